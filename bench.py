@@ -1,0 +1,322 @@
+"""Benchmark: GLL-point updates/s of the explicit spectral-element time step.
+
+Workload (default): 3-D elastic Hexahedron<Elastic3D>, 64^3 hexes of 200 m,
+order 4 (125 GLL points per element, G = 257^3 = 16,974,593 nodes, 3
+components), FP32 fields with FP64-computed geometry, Gaussian random-field
+model, moment-tensor Ricker source, 64 surface receivers.  A step is one time
+step of the whole mesh.  Per-step inputs (~3.6 GB of geometry, material and
+wavefields) exceed the 126 MB L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica on its own GPU (the
+path does not shard: replicas only); value = total updates / max rank time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GLL-point updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nel", type=int, default=64)
+    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="run a few steps only (for ncu captures); prints no JSON")
+    return ap.parse_args()
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def workload(args):
+    return {"workload": f"elastic3d hex {args.nel}^3 order {args.order}, 64 receivers, "
+                        f"moment-tensor Ricker, GRF model",
+            "shape": "Hexahedron<Elastic3D>", "elements": args.nel ** 3, "order": args.order,
+            "fields": "fp32 (geometry computed fp64)", "l2": "inputs larger than L2 (no flush)"}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return None
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_leg(args, nel_sample, steps, warm):
+    """Time the FP64 CPU oracle in reference-faithful mode (per-point Jacobian
+    rebuilds, Hexahedra.cpp:600,702) on a bounded sample of the workload."""
+    from oracle import pyoracle as po
+    from salvus_b200 import configs
+    thr = cpu_threads()
+    cfg = configs.elastic_hex(nel=nel_sample, order=args.order)
+    o = po.Problem(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                   configs.oracle_params(cfg), flags=po.FAITHFUL_RECOMPUTE, threads=thr)
+    s = cfg["sources"][0]
+    o.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                 s["moment_tensor"], kind=1)
+    for r in cfg["receivers"]:
+        o.add_receiver(r)
+    dt = 1e-3
+    if warm:
+        o.run(warm, dt)
+    t0 = time.perf_counter()
+    o.run(steps, dt)
+    el = time.perf_counter() - t0
+    rate = o.G * steps / el
+    sample = (f"oracle (FP64 reference-faithful restatement, OpenMP over element colours) on "
+              f"{nel_sample}^3 elements (G={o.G}) x {steps} steps after {warm} warm-up; "
+              f"{el:.2f} s")
+    return rate, thr, sample, el
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+
+    def start(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        busy = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": float(np.median(busy)) if busy else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    nel_sample = min(args.nel, 32)
+    steps = max(1, min(args.steps, 3))
+    warm = 1 if args.warmup > 0 else 0
+    rate, thr, sample, el = cpu_leg(args, nel_sample, steps, warm)
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC,
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm, "higher_is_better": True,
+            "ms_per_step": 1e3 * el / steps, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "config": workload(args),
+            "cpu_baseline": {"value": rate, "unit": METRIC, "cores": thr, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference needs PETSc/Eigen/HDF5/Exodus (absent); its CPU path is "
+                    "timed through the oracle port, which restates it and keeps its per-point "
+                    "Jacobian rebuild cost"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = env_rank()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+
+    import torch
+    from salvus_b200 import configs, core
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    cfg = configs.elastic_hex(nel=args.nel, order=args.order)
+    mesh = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                     cfg["params"], device=local)
+    G = mesh.n_nodes
+    dt = 0.4 * mesh.critical_dt(iterations=60)
+
+    def make_problem():
+        p = core.Problem(mesh, core.FP32, dt=dt)
+        s = cfg["sources"][0]
+        p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                     moment_tensor=s["moment_tensor"])
+        for r in cfg["receivers"]:
+            p.add_receiver(r)
+        p.set_seismogram_capacity(args.steps + args.warmup + 64)
+        return p
+
+    p = make_problem()
+    if args.profile_only:
+        p.run(max(args.steps, 3), core.RUN_PLAIN)
+        p.synchronize()
+        return
+    stream = torch.cuda.ExternalStream(p.stream_handle())
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def timed(fn):
+        barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = a.elapsed_time(b)
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    clocks = Clocks(local)
+    # warm-up (graph capture happens here)
+    p.run(args.warmup, core.RUN_GRAPH)
+    p.synchronize()
+    clocks.start()
+    l0 = core.launch_count()
+    ms = timed(lambda: p.run(args.steps, core.RUN_GRAPH))
+    launches = core.launch_count() - l0
+    ck = clocks.stop()
+    value = world * G * args.steps / (ms / 1e3)
+
+    # plain form: one host launch sequence per step
+    kp = min(args.steps, 200)
+    ms_plain = timed(lambda: p.run(kp, core.RUN_PLAIN))
+    plain = world * G * kp / (ms_plain / 1e3)
+
+    # per-kernel device time (events around each launch, plain form)
+    p.profile(True)
+    p.run(min(args.steps, 100), core.RUN_PLAIN)
+    prof = p.profile_read()
+    p.profile(False)
+
+    E, P = mesh.n_elements, mesh.points_per_element
+    # algorithmic bytes per stiffness launch: per point 48 B record (invJ 9,
+    # lambda wdetJ, mu wdetJ, conn) + compulsory u read 12 B/node + the
+    # element-local residual write 12 B/point
+    b_stiff = E * P * 48 + G * 12 + E * P * 12
+    # gather/update: residual read 12 B/point + incidence index 4 B/point +
+    # offsets 4 B/node + (u, v, a_) read and write 72 B/node + inverse mass 4 B/node
+    b_upd = E * P * 16 + G * (4 + 72 + 4)
+    peaks = measured_peaks()
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    k_ms, k_n = prof.get("stiffness", (0.0, 1))
+    u_ms, u_n = prof.get("gather_update", (0.0, 1))
+    st_ms = k_ms / max(k_n, 1)
+    up_ms = u_ms / max(u_n, 1)
+    ach = b_stiff / (st_ms / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic_elastic_hex_stiffness.txt")
+    if os.path.exists(tf):
+        for line in open(tf):
+            if line.startswith("dram_bytes_per_launch_fullsize="):
+                traffic = float(line.split("=")[1])
+
+    # end-to-end through the public API with host buffers: initial state from
+    # host (u0, v0 FP64), K steps, seismograms back to the host
+    p2 = make_problem()
+    rng = np.random.default_rng(7)
+    u0 = (1e-6 * rng.standard_normal((G, 3)))
+    v0 = np.zeros((G, 3))
+    seis_holder = {}
+
+    def e2e_job():
+        p2.set_field("u", u0)
+        p2.set_field("v", v0)
+        p2.run(args.steps, core.RUN_GRAPH)
+        seis_holder["s"] = p2.seismograms(0, args.steps)
+
+    ms_e2e = timed(e2e_job)
+    e2e = world * G * args.steps / (ms_e2e / 1e3)
+    h2d = 2 * G * 3 * 8 / args.steps
+    d2h = len(cfg["receivers"]) * 3 * 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, thr, sample, _ = cpu_leg(args, min(args.nel, 32), 2, 1)
+        cpu = {"value": rate, "unit": METRIC, "cores": thr, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded GRF model, structured hex mesh)",
+            "config": dict(workload(args), parallelism=f"replicas x{world}", form="graph-replayed fused step"),
+            "plain": {"value": plain, "unit": METRIC, "steps": kp, "ms_per_step": ms_plain / kp,
+                      "form": "host-launched fused step"},
+            "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+            "roofline": {"bound": "hbm", "kernel": "elastic_hex_stiffness", "achieved": ach,
+                         "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": traffic,
+                         "algorithmic_bytes": b_stiff,
+                         "peak_source": "measured" if peaks else "fallback"},
+            "roofline_update": {"kernel": "gather_update", "achieved": b_upd / (up_ms / 1e3) / 1e9,
+                                "peak": peak, "unit": "GB/s",
+                                "frac": b_upd / (up_ms / 1e3) / 1e9 / peak},
+            "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "form": "C-ABI job: FP64 host u0/v0 upload, K graph-replayed steps, "
+                            "seismogram read-back; h2d amortised over K"},
+            "gpu_launches": launches,
+            "clocks": ck,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

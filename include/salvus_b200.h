@@ -1,0 +1,183 @@
+/*
+ * salvus_b200.h -- C ABI of the B200 spectral-element time step.
+ *
+ * The reference boundary is Salvus's C++ plugin API: the time loop in
+ * src/cxx/Main.cpp:45-66 calls, once per step,
+ *   Problem::assembleIntoGlobalDof   (include/Problem/Problem.h:84-90,
+ *                                     src/cxx/Problem/Problem.cpp:143-214)
+ *   Problem::applyInverseMassMatrix  (Problem.h:112, Order2Newmark.cpp:68-83)
+ *   Problem::takeTimeStep            (Problem.h:120-121, Order2Newmark.cpp:85-114)
+ * on elements built by Element::Factory (src/cxx/Element/Element.cpp:117-304)
+ * from a DMPlex mesh (src/cxx/Mesh/Mesh.cpp:53-86,361-452) and an Exodus
+ * model (src/cxx/Model/ExodusModel.cpp:422-471).  This ABI replaces those
+ * calls; every entry point below names the reference interface it replaces.
+ *
+ * Conventions: plain C types only.  Every function returns SALVUS_OK (0) or a
+ * negative status and records a message readable with salvus_last_error()
+ * (thread-local).  The library owns device memory; callers own host arrays.
+ * Handles are opaque.  Calls on one problem are serialised on that problem's
+ * CUDA stream.
+ */
+#ifndef SALVUS_B200_H
+#define SALVUS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SALVUS_OK 0
+#define SALVUS_E_INVALID (-1)     /* bad argument / mesh (reference: std::runtime_error) */
+#define SALVUS_E_OOM (-2)         /* device or host allocation failed */
+#define SALVUS_E_CUDA (-3)        /* CUDA runtime error */
+#define SALVUS_E_TIMEOUT (-4)     /* a bounded device wait gave up */
+#define SALVUS_E_NONFINITE (-5)   /* NaN / Inf detected in a wavefield */
+#define SALVUS_E_STATE (-6)       /* call out of order (e.g. no dt set) */
+#define SALVUS_E_UNSUPPORTED (-7) /* order / shape / physics not built */
+#define SALVUS_E_NOT_FOUND (-8)   /* source / receiver outside the mesh */
+
+enum salvus_shape { SALVUS_QUAD = 0, SALVUS_HEX = 1, SALVUS_TRI = 2, SALVUS_TET = 3 };
+enum salvus_physics { SALVUS_ACOUSTIC = 0, SALVUS_ELASTIC3D = 1 };
+enum salvus_precision { SALVUS_FP32 = 0, SALVUS_FP64 = 1 };
+enum salvus_field { SALVUS_FIELD_U = 0, SALVUS_FIELD_V = 1, SALVUS_FIELD_A = 2,
+                    SALVUS_FIELD_A_PREV = 3 };
+enum salvus_source_kind { SALVUS_SOURCE_FORCE = 0, SALVUS_SOURCE_MOMENT_TENSOR = 1 };
+enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
+
+/* Mesh description.  Replaces Mesh::read + ExodusModel::read +
+ * Mesh::setupGlobalDof (Mesh.cpp:53-86, 361-452; ExodusModel.cpp:37,422).
+ * cells use the reference's right-hand (PETSc) vertex order:
+ *   quad v0(-,-) v1(+,-) v2(+,+) v3(-,+)                  (QuadP1.h:98-108)
+ *   hex  v0(-,-,-) v1(-,+,-) v2(+,+,-) v3(+,-,-)
+ *        v4(-,-,+) v5(+,-,+) v6(+,+,+) v7(-,+,+)         (HexP1.cpp:86-122)
+ * params are per element, per element vertex (Exodus NAME_0..NAME_k):
+ *   acoustic : [1][n_elements][nv]  VP                    (Scalar.cpp:23-25)
+ *   elastic3d: [3][n_elements][nv]  RHO, VP, VS  (isotropic form of
+ *              Elastic3D.cpp:33-54 with VPV=VPH=VP, VSV=VSH=VS, ETA=1) */
+typedef struct {
+  int32_t shape;   /* enum salvus_shape */
+  int32_t order;   /* polynomial order: quad 1..10, hex 1..6 */
+  int32_t physics; /* enum salvus_physics */
+  int32_t reserved;
+  int64_t n_vertices;
+  const double *vertices; /* [n_vertices][dim] */
+  int64_t n_elements;
+  const int64_t *cells;   /* [n_elements][4 | 8] */
+  const double *params;
+} salvus_mesh_desc;
+
+/* One Ricker point source (Ricker::fire, Ricker.cpp:27-33; Source.h:75).
+ * FORCE: comp[0..c-1] is the direction (c = 1 acoustic, 3 elastic).
+ * MOMENT_TENSOR (elastic only, no reference counterpart): comp = [Mxx, Myy,
+ * Mzz, Myz, Mxz, Mxy]; nodal force f_{i,a} = sum_b M_ab dphi_i/dx_b (x_s). */
+typedef struct {
+  double location[3];
+  double center_freq;
+  double time_delay;
+  double amplitude;
+  int32_t kind;
+  int32_t shot; /* which shot of a batched problem (0 for single-shot) */
+  double comp[6];
+} salvus_source;
+
+typedef struct salvus_mesh salvus_mesh;
+typedef struct salvus_problem salvus_problem;
+
+const char *salvus_last_error(void);
+/* Library build string (compile arch, version). */
+const char *salvus_version(void);
+
+/* ---- mesh ---- */
+/* Flattens the mesh once: GLL connectivity by topological keys, FP64
+ * Jacobians / material / diagonal mass computed on the GPU and stored in the
+ * problem precision.  Replaces Problem::initializeElements (Problem.cpp:34-140),
+ * Mesh::setupGlobalDof and Order2Newmark::initializeGlobalDofs
+ * (Order2Newmark.cpp:32-66).  device < 0 builds the host-side numbering and
+ * node coordinates only (no GPU needed); such a mesh cannot hold problems. */
+int salvus_mesh_create(const salvus_mesh_desc *desc, int device, salvus_mesh **out);
+int salvus_mesh_destroy(salvus_mesh *mesh);
+/* Unique global GLL nodes G and components c. */
+int salvus_mesh_info(const salvus_mesh *mesh, int64_t *n_nodes, int32_t *n_components,
+                     int32_t *points_per_element);
+/* Node coordinates [G][dim] (QuadP1::buildNodalPoints QuadP1.cpp:176-216,
+ * HexP1::buildNodalPoints HexP1.cpp:312-354). */
+int salvus_mesh_node_coords(const salvus_mesh *mesh, double *xyz);
+/* Element-local to global node map [E][P] (the closure, Problem.cpp:302-318). */
+int salvus_mesh_connectivity(const salvus_mesh *mesh, int64_t *conn);
+/* Diagonal inverse mass [G] in FP64 (VecReciprocal, Order2Newmark.cpp:52). */
+int salvus_mesh_inverse_mass(const salvus_mesh *mesh, double *mi);
+/* Estimate lambda_max(M^-1 K) by power iteration on the GPU (FP64);
+ * dt_crit = 2 / sqrt(lambda_max).  The reference has no quad/hex CFL
+ * (Mesh.h:60 is the constant 1.0). */
+int salvus_mesh_max_eigenvalue(salvus_mesh *mesh, int32_t iterations, uint64_t seed,
+                               double *lambda_max);
+
+/* ---- problem (one wavefield set on a mesh) ---- */
+/* Replaces Problem::Factory + Order2Newmark (Problem.cpp:11,
+ * Order2Newmark.cpp:116-118).  n_shots > 1 selects the shot-batched layout. */
+int salvus_problem_create(salvus_mesh *mesh, int32_t precision, int32_t n_shots,
+                          salvus_problem **out);
+int salvus_problem_destroy(salvus_problem *p);
+int salvus_problem_set_dt(salvus_problem *p, double dt);
+/* Element::attachSource / Source::Factory (TensorQuad.cpp:270-284,
+ * Hexahedra.cpp:448-464): first element in element order whose hull holds
+ * the point, then the Newton inverse map. */
+int salvus_problem_add_source(salvus_problem *p, const salvus_source *src);
+/* Element::attachReceiver (TensorQuad.cpp:253-268, Hexahedra.cpp:429-446).
+ * Receivers are shared by all shots.  Returns SALVUS_OK; samples of u are
+ * taken after every step (FP64 sum of Lagrange-weighted nodes). */
+int salvus_problem_add_receiver(salvus_problem *p, const double *xyz);
+/* Capacity of the on-device seismogram ring, in steps (default 4096). */
+int salvus_problem_set_seismogram_capacity(salvus_problem *p, int64_t steps);
+/* Host <-> device field copies, [G][c] FP64 for one shot
+ * (Problem::insertElementalFieldIntoMesh Problem.cpp:286-300,
+ * getFieldOnElement Problem.cpp:302-318). */
+int salvus_problem_set_field(salvus_problem *p, int32_t field, int32_t shot, const double *vals);
+int salvus_problem_get_field(salvus_problem *p, int32_t field, int32_t shot, double *vals);
+
+/* ---- the reference's three per-step calls (literal form) ---- */
+/* a = f(t_n) - K u, assembled; t_n = step * dt.
+ * Problem::assembleIntoGlobalDof (Problem.cpp:143-214). */
+int salvus_assemble(salvus_problem *p);
+/* a <- M^-1 a.  Order2Newmark::applyInverseMassMatrix (Order2Newmark.cpp:68-83). */
+int salvus_apply_inverse_mass(salvus_problem *p);
+/* v += dt/2 (a + a_prev); u += dt v + dt^2/2 a; a_prev = a; step += 1;
+ * receivers sampled.  Order2Newmark::takeTimeStep (Order2Newmark.cpp:85-114). */
+int salvus_take_time_step(salvus_problem *p);
+
+/* ---- fused forms ---- */
+/* One fused step (the three calls above in one stiffness + one gather/update
+ * launch).  Same result as the three-call sequence. */
+int salvus_step(salvus_problem *p);
+/* n steps of the Main.cpp:45-66 loop; mode PLAIN launches each step from the
+ * host, GRAPH replays a captured CUDA graph of steps. */
+int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode);
+int salvus_synchronize(salvus_problem *p);
+int64_t salvus_problem_step_index(const salvus_problem *p);
+/* The problem's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events after this problem's kernels. */
+int salvus_problem_stream(const salvus_problem *p, void **stream);
+
+/* Seismograms [n_shots][n_receivers][c][n_steps] FP64 for steps
+ * [first_step, first_step + n_steps) still held in the ring. */
+int salvus_get_seismograms(salvus_problem *p, int64_t first_step, int64_t n_steps, double *out);
+int salvus_problem_info(const salvus_problem *p, int32_t *n_shots, int32_t *n_receivers,
+                        int32_t *n_components);
+
+/* ---- measurement ---- */
+/* Device time of the kernels launched by the last salvus_run / salvus_step
+ * calls since the last reset, per kernel class (CUDA events on the problem
+ * stream): names[i] (static strings), total_ms[i], launches[i].  Profiling
+ * adds an event pair per launch; enable only for measurement. */
+int salvus_profile_enable(salvus_problem *p, int32_t enable);
+int salvus_profile_read(salvus_problem *p, int32_t max_entries, const char **names,
+                        double *total_ms, int64_t *launches, int32_t *n_entries);
+/* Total kernel launches issued by this library in this process. */
+int64_t salvus_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

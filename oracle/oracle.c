@@ -1,0 +1,1090 @@
+/*
+ * oracle.c -- FP64 CPU restatement of the Salvus spectral-element time step.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker).  The CUDA product never links,
+ * loads or calls this file.  Each function cites the reference lines it
+ * restates; reference paths are relative to the reference project root.
+ *
+ * Parity is pinned by (a) the reference's own sympy-generated GLL / Lagrange
+ * tables (golden fixtures produced from the reference sources), (b) the
+ * reference's element KATs restated as properties, (c) the Ricker closed
+ * form, and (d) the analytic Neumann standing wave.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* quads up to order 10 (TensorQuad.h:69), hexes up to order 6 (the
+ * reference's order7_hex.c is missing, Hexahedra.h:14-17). */
+#define ORC_MAX_N 11
+#define ORC_MAX_P 343
+
+static __thread char g_err[512];
+static void set_err(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+const char *orc_last_error(void) { return g_err; }
+
+/* ------------------------------------------------------------------------ */
+/* Legendre polynomial P_N(x) and P_{N-1}(x) by the three-term recurrence.   */
+static void legendre(int N, double x, double *pn, double *pnm1) {
+  double p0 = 1.0, p1 = x;
+  if (N == 0) { *pn = 1.0; *pnm1 = 0.0; return; }
+  for (int k = 2; k <= N; ++k) {
+    double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+    p0 = p1;
+    p1 = p2;
+  }
+  *pn = p1;
+  *pnm1 = p0;
+}
+
+/* GLL points = roots of (1-x^2) P_N'(x); weights 2/(N(N+1) P_N(x_i)^2).
+ * Restates quadrature_points_weights.py:55-93 (the generator of
+ * gll_coordinates_orderN_square / gll_weights_orderN_square,
+ * src/cxx/Element/HyperCube/Quad/Autogen/order4_square.c:131-149). */
+int orc_gll(int order, double *pts, double *wts) {
+  if (order < 1 || order >= ORC_MAX_N) { set_err("order %d unsupported", order); return -1; }
+  const int N = order, n = N + 1;
+  for (int i = 0; i < n; ++i) {
+    double x = -cos(M_PI * i / N);
+    if (i > 0 && i < N) {
+      /* Newton on q(x) = P_{N+1} - P_{N-1}; q' = (2N+1) P_N. */
+      for (int it = 0; it < 100; ++it) {
+        double pn, pnm1, pnp1, dummy;
+        legendre(N, x, &pn, &pnm1);
+        legendre(N + 1, x, &pnp1, &dummy);
+        double dx = (pnp1 - pnm1) / ((2.0 * N + 1.0) * pn);
+        x -= dx;
+        if (fabs(dx) < 1e-17) break;
+      }
+    }
+    pts[i] = x;
+  }
+  /* exact antisymmetry */
+  for (int i = 0; i < n / 2; ++i) {
+    double m = 0.5 * (pts[n - 1 - i] - pts[i]);
+    pts[i] = -m;
+    pts[n - 1 - i] = m;
+  }
+  if (n % 2) pts[n / 2] = 0.0;
+  pts[0] = -1.0;
+  pts[N] = 1.0;
+  if (wts) {
+    for (int i = 0; i < n; ++i) {
+      double pn, pnm1;
+      legendre(N, pts[i], &pn, &pnm1);
+      wts[i] = 2.0 / (N * (N + 1.0) * pn * pn);
+    }
+  }
+  return 0;
+}
+
+/* D[i][j] = l_j'(xi_i) -- the layout of mGrd (TensorQuad.cpp:107-142,
+ * Hexahedra.cpp:535-577).  Barycentric form; diagonal = minus row sum. */
+int orc_deriv_matrix(int order, double *D) {
+  double x[ORC_MAX_N], lam[ORC_MAX_N];
+  if (orc_gll(order, x, NULL)) return -1;
+  const int n = order + 1;
+  for (int j = 0; j < n; ++j) {
+    double prod = 1.0;
+    for (int k = 0; k < n; ++k)
+      if (k != j) prod *= (x[j] - x[k]);
+    lam[j] = 1.0 / prod;
+  }
+  for (int i = 0; i < n; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) {
+      if (i == j) continue;
+      double v = (lam[j] / lam[i]) / (x[i] - x[j]);
+      D[i * n + j] = v;
+      s += v;
+    }
+    D[i * n + i] = -s;
+  }
+  return 0;
+}
+
+/* 1-D Lagrange basis on GLL nodes and its derivative at xi
+ * (code_generator.py:13-43, interpolate_orderN_square). */
+int orc_lagrange(int order, double xi, double *l, double *dl) {
+  double x[ORC_MAX_N];
+  if (orc_gll(order, x, NULL)) return -1;
+  const int n = order + 1;
+  for (int j = 0; j < n; ++j) {
+    double v = 1.0;
+    for (int k = 0; k < n; ++k)
+      if (k != j) v *= (xi - x[k]) / (x[j] - x[k]);
+    l[j] = v;
+    if (dl) {
+      double d = 0.0;
+      for (int m = 0; m < n; ++m) {
+        if (m == j) continue;
+        double t = 1.0 / (x[j] - x[m]);
+        for (int k = 0; k < n; ++k)
+          if (k != j && k != m) t *= (xi - x[k]) / (x[j] - x[k]);
+        d += t;
+      }
+      dl[j] = d;
+    }
+  }
+  return 0;
+}
+
+/* Ricker::fire, src/cxx/Source/Ricker.cpp:27-33. */
+double orc_ricker(double t, double f0, double t0, double amp) {
+  const double factor = M_PI * M_PI * f0 * f0 * (t - t0) * (t - t0);
+  return amp * ((1 - 2 * factor) * exp(-1 * factor));
+}
+
+/* ------------------------------------------------------------------------ */
+/* P1 geometry.                                                              */
+/* Quad vertex signs (QuadP1.h:98-108): v0(-,-) v1(+,-) v2(+,+) v3(-,+).     */
+static const double QS[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+/* Hex vertex signs (HexP1.cpp:86-122, 242-298): PETSc right-hand order.    */
+static const double HS[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1},
+                                {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+
+int orc_p1_interpolate(int shape, const double *ref, double *w) {
+  if (shape == ORC_QUAD) {
+    for (int k = 0; k < 4; ++k)
+      w[k] = 0.25 * (1 + QS[k][0] * ref[0]) * (1 + QS[k][1] * ref[1]);
+  } else {
+    for (int k = 0; k < 8; ++k)
+      w[k] = 0.125 * (1 + HS[k][0] * ref[0]) * (1 + HS[k][1] * ref[1]) * (1 + HS[k][2] * ref[2]);
+  }
+  return 0;
+}
+
+static int inv2(const double J[4], double *det, double *inv) {
+  double d = J[0] * J[3] - J[1] * J[2];
+  *det = d;
+  if (inv) {
+    inv[0] = J[3] / d; inv[1] = -J[1] / d;
+    inv[2] = -J[2] / d; inv[3] = J[0] / d;
+  }
+  return 0;
+}
+static int inv3(const double J[9], double *det, double *inv) {
+  double c00 = J[4] * J[8] - J[5] * J[7];
+  double c01 = J[5] * J[6] - J[3] * J[8];
+  double c02 = J[3] * J[7] - J[4] * J[6];
+  double d = J[0] * c00 + J[1] * c01 + J[2] * c02;
+  *det = d;
+  if (inv) {
+    double id = 1.0 / d;
+    inv[0] = c00 * id;
+    inv[1] = (J[2] * J[7] - J[1] * J[8]) * id;
+    inv[2] = (J[1] * J[5] - J[2] * J[4]) * id;
+    inv[3] = c01 * id;
+    inv[4] = (J[0] * J[8] - J[2] * J[6]) * id;
+    inv[5] = (J[2] * J[3] - J[0] * J[5]) * id;
+    inv[6] = c02 * id;
+    inv[7] = (J[1] * J[6] - J[0] * J[7]) * id;
+    inv[8] = (J[0] * J[4] - J[1] * J[3]) * id;
+  }
+  return 0;
+}
+
+/* Jacobian J[i][k] = d x_k / d xi_i (rows = reference directions), its
+ * determinant and inverse; gradient = invJ * reference gradient.
+ * QuadP1::inverseJacobianAtPoint QuadP1.h:79-90; HexP1::inverseJacobianAtPoint
+ * HexP1.cpp:189-240. */
+int orc_p1_jacobian(int shape, const double *vtx, const double *ref, unsigned flags,
+                    double *detJ, double *invJ) {
+  if (shape == ORC_QUAD) {
+    double J[4] = {0, 0, 0, 0};
+    double r = ref[0], s = ref[1];
+    for (int k = 0; k < 4; ++k) {
+      double dr, ds;
+      if (flags & ORC_Q17_QUAD_SWAPPED_JAC) {
+        /* QuadP1.h:20-27 evaluate dN/dr at r and dN/ds at s. */
+        dr = 0.25 * QS[k][0] * (1 + QS[k][1] * r);
+        ds = 0.25 * QS[k][1] * (1 + QS[k][0] * s);
+      } else {
+        dr = 0.25 * QS[k][0] * (1 + QS[k][1] * s);
+        ds = 0.25 * QS[k][1] * (1 + QS[k][0] * r);
+      }
+      J[0] += dr * vtx[2 * k + 0];
+      J[1] += dr * vtx[2 * k + 1];
+      J[2] += ds * vtx[2 * k + 0];
+      J[3] += ds * vtx[2 * k + 1];
+    }
+    return inv2(J, detJ, invJ);
+  } else {
+    double J[9] = {0};
+    for (int k = 0; k < 8; ++k) {
+      double a = 1 + HS[k][0] * ref[0], b = 1 + HS[k][1] * ref[1], c = 1 + HS[k][2] * ref[2];
+      double d0 = 0.125 * HS[k][0] * b * c;
+      double d1 = 0.125 * HS[k][1] * a * c;
+      double d2 = 0.125 * HS[k][2] * a * b;
+      for (int m = 0; m < 3; ++m) {
+        J[0 + m] += d0 * vtx[3 * k + m];
+        J[3 + m] += d1 * vtx[3 * k + m];
+        J[6 + m] += d2 * vtx[3 * k + m];
+      }
+    }
+    return inv3(J, detJ, invJ);
+  }
+}
+
+static void p1_map(int shape, const double *vtx, const double *ref, double *x) {
+  double w[8];
+  orc_p1_interpolate(shape, ref, w);
+  int nv = shape == ORC_QUAD ? 4 : 8, d = shape == ORC_QUAD ? 2 : 3;
+  for (int m = 0; m < d; ++m) {
+    double s = 0;
+    for (int k = 0; k < nv; ++k) s += w[k] * vtx[d * k + m];
+    x[m] = s;
+  }
+}
+
+/* QuadP1::checkHull QuadP1.cpp:8-39; HexP1::checkHull HexP1.cpp:8-84. */
+int orc_check_hull(int shape, const double *vtx, const double *x) {
+  double det, ref0[3] = {0, 0, 0};
+  orc_p1_jacobian(shape, vtx, ref0, 0, &det, NULL);
+  if (det <= 0) { set_err("poorly behaved element (detJ <= 0)"); return -1; }
+  if (shape == ORC_QUAD) {
+    int nneg = 0, npos = 0;
+    static const int em[5] = {0, 1, 2, 3, 0};
+    for (int i = 0; i < 4; ++i) {
+      const double *p0 = vtx + 2 * em[i], *p1 = vtx + 2 * em[i + 1];
+      double vx = p1[0] - p0[0], vy = p1[1] - p0[1];
+      double px = x[0] - p0[0], py = x[1] - p0[1];
+      double x0 = vx * py - vy * px;
+      if (x0 < 0) nneg++;
+      else if (x0 > 0) npos++;
+      else { npos++; nneg++; }
+    }
+    return (nneg == 4 || npos == 4) ? 1 : 0;
+  } else {
+    static const int sides[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 3, 5, 4},
+                                    {2, 1, 7, 6}, {0, 4, 7, 1}, {2, 6, 5, 3}};
+    for (int sd = 0; sd < 6; ++sd) {
+      const double *a = vtx + 3 * sides[sd][0], *b = vtx + 3 * sides[sd][1],
+                   *dd = vtx + 3 * sides[sd][3];
+      double l1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+      double l2[3] = {dd[0] - a[0], dd[1] - a[1], dd[2] - a[2]};
+      double nrm[3] = {l1[1] * l2[2] - l1[2] * l2[1], l1[2] * l2[0] - l1[0] * l2[2],
+                       l1[0] * l2[1] - l1[1] * l2[0]};
+      double dot = nrm[0] * (x[0] - a[0]) + nrm[1] * (x[1] - a[1]) + nrm[2] * (x[2] - a[2]);
+      if (dot > 0) return 0;
+    }
+    return 1;
+  }
+}
+
+/* Newton inverse map, tol 1e-6 on the physical residual, <= 10 iterations:
+ * QuadP1::inverseCoordinateTransform QuadP1.cpp:41-92,
+ * HexP1::inverseCoordinateTransform HexP1.cpp:135-187. */
+int orc_inverse_map(int shape, const double *vtx, const double *x, double *ref) {
+  const int d = shape == ORC_QUAD ? 2 : 3;
+  double sol[3] = {0, 0, 0};
+  for (int it = 0;; ++it) {
+    double X[3], det, inv[9];
+    p1_map(shape, vtx, sol, X);
+    double obj[3] = {x[0] - X[0], x[1] - X[1], d == 3 ? x[2] - X[2] : 0.0};
+    int ok = 1;
+    for (int m = 0; m < d; ++m)
+      if (!(fabs(obj[m]) < 1e-6)) ok = 0;
+    if (ok) break;
+    /* dx/dxi = J^T, so the Newton step is (J^T)^-1 obj = invJ^T obj. */
+    orc_p1_jacobian(shape, vtx, sol, 0, &det, inv);
+    for (int a = 0; a < d; ++a) {
+      double s = 0;
+      for (int b = 0; b < d; ++b) s += inv[b * d + a] * obj[b];
+      sol[a] += s;
+    }
+    if (it > 10) { set_err("inverse map failed to converge after 10 iterations"); return -1; }
+  }
+  for (int m = 0; m < d; ++m) ref[m] = sol[m];
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Tensor element operators (single element).                                */
+typedef struct {
+  int shape, dim, n, P, nv;
+  double xi[ORC_MAX_N], w[ORC_MAX_N], D[ORC_MAX_N * ORC_MAX_N];
+} basis_t;
+
+static int basis_init(basis_t *b, int shape, int order) {
+  b->shape = shape;
+  b->dim = shape == ORC_QUAD ? 2 : 3;
+  b->n = order + 1;
+  b->P = b->dim == 2 ? b->n * b->n : b->n * b->n * b->n;
+  b->nv = shape == ORC_QUAD ? 4 : 8;
+  if (b->P > ORC_MAX_P) { set_err("order %d unsupported for this shape", order); return -1; }
+  if (orc_gll(order, b->xi, b->w)) return -1;
+  return orc_deriv_matrix(order, b->D);
+}
+
+static inline void point_ref(const basis_t *b, int p, double *ref) {
+  int n = b->n;
+  ref[0] = b->xi[p % n];
+  ref[1] = b->xi[(p / n) % n];
+  ref[2] = b->dim == 3 ? b->xi[p / (n * n)] : 0.0;
+}
+static inline double point_w(const basis_t *b, int p) {
+  int n = b->n;
+  double w = b->w[p % n] * b->w[(p / n) % n];
+  if (b->dim == 3) w *= b->w[p / (n * n)];
+  return w;
+}
+
+/* Reference-direction gradient at every point.  TensorQuad.cpp:198-201,
+ * Hexahedra.cpp:611-616. */
+static void ref_gradient(const basis_t *b, const double *u, double *gr /* [P][dim] */) {
+  const int n = b->n, d = b->dim;
+  for (int p = 0; p < b->P; ++p) {
+    int r = p % n, s = (p / n) % n, t = p / (n * n);
+    double g0 = 0, g1 = 0, g2 = 0;
+    for (int i = 0; i < n; ++i) {
+      g0 += b->D[r * n + i] * u[i + s * n + t * n * n];
+      g1 += b->D[s * n + i] * u[r + i * n + t * n * n];
+      if (d == 3) g2 += b->D[t * n + i] * u[r + s * n + i * n * n];
+    }
+    gr[p * d + 0] = g0;
+    gr[p * d + 1] = g1;
+    if (d == 3) gr[p * d + 2] = g2;
+  }
+}
+
+/* Per-point geometry of one element: detJ[P], invJ[P][d*d]. */
+static void element_geometry(const basis_t *b, const double *vtx, unsigned flags,
+                             double *detJ, double *invJ) {
+  for (int p = 0; p < b->P; ++p) {
+    double ref[3];
+    point_ref(b, p, ref);
+    orc_p1_jacobian(b->shape, vtx, ref, flags, &detJ[p], &invJ[p * b->dim * b->dim]);
+  }
+}
+
+/* computeGradient: physical gradient = invJ * ref gradient. */
+static void grad_from_geom(const basis_t *b, const double *invJ, const double *u, double *g) {
+  double gr[ORC_MAX_P * 3];
+  const int d = b->dim;
+  ref_gradient(b, u, gr);
+  for (int p = 0; p < b->P; ++p) {
+    const double *iJ = invJ + p * d * d;
+    for (int a = 0; a < d; ++a) {
+      double s = 0;
+      for (int k = 0; k < d; ++k) s += iJ[a * d + k] * gr[p * d + k];
+      g[p * d + a] = s;
+    }
+  }
+}
+
+/* Gradient-test integral, per-quadrature-point form (Hexahedra.cpp:689-754;
+ * corrected 2-D form).  F = invJ^T f at each point, then D^T sums weighted
+ * by w detJ. */
+static void grad_test_from_geom(const basis_t *b, const double *detJ, const double *invJ,
+                                const double *f, double *out) {
+  const int n = b->n, d = b->dim;
+  double F[ORC_MAX_P * 3];
+  for (int p = 0; p < b->P; ++p) {
+    const double *iJ = invJ + p * d * d;
+    for (int k = 0; k < d; ++k) {
+      double s = 0;
+      for (int a = 0; a < d; ++a) s += iJ[a * d + k] * f[p * d + a];
+      F[p * d + k] = s * detJ[p];
+    }
+  }
+  for (int p = 0; p < b->P; ++p) {
+    int r = p % n, s = (p / n) % n, t = p / (n * n);
+    double sr = 0, ss = 0, st = 0;
+    for (int i = 0; i < n; ++i) {
+      int ri = i + s * n + t * n * n, si = r + i * n + t * n * n, ti = r + s * n + i * n * n;
+      sr += F[ri * d + 0] * b->D[i * n + r] * b->w[i];
+      ss += F[si * d + 1] * b->D[i * n + s] * b->w[i];
+      if (d == 3) st += F[ti * d + 2] * b->D[i * n + t] * b->w[i];
+    }
+    if (d == 2) {
+      out[p] = sr * b->w[s] + ss * b->w[r];
+    } else {
+      out[p] = sr * b->w[s] * b->w[t] + ss * b->w[r] * b->w[t] + st * b->w[r] * b->w[s];
+    }
+  }
+}
+
+/* 2-D reference-literal gradient-test (TensorQuad.cpp:351-397): sums use
+ * detJ at the quadrature points, J^-1 is applied at the output point. */
+static void grad_test_quad_literal(const basis_t *b, const double *vtx, unsigned flags,
+                                   const double *detJ, const double *f, double *out) {
+  const int n = b->n;
+  for (int p = 0; p < b->P; ++p) {
+    int r = p % n, s = p / n;
+    double dfx0 = 0, dfx1 = 0, dfy0 = 0, dfy1 = 0;
+    for (int i = 0; i < n; ++i) {
+      int ri = i + s * n, si = r + i * n;
+      dfx0 += detJ[ri] * f[ri * 2 + 0] * b->D[i * n + r] * b->w[i];
+      dfx1 += detJ[si] * f[si * 2 + 0] * b->D[i * n + s] * b->w[i];
+      dfy0 += detJ[ri] * f[ri * 2 + 1] * b->D[i * n + r] * b->w[i];
+      dfy1 += detJ[si] * f[si * 2 + 1] * b->D[i * n + s] * b->w[i];
+    }
+    dfx0 *= b->w[s]; dfx1 *= b->w[r]; dfy0 *= b->w[s]; dfy1 *= b->w[r];
+    double ref[3], dj, iJ[4];
+    point_ref(b, p, ref);
+    orc_p1_jacobian(b->shape, vtx, ref, flags, &dj, iJ);
+    out[p] = iJ[0] * dfx0 + iJ[1] * dfx1 + iJ[2] * dfy0 + iJ[3] * dfy1;
+  }
+}
+
+int orc_element_gradient(int shape, int order, const double *vtx, unsigned flags,
+                         const double *u, double *grad) {
+  basis_t b;
+  if (basis_init(&b, shape, order)) return -1;
+  double detJ[ORC_MAX_P], invJ[ORC_MAX_P * 9];
+  element_geometry(&b, vtx, flags, detJ, invJ);
+  grad_from_geom(&b, invJ, u, grad);
+  return 0;
+}
+
+int orc_element_grad_test(int shape, int order, const double *vtx, unsigned flags,
+                          const double *f, double *out) {
+  basis_t b;
+  if (basis_init(&b, shape, order)) return -1;
+  double detJ[ORC_MAX_P], invJ[ORC_MAX_P * 9];
+  element_geometry(&b, vtx, flags, detJ, invJ);
+  if (shape == ORC_QUAD && (flags & ORC_Q3_QUAD_INVJ_AT_OUTPUT))
+    grad_test_quad_literal(&b, vtx, flags, detJ, f, out);
+  else
+    grad_test_from_geom(&b, detJ, invJ, f, out);
+  return 0;
+}
+
+/* applyTestAndIntegrate TensorQuad.cpp:326-348, Hexahedra.cpp:659-686. */
+int orc_element_test(int shape, int order, const double *vtx, unsigned flags,
+                     const double *f, double *out) {
+  basis_t b;
+  if (basis_init(&b, shape, order)) return -1;
+  for (int p = 0; p < b.P; ++p) {
+    double ref[3], dj;
+    point_ref(&b, p, ref);
+    orc_p1_jacobian(shape, vtx, ref, flags, &dj, NULL);
+    out[p] = f[p] * dj * point_w(&b, p);
+  }
+  return 0;
+}
+
+static void tensor_lagrange(const basis_t *b, const double *ref, double *l, double *dl /* [P][d] or NULL */) {
+  double lr[ORC_MAX_N], ls[ORC_MAX_N], lt[ORC_MAX_N], dr[ORC_MAX_N], ds[ORC_MAX_N], dt[ORC_MAX_N];
+  const int n = b->n;
+  orc_lagrange(n - 1, ref[0], lr, dr);
+  orc_lagrange(n - 1, ref[1], ls, ds);
+  if (b->dim == 3) orc_lagrange(n - 1, ref[2], lt, dt);
+  for (int p = 0; p < b->P; ++p) {
+    int r = p % n, s = (p / n) % n, t = p / (n * n);
+    if (b->dim == 2) {
+      l[p] = lr[r] * ls[s];
+      if (dl) { dl[p * 2 + 0] = dr[r] * ls[s]; dl[p * 2 + 1] = lr[r] * ds[s]; }
+    } else {
+      l[p] = lr[r] * ls[s] * lt[t];
+      if (dl) {
+        dl[p * 3 + 0] = dr[r] * ls[s] * lt[t];
+        dl[p * 3 + 1] = lr[r] * ds[s] * lt[t];
+        dl[p * 3 + 2] = lr[r] * ls[s] * dt[t];
+      }
+    }
+  }
+}
+
+/* getDeltaFunctionCoefficients TensorQuad.cpp:287-306, Hexahedra.cpp:467-490. */
+int orc_element_delta(int shape, int order, const double *vtx, unsigned flags,
+                      const double *ref, double *out) {
+  basis_t b;
+  if (basis_init(&b, shape, order)) return -1;
+  tensor_lagrange(&b, ref, out, NULL);
+  for (int p = 0; p < b.P; ++p) {
+    double pr[3], dj;
+    point_ref(&b, p, pr);
+    orc_p1_jacobian(shape, vtx, pr, flags, &dj, NULL);
+    out[p] /= (point_w(&b, p) * dj);
+  }
+  return 0;
+}
+
+/* ParAtIntPts TensorQuad.cpp:309-323, Hexahedra.cpp:635-656. */
+int orc_element_par(int shape, int order, const double *par_vtx, double *out) {
+  basis_t b;
+  if (basis_init(&b, shape, order)) return -1;
+  for (int p = 0; p < b.P; ++p) {
+    double ref[3], w[8];
+    point_ref(&b, p, ref);
+    orc_p1_interpolate(shape, ref, w);
+    double s = 0;
+    for (int k = 0; k < b.nv; ++k) s += w[k] * par_vtx[k];
+    out[p] = s;
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Problem.                                                                  */
+typedef struct {
+  int64_t elem;
+  double ref[3];
+  double f0, t0, amp;
+  double *wts; /* [P][c] nodal weights multiplied by the source time function */
+} src_t;
+
+typedef struct {
+  int64_t elem;
+  double *l; /* [P] Lagrange weights */
+} rec_t;
+
+struct orc_problem {
+  orc_desc d;
+  basis_t b;
+  int c, npar;
+  int64_t E, G;
+  double *vtx;     /* [E][nv][dim] */
+  double *par;     /* [npar][E][nv] */
+  int64_t *conn;   /* [E][P] */
+  double *xyz;     /* [G][dim] */
+  /* cached per-point data (not used in faithful mode) */
+  double *detJ, *invJ, *mat; /* mat: acoustic vp^2 [E][P]; elastic 9 c_ij [E][9][P] */
+  double *mi;      /* [G] inverse diagonal mass */
+  double *u, *v, *a, *a_; /* [G][c] */
+  int64_t step;
+  /* colouring for threaded assembly */
+  int ncolours;
+  int64_t *col_off, *col_elems;
+  src_t *src; int nsrc;
+  rec_t *rec; int nrec;
+};
+
+static void *xcalloc(size_t n, size_t s) {
+  void *p = calloc(n ? n : 1, s);
+  if (!p) { fprintf(stderr, "oracle: out of memory\n"); abort(); }
+  return p;
+}
+
+/* -- coordinate-keyed node numbering (independent of the product's
+ *    topological numbering; semantics of Mesh::setupGlobalDof Mesh.cpp:361-452) */
+typedef struct { int64_t k[3]; int64_t id; } hent_t;
+
+static uint64_t mix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+static int number_nodes(orc_problem *p) {
+  const basis_t *b = &p->b;
+  const int d = b->dim;
+  /* tolerance: 1e-7 of the smallest element-vertex spacing */
+  double hmin = INFINITY;
+  for (int64_t e = 0; e < p->E; ++e) {
+    const double *v = p->vtx + e * b->nv * d;
+    for (int k = 1; k < b->nv; ++k) {
+      double s = 0;
+      for (int m = 0; m < d; ++m) s += (v[k * d + m] - v[m]) * (v[k * d + m] - v[m]);
+      if (s > 0 && sqrt(s) < hmin) hmin = sqrt(s);
+    }
+  }
+  const double tol = 1e-7 * hmin;
+  size_t cap = 1024;
+  while (cap < (size_t)(p->E * b->P)) cap <<= 1;
+  hent_t *tab = (hent_t *)malloc(cap * sizeof(hent_t));
+  if (!tab) { set_err("oom"); return -1; }
+  for (size_t i = 0; i < cap; ++i) tab[i].id = -1;
+  p->conn = (int64_t *)xcalloc((size_t)(p->E * b->P), sizeof(int64_t));
+  double *xyz = (double *)xcalloc((size_t)(p->E * b->P) * d, sizeof(double));
+  int64_t G = 0;
+  for (int64_t e = 0; e < p->E; ++e) {
+    const double *v = p->vtx + e * b->nv * d;
+    for (int q = 0; q < b->P; ++q) {
+      double ref[3], x[3] = {0, 0, 0};
+      point_ref(b, q, ref);
+      p1_map(b->shape, v, ref, x);
+      int64_t key[3];
+      for (int m = 0; m < 3; ++m) key[m] = (m < d) ? (int64_t)llround(x[m] / tol) : 0;
+      uint64_t h = mix64((uint64_t)key[0] ^ mix64((uint64_t)key[1] ^ mix64((uint64_t)key[2])));
+      size_t i = h & (cap - 1);
+      for (;;) {
+        if (tab[i].id < 0) {
+          tab[i].k[0] = key[0]; tab[i].k[1] = key[1]; tab[i].k[2] = key[2];
+          tab[i].id = G;
+          for (int m = 0; m < d; ++m) xyz[G * d + m] = x[m];
+          p->conn[e * b->P + q] = G++;
+          break;
+        }
+        if (tab[i].k[0] == key[0] && tab[i].k[1] == key[1] && tab[i].k[2] == key[2]) {
+          p->conn[e * b->P + q] = tab[i].id;
+          break;
+        }
+        i = (i + 1) & (cap - 1);
+      }
+    }
+  }
+  free(tab);
+  p->G = G;
+  p->xyz = (double *)realloc(xyz, (size_t)G * d * sizeof(double));
+  return 0;
+}
+
+static void colour_elements(orc_problem *p) {
+  const int P = p->b.P;
+  uint64_t *mask = (uint64_t *)xcalloc((size_t)p->G, sizeof(uint64_t));
+  int *col = (int *)xcalloc((size_t)p->E, sizeof(int));
+  int nc = 0;
+  for (int64_t e = 0; e < p->E; ++e) {
+    uint64_t used = 0;
+    for (int q = 0; q < P; ++q) used |= mask[p->conn[e * P + q]];
+    int c = 0;
+    while (c < 64 && (used >> c) & 1) ++c;
+    if (c >= 64) { fprintf(stderr, "oracle: colouring overflow\n"); abort(); }
+    col[e] = c;
+    if (c + 1 > nc) nc = c + 1;
+    for (int q = 0; q < P; ++q) mask[p->conn[e * P + q]] |= (1ull << c);
+  }
+  p->ncolours = nc;
+  p->col_off = (int64_t *)xcalloc((size_t)nc + 1, sizeof(int64_t));
+  p->col_elems = (int64_t *)xcalloc((size_t)p->E, sizeof(int64_t));
+  for (int64_t e = 0; e < p->E; ++e) p->col_off[col[e] + 1]++;
+  for (int c = 0; c < nc; ++c) p->col_off[c + 1] += p->col_off[c];
+  int64_t *fill = (int64_t *)xcalloc((size_t)nc, sizeof(int64_t));
+  for (int64_t e = 0; e < p->E; ++e) p->col_elems[p->col_off[col[e]] + fill[col[e]]++] = e;
+  free(fill); free(col); free(mask);
+}
+
+/* Material at GLL points of element e: acoustic vp^2 (Scalar.cpp:45);
+ * elastic c_ij (Elastic3D.cpp:42-53, c11 c12 c13 c22 c23 c33 c44 c55 c66). */
+static void element_material(const orc_problem *p, int64_t e, double *m, double *rho) {
+  const basis_t *b = &p->b;
+  const int P = b->P, nv = b->nv;
+  double tmp[6][ORC_MAX_P];
+  for (int k = 0; k < p->npar; ++k)
+    orc_element_par(b->shape, b->n - 1, p->par + ((size_t)k * p->E + e) * nv, tmp[k]);
+  if (p->d.physics == ORC_ACOUSTIC) {
+    for (int q = 0; q < P; ++q) m[q] = pow(tmp[0][q], 2);
+    if (rho) for (int q = 0; q < P; ++q) rho[q] = 1.0;
+  } else {
+    for (int q = 0; q < P; ++q) {
+      double r = tmp[0][q], vpv = tmp[1][q], vph = tmp[2][q], vsv = tmp[3][q], vsh = tmp[4][q],
+             eta = tmp[5][q];
+      double c11 = r * pow(vph, 2), c22 = r * pow(vph, 2), c33 = r * pow(vpv, 2);
+      double c44 = r * pow(vsv, 2), c55 = r * pow(vsv, 2), c66 = r * pow(vsh, 2);
+      double c12 = c11 - 2 * c66, c13 = eta * (c11 - 2 * c44), c23 = eta * (c11 - 2 * c44);
+      m[0 * P + q] = c11; m[1 * P + q] = c12; m[2 * P + q] = c13;
+      m[3 * P + q] = c22; m[4 * P + q] = c23; m[5 * P + q] = c33;
+      m[6 * P + q] = c44; m[7 * P + q] = c55; m[8 * P + q] = c66;
+      if (rho) rho[q] = r;
+    }
+  }
+}
+
+/* Element stiffness K_e u_e, [P][c] in and out.
+ * Scalar::computeStiffnessTerm Scalar.cpp:58-71 / computeStress :42-55;
+ * Elastic3D::computeStiffnessTerm Elastic3D.cpp:70-103 / computeStress :106-118. */
+static void element_stiffness(const orc_problem *p, int64_t e, const double *ue, double *ke) {
+  const basis_t *b = &p->b;
+  const int P = b->P, d = b->dim;
+  const unsigned fl = p->d.flags;
+  const double *vtx = p->vtx + e * b->nv * d;
+  double detJ_l[ORC_MAX_P], invJ_l[ORC_MAX_P * 9], mat_l[9 * ORC_MAX_P];
+  const double *detJ, *invJ, *mat;
+  const int faithful = (fl & ORC_FAITHFUL_RECOMPUTE) != 0;
+  if (faithful) {
+    element_geometry(b, vtx, fl, detJ_l, invJ_l);
+    detJ = detJ_l; invJ = invJ_l;
+    if (p->d.physics == ORC_ACOUSTIC) {
+      /* Scalar::computeStress re-interpolates VP every call (Scalar.cpp:45) */
+      element_material(p, e, mat_l, NULL);
+      mat = mat_l;
+    } else {
+      /* Elastic3D caches c_ij per element at attach time (Elastic3D.cpp:33-54) */
+      mat = p->mat + e * P * 9;
+    }
+  } else {
+    detJ = p->detJ + e * P;
+    invJ = p->invJ + e * P * d * d;
+    mat = p->mat + e * P * (p->d.physics == ORC_ACOUSTIC ? 1 : 9);
+  }
+  if (p->d.physics == ORC_ACOUSTIC) {
+    double g[ORC_MAX_P * 3];
+    grad_from_geom(b, invJ, ue, g);
+    for (int q = 0; q < P; ++q)
+      for (int a = 0; a < d; ++a) g[q * d + a] *= mat[q];
+    if (b->shape == ORC_QUAD && (fl & ORC_Q3_QUAD_INVJ_AT_OUTPUT)) {
+      grad_test_quad_literal(b, vtx, fl, detJ, g, ke);
+    } else {
+      if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l); /* Hexahedra.cpp:702 */
+      grad_test_from_geom(b, detJ, invJ, g, ke);
+    }
+    return;
+  }
+  /* elastic 3-D */
+  double ux[ORC_MAX_P], uy[ORC_MAX_P], uz[ORC_MAX_P];
+  for (int q = 0; q < P; ++q) { ux[q] = ue[q * 3]; uy[q] = ue[q * 3 + 1]; uz[q] = ue[q * 3 + 2]; }
+  double gx[ORC_MAX_P * 3], gy[ORC_MAX_P * 3], gz[ORC_MAX_P * 3];
+  grad_from_geom(b, invJ, ux, gx);
+  if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+  grad_from_geom(b, invJ, uy, gy);
+  if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+  grad_from_geom(b, invJ, uz, gz);
+  double sx[ORC_MAX_P * 3], sy[ORC_MAX_P * 3], sz[ORC_MAX_P * 3];
+  for (int q = 0; q < P; ++q) {
+    double e0 = gx[q * 3 + 0], e1 = gy[q * 3 + 1], e2 = gz[q * 3 + 2];
+    double e3 = gy[q * 3 + 2] + gz[q * 3 + 1];
+    double e4 = gx[q * 3 + 2] + gz[q * 3 + 0];
+    double e5 = gx[q * 3 + 1] + gy[q * 3 + 0];
+    double c11 = mat[0 * P + q], c12 = mat[1 * P + q], c13 = mat[2 * P + q];
+    double c22 = mat[3 * P + q], c23 = mat[4 * P + q], c33 = mat[5 * P + q];
+    double c44 = mat[6 * P + q], c55 = mat[7 * P + q], c66 = mat[8 * P + q];
+    double s0 = c11 * e0 + c12 * e1 + c13 * e2;
+    double s1 = c12 * e0 + c22 * e1 + c23 * e2;
+    double s2 = c13 * e0 + c23 * e1 + c33 * e2;
+    double s3 = c44 * e3, s4 = c55 * e4, s5 = c66 * e5;
+    sx[q * 3 + 0] = s0; sx[q * 3 + 1] = s5; sx[q * 3 + 2] = s4;
+    sy[q * 3 + 0] = s5; sy[q * 3 + 1] = s1; sy[q * 3 + 2] = s3;
+    sz[q * 3 + 0] = s4; sz[q * 3 + 1] = s3; sz[q * 3 + 2] = s2;
+  }
+  double kx[ORC_MAX_P], ky[ORC_MAX_P], kz[ORC_MAX_P];
+  if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+  grad_test_from_geom(b, detJ, invJ, sx, kx);
+  if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+  grad_test_from_geom(b, detJ, invJ, sy, ky);
+  if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+  grad_test_from_geom(b, detJ, invJ, sz, kz);
+  for (int q = 0; q < P; ++q) { ke[q * 3] = kx[q]; ke[q * 3 + 1] = ky[q]; ke[q * 3 + 2] = kz[q]; }
+}
+
+orc_problem *orc_create(const orc_desc *d) {
+  if (!d || (d->shape != ORC_QUAD && d->shape != ORC_HEX)) { set_err("bad shape"); return NULL; }
+  if (d->physics == ORC_ELASTIC3D && d->shape != ORC_HEX) {
+    set_err("elastic 3-D physics needs hexahedra (Elastic3D.cpp:137)");
+    return NULL;
+  }
+  orc_problem *p = (orc_problem *)xcalloc(1, sizeof(orc_problem));
+  p->d = *d;
+  if (p->d.threads < 1) p->d.threads = 1;
+  if (basis_init(&p->b, d->shape, d->order)) { free(p); return NULL; }
+  const basis_t *b = &p->b;
+  const int dim = b->dim, nv = b->nv, P = b->P;
+  p->c = d->physics == ORC_ACOUSTIC ? 1 : 3;
+  p->npar = d->physics == ORC_ACOUSTIC ? 1 : 6;
+  p->E = d->n_elements;
+  p->vtx = (double *)xcalloc((size_t)(p->E * nv * dim), sizeof(double));
+  for (int64_t e = 0; e < p->E; ++e)
+    for (int k = 0; k < nv; ++k) {
+      int64_t vi = d->cells[e * nv + k];
+      if (vi < 0 || vi >= d->n_vertices) { set_err("cell vertex out of range"); orc_destroy(p); return NULL; }
+      for (int m = 0; m < dim; ++m) p->vtx[(e * nv + k) * dim + m] = d->vertices[vi * dim + m];
+    }
+  p->par = (double *)xcalloc((size_t)(p->npar * p->E * nv), sizeof(double));
+  memcpy(p->par, d->params, sizeof(double) * (size_t)(p->npar * p->E * nv));
+  /* element sanity (checkHull's right-hand-rule check) */
+  for (int64_t e = 0; e < p->E; ++e) {
+    double det, ref0[3] = {0, 0, 0};
+    orc_p1_jacobian(b->shape, p->vtx + e * nv * dim, ref0, 0, &det, NULL);
+    if (!(det > 0)) { set_err("element %lld has detJ <= 0", (long long)e); orc_destroy(p); return NULL; }
+  }
+  if (number_nodes(p)) { orc_destroy(p); return NULL; }
+  colour_elements(p);
+  const int nm = d->physics == ORC_ACOUSTIC ? 1 : 9;
+  const int faithful = (d->flags & ORC_FAITHFUL_RECOMPUTE) != 0;
+  if (!faithful) {
+    p->detJ = (double *)xcalloc((size_t)(p->E * P), sizeof(double));
+    p->invJ = (double *)xcalloc((size_t)(p->E * P * dim * dim), sizeof(double));
+    for (int64_t e = 0; e < p->E; ++e)
+      element_geometry(b, p->vtx + e * nv * dim, d->flags, p->detJ + e * P, p->invJ + e * P * dim * dim);
+  }
+  if (!faithful || d->physics == ORC_ELASTIC3D) {
+    p->mat = (double *)xcalloc((size_t)(p->E * P * nm), sizeof(double));
+    for (int64_t e = 0; e < p->E; ++e) element_material(p, e, p->mat + e * P * nm, NULL);
+  }
+  /* Diagonal mass: Scalar.cpp:34-39 (no rho), Elastic3D.cpp:63-67 (rho);
+   * summed in element order then reciprocal (Order2Newmark.cpp:32-66). */
+  p->mi = (double *)xcalloc((size_t)p->G, sizeof(double));
+  for (int64_t e = 0; e < p->E; ++e) {
+    double m[9 * ORC_MAX_P], rho[ORC_MAX_P], me[ORC_MAX_P];
+    element_material(p, e, m, rho);
+    orc_element_test(b->shape, b->n - 1, p->vtx + e * nv * dim, d->flags, rho, me);
+    for (int q = 0; q < P; ++q) p->mi[p->conn[e * P + q]] += me[q];
+  }
+  for (int64_t g = 0; g < p->G; ++g) p->mi[g] = 1.0 / p->mi[g];
+  size_t nf = (size_t)(p->G * p->c);
+  p->u = (double *)xcalloc(nf, sizeof(double));
+  p->v = (double *)xcalloc(nf, sizeof(double));
+  p->a = (double *)xcalloc(nf, sizeof(double));
+  p->a_ = (double *)xcalloc(nf, sizeof(double));
+  return p;
+}
+
+void orc_destroy(orc_problem *p) {
+  if (!p) return;
+  free(p->vtx); free(p->par); free(p->conn); free(p->xyz);
+  free(p->detJ); free(p->invJ); free(p->mat); free(p->mi);
+  free(p->u); free(p->v); free(p->a); free(p->a_);
+  free(p->col_off); free(p->col_elems);
+  for (int i = 0; i < p->nsrc; ++i) free(p->src[i].wts);
+  for (int i = 0; i < p->nrec; ++i) free(p->rec[i].l);
+  free(p->src); free(p->rec);
+  free(p);
+}
+
+int64_t orc_num_nodes(const orc_problem *p) { return p->G; }
+int orc_num_components(const orc_problem *p) { return p->c; }
+int64_t orc_step_index(const orc_problem *p) { return p->step; }
+int orc_node_coords(const orc_problem *p, double *xyz) {
+  memcpy(xyz, p->xyz, sizeof(double) * (size_t)(p->G * p->b.dim));
+  return 0;
+}
+
+/* First element (in element order) whose hull holds x, as in
+ * Problem::initializeElements Problem.cpp:77-109 (rank-0 attach rule). */
+static int64_t locate(const orc_problem *p, const double *x, double *ref) {
+  const int nv = p->b.nv, d = p->b.dim;
+  for (int64_t e = 0; e < p->E; ++e) {
+    int h = orc_check_hull(p->b.shape, p->vtx + e * nv * d, x);
+    if (h < 0) return -2;
+    if (h == 1) {
+      if (orc_inverse_map(p->b.shape, p->vtx + e * nv * d, x, ref)) return -2;
+      return e;
+    }
+  }
+  set_err("point (%g, %g, %g) is outside the mesh", x[0], x[1], d == 3 ? x[2] : 0.0);
+  return -1;
+}
+
+int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double amp,
+                   int kind, const double *comp) {
+  const basis_t *b = &p->b;
+  const int P = b->P, c = p->c, d = b->dim;
+  if (kind == 1 && p->d.physics != ORC_ELASTIC3D) { set_err("moment tensor needs elastic physics"); return -1; }
+  double ref[3] = {0, 0, 0};
+  int64_t e = locate(p, x, ref);
+  if (e < 0) return -1;
+  p->src = (src_t *)realloc(p->src, sizeof(src_t) * (size_t)(p->nsrc + 1));
+  src_t *s = &p->src[p->nsrc];
+  s->elem = e; s->f0 = f0; s->t0 = t0; s->amp = amp;
+  memcpy(s->ref, ref, sizeof ref);
+  s->wts = (double *)xcalloc((size_t)(P * c), sizeof(double));
+  const double *vtx = p->vtx + e * b->nv * d;
+  if (kind == 0) {
+    /* delta coefficients l_p/(w_p detJ_p) (getDeltaFunctionCoefficients),
+     * times direction (Ricker::fire), then x w_p detJ_p
+     * (applyTestAndIntegrate, Scalar.cpp:87) -- omitted for elastic in the
+     * reference-literal mode (Elastic3D.cpp:126-133, quirk Q2). */
+    double delta[ORC_MAX_P], integ[ORC_MAX_P];
+    orc_element_delta(b->shape, b->n - 1, vtx, p->d.flags, ref, delta);
+    int scale = !(p->d.physics == ORC_ELASTIC3D && (p->d.flags & ORC_Q2_ELASTIC_SRC_UNSCALED));
+    if (scale) orc_element_test(b->shape, b->n - 1, vtx, p->d.flags, delta, integ);
+    for (int q = 0; q < P; ++q)
+      for (int a = 0; a < c; ++a)
+        s->wts[q * c + a] = (scale ? integ[q] : delta[q]) * comp[a];
+  } else {
+    /* moment tensor: f_{q,a} = sum_b M_ab dphi_q/dx_b (x_s) */
+    double l[ORC_MAX_P], dl[ORC_MAX_P * 3], det, iJ[9];
+    tensor_lagrange(b, ref, l, dl);
+    orc_p1_jacobian(b->shape, vtx, ref, p->d.flags, &det, iJ);
+    const double M[3][3] = {{comp[0], comp[5], comp[4]},
+                            {comp[5], comp[1], comp[3]},
+                            {comp[4], comp[3], comp[2]}};
+    for (int q = 0; q < P; ++q) {
+      double gx[3];
+      for (int a = 0; a < 3; ++a) {
+        double sacc = 0;
+        for (int k = 0; k < 3; ++k) sacc += iJ[a * 3 + k] * dl[q * 3 + k];
+        gx[a] = sacc;
+      }
+      for (int a = 0; a < 3; ++a)
+        s->wts[q * 3 + a] = M[a][0] * gx[0] + M[a][1] * gx[1] + M[a][2] * gx[2];
+    }
+  }
+  return p->nsrc++;
+}
+
+int orc_add_receiver(orc_problem *p, const double *x) {
+  double ref[3] = {0, 0, 0};
+  int64_t e = locate(p, x, ref);
+  if (e < 0) return -1;
+  p->rec = (rec_t *)realloc(p->rec, sizeof(rec_t) * (size_t)(p->nrec + 1));
+  rec_t *r = &p->rec[p->nrec];
+  r->elem = e;
+  r->l = (double *)xcalloc((size_t)p->b.P, sizeof(double));
+  tensor_lagrange(&p->b, ref, r->l, NULL);
+  return p->nrec++;
+}
+
+int orc_set_field(orc_problem *p, int which, const double *vals) {
+  double *f = which == 0 ? p->u : which == 1 ? p->v : NULL;
+  if (!f) { set_err("bad field"); return -1; }
+  memcpy(f, vals, sizeof(double) * (size_t)(p->G * p->c));
+  return 0;
+}
+
+int orc_get_field(const orc_problem *p, int which, double *vals) {
+  const double *f = which == 0 ? p->u : which == 1 ? p->v : which == 2 ? p->a : NULL;
+  if (!f) { set_err("bad field"); return -1; }
+  memcpy(vals, f, sizeof(double) * (size_t)(p->G * p->c));
+  return 0;
+}
+
+int orc_inverse_mass(const orc_problem *p, double *mi) {
+  memcpy(mi, p->mi, sizeof(double) * (size_t)p->G);
+  return 0;
+}
+
+/* a = f(t) - K u, assembled.  Problem::assembleIntoGlobalDof Problem.cpp:143-214. */
+static void assemble(orc_problem *p, const double *u, double t, double *a, int with_src) {
+  const int P = p->b.P, c = p->c;
+  memset(a, 0, sizeof(double) * (size_t)(p->G * c));
+  if (p->d.threads <= 1) {
+    double ue[ORC_MAX_P * 3], ke[ORC_MAX_P * 3];
+    for (int64_t e = 0; e < p->E; ++e) {
+      const int64_t *cn = p->conn + e * P;
+      for (int q = 0; q < P; ++q)
+        for (int k = 0; k < c; ++k) ue[q * c + k] = u[cn[q] * c + k];
+      element_stiffness(p, e, ue, ke);
+      for (int q = 0; q < P; ++q)
+        for (int k = 0; k < c; ++k) a[cn[q] * c + k] += -ke[q * c + k];
+    }
+  } else {
+    for (int col = 0; col < p->ncolours; ++col) {
+      const int64_t lo = p->col_off[col], hi = p->col_off[col + 1];
+#pragma omp parallel for num_threads(p->d.threads) schedule(static)
+      for (int64_t i = lo; i < hi; ++i) {
+        double ue[ORC_MAX_P * 3], ke[ORC_MAX_P * 3];
+        const int64_t e = p->col_elems[i];
+        const int64_t *cn = p->conn + e * P;
+        for (int q = 0; q < P; ++q)
+          for (int k = 0; k < c; ++k) ue[q * c + k] = u[cn[q] * c + k];
+        element_stiffness(p, e, ue, ke);
+        for (int q = 0; q < P; ++q)
+          for (int k = 0; k < c; ++k) a[cn[q] * c + k] += -ke[q * c + k];
+      }
+    }
+  }
+  if (with_src) {
+    /* computeSourceTerm at time t (Problem.cpp:196; Scalar.cpp:79-88;
+     * Elastic3D.cpp:126-133), sources in attach order. */
+    for (int i = 0; i < p->nsrc; ++i) {
+      const src_t *s = &p->src[i];
+      double stf = orc_ricker(t, s->f0, s->t0, s->amp);
+      const int64_t *cn = p->conn + s->elem * P;
+      for (int q = 0; q < P; ++q)
+        for (int k = 0; k < c; ++k) a[cn[q] * c + k] += s->wts[q * c + k] * stf;
+    }
+  }
+}
+
+int orc_acceleration(orc_problem *p, double t, double *a) {
+  assemble(p, p->u, t, a, 1);
+  const int c = p->c;
+  for (int64_t g = 0; g < p->G; ++g)
+    for (int k = 0; k < c; ++k) a[g * c + k] *= p->mi[g];
+  return 0;
+}
+
+int orc_run(orc_problem *p, int64_t nsteps, double dt, double *seis) {
+  const int c = p->c, P = p->b.P;
+  const int64_t G = p->G;
+  const double acl = 0.5 * dt, dsp = 0.5 * dt * dt;
+  /* components advanced by takeTimeStep: Order2Newmark.cpp:93-96 lists
+   * {"ax","ay","ax","a"}; corrected mode advances each component once. */
+  int comps[4], ncomp = 0;
+  if (c == 1) {
+    comps[ncomp++] = 0;
+  } else if (p->d.flags & ORC_Q1_Z_NOT_ADVANCED) {
+    comps[ncomp++] = 0; comps[ncomp++] = 1; comps[ncomp++] = 0;
+  } else {
+    comps[ncomp++] = 0; comps[ncomp++] = 1; comps[ncomp++] = 2;
+  }
+  for (int64_t n = 0; n < nsteps; ++n) {
+    const double t = (double)p->step * dt; /* integer step count (quirk Q11) */
+    assemble(p, p->u, t, p->a, 1);
+    /* applyInverseMassMatrix Order2Newmark.cpp:68-83 */
+    for (int64_t g = 0; g < G; ++g)
+      for (int k = 0; k < c; ++k) p->a[g * c + k] *= p->mi[g];
+    /* takeTimeStep Order2Newmark.cpp:85-114 (VecAXPBYPCZ twice + VecCopy) */
+    for (int ci = 0; ci < ncomp; ++ci) {
+      const int k = comps[ci];
+      for (int64_t g = 0; g < G; ++g) {
+        const int64_t i = g * c + k;
+        p->v[i] = acl * p->a[i] + acl * p->a_[i] + 1.0 * p->v[i];
+        p->u[i] = dt * p->v[i] + dsp * p->a[i] + 1.0 * p->u[i];
+        p->a_[i] = p->a[i];
+      }
+    }
+    p->step++;
+    if (seis) {
+      for (int r = 0; r < p->nrec; ++r) {
+        const rec_t *rc = &p->rec[r];
+        const int64_t *cn = p->conn + rc->elem * P;
+        for (int k = 0; k < c; ++k) {
+          /* Kahan-compensated FP64 sum */
+          double s = 0, comp = 0;
+          for (int q = 0; q < P; ++q) {
+            double y = rc->l[q] * p->u[cn[q] * c + k] - comp;
+            double tt = s + y;
+            comp = (tt - s) - y;
+            s = tt;
+          }
+          seis[((int64_t)r * c + k) * nsteps + n] = s;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+double orc_max_eigenvalue(orc_problem *p, int iters, uint64_t seed) {
+  const int c = p->c;
+  const int64_t N = p->G * c;
+  double *x = (double *)xcalloc((size_t)N, sizeof(double));
+  double *y = (double *)xcalloc((size_t)N, sizeof(double));
+  uint64_t st = seed ? seed : 1;
+  for (int64_t i = 0; i < N; ++i) {
+    st = mix64(st);
+    x[i] = ((st >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+  }
+  double lam = 0;
+  for (int it = 0; it < iters; ++it) {
+    /* y = M^-1 K x  (assemble gives -K x) */
+    assemble(p, x, 0.0, y, 0);
+    double num = 0, den = 0;
+    for (int64_t g = 0; g < p->G; ++g)
+      for (int k = 0; k < c; ++k) {
+        int64_t i = g * c + k;
+        y[i] = -y[i] * p->mi[g];
+        num += y[i] * y[i] / p->mi[g];
+        den += x[i] * y[i] / p->mi[g];
+      }
+    lam = num / den;
+    double nrm = 0;
+    for (int64_t i = 0; i < N; ++i) nrm = fmax(nrm, fabs(y[i]));
+    for (int64_t i = 0; i < N; ++i) x[i] = y[i] / nrm;
+  }
+  free(x); free(y);
+  return lam;
+}
+
+double orc_energy(orc_problem *p) {
+  const int c = p->c;
+  const int64_t N = p->G * c;
+  double *ku = (double *)xcalloc((size_t)N, sizeof(double));
+  assemble(p, p->u, 0.0, ku, 0); /* -K u */
+  double ek = 0, ep = 0;
+  for (int64_t g = 0; g < p->G; ++g)
+    for (int k = 0; k < c; ++k) {
+      int64_t i = g * c + k;
+      ek += 0.5 * p->v[i] * p->v[i] / p->mi[g];
+      ep += -0.5 * p->u[i] * ku[i];
+    }
+  free(ku);
+  return ek + ep;
+}

@@ -1,0 +1,121 @@
+/*
+ * oracle.h -- FP64 CPU restatement of the Salvus explicit spectral-element time
+ * step.  TEST INFRASTRUCTURE ONLY: this library is the checker for the CUDA
+ * product path.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline legs may load it; the product never links or calls it.
+ *
+ * Every routine restates the reference algorithm from the cited reference
+ * source lines (paths relative to the reference project root).  Node
+ * numbering deliberately uses a different method (coordinate keys) from the
+ * product (topological keys) so the two implementations share no code.
+ */
+#ifndef SALVUS_ORACLE_H
+#define SALVUS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_QUAD = 0, ORC_HEX = 1 };
+enum { ORC_ACOUSTIC = 0, ORC_ELASTIC3D = 1 };
+
+/* Reference quirk switches ("reference-literal" mode).  The default (0) is the
+ * corrected physics that the GPU path is checked against. */
+enum {
+  /* Order2Newmark.cpp:93-96 lists {"ax","ay","ax","a"}: uz never advances. */
+  ORC_Q1_Z_NOT_ADVANCED = 1u << 0,
+  /* Elastic3D.cpp:126-133 omits applyTestAndIntegrate on the source term. */
+  ORC_Q2_ELASTIC_SRC_UNSCALED = 1u << 1,
+  /* TensorQuad.cpp:383-390 applies J^-1 at the output point (not per
+   * quadrature point) in the 2-D gradient-test integral. */
+  ORC_Q3_QUAD_INVJ_AT_OUTPUT = 1u << 2,
+  /* QuadP1.h:20-27,85-86 evaluates dN/dr with r and dN/ds with s swapped
+   * (exact only on parallelograms). */
+  ORC_Q17_QUAD_SWAPPED_JAC = 1u << 3,
+  /* Scalar.cpp:45 / TensorQuad.cpp:194,385 / Hexahedra.cpp:600,702: rebuild
+   * the Jacobian and re-interpolate material at every GLL point every call
+   * (reference operation count; used for the faithful CPU timing). */
+  ORC_FAITHFUL_RECOMPUTE = 1u << 4,
+};
+
+typedef struct {
+  int shape;             /* ORC_QUAD or ORC_HEX */
+  int order;             /* polynomial order N (n = N + 1 GLL points per dim) */
+  int physics;           /* ORC_ACOUSTIC or ORC_ELASTIC3D */
+  int64_t n_vertices;
+  const double *vertices;   /* [n_vertices][dim] */
+  int64_t n_elements;
+  const int64_t *cells;     /* [n_elements][4 | 8], PETSc right-hand order */
+  /* Per element, per element-vertex material (ExodusModel NAME_0..NAME_k
+   * convention, ExodusModel.cpp:455-470):
+   *   acoustic: [1][n_elements][nv] = VP
+   *   elastic : [6][n_elements][nv] = RHO, VPV, VPH, VSV, VSH, ETA */
+  const double *params;
+  unsigned flags;
+  int threads;              /* OpenMP threads for element loops (>=1) */
+} orc_desc;
+
+typedef struct orc_problem orc_problem;
+
+/* ---- GLL / Lagrange tables (math restatement of the sympy code generator,
+ * src/py/pysalvus/code_generation/quadrature_points_weights.py:55-93,
+ * code_generator.py:13-43) ---- */
+int orc_gll(int order, double *points, double *weights);
+int orc_deriv_matrix(int order, double *D /* [n][n], D[i*n+j] = l_j'(xi_i) */);
+int orc_lagrange(int order, double xi, double *l /* [n] */, double *dl /* [n] or NULL */);
+double orc_ricker(double t, double f0, double t0, double amp);
+
+/* ---- element level (single element, no mesh) ---- */
+int orc_p1_jacobian(int shape, const double *vtx, const double *ref, unsigned flags,
+                    double *detJ, double *invJ /* [d][d] */);
+int orc_p1_interpolate(int shape, const double *ref, double *w /* [4|8] */);
+int orc_check_hull(int shape, const double *vtx, const double *x);
+int orc_inverse_map(int shape, const double *vtx, const double *x, double *ref);
+/* grad[p][d] of nodal field u[p] (computeGradient). */
+int orc_element_gradient(int shape, int order, const double *vtx, unsigned flags,
+                         const double *u, double *grad);
+/* out[p] = integral of grad(phi_p) . f (applyGradTestAndIntegrate). */
+int orc_element_grad_test(int shape, int order, const double *vtx, unsigned flags,
+                          const double *f /* [P][d] */, double *out);
+/* out[p] = f[p] w_p detJ_p (applyTestAndIntegrate). */
+int orc_element_test(int shape, int order, const double *vtx, unsigned flags,
+                     const double *f, double *out);
+/* delta-function coefficients l_p(ref)/(w_p detJ_p) (getDeltaFunctionCoefficients). */
+int orc_element_delta(int shape, int order, const double *vtx, unsigned flags,
+                      const double *ref, double *out);
+/* P1 vertex parameter interpolated to GLL points (ParAtIntPts). */
+int orc_element_par(int shape, int order, const double *par_vtx, double *out);
+
+/* ---- problem level ---- */
+orc_problem *orc_create(const orc_desc *d);
+void orc_destroy(orc_problem *p);
+const char *orc_last_error(void);
+int64_t orc_num_nodes(const orc_problem *p);
+int orc_num_components(const orc_problem *p);
+int orc_node_coords(const orc_problem *p, double *xyz /* [G][dim] */);
+/* kind 0: force, comp = direction [c]; kind 1: moment tensor
+ * comp = [Mxx, Myy, Mzz, Myz, Mxz, Mxy]. Returns source index or <0. */
+int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double amp,
+                   int kind, const double *comp);
+int orc_add_receiver(orc_problem *p, const double *x);
+/* which: 0 = u, 1 = v.  Arrays are [G][c]. */
+int orc_set_field(orc_problem *p, int which, const double *vals);
+int orc_get_field(const orc_problem *p, int which, double *vals);
+int orc_inverse_mass(const orc_problem *p, double *mi /* [G] */);
+/* Advance nsteps (Main.cpp:45-66 loop body).  seis may be NULL, else
+ * [n_receivers][c][nsteps] of u sampled after each step. */
+int orc_run(orc_problem *p, int64_t nsteps, double dt, double *seis);
+/* a = M^-1 (f(t) - K u) for the current state, [G][c]. */
+int orc_acceleration(orc_problem *p, double t, double *a);
+/* lambda_max of M^-1 K by power iteration (dt_crit = 2/sqrt(lambda)). */
+double orc_max_eigenvalue(orc_problem *p, int iters, uint64_t seed);
+/* Kinetic + strain energy 0.5 v^T M v + 0.5 u^T K u (FP64, fixed order). */
+double orc_energy(orc_problem *p);
+int64_t orc_step_index(const orc_problem *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,94 @@
+"""Seeded synthetic workloads for the headline configurations.
+
+All inputs are synthetic (no datasets): structured meshes, Gaussian random
+field models and seeded source / receiver positions.  Sizes are parameters so
+that tests can run the same physics at reduced size.
+"""
+import numpy as np
+
+from . import meshgen
+from .core import ACOUSTIC, ELASTIC3D, HEX, QUAD
+
+
+def standing_wave_2d(nel=40, order=4, L=1.0e4, vp=4000.0):
+    """2-D acoustic quad mesh of an L x L square, homogeneous vp, free
+    (Neumann) boundaries.  Initial condition u = cos(pi x/L) cos(pi y/L)."""
+    V, C = meshgen.structured_quad(nel, nel, L, L)
+    par = np.full((1, len(C), 4), vp)
+    return dict(shape=QUAD, order=order, physics=ACOUSTIC, vertices=V, cells=C, params=par,
+                L=L, vp=vp, omega=np.sqrt(2.0) * np.pi * vp / L)
+
+
+def standing_wave_initial(xyz, L):
+    return np.prod(np.cos(np.pi * xyz / L), axis=1)
+
+
+def ricker_2d(nel=40, order=4, L=1.0e4, vp=4000.0, f0=2.0, n_receivers=16, radius=3.0e3, seed=0):
+    """Point Ricker source at the centre and a seeded ring of receivers."""
+    cfg = standing_wave_2d(nel, order, L, vp)
+    center = (L / 2, L / 2)
+    cfg.update(
+        sources=[dict(location=center, center_freq=f0, time_delay=1.2 / f0, amplitude=1.0,
+                      direction=[1.0])],
+        receivers=meshgen.ring_positions(center, radius, n_receivers, seed),
+    )
+    return cfg
+
+
+def elastic_hex(nel=64, order=4, h=200.0, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
+                corr=1000.0, f0=1.5, n_receivers=64, seed=1):
+    """3-D elastic hex cube with a Gaussian random-field perturbation of
+    vp, vs and rho, a moment-tensor Ricker source at the centre and receivers
+    at seeded positions on the top surface."""
+    L = nel * h
+    V, C = meshgen.structured_hex(nel, nel, nel, L, L, L)
+    grf = meshgen.gaussian_random_field((nel + 1,) * 3, h, corr, seed)  # [z][y][x]
+    pert = 1.0 + std * grf.ravel()
+    vpv, vsv, rhov = vp * pert, vs * pert, rho * pert
+    params = np.stack([meshgen.per_element_vertex(rhov, C), meshgen.per_element_vertex(vpv, C),
+                       meshgen.per_element_vertex(vsv, C)])
+    rng = np.random.default_rng(seed)
+    mt = rng.standard_normal(6)
+    rec_xy = rng.uniform(0.02 * L, 0.98 * L, size=(n_receivers, 2))
+    receivers = np.concatenate([rec_xy, np.full((n_receivers, 1), L)], axis=1)
+    return dict(shape=HEX, order=order, physics=ELASTIC3D, vertices=V, cells=C, params=params,
+                L=L, sources=[dict(location=(L / 2 + 0.37 * h, L / 2 - 0.21 * h, L / 2 + 0.13 * h),
+                                   center_freq=f0, time_delay=1.2 / f0, amplitude=1.0e13,
+                                   moment_tensor=mt)],
+                receivers=receivers)
+
+
+def acoustic_hex(nel=8, order=4, L=1.0e4, vp=4000.0):
+    V, C = meshgen.structured_hex(nel, nel, nel, L, L, L)
+    par = np.full((1, len(C), 8), vp)
+    return dict(shape=HEX, order=order, physics=ACOUSTIC, vertices=V, cells=C, params=par, L=L,
+                vp=vp, omega=np.sqrt(3.0) * np.pi * vp / L)
+
+
+def batched_quad(nel=200, order=4, L=1.0e4, vmin=2500.0, vmax=5500.0, corr=800.0, n_shots=256,
+                 n_receivers=16, seed=2):
+    """Smooth random velocity model on an nel x nel quad mesh and n_shots
+    Ricker sources (f0 uniform in 1.5-3 Hz, positions uniform in the interior)."""
+    V, C = meshgen.structured_quad(nel, nel, L, L)
+    h = L / nel
+    grf = meshgen.gaussian_random_field((nel + 1, nel + 1), h, corr, seed).ravel()
+    lo, hi = grf.min(), grf.max()
+    vpv = vmin + (vmax - vmin) * (grf - lo) / (hi - lo)
+    par = meshgen.per_element_vertex(vpv, C)[None]
+    rng = np.random.default_rng(seed)
+    f0 = rng.uniform(1.5, 3.0, n_shots)
+    pos = rng.uniform(0.1 * L, 0.9 * L, size=(n_shots, 2))
+    sources = [dict(location=tuple(pos[s]), center_freq=f0[s], time_delay=1.2 / f0[s],
+                    amplitude=1.0, direction=[1.0], shot=s) for s in range(n_shots)]
+    receivers = meshgen.ring_positions((L / 2, L / 2), 0.35 * L, n_receivers, seed)
+    return dict(shape=QUAD, order=order, physics=ACOUSTIC, vertices=V, cells=C, params=par, L=L,
+                sources=sources, receivers=receivers)
+
+
+def oracle_params(cfg):
+    """Parameter array in the oracle's layout (elastic: RHO VPV VPH VSV VSH ETA)."""
+    p = cfg["params"]
+    if cfg["physics"] == ACOUSTIC:
+        return p
+    rho, vp, vs = p
+    return np.stack([rho, vp, vp, vs, vs, np.ones_like(rho)])

@@ -1,0 +1,905 @@
+// abi.cu -- extern "C" entry points (include/salvus_b200.h): mesh flattening,
+// device residency, and the per-step launch sequence
+//   stiffness (element-local residual) -> sources -> node gather + inverse
+//   mass + Newmark -> receivers.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <vector>
+
+#include "internal.h"
+#include "kernels_setup.cuh"
+#include "kernels_stiffness.cuh"
+#include "kernels_step.cuh"
+
+namespace salvus {
+const char *last_error();
+int flatten_mesh(salvus_mesh *m, const int64_t *cells, int64_t n_vertices);
+int locate_point(const salvus_mesh *m, const double *x, int64_t *elem, double *ref);
+
+static std::atomic<int64_t> g_launches{0};
+
+enum Kind { K_STIFF = 0, K_SRC, K_UPDATE, K_REC, K_GATHER, K_MINV, K_NEWMARK, K_GRAPH, K_NKINDS };
+static const char *kKindNames[K_NKINDS] = {"stiffness", "source",        "gather_update",
+                                           "receivers", "gather",        "inverse_mass",
+                                           "newmark",   "graph_replay"};
+
+struct ProfScope {
+  salvus_problem *p;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(salvus_problem *p_, int k) : p(p_), kind(k) {
+    if (p && p->profiling) {
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      cudaEventRecord(a, p->stream);
+    }
+  }
+  ~ProfScope() {
+    if (a) {
+      cudaEventRecord(b, p->stream);
+      p->events.push_back({kind, a, b});
+    }
+  }
+};
+
+static inline unsigned blocks_for(int64_t n, int threads) {
+  return (unsigned)((n + threads - 1) / threads);
+}
+
+template <typename real>
+static DMatrix<real> dmatrix(const Basis &b) {
+  DMatrix<real> d{};
+  for (int i = 0; i < b.n * b.n; ++i) d.d[i] = (real)b.D[i];
+  return d;
+}
+
+static int check_launch(const char *what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(SALVUS_E_CUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
+  return SALVUS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stiffness dispatch
+template <int DIM, int N, typename real>
+static int launch_acoustic(const salvus_mesh *m, const real *rec, const real *u, real *r,
+                           cudaStream_t st) {
+  using S = AcousticShape<DIM, N>;
+  const unsigned grid = blocks_for(m->E, S::EPB);
+  acoustic_stiffness_kernel<DIM, N, real><<<grid, S::THREADS, 0, st>>>(
+      m->E, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
+  g_launches++;
+  return check_launch("acoustic stiffness");
+}
+
+template <int N, typename real>
+static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, real *r,
+                          cudaStream_t st) {
+  using S = ElasticShape<N, real>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(elastic_hex_stiffness_kernel<N, real>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+    attr_set = true;
+  }
+  const unsigned grid = blocks_for(m->E, S::EPB);
+  elastic_hex_stiffness_kernel<N, real><<<grid, S::THREADS, S::SMEM, st>>>(
+      m->E, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
+  g_launches++;
+  return check_launch("elastic stiffness");
+}
+
+template <int N, typename real>
+static int acoustic2(const salvus_mesh *m, const real *rec, const real *u, real *r, cudaStream_t s) {
+  return launch_acoustic<2, N, real>(m, rec, u, r, s);
+}
+template <int N, typename real>
+static int acoustic3(const salvus_mesh *m, const real *rec, const real *u, real *r, cudaStream_t s) {
+  return launch_acoustic<3, N, real>(m, rec, u, r, s);
+}
+
+template <typename real>
+static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u, real *r,
+                            cudaStream_t st) {
+  if (m->physics == SALVUS_ELASTIC3D) {
+    switch (m->order) {
+      case 1: return launch_elastic<1, real>(m, rec, u, r, st);
+      case 2: return launch_elastic<2, real>(m, rec, u, r, st);
+      case 3: return launch_elastic<3, real>(m, rec, u, r, st);
+      case 4: return launch_elastic<4, real>(m, rec, u, r, st);
+      case 5: return launch_elastic<5, real>(m, rec, u, r, st);
+      case 6: return launch_elastic<6, real>(m, rec, u, r, st);
+    }
+  } else if (m->shape == SALVUS_QUAD) {
+    switch (m->order) {
+      case 1: return acoustic2<1, real>(m, rec, u, r, st);
+      case 2: return acoustic2<2, real>(m, rec, u, r, st);
+      case 3: return acoustic2<3, real>(m, rec, u, r, st);
+      case 4: return acoustic2<4, real>(m, rec, u, r, st);
+      case 5: return acoustic2<5, real>(m, rec, u, r, st);
+      case 6: return acoustic2<6, real>(m, rec, u, r, st);
+      case 7: return acoustic2<7, real>(m, rec, u, r, st);
+      case 8: return acoustic2<8, real>(m, rec, u, r, st);
+      case 9: return acoustic2<9, real>(m, rec, u, r, st);
+      case 10: return acoustic2<10, real>(m, rec, u, r, st);
+    }
+  } else {
+    switch (m->order) {
+      case 1: return acoustic3<1, real>(m, rec, u, r, st);
+      case 2: return acoustic3<2, real>(m, rec, u, r, st);
+      case 3: return acoustic3<3, real>(m, rec, u, r, st);
+      case 4: return acoustic3<4, real>(m, rec, u, r, st);
+      case 5: return acoustic3<5, real>(m, rec, u, r, st);
+      case 6: return acoustic3<6, real>(m, rec, u, r, st);
+    }
+  }
+  return fail(SALVUS_E_UNSUPPORTED, "no stiffness kernel for shape %d order %d", m->shape, m->order);
+}
+
+// ---------------------------------------------------------------------------
+// mesh setup
+template <typename real, bool kPack>
+static int build_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &mass_local) {
+  const int rw = record_words(m->shape, m->physics, sizeof(real) == 8);
+  int rc = out.alloc(sizeof(real) * (size_t)(m->E * m->P) * rw);
+  if (rc) return rc;
+  GllTable gll{};
+  for (int i = 0; i < m->n; ++i) {
+    gll.xi[i] = m->basis.xi[i];
+    gll.w[i] = m->basis.w[i];
+  }
+  const int64_t total = m->E * m->P;
+  geometry_kernel<real, kPack><<<blocks_for(total, 128), 128, 0, m->stream>>>(
+      m->E, m->dim, m->n, m->P, m->physics, rw, m->d_vtx.as<double>(), m->d_par.as<double>(),
+      m->d_conn.as<int32_t>(), gll, out.as<real>(), mass_local.as<double>());
+  g_launches++;
+  return check_launch("geometry");
+}
+
+static int mesh_setup_device(salvus_mesh *m) {
+  int rc;
+  SALVUS_CUDA(cudaSetDevice(m->device));
+  SALVUS_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  const int64_t EP = m->E * m->P;
+  if ((rc = m->d_conn.alloc(sizeof(int32_t) * EP))) return rc;
+  if ((rc = m->d_inc_off.alloc(sizeof(int32_t) * (m->G + 1)))) return rc;
+  if ((rc = m->d_inc_idx.alloc(sizeof(int32_t) * EP))) return rc;
+  if ((rc = m->d_vtx.alloc(sizeof(double) * m->vtx.size()))) return rc;
+  if ((rc = m->d_par.alloc(sizeof(double) * m->par.size()))) return rc;
+  if ((rc = m->d_mi64.alloc(sizeof(double) * m->G))) return rc;
+  if ((rc = m->d_mi32.alloc(sizeof(float) * m->G))) return rc;
+  SALVUS_CUDA(cudaMemcpyAsync(m->d_conn.ptr, m->conn.data(), sizeof(int32_t) * EP,
+                              cudaMemcpyHostToDevice, m->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(m->d_inc_off.ptr, m->inc_off.data(), sizeof(int32_t) * (m->G + 1),
+                              cudaMemcpyHostToDevice, m->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(m->d_inc_idx.ptr, m->inc_idx.data(), sizeof(int32_t) * EP,
+                              cudaMemcpyHostToDevice, m->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(m->d_vtx.ptr, m->vtx.data(), sizeof(double) * m->vtx.size(),
+                              cudaMemcpyHostToDevice, m->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(m->d_par.ptr, m->par.data(), sizeof(double) * m->par.size(),
+                              cudaMemcpyHostToDevice, m->stream));
+  DeviceBuffer mass_local;
+  if ((rc = mass_local.alloc(sizeof(double) * EP))) return rc;
+  if ((rc = build_records<float, true>(m, m->d_rec32, mass_local))) return rc;
+  if ((rc = build_records<double, false>(m, m->d_rec64, mass_local))) return rc;
+  mass_gather_kernel<<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
+      m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), mass_local.as<double>(),
+      m->d_mi64.as<double>(), m->d_mi32.as<float>());
+  g_launches++;
+  if ((rc = check_launch("mass"))) return rc;
+  m->mi.resize(m->G);
+  SALVUS_CUDA(cudaMemcpyAsync(m->mi.data(), m->d_mi64.ptr, sizeof(double) * m->G,
+                              cudaMemcpyDeviceToHost, m->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(m->stream));
+  return SALVUS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// problem helpers
+template <typename real>
+static real *F(const DeviceBuffer &b) { return b.as<real>(); }
+
+static int upload_sources(salvus_problem *p) {
+  if (!p->src_dirty) return SALVUS_OK;
+  const salvus_mesh *m = p->mesh;
+  const size_t ns = p->srcs.size();
+  int rc;
+  if (ns) {
+    std::vector<int64_t> el(ns);
+    std::vector<double> par(3 * ns), w(ns * m->P * p->c);
+    for (size_t s = 0; s < ns; ++s) {
+      el[s] = p->srcs[s].elem;
+      par[3 * s] = p->srcs[s].desc.center_freq;
+      par[3 * s + 1] = p->srcs[s].desc.time_delay;
+      par[3 * s + 2] = p->srcs[s].desc.amplitude;
+      std::memcpy(&w[s * m->P * p->c], p->srcs[s].wts.data(), sizeof(double) * m->P * p->c);
+    }
+    if ((rc = p->d_src_elem.alloc(sizeof(int64_t) * ns))) return rc;
+    if ((rc = p->d_src_par.alloc(sizeof(double) * par.size()))) return rc;
+    if ((rc = p->d_src_wts.alloc(sizeof(double) * w.size()))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_src_elem.ptr, el.data(), sizeof(int64_t) * ns,
+                                cudaMemcpyHostToDevice, p->stream));
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_src_par.ptr, par.data(), sizeof(double) * par.size(),
+                                cudaMemcpyHostToDevice, p->stream));
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_src_wts.ptr, w.data(), sizeof(double) * w.size(),
+                                cudaMemcpyHostToDevice, p->stream));
+    SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  }
+  p->src_dirty = false;
+  return SALVUS_OK;
+}
+
+static int upload_receivers(salvus_problem *p) {
+  if (!p->rec_dirty) return SALVUS_OK;
+  const salvus_mesh *m = p->mesh;
+  const size_t nr = p->recs.size();
+  int rc;
+  std::vector<int64_t> el(nr ? nr : 1, 0);
+  std::vector<double> l(nr ? nr * m->P : 1, 0.0);
+  for (size_t r = 0; r < nr; ++r) {
+    el[r] = p->recs[r].elem;
+    std::memcpy(&l[r * m->P], p->recs[r].l.data(), sizeof(double) * m->P);
+  }
+  if ((rc = p->d_rec_elem.alloc(sizeof(int64_t) * el.size()))) return rc;
+  if ((rc = p->d_rec_l.alloc(sizeof(double) * l.size()))) return rc;
+  size_t sz = sizeof(double) * (size_t)(nr ? nr : 1) * p->c * p->seis_cap;
+  if ((rc = p->d_seis.alloc(sz))) return rc;
+  SALVUS_CUDA(cudaMemsetAsync(p->d_seis.ptr, 0, sz, p->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(p->d_rec_elem.ptr, el.data(), sizeof(int64_t) * el.size(),
+                              cudaMemcpyHostToDevice, p->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(p->d_rec_l.ptr, l.data(), sizeof(double) * l.size(),
+                              cudaMemcpyHostToDevice, p->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  p->rec_dirty = false;
+  return SALVUS_OK;
+}
+
+static void drop_graph(salvus_problem *p) {
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  p->graph_exec = nullptr;
+  p->graph_steps = 0;
+}
+
+template <typename real, int C>
+static int launch_sources(salvus_problem *p) {
+  if (p->srcs.empty()) return SALVUS_OK;
+  ProfScope ps(p, K_SRC);
+  source_kernel<real, C><<<1, 256, 0, p->stream>>>(
+      (int)p->srcs.size(), p->mesh->P, p->d_src_elem.as<int64_t>(), p->d_src_par.as<double>(),
+      p->d_src_wts.as<double>(), p->d_step.as<int64_t>(), p->dt, F<real>(p->d_r));
+  g_launches++;
+  return check_launch("source");
+}
+
+template <typename real, int C>
+static int launch_receivers(salvus_problem *p) {
+  ProfScope ps(p, K_REC);
+  const int nr = (int)p->recs.size();
+  const int threads = nr * C > 0 ? (nr * C > 1024 ? 1024 : ((nr * C + 31) / 32) * 32) : 32;
+  receiver_kernel<real, C><<<1, threads, 0, p->stream>>>(
+      nr, p->mesh->P, p->d_rec_elem.as<int64_t>(), p->d_rec_l.as<double>(),
+      p->mesh->d_conn.as<int32_t>(), F<real>(p->d_u), p->d_seis.as<double>(), p->seis_cap,
+      p->d_step.as<int64_t>());
+  g_launches++;
+  return check_launch("receivers");
+}
+
+template <typename real>
+static const real *records(const salvus_problem *p) {
+  return sizeof(real) == 4 ? (const real *)p->mesh->d_rec32.ptr : (const real *)p->mesh->d_rec64.ptr;
+}
+template <typename real>
+static const real *inv_mass(const salvus_problem *p) {
+  return sizeof(real) == 4 ? (const real *)p->mesh->d_mi32.ptr : (const real *)p->mesh->d_mi64.ptr;
+}
+
+template <typename real, int C>
+static int step_fused_t(salvus_problem *p) {
+  const salvus_mesh *m = p->mesh;
+  int rc;
+  {
+    ProfScope ps(p, K_STIFF);
+    if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream)))
+      return rc;
+  }
+  if ((rc = launch_sources<real, C>(p))) return rc;
+  {
+    ProfScope ps(p, K_UPDATE);
+    gather_kernel<real, C, 0><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(
+        m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), F<real>(p->d_r),
+        inv_mass<real>(p), F<real>(p->d_u), F<real>(p->d_v), F<real>(p->d_ap), F<real>(p->d_a),
+        (real)p->dt);
+    g_launches++;
+    if ((rc = check_launch("gather update"))) return rc;
+  }
+  return launch_receivers<real, C>(p);
+}
+
+static int step_fused(salvus_problem *p) {
+  if (p->prec == SALVUS_FP32) return p->c == 1 ? step_fused_t<float, 1>(p) : step_fused_t<float, 3>(p);
+  return p->c == 1 ? step_fused_t<double, 1>(p) : step_fused_t<double, 3>(p);
+}
+
+template <typename real, int C>
+static int assemble_t(salvus_problem *p) {
+  const salvus_mesh *m = p->mesh;
+  int rc;
+  {
+    ProfScope ps(p, K_STIFF);
+    if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream)))
+      return rc;
+  }
+  if ((rc = launch_sources<real, C>(p))) return rc;
+  ProfScope ps(p, K_GATHER);
+  gather_kernel<real, C, 1><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(
+      m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), F<real>(p->d_r), nullptr,
+      nullptr, nullptr, nullptr, F<real>(p->d_a), (real)0);
+  g_launches++;
+  return check_launch("gather");
+}
+
+template <typename real, int C>
+static int minv_t(salvus_problem *p) {
+  ProfScope ps(p, K_MINV);
+  const int64_t N = p->mesh->G * C;
+  inverse_mass_kernel<real, C><<<blocks_for(N, 256), 256, 0, p->stream>>>(
+      p->mesh->G, inv_mass<real>(p), F<real>(p->d_a));
+  g_launches++;
+  return check_launch("inverse mass");
+}
+
+template <typename real, int C>
+static int newmark_t(salvus_problem *p) {
+  int rc;
+  {
+    ProfScope ps(p, K_NEWMARK);
+    const int64_t N = p->mesh->G * C;
+    newmark_kernel<real><<<blocks_for(N, 256), 256, 0, p->stream>>>(
+        N, F<real>(p->d_a), F<real>(p->d_u), F<real>(p->d_v), F<real>(p->d_ap), (real)p->dt);
+    g_launches++;
+    if ((rc = check_launch("newmark"))) return rc;
+  }
+  return launch_receivers<real, C>(p);
+}
+
+static int ready(salvus_problem *p) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  if (!p->dt_set) return fail(SALVUS_E_STATE, "time step not set (salvus_problem_set_dt)");
+  int rc;
+  if ((rc = upload_sources(p))) return rc;
+  if ((rc = upload_receivers(p))) return rc;
+  return SALVUS_OK;
+}
+
+}  // namespace salvus
+
+using namespace salvus;
+
+// ===========================================================================
+extern "C" {
+
+const char *salvus_last_error(void) { return salvus::last_error(); }
+
+const char *salvus_version(void) {
+  return "salvus_b200 0.1 (sm_100a; FP32/FP64 tensor-product SEM; deterministic gather assembly)";
+}
+
+int64_t salvus_launch_count(void) { return g_launches.load(); }
+
+int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out) {
+  if (!d || !out) return fail(SALVUS_E_INVALID, "null argument");
+  *out = nullptr;
+  if (d->shape != SALVUS_QUAD && d->shape != SALVUS_HEX)
+    return fail(SALVUS_E_UNSUPPORTED, "shape %d not supported by the tensor path", d->shape);
+  if (d->physics == SALVUS_ELASTIC3D && d->shape != SALVUS_HEX)
+    return fail(SALVUS_E_UNSUPPORTED, "elastic 3-D physics needs hexahedra (Elastic3D.cpp:137)");
+  if (d->physics != SALVUS_ACOUSTIC && d->physics != SALVUS_ELASTIC3D)
+    return fail(SALVUS_E_INVALID, "unknown physics %d", d->physics);
+  if (d->n_elements <= 0 || d->n_vertices <= 0 || !d->vertices || !d->cells || !d->params)
+    return fail(SALVUS_E_INVALID, "empty mesh");
+  std::unique_ptr<salvus_mesh> m(new salvus_mesh());
+  m->device = device;
+  m->shape = d->shape;
+  m->order = d->order;
+  m->physics = d->physics;
+  int rc = make_basis(d->shape, d->order, &m->basis);
+  if (rc) return rc;
+  m->dim = m->basis.dim;
+  m->nv = m->basis.nv;
+  m->n = m->basis.n;
+  m->P = m->basis.P;
+  m->c = d->physics == SALVUS_ELASTIC3D ? 3 : 1;
+  m->npar = d->physics == SALVUS_ELASTIC3D ? 3 : 1;
+  m->E = d->n_elements;
+  m->vtx.resize((size_t)(m->E * m->nv * m->dim));
+  for (int64_t e = 0; e < m->E; ++e)
+    for (int k = 0; k < m->nv; ++k) {
+      int64_t vi = d->cells[e * m->nv + k];
+      if (vi < 0 || vi >= d->n_vertices)
+        return fail(SALVUS_E_INVALID, "element %lld references vertex %lld out of range",
+                    (long long)e, (long long)vi);
+      for (int a = 0; a < m->dim; ++a)
+        m->vtx[(size_t)((e * m->nv + k) * m->dim + a)] = d->vertices[vi * m->dim + a];
+    }
+  for (int64_t e = 0; e < m->E; ++e) {
+    // right-hand rule check (QuadP1::checkHull / HexP1::checkHull)
+    const double *v = m->vtx.data() + e * m->nv * m->dim;
+    for (int q = 0; q < (m->dim == 2 ? 4 : 8); ++q) {
+      double ref[3];
+      for (int a = 0; a < m->dim; ++a) ref[a] = (m->dim == 2 ? (q >> a) & 1 : (q >> a) & 1) ? 1.0 : -1.0;
+      double det;
+      p1_jacobian(m->dim, v, ref, &det, nullptr);
+      if (!(det > 0))
+        return fail(SALVUS_E_INVALID, "element %lld is inverted or degenerate (detJ <= 0)",
+                    (long long)e);
+    }
+  }
+  const size_t npar_total = (size_t)m->npar * m->E * m->nv;
+  m->par.assign(d->params, d->params + npar_total);
+  for (size_t i = 0; i < npar_total; ++i)
+    if (!std::isfinite(m->par[i])) return fail(SALVUS_E_INVALID, "non-finite material parameter");
+  if ((rc = flatten_mesh(m.get(), d->cells, d->n_vertices))) return rc;
+  if (device >= 0) {
+    if ((rc = mesh_setup_device(m.get()))) return rc;
+  } else {
+    m->host_only = true;  // numbering and coordinates only; no GPU residency
+  }
+  *out = m.release();
+  return SALVUS_OK;
+}
+
+int salvus_mesh_destroy(salvus_mesh *m) {
+  if (!m) return SALVUS_OK;
+  if (m->host_only) {
+    delete m;
+    return SALVUS_OK;
+  }
+  cudaSetDevice(m->device);
+  if (m->stream) cudaStreamSynchronize(m->stream);
+  cudaStream_t s = m->stream;
+  delete m;
+  if (s) cudaStreamDestroy(s);
+  return SALVUS_OK;
+}
+
+int salvus_mesh_info(const salvus_mesh *m, int64_t *G, int32_t *c, int32_t *P) {
+  if (!m) return fail(SALVUS_E_INVALID, "null mesh");
+  if (G) *G = m->G;
+  if (c) *c = m->c;
+  if (P) *P = m->P;
+  return SALVUS_OK;
+}
+
+int salvus_mesh_node_coords(const salvus_mesh *m, double *xyz) {
+  if (!m || !xyz) return fail(SALVUS_E_INVALID, "null argument");
+  std::memcpy(xyz, m->xyz.data(), sizeof(double) * m->xyz.size());
+  return SALVUS_OK;
+}
+
+int salvus_mesh_connectivity(const salvus_mesh *m, int64_t *conn) {
+  if (!m || !conn) return fail(SALVUS_E_INVALID, "null argument");
+  for (size_t i = 0; i < m->conn.size(); ++i) conn[i] = m->conn[i];
+  return SALVUS_OK;
+}
+
+int salvus_mesh_inverse_mass(const salvus_mesh *m, double *mi) {
+  if (!m || !mi) return fail(SALVUS_E_INVALID, "null argument");
+  if (m->host_only) return fail(SALVUS_E_STATE, "host-only mesh has no mass matrix");
+  std::memcpy(mi, m->mi.data(), sizeof(double) * m->G);
+  return SALVUS_OK;
+}
+
+int salvus_mesh_max_eigenvalue(salvus_mesh *m, int32_t iters, uint64_t seed, double *lam_out) {
+  if (!m || !lam_out) return fail(SALVUS_E_INVALID, "null argument");
+  if (m->host_only) return fail(SALVUS_E_STATE, "host-only mesh");
+  SALVUS_CUDA(cudaSetDevice(m->device));
+  const int64_t N = m->G * m->c;
+  DeviceBuffer x, y, r, mass, part;
+  int rc;
+  if ((rc = x.alloc(8 * N)) || (rc = y.alloc(8 * N)) || (rc = r.alloc(8 * m->E * m->P * m->c)) ||
+      (rc = mass.alloc(8 * m->G)) || (rc = part.alloc(8 * 1024)))
+    return rc;
+  std::vector<double> h(N), mh(m->G);
+  std::mt19937_64 rng(seed ? seed : 1);
+  std::uniform_real_distribution<double> U(-0.5, 0.5);
+  for (auto &v : h) v = U(rng);
+  for (int64_t g = 0; g < m->G; ++g) mh[g] = 1.0 / m->mi[g];
+  SALVUS_CUDA(cudaMemcpyAsync(x.ptr, h.data(), 8 * N, cudaMemcpyHostToDevice, m->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(mass.ptr, mh.data(), 8 * m->G, cudaMemcpyHostToDevice, m->stream));
+  const int nb = 512;
+  std::vector<double> hp(nb);
+  auto dot = [&](const double *a, const double *b, double &out) -> int {
+    dot_kernel<double><<<nb, 256, 0, m->stream>>>(N, m->c, a, b, mass.as<double>(), part.as<double>());
+    g_launches++;
+    SALVUS_CUDA(cudaMemcpyAsync(hp.data(), part.ptr, 8 * nb, cudaMemcpyDeviceToHost, m->stream));
+    SALVUS_CUDA(cudaStreamSynchronize(m->stream));
+    double s = 0;
+    for (int i = 0; i < nb; ++i) s += hp[i];
+    out = s;
+    return SALVUS_OK;
+  };
+  double lam = 0;
+  for (int it = 0; it < iters; ++it) {
+    if ((rc = launch_stiffness<double>(m, m->d_rec64.as<double>(), x.as<double>(), r.as<double>(),
+                                       m->stream)))
+      return rc;
+    // y = -gather(r) = K x ; then M^-1
+    if (m->c == 1)
+      gather_kernel<double, 1, 1><<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
+          m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), r.as<double>(), nullptr,
+          nullptr, nullptr, nullptr, y.as<double>(), 0.0);
+    else
+      gather_kernel<double, 3, 1><<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
+          m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), r.as<double>(), nullptr,
+          nullptr, nullptr, nullptr, y.as<double>(), 0.0);
+    g_launches++;
+    if (m->c == 1)
+      inverse_mass_kernel<double, 1><<<blocks_for(N, 256), 256, 0, m->stream>>>(
+          m->G, m->d_mi64.as<double>(), y.as<double>());
+    else
+      inverse_mass_kernel<double, 3><<<blocks_for(N, 256), 256, 0, m->stream>>>(
+          m->G, m->d_mi64.as<double>(), y.as<double>());
+    g_launches++;
+    scale_kernel<double><<<blocks_for(N, 256), 256, 0, m->stream>>>(N, y.as<double>(), -1.0);
+    g_launches++;
+    double xy, xx, yy;
+    if ((rc = dot(x.as<double>(), y.as<double>(), xy)) || (rc = dot(x.as<double>(), x.as<double>(), xx)) ||
+        (rc = dot(y.as<double>(), y.as<double>(), yy)))
+      return rc;
+    lam = xy / xx;
+    std::swap(x.ptr, y.ptr);
+    scale_kernel<double><<<blocks_for(N, 256), 256, 0, m->stream>>>(N, x.as<double>(),
+                                                                     1.0 / std::sqrt(yy));
+    g_launches++;
+  }
+  SALVUS_CUDA(cudaStreamSynchronize(m->stream));
+  *lam_out = lam;
+  return SALVUS_OK;
+}
+
+int salvus_problem_create(salvus_mesh *m, int32_t precision, int32_t n_shots, salvus_problem **out) {
+  if (!m || !out) return fail(SALVUS_E_INVALID, "null argument");
+  *out = nullptr;
+  if (m->host_only) return fail(SALVUS_E_STATE, "mesh was created host-only (device < 0)");
+  if (precision != SALVUS_FP32 && precision != SALVUS_FP64)
+    return fail(SALVUS_E_INVALID, "unknown precision %d", precision);
+  if (n_shots != 1) return fail(SALVUS_E_UNSUPPORTED, "batched shots use salvus_batch_* (n_shots=%d)", n_shots);
+  SALVUS_CUDA(cudaSetDevice(m->device));
+  std::unique_ptr<salvus_problem> p(new salvus_problem());
+  p->mesh = m;
+  p->prec = precision;
+  p->shots = 1;
+  p->c = m->c;
+  p->rsize = precision == SALVUS_FP32 ? 4 : 8;
+  SALVUS_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+  const size_t nf = (size_t)m->G * p->c * p->rsize;
+  int rc;
+  if ((rc = p->d_u.alloc(nf)) || (rc = p->d_v.alloc(nf)) || (rc = p->d_a.alloc(nf)) ||
+      (rc = p->d_ap.alloc(nf)) || (rc = p->d_r.alloc((size_t)m->E * m->P * p->c * p->rsize)) ||
+      (rc = p->d_step.alloc(sizeof(int64_t))))
+    return rc;
+  SALVUS_CUDA(cudaMemsetAsync(p->d_u.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(p->d_v.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(p->d_a.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(p->d_ap.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(p->d_step.ptr, 0, sizeof(int64_t), p->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  p->prof_ms.assign(K_NKINDS, 0.0);
+  p->prof_n.assign(K_NKINDS, 0);
+  *out = p.release();
+  return SALVUS_OK;
+}
+
+int salvus_problem_destroy(salvus_problem *p) {
+  if (!p) return SALVUS_OK;
+  cudaSetDevice(p->mesh->device);
+  cudaStreamSynchronize(p->stream);
+  drop_graph(p);
+  for (auto &e : p->events) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  cudaStream_t s = p->stream;
+  delete p;
+  if (s) cudaStreamDestroy(s);
+  return SALVUS_OK;
+}
+
+int salvus_problem_set_dt(salvus_problem *p, double dt) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(SALVUS_E_INVALID, "dt must be positive");
+  if (p->dt != dt) drop_graph(p);
+  p->dt = dt;
+  p->dt_set = true;
+  return SALVUS_OK;
+}
+
+int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
+  if (!p || !s) return fail(SALVUS_E_INVALID, "null argument");
+  const salvus_mesh *m = p->mesh;
+  if (s->shot != 0) return fail(SALVUS_E_INVALID, "shot index %d out of range", s->shot);
+  if (s->kind == SALVUS_SOURCE_MOMENT_TENSOR && m->physics != SALVUS_ELASTIC3D)
+    return fail(SALVUS_E_INVALID, "moment-tensor sources need elastic physics");
+  if (s->kind != SALVUS_SOURCE_FORCE && s->kind != SALVUS_SOURCE_MOMENT_TENSOR)
+    return fail(SALVUS_E_INVALID, "unknown source kind %d", s->kind);
+  salvus_problem::Src src;
+  src.desc = *s;
+  int rc = locate_point(m, s->location, &src.elem, src.ref);
+  if (rc) return rc;
+  const int n = m->n, P = m->P, c = p->c;
+  std::vector<double> lr(n), ls(n), lt(n, 1.0), dr(n), ds(n), dt(n, 0.0);
+  lagrange_1d(m->basis, src.ref[0], lr.data(), dr.data());
+  lagrange_1d(m->basis, src.ref[1], ls.data(), ds.data());
+  if (m->dim == 3) lagrange_1d(m->basis, src.ref[2], lt.data(), dt.data());
+  src.wts.assign((size_t)P * c, 0.0);
+  if (s->kind == SALVUS_SOURCE_FORCE) {
+    for (int q = 0; q < P; ++q) {
+      const int i = q % n, j = (q / n) % n, k = q / (n * n);
+      const double l = lr[i] * ls[j] * (m->dim == 3 ? lt[k] : 1.0);
+      for (int a = 0; a < c; ++a) src.wts[(size_t)q * c + a] = l * s->comp[a];
+    }
+  } else {
+    double det, iJ[9];
+    p1_jacobian(3, m->vtx.data() + src.elem * 8 * 3, src.ref, &det, iJ);
+    const double M[3][3] = {{s->comp[0], s->comp[5], s->comp[4]},
+                            {s->comp[5], s->comp[1], s->comp[3]},
+                            {s->comp[4], s->comp[3], s->comp[2]}};
+    for (int q = 0; q < P; ++q) {
+      const int i = q % n, j = (q / n) % n, k = q / (n * n);
+      const double gref[3] = {dr[i] * ls[j] * lt[k], lr[i] * ds[j] * lt[k], lr[i] * ls[j] * dt[k]};
+      double gx[3];
+      for (int a = 0; a < 3; ++a) gx[a] = iJ[a * 3] * gref[0] + iJ[a * 3 + 1] * gref[1] + iJ[a * 3 + 2] * gref[2];
+      for (int a = 0; a < 3; ++a)
+        src.wts[(size_t)q * 3 + a] = M[a][0] * gx[0] + M[a][1] * gx[1] + M[a][2] * gx[2];
+    }
+  }
+  p->srcs.push_back(std::move(src));
+  p->src_dirty = true;
+  drop_graph(p);
+  return SALVUS_OK;
+}
+
+int salvus_problem_add_receiver(salvus_problem *p, const double *xyz) {
+  if (!p || !xyz) return fail(SALVUS_E_INVALID, "null argument");
+  const salvus_mesh *m = p->mesh;
+  salvus_problem::Rec r;
+  for (int a = 0; a < 3; ++a) r.xyz[a] = a < m->dim ? xyz[a] : 0.0;
+  int rc = locate_point(m, r.xyz, &r.elem, r.ref);
+  if (rc) return rc;
+  const int n = m->n;
+  std::vector<double> lr(n), ls(n), lt(n, 1.0);
+  lagrange_1d(m->basis, r.ref[0], lr.data(), nullptr);
+  lagrange_1d(m->basis, r.ref[1], ls.data(), nullptr);
+  if (m->dim == 3) lagrange_1d(m->basis, r.ref[2], lt.data(), nullptr);
+  r.l.resize(m->P);
+  for (int q = 0; q < m->P; ++q) r.l[q] = lr[q % n] * ls[(q / n) % n] * (m->dim == 3 ? lt[q / (n * n)] : 1.0);
+  p->recs.push_back(std::move(r));
+  p->rec_dirty = true;
+  drop_graph(p);
+  return SALVUS_OK;
+}
+
+int salvus_problem_set_seismogram_capacity(salvus_problem *p, int64_t steps) {
+  if (!p || steps <= 0) return fail(SALVUS_E_INVALID, "bad capacity");
+  p->seis_cap = steps;
+  p->rec_dirty = true;
+  drop_graph(p);
+  return SALVUS_OK;
+}
+
+static salvus::DeviceBuffer *field_buffer(salvus_problem *p, int32_t f) {
+  switch (f) {
+    case SALVUS_FIELD_U: return &p->d_u;
+    case SALVUS_FIELD_V: return &p->d_v;
+    case SALVUS_FIELD_A: return &p->d_a;
+    case SALVUS_FIELD_A_PREV: return &p->d_ap;
+  }
+  return nullptr;
+}
+
+int salvus_problem_set_field(salvus_problem *p, int32_t f, int32_t shot, const double *vals) {
+  if (!p || !vals) return fail(SALVUS_E_INVALID, "null argument");
+  DeviceBuffer *b = field_buffer(p, f);
+  if (!b || shot != 0) return fail(SALVUS_E_INVALID, "bad field %d / shot %d", f, shot);
+  const size_t N = (size_t)p->mesh->G * p->c;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if (p->prec == SALVUS_FP64) {
+    SALVUS_CUDA(cudaMemcpyAsync(b->ptr, vals, 8 * N, cudaMemcpyHostToDevice, p->stream));
+  } else {
+    // FP64 host array -> FP64 staging on the device -> FP32 field
+    int rc;
+    if (p->d_stage.bytes < 8 * N && (rc = p->d_stage.alloc(8 * N))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_stage.ptr, vals, 8 * N, cudaMemcpyHostToDevice, p->stream));
+    convert_kernel<double, float><<<blocks_for((int64_t)N, 256), 256, 0, p->stream>>>(
+        (int64_t)N, p->d_stage.as<double>(), b->as<float>());
+    g_launches++;
+    if ((rc = check_launch("convert"))) return rc;
+  }
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  return SALVUS_OK;
+}
+
+int salvus_problem_get_field(salvus_problem *p, int32_t f, int32_t shot, double *vals) {
+  if (!p || !vals) return fail(SALVUS_E_INVALID, "null argument");
+  DeviceBuffer *b = field_buffer(p, f);
+  if (!b || shot != 0) return fail(SALVUS_E_INVALID, "bad field %d / shot %d", f, shot);
+  const size_t N = (size_t)p->mesh->G * p->c;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if (p->prec == SALVUS_FP64) {
+    SALVUS_CUDA(cudaMemcpyAsync(vals, b->ptr, 8 * N, cudaMemcpyDeviceToHost, p->stream));
+  } else {
+    int rc;
+    if (p->d_stage.bytes < 8 * N && (rc = p->d_stage.alloc(8 * N))) return rc;
+    convert_kernel<float, double><<<blocks_for((int64_t)N, 256), 256, 0, p->stream>>>(
+        (int64_t)N, b->as<float>(), p->d_stage.as<double>());
+    g_launches++;
+    if ((rc = check_launch("convert"))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(vals, p->d_stage.ptr, 8 * N, cudaMemcpyDeviceToHost, p->stream));
+  }
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  return SALVUS_OK;
+}
+
+int salvus_assemble(salvus_problem *p) {
+  int rc = ready(p);
+  if (rc) return rc;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if (p->prec == SALVUS_FP32) return p->c == 1 ? assemble_t<float, 1>(p) : assemble_t<float, 3>(p);
+  return p->c == 1 ? assemble_t<double, 1>(p) : assemble_t<double, 3>(p);
+}
+
+int salvus_apply_inverse_mass(salvus_problem *p) {
+  int rc = ready(p);
+  if (rc) return rc;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if (p->prec == SALVUS_FP32) return p->c == 1 ? minv_t<float, 1>(p) : minv_t<float, 3>(p);
+  return p->c == 1 ? minv_t<double, 1>(p) : minv_t<double, 3>(p);
+}
+
+int salvus_take_time_step(salvus_problem *p) {
+  int rc = ready(p);
+  if (rc) return rc;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if (p->prec == SALVUS_FP32) rc = p->c == 1 ? newmark_t<float, 1>(p) : newmark_t<float, 3>(p);
+  else rc = p->c == 1 ? newmark_t<double, 1>(p) : newmark_t<double, 3>(p);
+  if (rc == SALVUS_OK) p->step++;
+  return rc;
+}
+
+int salvus_step(salvus_problem *p) {
+  int rc = ready(p);
+  if (rc) return rc;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  rc = step_fused(p);
+  if (rc == SALVUS_OK) p->step++;
+  return rc;
+}
+
+int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
+  int rc = ready(p);
+  if (rc) return rc;
+  if (n_steps < 0) return fail(SALVUS_E_INVALID, "negative step count");
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if (mode == SALVUS_RUN_PLAIN || n_steps < 8) {
+    for (int64_t s = 0; s < n_steps; ++s) {
+      if ((rc = step_fused(p))) return rc;
+      p->step++;
+    }
+    return SALVUS_OK;
+  }
+  if (mode != SALVUS_RUN_GRAPH) return fail(SALVUS_E_INVALID, "unknown run mode %d", mode);
+  const int chunk = 32;
+  if (!p->graph_exec) {
+    const bool prof = p->profiling;
+    p->profiling = false;
+    cudaGraph_t graph;
+    SALVUS_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+    int crc = SALVUS_OK;
+    for (int s = 0; s < chunk && crc == SALVUS_OK; ++s) crc = step_fused(p);
+    cudaError_t ce = cudaStreamEndCapture(p->stream, &graph);
+    p->profiling = prof;
+    if (crc) return crc;
+    if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&p->graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+    p->graph_steps = chunk;
+  }
+  int64_t done = 0;
+  while (n_steps - done >= p->graph_steps) {
+    ProfScope ps(p, K_GRAPH);
+    SALVUS_CUDA(cudaGraphLaunch(p->graph_exec, p->stream));
+    g_launches += (int64_t)p->graph_steps * (3 + (p->srcs.empty() ? 0 : 1));
+    done += p->graph_steps;
+    p->step += p->graph_steps;
+  }
+  for (; done < n_steps; ++done) {
+    if ((rc = step_fused(p))) return rc;
+    p->step++;
+  }
+  return SALVUS_OK;
+}
+
+int salvus_synchronize(salvus_problem *p) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  return SALVUS_OK;
+}
+
+int64_t salvus_problem_step_index(const salvus_problem *p) { return p ? p->step : -1; }
+
+int salvus_problem_stream(const salvus_problem *p, void **stream) {
+  if (!p || !stream) return fail(SALVUS_E_INVALID, "null argument");
+  *stream = (void *)p->stream;
+  return SALVUS_OK;
+}
+
+int salvus_problem_info(const salvus_problem *p, int32_t *shots, int32_t *nrec, int32_t *c) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  if (shots) *shots = p->shots;
+  if (nrec) *nrec = (int32_t)p->recs.size();
+  if (c) *c = p->c;
+  return SALVUS_OK;
+}
+
+int salvus_get_seismograms(salvus_problem *p, int64_t first, int64_t count, double *out) {
+  if (!p || !out) return fail(SALVUS_E_INVALID, "null argument");
+  if (count < 0 || first < 0 || first + count > p->step || first < p->step - p->seis_cap)
+    return fail(SALVUS_E_INVALID, "steps [%lld, %lld) not held (step %lld, capacity %lld)",
+                (long long)first, (long long)(first + count), (long long)p->step,
+                (long long)p->seis_cap);
+  if (p->recs.empty() || count == 0) return SALVUS_OK;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  const int64_t rows = (int64_t)p->recs.size() * p->c;
+  std::vector<double> ring((size_t)(rows * p->seis_cap));
+  SALVUS_CUDA(cudaMemcpyAsync(ring.data(), p->d_seis.ptr, 8 * ring.size(), cudaMemcpyDeviceToHost,
+                              p->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  for (int64_t rr = 0; rr < rows; ++rr)
+    for (int64_t s = 0; s < count; ++s)
+      out[rr * count + s] = ring[(size_t)(rr * p->seis_cap + (first + s) % p->seis_cap)];
+  return SALVUS_OK;
+}
+
+int salvus_profile_enable(salvus_problem *p, int32_t enable) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  p->profiling = enable != 0;
+  return SALVUS_OK;
+}
+
+int salvus_profile_read(salvus_problem *p, int32_t max_entries, const char **names, double *ms,
+                        int64_t *launches, int32_t *n_entries) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  for (auto &e : p->events) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e.a, e.b);
+    p->prof_ms[e.kind] += t;
+    p->prof_n[e.kind] += 1;
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  p->events.clear();
+  int k = 0;
+  for (int i = 0; i < K_NKINDS && k < max_entries; ++i) {
+    if (!p->prof_n[i]) continue;
+    if (names) names[k] = kKindNames[i];
+    if (ms) ms[k] = p->prof_ms[i];
+    if (launches) launches[k] = p->prof_n[i];
+    ++k;
+  }
+  if (n_entries) *n_entries = k;
+  std::fill(p->prof_ms.begin(), p->prof_ms.end(), 0.0);
+  std::fill(p->prof_n.begin(), p->prof_n.end(), 0);
+  return SALVUS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,124 @@
+// internal.h -- host-side structures of the B200 spectral-element library.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/salvus_b200.h"
+
+namespace salvus {
+
+// Largest supported polynomial orders (reference limits: TensorQuad.h:69 for
+// quads, Hexahedra.h:14-17 with order7_hex.c missing for hexes).
+constexpr int kMaxQuadOrder = 10;
+constexpr int kMaxHexOrder = 6;
+
+void set_error(const char *fmt, ...);
+int fail(int code, const char *fmt, ...);
+#define SALVUS_CUDA(call)                                                       \
+  do {                                                                         \
+    cudaError_t e_ = (call);                                                   \
+    if (e_ != cudaSuccess)                                                     \
+      return ::salvus::fail(SALVUS_E_CUDA, "%s failed: %s (%s:%d)", #call,     \
+                            cudaGetErrorString(e_), __FILE__, __LINE__);       \
+  } while (0)
+
+// 1-D GLL basis of order N computed from the mathematics in FP64.
+struct Basis {
+  int order = 0, n = 0, dim = 0, P = 0, nv = 0;
+  std::vector<double> xi, w, D;  // D[i*n+j] = l_j'(xi_i)
+};
+int make_basis(int shape, int order, Basis *b);
+void lagrange_1d(const Basis &b, double x, double *l, double *dl);
+
+// P1 geometry of one element (vertex signs of QuadP1.h:98-108 / HexP1.cpp).
+void p1_jacobian(int dim, const double *vtx, const double *ref, double *detJ, double *invJ);
+void p1_map(int dim, const double *vtx, const double *ref, double *x);
+int check_hull(int dim, const double *vtx, const double *x);  // 1 in, 0 out, <0 error
+int inverse_map(int dim, const double *vtx, const double *x, double *ref);
+
+struct DeviceBuffer {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  int alloc(size_t n);
+  void release();
+  ~DeviceBuffer() { release(); }
+  template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Number of float / double words per element-point record in the stiffness
+// kernels (geometry + folded material [+ packed connectivity for FP32]).
+int record_words(int shape, int physics, int fp64);
+
+}  // namespace salvus
+
+struct salvus_mesh {
+  int device = 0;
+  bool host_only = false;
+  int shape = 0, order = 0, physics = 0, dim = 0, nv = 0, n = 0, P = 0, c = 0, npar = 0;
+  int64_t E = 0, G = 0;
+  salvus::Basis basis;
+  std::vector<double> vtx;        // [E][nv][dim]
+  std::vector<double> par;        // [npar][E][nv]
+  std::vector<int32_t> conn;      // [E][P]
+  std::vector<double> xyz;        // [G][dim]
+  std::vector<int32_t> inc_off;   // [G+1]   node -> incident element points
+  std::vector<int32_t> inc_idx;   // [E*P]   e*P + p, sorted by element
+  std::vector<double> mi;         // [G] inverse mass (FP64, host copy)
+  // device
+  salvus::DeviceBuffer d_conn, d_inc_off, d_inc_idx, d_vtx, d_par;
+  salvus::DeviceBuffer d_mi64, d_mi32;
+  salvus::DeviceBuffer d_rec32, d_rec64;  // stiffness records per precision
+  cudaStream_t stream = nullptr;
+};
+
+struct salvus_problem {
+  salvus_mesh *mesh = nullptr;
+  int prec = SALVUS_FP32;
+  int shots = 1;
+  int c = 1;
+  double dt = 0.0;
+  bool dt_set = false;
+  int64_t step = 0;
+  size_t rsize = 4;  // sizeof(real)
+  salvus::DeviceBuffer d_u, d_v, d_a, d_ap, d_r;
+  salvus::DeviceBuffer d_step;   // int64 device step counter
+  salvus::DeviceBuffer d_stage;  // FP64 staging for host field copies
+  // sources (host mirror + device)
+  struct Src {
+    salvus_source desc;
+    int64_t elem;
+    double ref[3];
+    std::vector<double> wts;  // [P][c]
+  };
+  std::vector<Src> srcs;
+  salvus::DeviceBuffer d_src_elem, d_src_par, d_src_wts;
+  bool src_dirty = true;
+  // receivers
+  struct Rec {
+    double xyz[3];
+    int64_t elem;
+    double ref[3];
+    std::vector<double> l;  // [P]
+  };
+  std::vector<Rec> recs;
+  salvus::DeviceBuffer d_rec_elem, d_rec_l, d_seis;
+  int64_t seis_cap = 4096;
+  bool rec_dirty = true;
+  // graphs
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_steps = 0;
+  cudaStream_t stream = nullptr;
+  // profiling
+  bool profiling = false;
+  struct Ev {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Ev> events;
+  std::vector<double> prof_ms;
+  std::vector<int64_t> prof_n;
+};

@@ -1,0 +1,170 @@
+// kernels_setup.cuh -- one-time FP64 setup on the GPU: per-GLL-point
+// Jacobians, P1-interpolated material, folded stiffness records (stored in
+// the problem precision) and the element-local diagonal mass.
+//
+// Reference arithmetic restated: HexP1::inverseJacobianAtPoint
+// (HexP1.cpp:189-240), QuadP1::inverseJacobianAtPoint (QuadP1.h:79-90, with
+// the correct dN/dr(s), dN/ds(r) arguments), ParAtIntPts (TensorQuad.cpp:
+// 309-323, Hexahedra.cpp:635-656), Elastic3D::attachMaterialProperties
+// (Elastic3D.cpp:33-54), assembleElementMassMatrix (Scalar.cpp:34-39,
+// Elastic3D.cpp:63-67), Order2Newmark::initializeGlobalDofs
+// (Order2Newmark.cpp:32-66).
+#pragma once
+
+#include <cstdint>
+
+namespace salvus {
+
+constexpr int kMaxN = 11;
+
+struct GllTable {
+  double xi[kMaxN];
+  double w[kMaxN];
+};
+
+__device__ __forceinline__ void p1_jac_dev(int dim, const double *v, const double *ref,
+                                           double *detJ, double *invJ) {
+  if (dim == 2) {
+    const double sg[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
+    double J0 = 0, J1 = 0, J2 = 0, J3 = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      double dr = 0.25 * sg[k][0] * (1 + sg[k][1] * ref[1]);
+      double ds = 0.25 * sg[k][1] * (1 + sg[k][0] * ref[0]);
+      J0 += dr * v[2 * k]; J1 += dr * v[2 * k + 1];
+      J2 += ds * v[2 * k]; J3 += ds * v[2 * k + 1];
+    }
+    double d = J0 * J3 - J1 * J2;
+    *detJ = d;
+    invJ[0] = J3 / d; invJ[1] = -J1 / d; invJ[2] = -J2 / d; invJ[3] = J0 / d;
+    return;
+  }
+  const double sg[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1},
+                           {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+  double J[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    double a = 1 + sg[k][0] * ref[0], b = 1 + sg[k][1] * ref[1], c = 1 + sg[k][2] * ref[2];
+    double d0 = 0.125 * sg[k][0] * b * c, d1 = 0.125 * sg[k][1] * a * c,
+           d2 = 0.125 * sg[k][2] * a * b;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      J[m] += d0 * v[3 * k + m];
+      J[3 + m] += d1 * v[3 * k + m];
+      J[6 + m] += d2 * v[3 * k + m];
+    }
+  }
+  double m00 = J[4] * J[8] - J[5] * J[7], m01 = J[5] * J[6] - J[3] * J[8],
+         m02 = J[3] * J[7] - J[4] * J[6];
+  double d = J[0] * m00 + J[1] * m01 + J[2] * m02;
+  double id = 1.0 / d;
+  *detJ = d;
+  invJ[0] = m00 * id;
+  invJ[1] = (J[2] * J[7] - J[1] * J[8]) * id;
+  invJ[2] = (J[1] * J[5] - J[2] * J[4]) * id;
+  invJ[3] = m01 * id;
+  invJ[4] = (J[0] * J[8] - J[2] * J[6]) * id;
+  invJ[5] = (J[2] * J[3] - J[0] * J[5]) * id;
+  invJ[6] = m02 * id;
+  invJ[7] = (J[1] * J[6] - J[0] * J[7]) * id;
+  invJ[8] = (J[0] * J[4] - J[1] * J[3]) * id;
+}
+
+__device__ __forceinline__ double p1_interp_dev(int dim, const double *vals, const double *ref) {
+  if (dim == 2) {
+    return 0.25 * ((1 - ref[0]) * (1 - ref[1]) * vals[0] + (1 + ref[0]) * (1 - ref[1]) * vals[1] +
+                   (1 + ref[0]) * (1 + ref[1]) * vals[2] + (1 - ref[0]) * (1 + ref[1]) * vals[3]);
+  }
+  const double sg[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1},
+                           {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+  double s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    s += 0.125 * (1 + sg[k][0] * ref[0]) * (1 + sg[k][1] * ref[1]) * (1 + sg[k][2] * ref[2]) *
+         vals[k];
+  return s;
+}
+
+// One thread per element point.  Writes the stiffness record (FP32 packed
+// with connectivity, or FP64) and the element-local mass w detJ (rho).
+// Records:
+//   acoustic : G = w detJ vp^2 invJ^T invJ (symmetric; 3 or 6 words)
+//   elastic  : invJ (row-major [x_a][xi_b], 9 words), lambda w detJ, mu w detJ
+template <typename real, bool kPackConn>
+__global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, int rw,
+                                const double *__restrict__ vtx, const double *__restrict__ par,
+                                const int32_t *__restrict__ conn, GllTable gll,
+                                real *__restrict__ rec, double *__restrict__ mass_local) {
+  int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= E * P) return;
+  const int64_t e = tid / P;
+  const int p = (int)(tid - e * P);
+  const int nv = dim == 2 ? 4 : 8;
+  const int i = p % n, j = (p / n) % n, k = p / (n * n);
+  double ref[3] = {gll.xi[i], gll.xi[j], dim == 3 ? gll.xi[k] : 0.0};
+  double wq = gll.w[i] * gll.w[j] * (dim == 3 ? gll.w[k] : 1.0);
+  double v[24];
+  for (int a = 0; a < nv * dim; ++a) v[a] = vtx[e * nv * dim + a];
+  double detJ, iJ[9];
+  p1_jac_dev(dim, v, ref, &detJ, iJ);
+  const double wd = wq * detJ;
+  real *out = rec + tid * rw;
+  if (physics == 0) {
+    double vals[8];
+    for (int a = 0; a < nv; ++a) vals[a] = par[e * nv + a];
+    double vp = p1_interp_dev(dim, vals, ref);
+    double s = wd * vp * vp;
+    if (dim == 2) {
+      // G_bc = sum_a invJ[a][b] invJ[a][c]
+      double g00 = iJ[0] * iJ[0] + iJ[2] * iJ[2];
+      double g01 = iJ[0] * iJ[1] + iJ[2] * iJ[3];
+      double g11 = iJ[1] * iJ[1] + iJ[3] * iJ[3];
+      out[0] = (real)(s * g00); out[1] = (real)(s * g01); out[2] = (real)(s * g11);
+    } else {
+      int q = 0;
+      for (int b = 0; b < 3; ++b)
+        for (int c = b; c < 3; ++c) {
+          double g = iJ[0 * 3 + b] * iJ[0 * 3 + c] + iJ[1 * 3 + b] * iJ[1 * 3 + c] +
+                     iJ[2 * 3 + b] * iJ[2 * 3 + c];
+          out[q++] = (real)(s * g);
+        }
+    }
+    mass_local[tid] = wd;  // Scalar mass: no density (Scalar.cpp:34-39)
+  } else {
+    double vals[8], rho, vp, vs;
+    for (int a = 0; a < 8; ++a) vals[a] = par[(0 * E + e) * 8 + a];
+    rho = p1_interp_dev(3, vals, ref);
+    for (int a = 0; a < 8; ++a) vals[a] = par[(1 * E + e) * 8 + a];
+    vp = p1_interp_dev(3, vals, ref);
+    for (int a = 0; a < 8; ++a) vals[a] = par[(2 * E + e) * 8 + a];
+    vs = p1_interp_dev(3, vals, ref);
+    // c11 = rho vp^2, c66 = rho vs^2, c12 = c11 - 2 c66 (Elastic3D.cpp:42-53)
+    double mu = rho * vs * vs;
+    double lam = rho * vp * vp - 2.0 * mu;
+    for (int a = 0; a < 9; ++a) out[a] = (real)iJ[a];
+    out[9] = (real)(wd * lam);
+    out[10] = (real)(wd * mu);
+    mass_local[tid] = wd * rho;
+  }
+  if (kPackConn) {
+    int32_t c = conn[tid];
+    reinterpret_cast<int32_t *>(out)[rw - (dim == 3 && physics == 0 ? 2 : 1)] = c;
+    if (dim == 3 && physics == 0) reinterpret_cast<int32_t *>(out)[rw - 1] = 0;
+  }
+}
+
+// Diagonal mass by node gather in ascending element order, then reciprocal.
+__global__ void mass_gather_kernel(int64_t G, const int32_t *__restrict__ off,
+                                   const int32_t *__restrict__ idx,
+                                   const double *__restrict__ mass_local,
+                                   double *__restrict__ mi64, float *__restrict__ mi32) {
+  int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G) return;
+  double s = 0.0;
+  for (int32_t q = off[g]; q < off[g + 1]; ++q) s += mass_local[idx[q]];
+  double m = 1.0 / s;
+  mi64[g] = m;
+  mi32[g] = (float)m;
+}
+
+}  // namespace salvus
