@@ -106,6 +106,12 @@ int salvus_mesh_info(const salvus_mesh *mesh, int64_t *n_nodes, int32_t *n_compo
 int salvus_mesh_node_coords(const salvus_mesh *mesh, double *xyz);
 /* Element-local to global node map [E][P] (the closure, Problem.cpp:302-318). */
 int salvus_mesh_connectivity(const salvus_mesh *mesh, int64_t *conn);
+/* Owning element (first in element order whose hull holds the point) and
+ * reference coordinates of a physical point: QuadP1::checkHull +
+ * inverseCoordinateTransform (QuadP1.cpp:8-92), HexP1 (HexP1.cpp:8-187), as
+ * used by attachSource / attachReceiver.  Works on host-only meshes. */
+int salvus_mesh_locate_point(const salvus_mesh *mesh, const double *xyz, int64_t *element,
+                             double *ref);
 /* Diagonal inverse mass [G] in FP64 (VecReciprocal, Order2Newmark.cpp:52). */
 int salvus_mesh_inverse_mass(const salvus_mesh *mesh, double *mi);
 /* Estimate lambda_max(M^-1 K) by power iteration on the GPU (FP64);

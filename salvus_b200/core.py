@@ -61,6 +61,7 @@ SIGNATURES = [
     ("salvus_mesh_info", ctypes.c_int, [_VP, ctypes.POINTER(_I64), ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
     ("salvus_mesh_node_coords", ctypes.c_int, [_VP, _DP]),
     ("salvus_mesh_connectivity", ctypes.c_int, [_VP, ctypes.POINTER(_I64)]),
+    ("salvus_mesh_locate_point", ctypes.c_int, [_VP, _DP, ctypes.POINTER(_I64), _DP]),
     ("salvus_mesh_inverse_mass", ctypes.c_int, [_VP, _DP]),
     ("salvus_mesh_max_eigenvalue", ctypes.c_int, [_VP, _I32, ctypes.c_uint64, _DP]),
     ("salvus_problem_create", ctypes.c_int, [_VP, _I32, _I32, ctypes.POINTER(_VP)]),
@@ -154,6 +155,14 @@ class Mesh:
         c = np.zeros((self.n_elements, self.points_per_element), dtype=np.int64)
         _check(lib().salvus_mesh_connectivity(self.h, c.ctypes.data_as(ctypes.POINTER(_I64))))
         return c
+
+    def locate(self, xyz):
+        """(element, reference coordinates) of a physical point."""
+        x = np.zeros(3)
+        x[: len(xyz)] = xyz
+        e, r = _I64(), np.zeros(3)
+        _check(lib().salvus_mesh_locate_point(self.h, _dp(x), ctypes.byref(e), _dp(r)))
+        return e.value, r[: self.dim]
 
     def inverse_mass(self):
         m = np.zeros(self.n_nodes)

@@ -488,6 +488,15 @@ int salvus_mesh_connectivity(const salvus_mesh *m, int64_t *conn) {
   return SALVUS_OK;
 }
 
+int salvus_mesh_locate_point(const salvus_mesh *m, const double *xyz, int64_t *elem, double *ref) {
+  if (!m || !xyz || !elem || !ref) return fail(SALVUS_E_INVALID, "null argument");
+  double x[3] = {xyz[0], xyz[1], m->dim == 3 ? xyz[2] : 0.0}, r[3] = {0, 0, 0};
+  int rc = locate_point(m, x, elem, r);
+  if (rc) return rc;
+  for (int a = 0; a < m->dim; ++a) ref[a] = r[a];
+  return SALVUS_OK;
+}
+
 int salvus_mesh_inverse_mass(const salvus_mesh *m, double *mi) {
   if (!m || !mi) return fail(SALVUS_E_INVALID, "null argument");
   if (m->host_only) return fail(SALVUS_E_STATE, "host-only mesh has no mass matrix");

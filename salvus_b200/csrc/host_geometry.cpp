@@ -224,7 +224,9 @@ int check_hull(int dim, const double *vtx, const double *x) {
 // after the first step).
 int inverse_map(int dim, const double *vtx, const double *x, double *ref) {
   double r[3] = {0, 0, 0};
-  for (int it = 0; it < 50; ++it) {
+  double prev = INFINITY;
+  int stalled = 0;
+  for (int it = 0; it < 60; ++it) {
     double X[3] = {0, 0, 0}, det, inv[9];
     p1_map(dim, vtx, r, X);
     p1_jacobian(dim, vtx, r, &det, inv);
@@ -235,7 +237,11 @@ int inverse_map(int dim, const double *vtx, const double *x, double *ref) {
       step_norm = std::fmax(step_norm, std::fabs(dr[a]));
     }
     for (int a = 0; a < dim; ++a) r[a] += dr[a];
-    if (step_norm < 1e-15) {
+    // quadratic convergence until the step reaches the rounding floor of the
+    // physical coordinates; stop once it no longer shrinks
+    stalled = (step_norm >= 0.5 * prev) ? stalled + 1 : 0;
+    prev = step_norm;
+    if (step_norm < 1e-14 || (step_norm < 1e-10 && stalled >= 2)) {
       for (int a = 0; a < dim; ++a) ref[a] = r[a];
       return SALVUS_OK;
     }

@@ -112,6 +112,38 @@ def test_hex_numbering_rotated_cells():
             np.testing.assert_allclose(xm[conn[e, p]], w @ v, atol=1e-9)
 
 
+def _first_hull_element(shape, V, C, x):
+    for e in range(len(C)):
+        if po.check_hull(shape, V[C[e]], x) == 1:
+            return e
+    return -1
+
+
+@pytest.mark.parametrize("which", ["ring2d", "elastic3d"])
+def test_point_location_matches_oracle(which):
+    if which == "ring2d":
+        cfg = configs.ricker_2d(nel=40, order=4)
+        pts = list(cfg["receivers"]) + [s["location"] for s in cfg["sources"]] + [(2500.0, 2500.0)]
+    else:
+        cfg = configs.elastic_hex(nel=6, order=4, n_receivers=10)
+        pts = list(cfg["receivers"]) + [s["location"] for s in cfg["sources"]]
+    m = _host_mesh(cfg)
+    V, C = cfg["vertices"], cfg["cells"]
+    for x in pts:
+        e, ref = m.locate(x)
+        assert e == _first_hull_element(cfg["shape"], V, C, np.asarray(x, float))
+        np.testing.assert_allclose(ref, po.inverse_map(cfg["shape"], V[C[e]], x), atol=1e-6)
+        # the product's reference coordinates map back to the point exactly
+        d = len(ref)
+        signs = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], float) if d == 2 else np.array(
+            [[-1, -1, -1], [-1, 1, -1], [1, 1, -1], [1, -1, -1],
+             [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], float)
+        w = np.prod(1 + signs * ref, axis=1) / 2 ** d
+        np.testing.assert_allclose(w @ V[C[e]], x, rtol=1e-12, atol=1e-8)
+    with pytest.raises(core.SalvusError):
+        m.locate([-1.0] * m.dim)
+
+
 def test_invalid_meshes_rejected():
     V, C = meshgen.structured_quad(2, 2, 1.0, 1.0)
     par = np.ones((1, len(C), 4))
