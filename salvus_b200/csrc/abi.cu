@@ -16,6 +16,10 @@
 #include "kernels_setup.cuh"
 #include "kernels_stiffness.cuh"
 #include "kernels_step.cuh"
+#include "kernels_hex_tma.cuh"
+#include "kernels_hex_v2.cuh"
+#include <cstdlib>
+#include <type_traits>
 
 namespace salvus {
 const char *last_error();
@@ -78,9 +82,89 @@ static int launch_acoustic(const salvus_mesh *m, const real *rec, const real *u,
   return check_launch("acoustic stiffness");
 }
 
+// FP32 elastic hexahedra: SALVUS_HEX_KERNEL selects the variant
+//   persistent (default) TMA double-buffered persistent CTAs
+//   tma                  one TMA-staged group per CTA
+//   classic              register/shared-memory baseline (also the FP64 path)
+enum HexVariant {
+  HEX_PERSISTENT = 0, HEX_TMA = 1, HEX_CLASSIC = 2, HEX_V2 = 3, HEX_V2_E4 = 4, HEX_V3 = 5,
+  HEX_V3_E4 = 6
+};
+static int hex_variant() {
+  static int v = -1;
+  if (v < 0) {
+    const char *s = std::getenv("SALVUS_HEX_KERNEL");
+    v = HEX_V2;
+    if (s && std::strcmp(s, "v3") == 0) v = HEX_V3;
+    if (s && std::strcmp(s, "classic") == 0) v = HEX_CLASSIC;
+    if (s && std::strcmp(s, "tma") == 0) v = HEX_TMA;
+    if (s && std::strcmp(s, "persistent") == 0) v = HEX_PERSISTENT;
+    if (s && std::strcmp(s, "v2") == 0) v = HEX_V2;
+    if (s && std::strcmp(s, "v2e4") == 0) v = HEX_V2_E4;
+    if (s && std::strcmp(s, "v3e4") == 0) v = HEX_V3_E4;
+  }
+  return v;
+}
+
+template <int N, int EPB, bool kAsync>
+static int launch_elastic_v2(const salvus_mesh *m, const float *rec, const float *u, float *r,
+                             cudaStream_t st) {
+  using T = ElasticV2Shape<N, EPB, kAsync>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(elastic_hex_stiffness_v2_kernel<N, EPB, kAsync>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    attr = true;
+  }
+  const unsigned grid = blocks_for(m->E, EPB);
+  elastic_hex_stiffness_v2_kernel<N, EPB, kAsync><<<grid, T::THREADS, T::SMEM, st>>>(
+      m->E, rec, u, r, dmatrix<float>(m->basis));
+  g_launches++;
+  return check_launch("elastic stiffness (v2)");
+}
+
 template <int N, typename real>
 static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, real *r,
-                          cudaStream_t st) {
+                          cudaStream_t st, int *err) {
+  if constexpr (std::is_same<real, float>::value) {
+    const int var = hex_variant();
+    constexpr int n2 = (N + 1) * (N + 1);
+    constexpr int E8 = 200 / n2 > 0 ? 200 / n2 : 1, E4 = 100 / n2 > 0 ? 100 / n2 : 1;
+    if (var == HEX_V2) return launch_elastic_v2<N, E8, false>(m, rec, u, r, st);
+    if (var == HEX_V2_E4) return launch_elastic_v2<N, E4, false>(m, rec, u, r, st);
+    if (var == HEX_V3) return launch_elastic_v2<N, E8, true>(m, rec, u, r, st);
+    if (var == HEX_V3_E4) return launch_elastic_v2<N, E4, true>(m, rec, u, r, st);
+    if (var == HEX_TMA && err) {
+      using T = ElasticTmaShape<N>;
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(elastic_hex_stiffness_tma_kernel<N>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+        attr = true;
+      }
+      const unsigned grid = blocks_for(m->E, T::EPB);
+      elastic_hex_stiffness_tma_kernel<N><<<grid, T::THREADS, T::SMEM, st>>>(
+          m->E, rec, u, r, dmatrix<float>(m->basis), err);
+      g_launches++;
+      return check_launch("elastic stiffness (tma)");
+    }
+    if (var == HEX_PERSISTENT && err) {
+      using T = ElasticTmaShape<N>;
+      static bool attr = false;
+      if (!attr) {
+        cudaFuncSetAttribute(elastic_hex_stiffness_tma_persistent<N>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_PERSISTENT);
+        attr = true;
+      }
+      const int64_t groups = (m->E + T::EPB - 1) / T::EPB;
+      const int64_t slots = (int64_t)m->sm_count * 2;
+      const unsigned grid = (unsigned)(groups < slots ? groups : slots);
+      elastic_hex_stiffness_tma_persistent<N><<<grid, T::THREADS, T::SMEM_PERSISTENT, st>>>(
+          m->E, rec, u, r, dmatrix<float>(m->basis), err);
+      g_launches++;
+      return check_launch("elastic stiffness (persistent)");
+    }
+  }
   using S = ElasticShape<N, real>;
   static bool attr_set = false;
   if (!attr_set) {
@@ -106,15 +190,15 @@ static int acoustic3(const salvus_mesh *m, const real *rec, const real *u, real 
 
 template <typename real>
 static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u, real *r,
-                            cudaStream_t st) {
+                            cudaStream_t st, int *err = nullptr) {
   if (m->physics == SALVUS_ELASTIC3D) {
     switch (m->order) {
-      case 1: return launch_elastic<1, real>(m, rec, u, r, st);
-      case 2: return launch_elastic<2, real>(m, rec, u, r, st);
-      case 3: return launch_elastic<3, real>(m, rec, u, r, st);
-      case 4: return launch_elastic<4, real>(m, rec, u, r, st);
-      case 5: return launch_elastic<5, real>(m, rec, u, r, st);
-      case 6: return launch_elastic<6, real>(m, rec, u, r, st);
+      case 1: return launch_elastic<1, real>(m, rec, u, r, st, err);
+      case 2: return launch_elastic<2, real>(m, rec, u, r, st, err);
+      case 3: return launch_elastic<3, real>(m, rec, u, r, st, err);
+      case 4: return launch_elastic<4, real>(m, rec, u, r, st, err);
+      case 5: return launch_elastic<5, real>(m, rec, u, r, st, err);
+      case 6: return launch_elastic<6, real>(m, rec, u, r, st, err);
     }
   } else if (m->shape == SALVUS_QUAD) {
     switch (m->order) {
@@ -165,6 +249,7 @@ static int build_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &mass_l
 static int mesh_setup_device(salvus_mesh *m) {
   int rc;
   SALVUS_CUDA(cudaSetDevice(m->device));
+  SALVUS_CUDA(cudaDeviceGetAttribute(&m->sm_count, cudaDevAttrMultiProcessorCount, m->device));
   SALVUS_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
   const int64_t EP = m->E * m->P;
   if ((rc = m->d_conn.alloc(sizeof(int32_t) * EP))) return rc;
@@ -305,7 +390,8 @@ static int step_fused_t(salvus_problem *p) {
   int rc;
   {
     ProfScope ps(p, K_STIFF);
-    if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream)))
+    if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
+                                       p->d_err.as<int>())))
       return rc;
   }
   if ((rc = launch_sources<real, C>(p))) return rc;
@@ -332,7 +418,8 @@ static int assemble_t(salvus_problem *p) {
   int rc;
   {
     ProfScope ps(p, K_STIFF);
-    if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream)))
+    if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
+                                       p->d_err.as<int>())))
       return rc;
   }
   if ((rc = launch_sources<real, C>(p))) return rc;
@@ -366,6 +453,15 @@ static int newmark_t(salvus_problem *p) {
     if ((rc = check_launch("newmark"))) return rc;
   }
   return launch_receivers<real, C>(p);
+}
+
+// Reads the device error word (set by kernels whose bounded waits ran out).
+static int device_status(salvus_problem *p) {
+  int h = 0;
+  SALVUS_CUDA(cudaMemcpyAsync(&h, p->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  if (h) return fail(SALVUS_E_TIMEOUT, "a bounded device wait gave up (code %d); results invalid", h);
+  return SALVUS_OK;
 }
 
 static int ready(salvus_problem *p) {
@@ -591,8 +687,9 @@ int salvus_problem_create(salvus_mesh *m, int32_t precision, int32_t n_shots, sa
   int rc;
   if ((rc = p->d_u.alloc(nf)) || (rc = p->d_v.alloc(nf)) || (rc = p->d_a.alloc(nf)) ||
       (rc = p->d_ap.alloc(nf)) || (rc = p->d_r.alloc((size_t)m->E * m->P * p->c * p->rsize)) ||
-      (rc = p->d_step.alloc(sizeof(int64_t))))
+      (rc = p->d_step.alloc(sizeof(int64_t))) || (rc = p->d_err.alloc(sizeof(int))))
     return rc;
+  SALVUS_CUDA(cudaMemsetAsync(p->d_err.ptr, 0, sizeof(int), p->stream));
   SALVUS_CUDA(cudaMemsetAsync(p->d_u.ptr, 0, nf, p->stream));
   SALVUS_CUDA(cudaMemsetAsync(p->d_v.ptr, 0, nf, p->stream));
   SALVUS_CUDA(cudaMemsetAsync(p->d_a.ptr, 0, nf, p->stream));
@@ -839,7 +936,7 @@ int salvus_synchronize(salvus_problem *p) {
   if (!p) return fail(SALVUS_E_INVALID, "null problem");
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
   SALVUS_CUDA(cudaStreamSynchronize(p->stream));
-  return SALVUS_OK;
+  return device_status(p);
 }
 
 int64_t salvus_problem_step_index(const salvus_problem *p) { return p ? p->step : -1; }
@@ -871,6 +968,7 @@ int salvus_get_seismograms(salvus_problem *p, int64_t first, int64_t count, doub
   SALVUS_CUDA(cudaMemcpyAsync(ring.data(), p->d_seis.ptr, 8 * ring.size(), cudaMemcpyDeviceToHost,
                               p->stream));
   SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  if (int rc = device_status(p)) return rc;
   for (int64_t rr = 0; rr < rows; ++rr)
     for (int64_t s = 0; s < count; ++s)
       out[rr * count + s] = ring[(size_t)(rr * p->seis_cap + (first + s) % p->seis_cap)];

@@ -57,6 +57,7 @@ int record_words(int shape, int physics, int fp64);
 
 struct salvus_mesh {
   int device = 0;
+  int sm_count = 148;
   bool host_only = false;
   int shape = 0, order = 0, physics = 0, dim = 0, nv = 0, n = 0, P = 0, c = 0, npar = 0;
   int64_t E = 0, G = 0;
@@ -87,6 +88,7 @@ struct salvus_problem {
   salvus::DeviceBuffer d_u, d_v, d_a, d_ap, d_r;
   salvus::DeviceBuffer d_step;   // int64 device step counter
   salvus::DeviceBuffer d_stage;  // FP64 staging for host field copies
+  salvus::DeviceBuffer d_err;    // int: device-side error word (bounded waits)
   // sources (host mirror + device)
   struct Src {
     salvus_source desc;

@@ -21,6 +21,25 @@
 
 namespace salvus {
 
+// One Newmark update with explicitly rounded operations, so that the fused
+// gather/update kernel and the three-call path (gather, inverse mass,
+// Newmark) produce bitwise identical wavefields whatever the compiler's
+// contraction choices.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+
+template <typename real>
+__device__ __forceinline__ void newmark_point(real an, real &ap, real &v, real &u, real dt) {
+  const real acl = mul_rn(real(0.5), dt), dsp = mul_rn(mul_rn(real(0.5), dt), dt);
+  // v_{n} = dt/2 a + dt/2 a_ + v ; u = dt v + dt^2/2 a + u  (Order2Newmark.cpp:104-107)
+  const real vn = add_rn(add_rn(mul_rn(acl, an), mul_rn(acl, ap)), v);
+  u = add_rn(add_rn(mul_rn(dt, vn), mul_rn(dsp, an)), u);
+  v = vn;
+  ap = an;
+}
+
 // mode 0: fused  a = mi * sum(r); Newmark update of (u, v, a_)
 // mode 1: gather a = sum(r)
 template <typename real, int C, int MODE>
@@ -31,30 +50,59 @@ __global__ void gather_kernel(int64_t G, const int32_t *__restrict__ off,
                               real dt) {
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= G) return;
+  // Newmark operands first: they do not depend on the gather, so their loads
+  // overlap the dependent index -> residual chain below.
+  real m = 0, uo[C], vo[C], apo[C];
+  if (MODE == 0) {
+    m = mi[g];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      uo[c] = u[g * C + c];
+      vo[c] = v[g * C + c];
+      apo[c] = ap[g * C + c];
+    }
+  }
   real acc[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) acc[c] = 0;
   const int32_t q0 = off[g], q1 = off[g + 1];
-  for (int32_t q = q0; q < q1; ++q) {
-    const int64_t ep = idx[q];
+  const int cnt = q1 - q0;
+  constexpr int kFast = 8;  // hexahedral / quadrilateral valence bound
+  if (cnt <= kFast) {
+    int32_t ep[kFast];
 #pragma unroll
-    for (int c = 0; c < C; ++c) acc[c] += r[ep * C + c];
+    for (int q = 0; q < kFast; ++q) ep[q] = q < cnt ? idx[q0 + q] : 0;
+    real rv[kFast][C];
+#pragma unroll
+    for (int q = 0; q < kFast; ++q)
+#pragma unroll
+      for (int c = 0; c < C; ++c) rv[q][c] = q < cnt ? r[(int64_t)ep[q] * C + c] : real(0);
+    // ascending element order, as in the general loop
+#pragma unroll
+    for (int q = 0; q < kFast; ++q)
+      if (q < cnt) {
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] += rv[q][c];
+      }
+  } else {
+    for (int32_t q = q0; q < q1; ++q) {
+      const int64_t e = idx[q];
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[c] += r[e * C + c];
+    }
   }
-  if (MODE == 1) {
+  if constexpr (MODE == 1) {
 #pragma unroll
     for (int c = 0; c < C; ++c) a[g * C + c] = acc[c];
-    return;
-  }
-  const real m = mi[g];
-  const real acl = real(0.5) * dt, dsp = real(0.5) * dt * dt;
+  } else {
 #pragma unroll
-  for (int c = 0; c < C; ++c) {
-    const int64_t i = g * C + c;
-    const real an = acc[c] * m;
-    const real vn = acl * an + acl * ap[i] + v[i];
-    u[i] = dt * vn + dsp * an + u[i];
-    v[i] = vn;
-    ap[i] = an;
+    for (int c = 0; c < C; ++c) {
+      const int64_t i = g * C + c;
+      newmark_point<real>(mul_rn(acc[c], m), apo[c], vo[c], uo[c], dt);
+      u[i] = uo[c];
+      v[i] = vo[c];
+      ap[i] = apo[c];
+    }
   }
 }
 
@@ -62,7 +110,7 @@ template <typename real, int C>
 __global__ void inverse_mass_kernel(int64_t G, const real *__restrict__ mi, real *__restrict__ a) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= G * C) return;
-  a[i] = a[i] * mi[i / C];
+  a[i] = mul_rn(a[i], mi[i / C]);
 }
 
 template <typename real>
@@ -70,12 +118,11 @@ __global__ void newmark_kernel(int64_t N, const real *__restrict__ a, real *__re
                                real *__restrict__ v, real *__restrict__ ap, real dt) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
-  const real acl = real(0.5) * dt, dsp = real(0.5) * dt * dt;
-  const real an = a[i];
-  const real vn = acl * an + acl * ap[i] + v[i];
-  u[i] = dt * vn + dsp * an + u[i];
-  v[i] = vn;
-  ap[i] = an;
+  real apv = ap[i], vv = v[i], uv = u[i];
+  newmark_point<real>(a[i], apv, vv, uv, dt);
+  u[i] = uv;
+  v[i] = vv;
+  ap[i] = apv;
 }
 
 __device__ __forceinline__ double ricker_dev(double t, double f0, double t0, double amp) {
