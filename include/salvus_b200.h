@@ -172,6 +172,23 @@ int salvus_get_seismograms(salvus_problem *p, int64_t first_step, int64_t n_step
 int salvus_problem_info(const salvus_problem *p, int32_t *n_shots, int32_t *n_receivers,
                         int32_t *n_components);
 
+/* ---- allocation-free stiffness action ---- */
+/* a = -K u, assembled over the mesh (no mass, no sources), for callers that
+ * cannot allocate device memory while they run: frameworks that own all
+ * device memory through their own pool, or code that must not touch the
+ * allocator mid-run.  This entry point has no counterpart in the reference.
+ * u and a are the caller's device buffers, [G][c] in `precision` (FP32 or
+ * FP64); stream is a cudaStream_t or NULL.  The call is asynchronous on that
+ * stream and allocates nothing: the element-local residual lives in a
+ * 32 MiB array inside the library that every GPU loading the library holds
+ * until exit.  Meshes needing more (E * P * c * sizeof(real) > 32 MiB) are
+ * rejected with SALVUS_E_INVALID.  All calls share that array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture. */
+int salvus_apply_stiffness_noalloc(const salvus_mesh *mesh, int32_t precision, const void *u,
+                                   void *a, void *stream);
+
 /* ---- measurement ---- */
 /* Device time of the kernels launched by the last salvus_run / salvus_step
  * calls since the last reset, per kernel class (CUDA events on the problem

@@ -86,6 +86,7 @@ SIGNATURES = [
     ("salvus_profile_read", ctypes.c_int, [_VP, _I32, ctypes.POINTER(ctypes.c_char_p), _DP,
                                            ctypes.POINTER(_I64), ctypes.POINTER(_I32)]),
     ("salvus_launch_count", _I64, []),
+    ("salvus_apply_stiffness_noalloc", ctypes.c_int, [_VP, _I32, _VP, _VP, _VP]),
 ]
 
 _LIB = None

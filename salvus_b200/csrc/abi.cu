@@ -455,6 +455,34 @@ static int newmark_t(salvus_problem *p) {
   return launch_receivers<real, C>(p);
 }
 
+// a = -K u for caller-owned device buffers, with the element-local residual
+// in caller-provided scratch (used by salvus_apply_stiffness_noalloc).
+template <typename real>
+static int apply_stiffness_into_t(const salvus_mesh *m, const real *rec, const real *u, real *a,
+                                  real *scratch, cudaStream_t st) {
+  int rc = launch_stiffness<real>(m, rec, u, scratch, st, nullptr);
+  if (rc) return rc;
+  if (m->c == 1)
+    gather_kernel<real, 1, 1><<<blocks_for(m->G, 256), 256, 0, st>>>(
+        m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), scratch, nullptr, nullptr,
+        nullptr, nullptr, a, (real)0);
+  else
+    gather_kernel<real, 3, 1><<<blocks_for(m->G, 256), 256, 0, st>>>(
+        m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), scratch, nullptr, nullptr,
+        nullptr, nullptr, a, (real)0);
+  g_launches++;
+  return check_launch("allocation-free gather");
+}
+
+int apply_stiffness_into(const salvus_mesh *m, int precision, const void *u, void *a,
+                         void *scratch, cudaStream_t st) {
+  if (precision == SALVUS_FP32)
+    return apply_stiffness_into_t<float>(m, m->d_rec32.as<float>(), (const float *)u, (float *)a,
+                                         (float *)scratch, st);
+  return apply_stiffness_into_t<double>(m, m->d_rec64.as<double>(), (const double *)u,
+                                        (double *)a, (double *)scratch, st);
+}
+
 // Reads the device error word (set by kernels whose bounded waits ran out).
 static int device_status(salvus_problem *p) {
   int h = 0;
