@@ -366,11 +366,14 @@ template <typename real, int C>
 static int launch_receivers(salvus_problem *p) {
   ProfScope ps(p, K_REC);
   const int nr = (int)p->recs.size();
-  const int threads = nr * C > 0 ? (nr * C > 1024 ? 1024 : ((nr * C + 31) / 32) * 32) : 32;
-  receiver_kernel<real, C><<<1, threads, 0, p->stream>>>(
-      nr, p->mesh->P, p->d_rec_elem.as<int64_t>(), p->d_rec_l.as<double>(),
-      p->mesh->d_conn.as<int32_t>(), F<real>(p->d_u), p->d_seis.as<double>(), p->seis_cap,
-      p->d_step.as<int64_t>());
+  if (nr > 0) {
+    receiver_kernel<real, C><<<nr, kRecThreads, 0, p->stream>>>(
+        p->mesh->P, p->d_rec_elem.as<int64_t>(), p->d_rec_l.as<double>(),
+        p->mesh->d_conn.as<int32_t>(), F<real>(p->d_u), p->d_seis.as<double>(), p->seis_cap,
+        p->d_step.as<int64_t>());
+    g_launches++;
+  }
+  advance_step_kernel<<<1, 1, 0, p->stream>>>(p->d_step.as<int64_t>());
   g_launches++;
   return check_launch("receivers");
 }

@@ -147,29 +147,48 @@ __global__ void source_kernel(int nsrc, int P, const int64_t *__restrict__ elem,
   }
 }
 
-// Receivers (one CTA): seis[(rec*C + c)*cap + step % cap] = sum_p l_p u;
-// then advances the device step counter.
+// Receivers: one CTA per receiver, one thread per element point (strided);
+// each thread keeps a Kahan-compensated FP64 partial per component, then a
+// fixed-order tree combines the partials (deterministic).
+// seis[(rec*C + c)*cap + step % cap] = sum_p l_p u_p.
+constexpr int kRecThreads = 128;
 template <typename real, int C>
-__global__ void receiver_kernel(int nrec, int P, const int64_t *__restrict__ elem,
-                                const double *__restrict__ lw, const int32_t *__restrict__ conn,
-                                const real *__restrict__ u, double *__restrict__ seis, int64_t cap,
-                                int64_t *__restrict__ step) {
-  const int64_t n = *step;
-  for (int q = threadIdx.x; q < nrec * C; q += blockDim.x) {
-    const int rc = q / C, c = q - rc * C;
-    const int64_t e = elem[rc];
-    double s = 0.0, comp = 0.0;
-    for (int p = 0; p < P; ++p) {
-      const double y = lw[(int64_t)rc * P + p] * (double)u[(int64_t)conn[e * P + p] * C + c] - comp;
-      const double tt = s + y;
-      comp = (tt - s) - y;
-      s = tt;
+__global__ void __launch_bounds__(kRecThreads)
+receiver_kernel(int P, const int64_t *__restrict__ elem, const double *__restrict__ lw,
+                const int32_t *__restrict__ conn, const real *__restrict__ u,
+                double *__restrict__ seis, int64_t cap, const int64_t *__restrict__ step) {
+  __shared__ double part[C][kRecThreads];
+  const int rc = blockIdx.x, t = threadIdx.x;
+  const int64_t e = elem[rc];
+  double s[C], comp[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) s[c] = comp[c] = 0.0;
+  for (int p = t; p < P; p += kRecThreads) {
+    const double l = lw[(int64_t)rc * P + p];
+    const int64_t node = conn[e * P + p];
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const double y = l * (double)u[node * C + c] - comp[c];
+      const double tt = s[c] + y;
+      comp[c] = (tt - s[c]) - y;
+      s[c] = tt;
     }
-    seis[(int64_t)q * cap + (n % cap)] = s;
   }
+#pragma unroll
+  for (int c = 0; c < C; ++c) part[c][t] = s[c];
   __syncthreads();
-  if (threadIdx.x == 0) *step = n + 1;
+  for (int o = kRecThreads / 2; o > 0; o >>= 1) {
+    if (t < o)
+#pragma unroll
+      for (int c = 0; c < C; ++c) part[c][t] += part[c][t + o];
+    __syncthreads();
+  }
+  if (t < C) seis[((int64_t)rc * C + t) * cap + (*step % cap)] = part[t][0];
 }
+
+// Advances the device step counter (one thread), after every kernel of the
+// step that reads it.
+__global__ void advance_step_kernel(int64_t *__restrict__ step) { *step += 1; }
 
 // Deterministic partial sums of x.y weighted by w (w may be null): one partial
 // per CTA, summed on the host in block order.
