@@ -1,0 +1,77 @@
+// Drives the C++ plugin facade the way the reference's Main.cpp:45-66 drives
+// its Problem: assembleIntoGlobalDof -> applyInverseMassMatrix ->
+// takeTimeStep, for Quad<Acoustic> and Hexahedron<Elastic3D>, and prints
+// the seismograms as JSON for comparison with the Python path.
+#include <cstdio>
+#include <vector>
+
+#include "salvus/salvus.hpp"
+
+using namespace salvus;
+
+static void quad_mesh(int n, double L, std::vector<double> &v, std::vector<int64_t> &c) {
+  for (int j = 0; j <= n; ++j)
+    for (int i = 0; i <= n; ++i) { v.push_back(L * i / n); v.push_back(L * j / n); }
+  auto id = [&](int i, int j) { return (int64_t)j * (n + 1) + i; };
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i < n; ++i) {
+      c.push_back(id(i, j)); c.push_back(id(i + 1, j)); c.push_back(id(i + 1, j + 1)); c.push_back(id(i, j + 1));
+    }
+}
+
+static void hex_mesh(int n, double L, std::vector<double> &v, std::vector<int64_t> &c) {
+  for (int k = 0; k <= n; ++k)
+    for (int j = 0; j <= n; ++j)
+      for (int i = 0; i <= n; ++i) { v.push_back(L * i / n); v.push_back(L * j / n); v.push_back(L * k / n); }
+  auto id = [&](int i, int j, int k) { return ((int64_t)k * (n + 1) + j) * (n + 1) + i; };
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        int64_t q[8] = {id(i, j, k), id(i, j + 1, k), id(i + 1, j + 1, k), id(i + 1, j, k),
+                        id(i, j, k + 1), id(i + 1, j, k + 1), id(i + 1, j + 1, k + 1), id(i, j + 1, k + 1)};
+        c.insert(c.end(), q, q + 8);
+      }
+}
+
+static void print(const char *name, const std::vector<double> &s, bool last) {
+  std::printf("\"%s\": [", name);
+  for (size_t i = 0; i < s.size(); ++i) std::printf("%s%.17g", i ? "," : "", s[i]);
+  std::printf("]%s\n", last ? "" : ",");
+}
+
+int main() {
+  std::printf("{\n");
+  {  // Quad<Acoustic>, literal three-call loop
+    std::vector<double> v; std::vector<int64_t> c;
+    quad_mesh(8, 1e4, v, c);
+    std::vector<double> vp(c.size(), 4000.0);
+    Mesh<Quad<Acoustic>> mesh(4, v, c, vp);
+    Order2Newmark<Quad<Acoustic>> problem(mesh, 2e-3);
+    Ricker src; src.location = {5123.0, 4987.0, 0.0}; src.center_freq = 4.0; src.time_delay = 0.3;
+    problem.addSource(src);
+    Receiver r1; r1.location = {2000.0, 3000.0, 0.0}; problem.addReceiver(r1);
+    Receiver r2; r2.location = {7000.0, 6100.0, 0.0}; problem.addReceiver(r2);
+    for (int n = 0; n < 150; ++n) {
+      problem.assembleIntoGlobalDof();
+      problem.applyInverseMassMatrix();
+      problem.takeTimeStep();
+    }
+    print("quad_acoustic", problem.seismograms(), false);
+  }
+  {  // Hexahedron<Elastic3D> through the string factory, graph replay
+    std::vector<double> v; std::vector<int64_t> c;
+    hex_mesh(3, 600.0, v, c);
+    const size_t E = c.size() / 8;
+    std::vector<double> par;
+    for (double val : {2700.0, 6000.0, 3464.0}) par.insert(par.end(), E * 8, val);
+    Simulation sim = makeProblem("hex", "3delastic", 4, v, c, par, 1e-3);
+    Ricker src; src.location = {311.0, 287.0, 305.0}; src.center_freq = 8.0; src.time_delay = 0.15;
+    src.amplitude = 1e10; src.moment_tensor = {1.0, -0.5, 0.3, 0.2, 0.1, -0.4};
+    sim.problem->addSource(src);
+    Receiver r; r.location = {100.0, 500.0, 600.0}; sim.problem->addReceiver(r);
+    sim.problem->run(120, true);
+    print("hex_elastic", sim.problem->seismograms(), true);
+  }
+  std::printf("}\n");
+  return 0;
+}
