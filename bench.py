@@ -37,6 +37,7 @@ def parse():
     ap.add_argument("--nel", type=int, default=64)
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-shots", action="store_true", help="skip the batched-shots leg")
     ap.add_argument("--profile-only", action="store_true",
                     help="run a few steps only (for ncu captures); prints no JSON")
     return ap.parse_args()
@@ -138,6 +139,48 @@ class Clocks:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
 
 
+def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
+    """Config 2: n_shots Ricker shots on a nel x nel order-4 quad mesh with a
+    seeded smooth velocity model.  Batched form (one graph-replayed launch
+    sequence per step for all shots) against the plain form (one shot, one
+    host-launched step at a time) on the same mesh."""
+    cfg = configs.batched_quad(nel=nel, order=4, n_shots=n_shots)
+    mesh = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                     cfg["params"], device=device)
+    dt = 0.4 * mesh.critical_dt(iterations=60)
+    G = mesh.n_nodes
+    p = core.Problem(mesh, core.FP32, dt=dt, n_shots=n_shots)
+    for s in cfg["sources"]:
+        p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                     direction=s["direction"], shot=s["shot"])
+    for r in cfg["receivers"]:
+        p.add_receiver(r)
+    p.set_seismogram_capacity(steps + 64)
+    tune = p.autotune()
+    p.run(5, core.RUN_GRAPH)
+    p.synchronize()
+    ms_b = timed(p, lambda: p.run(steps, core.RUN_GRAPH))
+    q = core.Problem(mesh, core.FP32, dt=dt)
+    s = cfg["sources"][0]
+    q.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                 direction=s["direction"])
+    for r in cfg["receivers"]:
+        q.add_receiver(r)
+    q.set_seismogram_capacity(steps + 64)
+    q.run(5, core.RUN_PLAIN)
+    q.synchronize()
+    ms_p = timed(q, lambda: q.run(steps, core.RUN_PLAIN))
+    batched = G * n_shots * steps / (ms_b / 1e3)
+    plain = G * steps / (ms_p / 1e3)
+    return {"workload": f"acoustic quad {nel}^2 order 4, {n_shots} Ricker shots, GRF model, "
+                        f"{len(cfg['receivers'])} receivers",
+            "value": batched, "unit": METRIC, "ms_per_step": ms_b / steps,
+            "plain_value": plain, "plain_ms_per_step": ms_p / steps,
+            "shot_throughput_ratio": batched / plain, "steps": steps,
+            "tuning": {"stiffness_shot_lanes": tune[0], "stiffness_elements_per_cta": tune[1],
+                       "gather_shot_lanes": tune[2], "gather_nodes_per_cta": tune[3]}}
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -200,13 +243,13 @@ def main():
         p.run(max(args.steps, 3), core.RUN_PLAIN)
         p.synchronize()
         return
-    stream = torch.cuda.ExternalStream(p.stream_handle())
-
     def barrier():
         if dist:
             dist.barrier()
 
-    def timed(fn):
+    def timed_on(prob, fn):
+        """CUDA events on the problem's own stream around fn(); max over ranks."""
+        stream = torch.cuda.ExternalStream(prob.stream_handle())
         barrier()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -221,6 +264,9 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
         return ms
+
+    def timed(fn):
+        return timed_on(p, fn)
 
     clocks = Clocks(local)
     # warm-up (graph capture happens here)
@@ -280,10 +326,14 @@ def main():
         p2.run(args.steps, core.RUN_GRAPH)
         seis_holder["s"] = p2.seismograms(0, args.steps)
 
-    ms_e2e = timed(e2e_job)
+    ms_e2e = timed_on(p2, e2e_job)
     e2e = world * G * args.steps / (ms_e2e / 1e3)
     h2d = 2 * G * 3 * 8 / args.steps
     d2h = len(cfg["receivers"]) * 3 * 8
+
+    shots = None
+    if not args.no_shots:
+        shots = shots_leg(core, configs, timed_on, steps=min(args.steps, 300), device=local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -314,6 +364,7 @@ def main():
             "gpu_launches": launches,
             "clocks": ck,
             "cpu_baseline": cpu,
+            "shots_batched": shots,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -162,6 +162,16 @@ int salvus_step(salvus_problem *p);
 int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode);
 int salvus_synchronize(salvus_problem *p);
 int64_t salvus_problem_step_index(const salvus_problem *p);
+/* Shot batching (n_shots > 1; FP32 acoustic quads): picks, by timing on this
+ * problem, the shot lanes and elements per CTA of the batched stiffness
+ * kernel and the shot lanes and nodes per CTA of the batched gather/update
+ * (no reference counterpart; the reference runs one source set per run).
+ * Runs automatically before the first batched step; results are cached per
+ * (order, shots, elements, device).  Single-shot problems report fixed
+ * values.  SALVUS_BATCH_CONFIG="i,j" pins the choice. */
+int salvus_problem_autotune(salvus_problem *p, int32_t *stiff_shot_lanes,
+                            int32_t *stiff_elements, int32_t *gather_shot_lanes,
+                            int32_t *gather_nodes);
 /* The problem's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events after this problem's kernels. */
 int salvus_problem_stream(const salvus_problem *p, void **stream);

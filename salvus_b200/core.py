@@ -87,6 +87,7 @@ SIGNATURES = [
                                            ctypes.POINTER(_I64), ctypes.POINTER(_I32)]),
     ("salvus_launch_count", _I64, []),
     ("salvus_apply_stiffness_noalloc", ctypes.c_int, [_VP, _I32, _VP, _VP, _VP]),
+    ("salvus_problem_autotune", ctypes.c_int, [_VP] + [ctypes.POINTER(_I32)] * 4),
 ]
 
 _LIB = None
@@ -182,11 +183,12 @@ class Mesh:
 class Problem:
     """One wavefield on a mesh: Order2Newmark with sources and receivers."""
 
-    def __init__(self, mesh, precision=FP32, dt=None):
+    def __init__(self, mesh, precision=FP32, dt=None, n_shots=1):
         self.mesh = mesh
         h = _VP()
-        _check(lib().salvus_problem_create(mesh.h, precision, 1, ctypes.byref(h)))
+        _check(lib().salvus_problem_create(mesh.h, precision, n_shots, ctypes.byref(h)))
         self.h = h
+        self.n_shots = n_shots
         self.precision = precision
         self.c = mesh.n_components
         self.n_receivers = 0
@@ -273,13 +275,20 @@ class Problem:
         return lib().salvus_problem_step_index(self.h)
 
     def seismograms(self, first=0, count=None):
-        """[n_receivers][c][count] FP64 samples of u after steps first..first+count-1."""
+        """FP64 samples of u after steps first..first+count-1: [n_receivers][c][count]
+        for one shot, [n_shots][n_receivers][c][count] for a batched problem."""
         if count is None:
             count = self.step_index - first
-        out = np.zeros((self.n_receivers, self.c, count))
+        out = np.zeros((self.n_shots, self.n_receivers, self.c, count))
         if self.n_receivers and count:
             _check(lib().salvus_get_seismograms(self.h, first, count, _dp(out)))
-        return out
+        return out[0] if self.n_shots == 1 else out
+
+    def autotune(self):
+        """(stiffness shot lanes, elements per CTA, gather shot lanes, nodes per CTA)."""
+        v = [_I32() for _ in range(4)]
+        _check(lib().salvus_problem_autotune(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
 
     def profile(self, enable=True):
         _check(lib().salvus_profile_enable(self.h, 1 if enable else 0))

@@ -18,6 +18,8 @@
 #include "kernels_step.cuh"
 #include "kernels_hex_tma.cuh"
 #include "kernels_hex_v2.cuh"
+#include "kernels_batch.cuh"
+#include <algorithm>
 #include <cstdlib>
 #include <type_traits>
 
@@ -296,15 +298,28 @@ static int upload_sources(salvus_problem *p) {
   const size_t ns = p->srcs.size();
   int rc;
   if (ns) {
+    // batched problems group sources by shot (attach order kept within a shot)
+    std::vector<size_t> order(ns);
+    for (size_t s = 0; s < ns; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      return p->srcs[a].desc.shot < p->srcs[b].desc.shot;
+    });
     std::vector<int64_t> el(ns);
     std::vector<double> par(3 * ns), w(ns * m->P * p->c);
-    for (size_t s = 0; s < ns; ++s) {
-      el[s] = p->srcs[s].elem;
-      par[3 * s] = p->srcs[s].desc.center_freq;
-      par[3 * s + 1] = p->srcs[s].desc.time_delay;
-      par[3 * s + 2] = p->srcs[s].desc.amplitude;
-      std::memcpy(&w[s * m->P * p->c], p->srcs[s].wts.data(), sizeof(double) * m->P * p->c);
+    std::vector<int32_t> shot_off(p->shots_pad + 1, 0);
+    for (size_t k = 0; k < ns; ++k) {
+      const auto &src = p->srcs[order[k]];
+      el[k] = src.elem;
+      par[3 * k] = src.desc.center_freq;
+      par[3 * k + 1] = src.desc.time_delay;
+      par[3 * k + 2] = src.desc.amplitude;
+      std::memcpy(&w[k * m->P * p->c], src.wts.data(), sizeof(double) * m->P * p->c);
+      shot_off[src.desc.shot + 1]++;
     }
+    for (int s = 0; s < p->shots_pad; ++s) shot_off[s + 1] += shot_off[s];
+    if ((rc = p->d_shot_off.alloc(sizeof(int32_t) * shot_off.size()))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_shot_off.ptr, shot_off.data(), sizeof(int32_t) * shot_off.size(),
+                                cudaMemcpyHostToDevice, p->stream));
     if ((rc = p->d_src_elem.alloc(sizeof(int64_t) * ns))) return rc;
     if ((rc = p->d_src_par.alloc(sizeof(double) * par.size()))) return rc;
     if ((rc = p->d_src_wts.alloc(sizeof(double) * w.size()))) return rc;
@@ -333,7 +348,7 @@ static int upload_receivers(salvus_problem *p) {
   }
   if ((rc = p->d_rec_elem.alloc(sizeof(int64_t) * el.size()))) return rc;
   if ((rc = p->d_rec_l.alloc(sizeof(double) * l.size()))) return rc;
-  size_t sz = sizeof(double) * (size_t)(nr ? nr : 1) * p->c * p->seis_cap;
+  size_t sz = sizeof(double) * (size_t)(nr ? nr : 1) * p->c * p->seis_cap * p->shots_pad;
   if ((rc = p->d_seis.alloc(sz))) return rc;
   SALVUS_CUDA(cudaMemsetAsync(p->d_seis.ptr, 0, sz, p->stream));
   SALVUS_CUDA(cudaMemcpyAsync(p->d_rec_elem.ptr, el.data(), sizeof(int64_t) * el.size(),
@@ -410,7 +425,201 @@ static int step_fused_t(salvus_problem *p) {
   return launch_receivers<real, C>(p);
 }
 
+// ---------------------------------------------------------------------------
+// shot-batched step (FP32 acoustic quads)
+struct BatchCfg {
+  int sc, epc;
+};
+static const BatchCfg kStiffCfg[] = {{32, 1}, {32, 2}, {32, 4}, {64, 1}, {64, 2},
+                                     {128, 1}, {128, 2}, {256, 1}};
+static const BatchCfg kGatherCfg[] = {{32, 4}, {32, 8}, {64, 2}, {64, 4}, {128, 1},
+                                      {128, 2}, {256, 1}};
+constexpr int kNumStiffCfg = sizeof(kStiffCfg) / sizeof(kStiffCfg[0]);
+constexpr int kNumGatherCfg = sizeof(kGatherCfg) / sizeof(kGatherCfg[0]);
+
+template <int N, int SC, int EPC>
+static void launch_qb(const salvus_problem *p, cudaStream_t st) {
+  const salvus_mesh *m = p->mesh;
+  dim3 grid((unsigned)((m->E + EPC - 1) / EPC), (unsigned)(p->shots_pad / SC));
+  quad_acoustic_batched_kernel<N, SC, EPC><<<grid, SC * EPC, 0, st>>>(
+      m->E, p->shots_pad, m->d_rec32.as<float>(), F<float>(p->d_u), F<float>(p->d_r),
+      dmatrix<float>(m->basis));
+}
+
+template <int N>
+static int launch_qb_cfg(const salvus_problem *p, int cfg, cudaStream_t st) {
+  switch (cfg) {
+    case 0: launch_qb<N, 32, 1>(p, st); break;
+    case 1: launch_qb<N, 32, 2>(p, st); break;
+    case 2: launch_qb<N, 32, 4>(p, st); break;
+    case 3: launch_qb<N, 64, 1>(p, st); break;
+    case 4: launch_qb<N, 64, 2>(p, st); break;
+    case 5: launch_qb<N, 128, 1>(p, st); break;
+    case 6: launch_qb<N, 128, 2>(p, st); break;
+    case 7: launch_qb<N, 256, 1>(p, st); break;
+    default: return fail(SALVUS_E_INVALID, "bad batch config %d", cfg);
+  }
+  g_launches++;
+  return check_launch("batched stiffness");
+}
+
+static int batched_stiffness(const salvus_problem *p, int cfg, cudaStream_t st) {
+  switch (p->mesh->order) {
+    case 1: return launch_qb_cfg<1>(p, cfg, st);
+    case 2: return launch_qb_cfg<2>(p, cfg, st);
+    case 3: return launch_qb_cfg<3>(p, cfg, st);
+    case 4: return launch_qb_cfg<4>(p, cfg, st);
+    case 5: return launch_qb_cfg<5>(p, cfg, st);
+    case 6: return launch_qb_cfg<6>(p, cfg, st);
+  }
+  return fail(SALVUS_E_UNSUPPORTED, "batched quads support orders 1..6");
+}
+
+template <int SC, int NPB>
+static void launch_bg(const salvus_problem *p, cudaStream_t st) {
+  const salvus_mesh *m = p->mesh;
+  dim3 grid((unsigned)((m->G + NPB - 1) / NPB), (unsigned)(p->shots_pad / SC));
+  batched_gather_update_kernel<SC, NPB><<<grid, SC * NPB, 0, st>>>(
+      m->G, p->shots_pad, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(),
+      F<float>(p->d_r), m->d_mi32.as<float>(), F<float>(p->d_u), F<float>(p->d_v), (float)p->dt);
+}
+
+static int batched_gather(const salvus_problem *p, int cfg, cudaStream_t st) {
+  switch (cfg) {
+    case 0: launch_bg<32, 4>(p, st); break;
+    case 1: launch_bg<32, 8>(p, st); break;
+    case 2: launch_bg<64, 2>(p, st); break;
+    case 3: launch_bg<64, 4>(p, st); break;
+    case 4: launch_bg<128, 1>(p, st); break;
+    case 5: launch_bg<128, 2>(p, st); break;
+    case 6: launch_bg<256, 1>(p, st); break;
+    default: return fail(SALVUS_E_INVALID, "bad gather config %d", cfg);
+  }
+  g_launches++;
+  return check_launch("batched gather");
+}
+
+// Times every admissible configuration of the batched stiffness and gather
+// kernels on this problem and keeps the fastest.  The stiffness timing writes
+// only the residual scratch; the gather timing runs on copies of u and w, so
+// the problem's state is untouched.  Results are cached per (order, padded
+// shots, elements, device) for the process.
+static int autotune(salvus_problem *p) {
+  if (p->tune_stiff >= 0 && p->tune_gather >= 0) return SALVUS_OK;
+  struct Key {
+    int order, shots;
+    int64_t E;
+    int dev;
+  };
+  static std::vector<std::pair<Key, std::pair<int, int>>> cache;
+  for (auto &c : cache)
+    if (c.first.order == p->mesh->order && c.first.shots == p->shots_pad && c.first.E == p->mesh->E &&
+        c.first.dev == p->mesh->device) {
+      p->tune_stiff = c.second.first;
+      p->tune_gather = c.second.second;
+      return SALVUS_OK;
+    }
+  const char *env = std::getenv("SALVUS_BATCH_CONFIG");  // "stiff,gather" fixes the choice
+  if (env) {
+    int a = -1, b = -1;
+    if (std::sscanf(env, "%d,%d", &a, &b) == 2 && a >= 0 && a < kNumStiffCfg && b >= 0 &&
+        b < kNumGatherCfg && p->shots_pad % kStiffCfg[a].sc == 0 && p->shots_pad % kGatherCfg[b].sc == 0) {
+      p->tune_stiff = a;
+      p->tune_gather = b;
+      return SALVUS_OK;
+    }
+  }
+  cudaEvent_t e0, e1;
+  SALVUS_CUDA(cudaEventCreate(&e0));
+  SALVUS_CUDA(cudaEventCreate(&e1));
+  int rc = SALVUS_OK;
+  auto time_it = [&](auto &&fn) -> float {
+    float best = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      cudaEventRecord(e0, p->stream);
+      if ((rc = fn())) return 1e30f;
+      cudaEventRecord(e1, p->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      best = std::min(best, ms);
+    }
+    return best;
+  };
+  float bs = 1e30f;
+  int cs = -1;
+  for (int c = 0; c < kNumStiffCfg && rc == SALVUS_OK; ++c) {
+    if (p->shots_pad % kStiffCfg[c].sc) continue;
+    float t = time_it([&] { return batched_stiffness(p, c, p->stream); });
+    if (t < bs) { bs = t; cs = c; }
+  }
+  // gather timing on scratch copies of u and w
+  const size_t nf = (size_t)p->mesh->G * p->shots_pad * sizeof(float);
+  DeviceBuffer su, sw;
+  if (rc == SALVUS_OK && ((rc = su.alloc(nf)) == SALVUS_OK) && ((rc = sw.alloc(nf)) == SALVUS_OK)) {
+    std::swap(p->d_u.ptr, su.ptr);
+    std::swap(p->d_v.ptr, sw.ptr);
+    cudaMemsetAsync(p->d_u.ptr, 0, nf, p->stream);
+    cudaMemsetAsync(p->d_v.ptr, 0, nf, p->stream);
+    float bg = 1e30f;
+    int cg = -1;
+    for (int c = 0; c < kNumGatherCfg && rc == SALVUS_OK; ++c) {
+      if (p->shots_pad % kGatherCfg[c].sc) continue;
+      float t = time_it([&] { return batched_gather(p, c, p->stream); });
+      if (t < bg) { bg = t; cg = c; }
+    }
+    std::swap(p->d_u.ptr, su.ptr);
+    std::swap(p->d_v.ptr, sw.ptr);
+    p->tune_gather = cg;
+  }
+  cudaStreamSynchronize(p->stream);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (cs < 0 || p->tune_gather < 0) return fail(SALVUS_E_INVALID, "no admissible batch configuration");
+  p->tune_stiff = cs;
+  cache.push_back({{p->mesh->order, p->shots_pad, p->mesh->E, p->mesh->device},
+                   {p->tune_stiff, p->tune_gather}});
+  return SALVUS_OK;
+}
+
+static int step_batched(salvus_problem *p) {
+  const salvus_mesh *m = p->mesh;
+  int rc;
+  {
+    ProfScope ps(p, K_STIFF);
+    if ((rc = batched_stiffness(p, p->tune_stiff, p->stream))) return rc;
+  }
+  if (!p->srcs.empty()) {
+    ProfScope ps(p, K_SRC);
+    const int threads = 256, total = p->shots_pad * m->P;
+    batched_source_kernel<<<(total + threads - 1) / threads, threads, 0, p->stream>>>(
+        p->shots_pad, m->P, p->d_shot_off.as<int32_t>(), p->d_src_elem.as<int64_t>(),
+        p->d_src_par.as<double>(), p->d_src_wts.as<double>(), p->d_step.as<int64_t>(), p->dt,
+        F<float>(p->d_r));
+    g_launches++;
+    if ((rc = check_launch("batched sources"))) return rc;
+  }
+  {
+    ProfScope ps(p, K_UPDATE);
+    if ((rc = batched_gather(p, p->tune_gather, p->stream))) return rc;
+  }
+  ProfScope ps(p, K_REC);
+  if (!p->recs.empty()) {
+    const int threads = p->shots_pad < 256 ? p->shots_pad : 256;
+    batched_receiver_kernel<<<(unsigned)p->recs.size(), threads, 0, p->stream>>>(
+        p->shots_pad, (int)p->recs.size(), m->P, p->d_rec_elem.as<int64_t>(),
+        p->d_rec_l.as<double>(), m->d_conn.as<int32_t>(), F<float>(p->d_u),
+        p->d_seis.as<double>(), p->seis_cap, p->d_step.as<int64_t>());
+    g_launches++;
+  }
+  advance_step_kernel<<<1, 1, 0, p->stream>>>(p->d_step.as<int64_t>());
+  g_launches++;
+  return check_launch("batched receivers");
+}
+
 static int step_fused(salvus_problem *p) {
+  if (p->shots > 1) return step_batched(p);
   if (p->prec == SALVUS_FP32) return p->c == 1 ? step_fused_t<float, 1>(p) : step_fused_t<float, 3>(p);
   return p->c == 1 ? step_fused_t<double, 1>(p) : step_fused_t<double, 3>(p);
 }
@@ -501,6 +710,7 @@ static int ready(salvus_problem *p) {
   int rc;
   if ((rc = upload_sources(p))) return rc;
   if ((rc = upload_receivers(p))) return rc;
+  if (p->shots > 1 && (rc = autotune(p))) return rc;
   return SALVUS_OK;
 }
 
@@ -705,26 +915,33 @@ int salvus_problem_create(salvus_mesh *m, int32_t precision, int32_t n_shots, sa
   if (m->host_only) return fail(SALVUS_E_STATE, "mesh was created host-only (device < 0)");
   if (precision != SALVUS_FP32 && precision != SALVUS_FP64)
     return fail(SALVUS_E_INVALID, "unknown precision %d", precision);
-  if (n_shots != 1) return fail(SALVUS_E_UNSUPPORTED, "batched shots use salvus_batch_* (n_shots=%d)", n_shots);
+  if (n_shots < 1) return fail(SALVUS_E_INVALID, "n_shots must be >= 1");
+  if (n_shots > 1 && (precision != SALVUS_FP32 || m->shape != SALVUS_QUAD || m->order > 6))
+    return fail(SALVUS_E_UNSUPPORTED,
+                "shot batching is built for FP32 acoustic quads of order 1..6 (got shape %d, "
+                "order %d, precision %d)", m->shape, m->order, precision);
   SALVUS_CUDA(cudaSetDevice(m->device));
   std::unique_ptr<salvus_problem> p(new salvus_problem());
   p->mesh = m;
   p->prec = precision;
-  p->shots = 1;
+  p->shots = n_shots;
+  p->shots_pad = n_shots == 1 ? 1 : (n_shots + 31) / 32 * 32;
   p->c = m->c;
   p->rsize = precision == SALVUS_FP32 ? 4 : 8;
   SALVUS_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
-  const size_t nf = (size_t)m->G * p->c * p->rsize;
+  const size_t nf = (size_t)m->G * p->c * p->rsize * p->shots_pad;
+  const size_t na = n_shots == 1 ? nf : 16;  // batched problems keep no a / a_ fields
   int rc;
-  if ((rc = p->d_u.alloc(nf)) || (rc = p->d_v.alloc(nf)) || (rc = p->d_a.alloc(nf)) ||
-      (rc = p->d_ap.alloc(nf)) || (rc = p->d_r.alloc((size_t)m->E * m->P * p->c * p->rsize)) ||
+  if ((rc = p->d_u.alloc(nf)) || (rc = p->d_v.alloc(nf)) || (rc = p->d_a.alloc(na)) ||
+      (rc = p->d_ap.alloc(na)) ||
+      (rc = p->d_r.alloc((size_t)m->E * m->P * p->c * p->rsize * p->shots_pad)) ||
       (rc = p->d_step.alloc(sizeof(int64_t))) || (rc = p->d_err.alloc(sizeof(int))))
     return rc;
   SALVUS_CUDA(cudaMemsetAsync(p->d_err.ptr, 0, sizeof(int), p->stream));
   SALVUS_CUDA(cudaMemsetAsync(p->d_u.ptr, 0, nf, p->stream));
   SALVUS_CUDA(cudaMemsetAsync(p->d_v.ptr, 0, nf, p->stream));
-  SALVUS_CUDA(cudaMemsetAsync(p->d_a.ptr, 0, nf, p->stream));
-  SALVUS_CUDA(cudaMemsetAsync(p->d_ap.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(p->d_a.ptr, 0, na, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(p->d_ap.ptr, 0, na, p->stream));
   SALVUS_CUDA(cudaMemsetAsync(p->d_step.ptr, 0, sizeof(int64_t), p->stream));
   SALVUS_CUDA(cudaStreamSynchronize(p->stream));
   p->prof_ms.assign(K_NKINDS, 0.0);
@@ -760,7 +977,8 @@ int salvus_problem_set_dt(salvus_problem *p, double dt) {
 int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
   if (!p || !s) return fail(SALVUS_E_INVALID, "null argument");
   const salvus_mesh *m = p->mesh;
-  if (s->shot != 0) return fail(SALVUS_E_INVALID, "shot index %d out of range", s->shot);
+  if (s->shot < 0 || s->shot >= p->shots)
+    return fail(SALVUS_E_INVALID, "shot index %d out of range", s->shot);
   if (s->kind == SALVUS_SOURCE_MOMENT_TENSOR && m->physics != SALVUS_ELASTIC3D)
     return fail(SALVUS_E_INVALID, "moment-tensor sources need elastic physics");
   if (s->kind != SALVUS_SOURCE_FORCE && s->kind != SALVUS_SOURCE_MOMENT_TENSOR)
@@ -840,8 +1058,35 @@ static salvus::DeviceBuffer *field_buffer(salvus_problem *p, int32_t f) {
   return nullptr;
 }
 
+// One shot's column of a shot-batched field (u, or the half-step velocity w
+// for SALVUS_FIELD_V; with a_ = 0 at the start, w = v there).
+static int batched_field(salvus_problem *p, int32_t f, int32_t shot, double *vals, bool set) {
+  if (f != SALVUS_FIELD_U && f != SALVUS_FIELD_V)
+    return fail(SALVUS_E_UNSUPPORTED, "batched problems hold u and the half-step velocity only");
+  if (shot < 0 || shot >= p->shots) return fail(SALVUS_E_INVALID, "shot %d out of range", shot);
+  DeviceBuffer *b = f == SALVUS_FIELD_U ? &p->d_u : &p->d_v;
+  const int64_t G = p->mesh->G;
+  int rc;
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if (p->d_stage.bytes < (size_t)(8 * G) && (rc = p->d_stage.alloc(8 * G))) return rc;
+  if (set) {
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_stage.ptr, vals, 8 * G, cudaMemcpyHostToDevice, p->stream));
+    shot_scatter_kernel<<<blocks_for(G, 256), 256, 0, p->stream>>>(G, p->shots_pad, shot,
+                                                                   p->d_stage.as<double>(), b->as<float>());
+  } else {
+    shot_gather_kernel<<<blocks_for(G, 256), 256, 0, p->stream>>>(G, p->shots_pad, shot, b->as<float>(),
+                                                                  p->d_stage.as<double>());
+    SALVUS_CUDA(cudaMemcpyAsync(vals, p->d_stage.ptr, 8 * G, cudaMemcpyDeviceToHost, p->stream));
+  }
+  g_launches++;
+  if ((rc = check_launch("shot field copy"))) return rc;
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  return SALVUS_OK;
+}
+
 int salvus_problem_set_field(salvus_problem *p, int32_t f, int32_t shot, const double *vals) {
   if (!p || !vals) return fail(SALVUS_E_INVALID, "null argument");
+  if (p->shots > 1) return batched_field(p, f, shot, const_cast<double *>(vals), true);
   DeviceBuffer *b = field_buffer(p, f);
   if (!b || shot != 0) return fail(SALVUS_E_INVALID, "bad field %d / shot %d", f, shot);
   const size_t N = (size_t)p->mesh->G * p->c;
@@ -864,6 +1109,7 @@ int salvus_problem_set_field(salvus_problem *p, int32_t f, int32_t shot, const d
 
 int salvus_problem_get_field(salvus_problem *p, int32_t f, int32_t shot, double *vals) {
   if (!p || !vals) return fail(SALVUS_E_INVALID, "null argument");
+  if (p->shots > 1) return batched_field(p, f, shot, vals, false);
   DeviceBuffer *b = field_buffer(p, f);
   if (!b || shot != 0) return fail(SALVUS_E_INVALID, "bad field %d / shot %d", f, shot);
   const size_t N = (size_t)p->mesh->G * p->c;
@@ -883,8 +1129,17 @@ int salvus_problem_get_field(salvus_problem *p, int32_t f, int32_t shot, double 
   return SALVUS_OK;
 }
 
+static int single_shot_only(salvus_problem *p) {
+  if (p && p->shots > 1)
+    return fail(SALVUS_E_UNSUPPORTED,
+                "the three-call form is single-shot; batched problems use salvus_step / salvus_run");
+  return SALVUS_OK;
+}
+
 int salvus_assemble(salvus_problem *p) {
-  int rc = ready(p);
+  int rc = single_shot_only(p);
+  if (rc) return rc;
+  rc = ready(p);
   if (rc) return rc;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
   if (p->prec == SALVUS_FP32) return p->c == 1 ? assemble_t<float, 1>(p) : assemble_t<float, 3>(p);
@@ -892,7 +1147,9 @@ int salvus_assemble(salvus_problem *p) {
 }
 
 int salvus_apply_inverse_mass(salvus_problem *p) {
-  int rc = ready(p);
+  int rc = single_shot_only(p);
+  if (rc) return rc;
+  rc = ready(p);
   if (rc) return rc;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
   if (p->prec == SALVUS_FP32) return p->c == 1 ? minv_t<float, 1>(p) : minv_t<float, 3>(p);
@@ -900,7 +1157,9 @@ int salvus_apply_inverse_mass(salvus_problem *p) {
 }
 
 int salvus_take_time_step(salvus_problem *p) {
-  int rc = ready(p);
+  int rc = single_shot_only(p);
+  if (rc) return rc;
+  rc = ready(p);
   if (rc) return rc;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
   if (p->prec == SALVUS_FP32) rc = p->c == 1 ? newmark_t<float, 1>(p) : newmark_t<float, 3>(p);
@@ -972,6 +1231,24 @@ int salvus_synchronize(salvus_problem *p) {
 
 int64_t salvus_problem_step_index(const salvus_problem *p) { return p ? p->step : -1; }
 
+int salvus_problem_autotune(salvus_problem *p, int32_t *stiff_shot_lanes, int32_t *stiff_elements,
+                            int32_t *gather_shot_lanes, int32_t *gather_nodes) {
+  int rc = ready(p);
+  if (rc) return rc;
+  if (p->shots == 1) {
+    if (stiff_shot_lanes) *stiff_shot_lanes = 1;
+    if (stiff_elements) *stiff_elements = 0;
+    if (gather_shot_lanes) *gather_shot_lanes = 1;
+    if (gather_nodes) *gather_nodes = 256;
+    return SALVUS_OK;
+  }
+  if (stiff_shot_lanes) *stiff_shot_lanes = kStiffCfg[p->tune_stiff].sc;
+  if (stiff_elements) *stiff_elements = kStiffCfg[p->tune_stiff].epc;
+  if (gather_shot_lanes) *gather_shot_lanes = kGatherCfg[p->tune_gather].sc;
+  if (gather_nodes) *gather_nodes = kGatherCfg[p->tune_gather].epc;
+  return SALVUS_OK;
+}
+
 int salvus_problem_stream(const salvus_problem *p, void **stream) {
   if (!p || !stream) return fail(SALVUS_E_INVALID, "null argument");
   *stream = (void *)p->stream;
@@ -994,7 +1271,7 @@ int salvus_get_seismograms(salvus_problem *p, int64_t first, int64_t count, doub
                 (long long)p->seis_cap);
   if (p->recs.empty() || count == 0) return SALVUS_OK;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
-  const int64_t rows = (int64_t)p->recs.size() * p->c;
+  const int64_t rows = (int64_t)p->shots * p->recs.size() * p->c;
   std::vector<double> ring((size_t)(rows * p->seis_cap));
   SALVUS_CUDA(cudaMemcpyAsync(ring.data(), p->d_seis.ptr, 8 * ring.size(), cudaMemcpyDeviceToHost,
                               p->stream));

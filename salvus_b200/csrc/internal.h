@@ -110,6 +110,11 @@ struct salvus_problem {
   salvus::DeviceBuffer d_rec_elem, d_rec_l, d_seis;
   int64_t seis_cap = 4096;
   bool rec_dirty = true;
+  // shot batching (shots > 1): fields are [G][c][S_pad]; d_v holds the
+  // half-step velocity w = v + dt/2 a_; sources grouped by shot
+  int shots_pad = 1;
+  salvus::DeviceBuffer d_shot_off;
+  int tune_stiff = -1, tune_gather = -1;  // autotuner choices (indices)
   // graphs
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;

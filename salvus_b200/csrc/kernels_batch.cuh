@@ -1,0 +1,146 @@
+// kernels_batch.cuh -- shot-batched kernels: S shots on one mesh advance
+// together.  Fields are shot-interleaved, f[node][S] (S padded to a multiple
+// of 32), so a warp's lanes are consecutive shots: every field load and store
+// is coalesced and each geometry / connectivity word is read once for all
+// shots of a CTA.
+//
+// The arithmetic per shot is the reference's (Scalar::computeStiffnessTerm,
+// Scalar.cpp:58-71; Ricker::fire, Ricker.cpp:27-33); the time update uses the
+// velocity-at-half-step form of the reference's Newmark scheme
+// (Order2Newmark.cpp:99-108): with w = v + dt/2 a_ the pair
+//   v += dt/2 (a + a_);  u += dt v + dt^2/2 a
+// is exactly  w += dt a;  u += dt w  (one fewer field to stream).
+#pragma once
+
+#include <cstdint>
+
+namespace salvus {
+
+// One thread = one shot of one quad element; the element's n^2 values of
+// that shot live in registers, so the tensor-product contractions need no
+// shared memory.  CTA = EPC elements x SC shots.
+template <int N, int SC, int EPC>
+__global__ void __launch_bounds__(SC *EPC)
+quad_acoustic_batched_kernel(int64_t E, int S, const float *__restrict__ rec,
+                             const float *__restrict__ u, float *__restrict__ r,
+                             DMatrix<float> Dm) {
+  constexpr int n = N + 1, P = n * n;
+  __shared__ float4 sg[EPC * P];  // G00 G01 G11 conn of the CTA's elements
+  const int64_t e0 = (int64_t)blockIdx.x * EPC;
+  for (int q = threadIdx.x; q < EPC * P; q += blockDim.x) {
+    const int64_t ee = e0 + q / P;
+    sg[q] = ee < E ? __ldg(reinterpret_cast<const float4 *>(rec) + e0 * P + q)
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncthreads();
+  const int ey = threadIdx.x / SC, lane = threadIdx.x - ey * SC;
+  const int64_t e = e0 + ey;
+  const int s = blockIdx.y * SC + lane;
+  if (e >= E || s >= S) return;
+  const float4 *g = sg + ey * P;
+  float uu[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) uu[p] = __ldg(u + (int64_t)__float_as_int(g[p].w) * S + s);
+  float Fr[P], Fs[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const int i = p % n, j = p / n;
+    float gr = 0.f, gs = 0.f;
+#pragma unroll
+    for (int l = 0; l < n; ++l) {
+      gr += Dm.d[i * n + l] * uu[l + n * j];
+      gs += Dm.d[j * n + l] * uu[i + n * l];
+    }
+    const float4 G = g[p];
+    Fr[p] = G.x * gr + G.y * gs;
+    Fs[p] = G.y * gr + G.z * gs;
+  }
+  float *out = r + (e * P) * S + s;
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const int i = p % n, j = p / n;
+    float o = 0.f;
+#pragma unroll
+    for (int l = 0; l < n; ++l) {
+      o += Dm.d[l * n + i] * Fr[l + n * j];
+      o += Dm.d[l * n + j] * Fs[i + n * l];
+    }
+    out[(int64_t)p * S] = -o;
+  }
+}
+
+// Ricker sources of every shot into the element-local residual.  Thread =
+// (shot, point); a shot's sources are applied in attach order.
+__global__ void batched_source_kernel(int S, int P, const int32_t *__restrict__ shot_off,
+                                      const int64_t *__restrict__ elem,
+                                      const double *__restrict__ par,
+                                      const double *__restrict__ wts,
+                                      const int64_t *__restrict__ step, double dt,
+                                      float *__restrict__ r) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= S * P) return;
+  const int p = q % P, s = q / P;
+  const double t = (double)(*step) * dt;
+  for (int k = shot_off[s]; k < shot_off[s + 1]; ++k) {
+    const double stf = ricker_dev(t, par[3 * k], par[3 * k + 1], par[3 * k + 2]);
+    r[(elem[k] * P + p) * S + s] += (float)(wts[(int64_t)k * P + p] * stf);
+  }
+}
+
+// Node gather + inverse mass + half-step-velocity update, thread = (node,
+// shot).  CTA = NPB nodes x SC shots.
+template <int SC, int NPB>
+__global__ void __launch_bounds__(SC *NPB)
+batched_gather_update_kernel(int64_t G, int S, const int32_t *__restrict__ off,
+                             const int32_t *__restrict__ idx, const float *__restrict__ r,
+                             const float *__restrict__ mi, float *__restrict__ u,
+                             float *__restrict__ w, float dt) {
+  const int ny = threadIdx.x / SC, lane = threadIdx.x - ny * SC;
+  const int64_t g = (int64_t)blockIdx.x * NPB + ny;
+  const int s = blockIdx.y * SC + lane;
+  if (g >= G || s >= S) return;
+  const int64_t i = g * S + s;
+  const float uo = u[i], wo = w[i], m = __ldg(mi + g);
+  const int32_t q0 = __ldg(off + g), q1 = __ldg(off + g + 1);
+  float acc = 0.f;
+  for (int32_t q = q0; q < q1; ++q) acc += __ldg(r + (int64_t)__ldg(idx + q) * S + s);
+  const float wn = wo + dt * (acc * m);
+  w[i] = wn;
+  u[i] = uo + dt * wn;
+}
+
+// Receivers of every shot: block = receiver, thread = shot; FP64 Kahan over
+// the element points.  seis[(s * R + rec) * cap + step % cap].
+__global__ void batched_receiver_kernel(int S, int R, int P, const int64_t *__restrict__ elem,
+                                        const double *__restrict__ lw,
+                                        const int32_t *__restrict__ conn,
+                                        const float *__restrict__ u, double *__restrict__ seis,
+                                        int64_t cap, const int64_t *__restrict__ step) {
+  const int rc = blockIdx.x;
+  const int64_t e = elem[rc];
+  const int64_t slot = *step % cap;
+  for (int s = threadIdx.x; s < S; s += blockDim.x) {
+    double acc = 0.0, comp = 0.0;
+    for (int p = 0; p < P; ++p) {
+      const double y = lw[(int64_t)rc * P + p] * (double)u[(int64_t)conn[e * P + p] * S + s] - comp;
+      const double tt = acc + y;
+      comp = (tt - acc) - y;
+      acc = tt;
+    }
+    seis[((int64_t)s * R + rc) * cap + slot] = acc;
+  }
+}
+
+// Column k of a shot-interleaved field <-> a contiguous FP64 array.
+__global__ void shot_scatter_kernel(int64_t G, int S, int k, const double *__restrict__ src,
+                                    float *__restrict__ f) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < G) f[g * S + k] = (float)src[g];
+}
+__global__ void shot_gather_kernel(int64_t G, int S, int k, const float *__restrict__ f,
+                                   double *__restrict__ dst) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < G) dst[g] = (double)f[g * S + k];
+}
+
+}  // namespace salvus
