@@ -56,11 +56,16 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  *   acoustic : [1][n_elements][nv]  VP                    (Scalar.cpp:23-25)
  *   elastic3d: [3][n_elements][nv]  RHO, VP, VS  (isotropic form of
  *              Elastic3D.cpp:33-54 with VPV=VPH=VP, VSV=VSH=VS, ETA=1) */
+/* salvus_mesh_desc.flags: build only the FP32 stiffness records (halves the
+ * per-mesh geometry memory; FP64 problems and the FP64 eigenvalue estimate
+ * are then unavailable on that mesh). */
+#define SALVUS_MESH_FP32_ONLY 1
+
 typedef struct {
   int32_t shape;   /* enum salvus_shape */
   int32_t order;   /* polynomial order: quad 1..10, hex 1..6 */
   int32_t physics; /* enum salvus_physics */
-  int32_t reserved;
+  int32_t reserved; /* flags: SALVUS_MESH_FP32_ONLY */
   int64_t n_vertices;
   const double *vertices; /* [n_vertices][dim] */
   int64_t n_elements;
@@ -198,6 +203,62 @@ int salvus_problem_info(const salvus_problem *p, int32_t *n_shots, int32_t *n_re
  * stream capture. */
 int salvus_apply_stiffness_noalloc(const salvus_mesh *mesh, int32_t precision, const void *u,
                                    void *a, void *stream);
+
+/* ---- serving: continuous batching of forward-modelling jobs ----
+ * No reference counterpart (the reference runs one simulation per process,
+ * Main.cpp:10-78).  A server owns one GPU and a device-memory budget.  A
+ * scheduler thread admits queued jobs while the budget and the running-job
+ * limit allow, prepares them on a worker thread (mesh flattening overlaps the
+ * GPU work of running jobs), advances every running job in graph-replayed
+ * chunks of steps on its own stream so their kernels overlap on the device,
+ * copies each chunk's seismogram samples to the host as it completes, and
+ * frees a job's device memory when it finishes.  Jobs never share device
+ * state, so a job's result is the same alone and in any mix. */
+typedef struct {
+  salvus_mesh_desc mesh; /* copied at submit */
+  int32_t precision;     /* SALVUS_FP32 or SALVUS_FP64 */
+  int32_t n_sources;
+  const salvus_source *sources;
+  int32_t n_receivers;
+  int32_t reserved;
+  const double *receivers; /* [n_receivers][3] */
+  double dt;
+  int64_t n_steps;
+} salvus_job_desc;
+
+enum salvus_job_state { SALVUS_JOB_QUEUED = 0, SALVUS_JOB_RUNNING = 1, SALVUS_JOB_DONE = 2,
+                        SALVUS_JOB_FAILED = 3, SALVUS_JOB_CANCELLED = 4 };
+
+typedef struct {
+  int64_t submitted, completed, failed, running, queued;
+  double p50_latency_s, p99_latency_s, mean_latency_s;
+  double gll_point_updates; /* sum over completed jobs of G * steps */
+  double busy_seconds;      /* wall time with at least one job admitted */
+  int64_t peak_device_bytes;
+} salvus_server_stats;
+
+typedef struct salvus_server salvus_server;
+
+int salvus_server_create(int device, int64_t memory_budget_bytes, int32_t max_running,
+                         int32_t chunk_steps, salvus_server **out);
+/* Copies the description (mesh arrays, sources, receivers); the caller's
+ * buffers may be reused at once.  Rejects jobs that can never fit the budget. */
+int salvus_server_submit(salvus_server *s, const salvus_job_desc *job, int64_t *job_id);
+int salvus_server_poll(salvus_server *s, int64_t job_id, int32_t *state, int64_t *steps_done,
+                       int64_t *n_nodes);
+/* Seismogram samples [receivers][c][count] for steps [first, first+count)
+ * already streamed back (count <= steps_done - first). */
+int salvus_server_seismograms(salvus_server *s, int64_t job_id, int64_t first, int64_t count,
+                              double *out);
+/* Blocks until the job is done / failed / cancelled or timeout_s passes
+ * (SALVUS_E_TIMEOUT). */
+int salvus_server_wait(salvus_server *s, int64_t job_id, double timeout_s);
+int salvus_server_cancel(salvus_server *s, int64_t job_id);
+/* Drops a finished job's host results. */
+int salvus_server_release(salvus_server *s, int64_t job_id);
+int salvus_server_stats_read(salvus_server *s, salvus_server_stats *out);
+/* Stops the scheduler (running jobs are cancelled) and frees everything. */
+int salvus_server_destroy(salvus_server *s);
 
 /* ---- measurement ---- */
 /* Device time of the kernels launched by the last salvus_run / salvus_step

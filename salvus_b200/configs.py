@@ -85,6 +85,45 @@ def batched_quad(nel=200, order=4, L=1.0e4, vmin=2500.0, vmax=5500.0, corr=800.0
                 sources=sources, receivers=receivers)
 
 
+def serving_job(kind, edge, seed, order=4, n_receivers=8):
+    """One forward-modelling job of the serving stream: a 2-D acoustic quad
+    job on a 10 km square (edge x edge elements, vp GRF in 2500-5500 m/s) or
+    a 3-D elastic hex job on a cube of 200 m hexes (vp, vs, rho with a 5 %
+    GRF), each with its own seeded model, Ricker source and receivers."""
+    rng = np.random.default_rng(seed)
+    if kind == "quad":
+        L = 1.0e4
+        cfg = batched_quad(nel=edge, order=order, n_shots=1, n_receivers=n_receivers, seed=seed)
+        src = cfg["sources"][0]
+        cfg["sources"] = [dict(location=src["location"], center_freq=src["center_freq"],
+                               time_delay=src["time_delay"], amplitude=1.0, direction=[1.0])]
+        cfg["h"] = L / edge
+        cfg["vmax"] = 5500.0
+        return cfg
+    cfg = elastic_hex(nel=edge, order=order, n_receivers=n_receivers, seed=seed,
+                      f0=float(rng.uniform(1.0, 2.0)))
+    cfg["h"] = 200.0
+    cfg["vmax"] = 6000.0 * 1.25
+    return cfg
+
+
+def serving_stream(n_jobs, seed=4, quad_edges=(50, 400), hex_edges=(16, 48), steps=(1000, 6000),
+                   rate_hz=1.0):
+    """Seeded job stream: half quads (edge ~ U{quad_edges}), half hexes (edge
+    ~ U{hex_edges}), steps ~ U{steps}, Poisson arrivals at rate_hz.  Returns
+    (kind, edge, seed, n_steps, arrival_s) tuples; meshes are built on demand."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for k in range(n_jobs):
+        t += rng.exponential(1.0 / rate_hz)
+        kind = "quad" if rng.random() < 0.5 else "hex"
+        lo, hi = quad_edges if kind == "quad" else hex_edges
+        out.append((kind, int(rng.integers(lo, hi + 1)), int(seed * 100003 + k),
+                    int(rng.integers(steps[0], steps[1] + 1)), t))
+    return out
+
+
 def oracle_params(cfg):
     """Parameter array in the oracle's layout (elastic: RHO VPV VPH VSV VSH ETA)."""
     p = cfg["params"]

@@ -274,7 +274,7 @@ static int mesh_setup_device(salvus_mesh *m) {
   DeviceBuffer mass_local;
   if ((rc = mass_local.alloc(sizeof(double) * EP))) return rc;
   if ((rc = build_records<float, true>(m, m->d_rec32, mass_local))) return rc;
-  if ((rc = build_records<double, false>(m, m->d_rec64, mass_local))) return rc;
+  if (!m->fp32_only && (rc = build_records<double, false>(m, m->d_rec64, mass_local))) return rc;
   mass_gather_kernel<<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
       m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), mass_local.as<double>(),
       m->d_mi64.as<double>(), m->d_mi32.as<float>());
@@ -742,6 +742,7 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
     return fail(SALVUS_E_INVALID, "empty mesh");
   std::unique_ptr<salvus_mesh> m(new salvus_mesh());
   m->device = device;
+  m->fp32_only = (d->reserved & SALVUS_MESH_FP32_ONLY) != 0;
   m->shape = d->shape;
   m->order = d->order;
   m->physics = d->physics;
@@ -844,6 +845,7 @@ int salvus_mesh_inverse_mass(const salvus_mesh *m, double *mi) {
 int salvus_mesh_max_eigenvalue(salvus_mesh *m, int32_t iters, uint64_t seed, double *lam_out) {
   if (!m || !lam_out) return fail(SALVUS_E_INVALID, "null argument");
   if (m->host_only) return fail(SALVUS_E_STATE, "host-only mesh");
+  if (m->fp32_only) return fail(SALVUS_E_STATE, "the eigenvalue estimate needs the FP64 records");
   SALVUS_CUDA(cudaSetDevice(m->device));
   const int64_t N = m->G * m->c;
   DeviceBuffer x, y, r, mass, part;
@@ -916,6 +918,8 @@ int salvus_problem_create(salvus_mesh *m, int32_t precision, int32_t n_shots, sa
   if (precision != SALVUS_FP32 && precision != SALVUS_FP64)
     return fail(SALVUS_E_INVALID, "unknown precision %d", precision);
   if (n_shots < 1) return fail(SALVUS_E_INVALID, "n_shots must be >= 1");
+  if (precision == SALVUS_FP64 && m->fp32_only)
+    return fail(SALVUS_E_STATE, "mesh was created with SALVUS_MESH_FP32_ONLY");
   if (n_shots > 1 && (precision != SALVUS_FP32 || m->shape != SALVUS_QUAD || m->order > 6))
     return fail(SALVUS_E_UNSUPPORTED,
                 "shot batching is built for FP32 acoustic quads of order 1..6 (got shape %d, "

@@ -59,6 +59,7 @@ struct salvus_mesh {
   int device = 0;
   int sm_count = 148;
   bool host_only = false;
+  bool fp32_only = false;
   int shape = 0, order = 0, physics = 0, dim = 0, nv = 0, n = 0, P = 0, c = 0, npar = 0;
   int64_t E = 0, G = 0;
   salvus::Basis basis;

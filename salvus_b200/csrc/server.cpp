@@ -1,0 +1,451 @@
+// server.cpp -- continuous batching of forward-modelling jobs on one GPU
+// (include/salvus_b200.h, "serving").
+//
+// Threads:
+//   scheduler  admits queued jobs while the device-memory budget and the
+//              running-job limit allow (any queued job that fits may pass a
+//              larger one ahead of it), enqueues one graph-replayed chunk of
+//              steps for every running job on the job's own stream (so the
+//              jobs' kernels overlap on the device), then collects each
+//              chunk: streams the new seismogram samples to the host and
+//              retires finished jobs, freeing their device memory.
+//   worker     prepares admitted jobs (mesh flattening on the host, device
+//              setup, sources, receivers) while the scheduler keeps running
+//              jobs busy.
+// Jobs never share device state, so a job's result does not depend on the
+// mix it ran in.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "internal.h"
+
+namespace salvus {
+const char *last_error();
+}
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+  int64_t id = 0;
+  // owned copies of the description
+  salvus_mesh_desc mesh{};
+  std::vector<double> vertices, params, receivers;
+  std::vector<int64_t> cells;
+  std::vector<salvus_source> sources;
+  int32_t precision = SALVUS_FP32;
+  double dt = 0;
+  int64_t n_steps = 0;
+  int c = 1;
+  // lifecycle
+  std::atomic<int> state{SALVUS_JOB_QUEUED};
+  std::atomic<int64_t> steps_done{0};
+  std::atomic<bool> cancel{false};
+  int64_t est_bytes = 0, G = 0;
+  std::string error;
+  std::vector<double> seis;  // [R][c][n_steps]
+  Clock::time_point submitted, done;
+  salvus_mesh *m = nullptr;
+  salvus_problem *p = nullptr;
+  int64_t chunk_first = 0, chunk_count = 0;
+};
+
+int64_t estimate_bytes(const salvus_mesh_desc &d, int precision) {
+  const int dim = d.shape == SALVUS_QUAD ? 2 : 3;
+  const int64_t n = d.order + 1;
+  const int64_t P = dim == 2 ? n * n : n * n * n;
+  const int64_t c = d.physics == SALVUS_ELASTIC3D ? 3 : 1;
+  const int64_t E = d.n_elements;
+  int64_t G = E;
+  for (int k = 0; k < dim; ++k) G *= d.order;
+  G = G * 5 / 4 + 4 * E;  // interior count plus a generous boundary allowance
+  const int64_t rw32 = salvus::record_words(d.shape, d.physics, 0);
+  const int64_t rw64 = salvus::record_words(d.shape, d.physics, 1);
+  const int64_t rs = precision == SALVUS_FP64 ? 8 : 4;
+  int64_t b = 0;
+  b += E * P * (4 * rw32 + 4 /*conn*/ + 4 /*incidence*/ + 8 /*setup mass, transient*/);
+  if (precision == SALVUS_FP64) b += E * P * 8 * rw64;
+  b += G * (4 + 8 + 4 + 8 * c);  // offsets, inverse mass, node coordinates
+  b += 4 * G * c * rs;             // u v a a_
+  b += E * P * c * rs;             // element-local residual
+  b += G * c * 8;                  // host-copy staging
+  b += E * 8 * dim * 8 + E * 8 * 3 * 8;  // vertices and vertex material
+  return b + (8 << 20);            // per-job slack (graphs, rings)
+}
+
+}  // namespace
+
+struct salvus_server {
+  int device = 0;
+  int64_t budget = 0;
+  int max_running = 8;
+  int chunk = 32;
+  std::mutex mu;
+  std::condition_variable cv_sched, cv_work, cv_done;
+  std::deque<Job *> queue, to_prepare, ready;
+  std::vector<Job *> running;
+  std::map<int64_t, std::unique_ptr<Job>> jobs;
+  int64_t next_id = 1;
+  int64_t mem_in_use = 0, peak_mem = 0;
+  int n_preparing = 0;
+  bool stop = false;
+  std::thread sched, worker;
+  // stats
+  std::vector<double> latencies;
+  double updates = 0;
+  double busy = 0;
+  int64_t submitted = 0, completed = 0, failed = 0;
+  Clock::time_point busy_since;
+  bool busy_now = false;
+};
+
+namespace {
+
+void finish_locked(salvus_server *s, Job *j, int state) {
+  j->state = state;
+  j->done = Clock::now();
+  s->mem_in_use -= j->est_bytes;
+  if (state == SALVUS_JOB_DONE) {
+    s->completed++;
+    s->latencies.push_back(std::chrono::duration<double>(j->done - j->submitted).count());
+    s->updates += (double)j->G * (double)j->n_steps;
+  } else if (state == SALVUS_JOB_FAILED) {
+    s->failed++;
+  }
+  s->cv_done.notify_all();
+  s->cv_sched.notify_all();
+}
+
+void release_device(Job *j) {
+  if (j->p) salvus_problem_destroy(j->p);
+  if (j->m) salvus_mesh_destroy(j->m);
+  j->p = nullptr;
+  j->m = nullptr;
+}
+
+// Host + device preparation of one job (worker thread).
+int prepare(salvus_server *s, Job *j) {
+  int rc = cudaSetDevice(s->device) == cudaSuccess ? SALVUS_OK : SALVUS_E_CUDA;
+  if (rc) return salvus::fail(rc, "cudaSetDevice failed");
+  salvus_mesh_desc d = j->mesh;
+  d.vertices = j->vertices.data();
+  d.cells = j->cells.data();
+  d.params = j->params.data();
+  if (j->precision == SALVUS_FP32) d.reserved |= SALVUS_MESH_FP32_ONLY;
+  if ((rc = salvus_mesh_create(&d, s->device, &j->m))) return rc;
+  int32_t c = 1;
+  if ((rc = salvus_mesh_info(j->m, &j->G, &c, nullptr))) return rc;
+  j->c = c;
+  if ((rc = salvus_problem_create(j->m, j->precision, 1, &j->p))) return rc;
+  if ((rc = salvus_problem_set_dt(j->p, j->dt))) return rc;
+  if ((rc = salvus_problem_set_seismogram_capacity(j->p, 2 * (int64_t)s->chunk + 8))) return rc;
+  for (auto &src : j->sources)
+    if ((rc = salvus_problem_add_source(j->p, &src))) return rc;
+  const int64_t R = (int64_t)j->receivers.size() / 3;
+  for (int64_t r = 0; r < R; ++r)
+    if ((rc = salvus_problem_add_receiver(j->p, &j->receivers[3 * r]))) return rc;
+  j->seis.assign((size_t)(R * j->c * j->n_steps), 0.0);
+  return SALVUS_OK;
+}
+
+void worker_loop(salvus_server *s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    Job *j = nullptr;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_work.wait(lk, [&] { return s->stop || !s->to_prepare.empty(); });
+      if (s->stop) return;
+      j = s->to_prepare.front();
+      s->to_prepare.pop_front();
+    }
+    int rc = j->cancel ? SALVUS_E_STATE : prepare(s, j);
+    std::string err = rc ? salvus::last_error() : "";
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->n_preparing--;
+    if (rc) {
+      release_device(j);
+      j->error = j->cancel ? "cancelled" : err;
+      finish_locked(s, j, j->cancel ? SALVUS_JOB_CANCELLED : SALVUS_JOB_FAILED);
+    } else {
+      s->ready.push_back(j);
+      s->cv_sched.notify_all();
+    }
+  }
+}
+
+void scheduler_loop(salvus_server *s) {
+  cudaSetDevice(s->device);
+  for (;;) {
+    std::vector<Job *> run;
+    {
+      std::unique_lock<std::mutex> lk(s->mu);
+      s->cv_sched.wait_for(lk, std::chrono::milliseconds(2), [&] {
+        return s->stop || !s->ready.empty() || !s->running.empty() || !s->queue.empty();
+      });
+      if (s->stop) return;
+      // admission: any queued job that fits the budget and the slot limit
+      for (auto it = s->queue.begin(); it != s->queue.end();) {
+        Job *j = *it;
+        const int active = (int)s->running.size() + (int)s->ready.size() + s->n_preparing;
+        if (active >= s->max_running) break;
+        if (j->cancel) {
+          j->state = SALVUS_JOB_CANCELLED;
+          it = s->queue.erase(it);
+          s->cv_done.notify_all();
+          continue;
+        }
+        if (s->mem_in_use + j->est_bytes <= s->budget) {
+          s->mem_in_use += j->est_bytes;
+          s->peak_mem = std::max(s->peak_mem, s->mem_in_use);
+          j->state = SALVUS_JOB_RUNNING;
+          s->n_preparing++;
+          s->to_prepare.push_back(j);
+          s->cv_work.notify_one();
+          it = s->queue.erase(it);
+        } else {
+          ++it;
+        }
+      }
+      while (!s->ready.empty()) {
+        s->running.push_back(s->ready.front());
+        s->ready.pop_front();
+      }
+      const bool busy = !s->running.empty() || s->n_preparing > 0;
+      if (busy && !s->busy_now) {
+        s->busy_now = true;
+        s->busy_since = Clock::now();
+      } else if (!busy && s->busy_now) {
+        s->busy_now = false;
+        s->busy += std::chrono::duration<double>(Clock::now() - s->busy_since).count();
+      }
+      run = s->running;
+    }
+    if (run.empty()) continue;
+    // enqueue one chunk per running job (their streams run concurrently)
+    for (Job *j : run) {
+      j->chunk_first = j->steps_done;
+      j->chunk_count = std::min<int64_t>(s->chunk, j->n_steps - j->steps_done);
+      if (j->cancel) j->chunk_count = 0;
+      if (j->chunk_count > 0 && salvus_run(j->p, j->chunk_count, SALVUS_RUN_GRAPH)) {
+        j->error = salvus::last_error();
+        j->chunk_count = -1;
+      }
+    }
+    // collect: stream samples back, retire finished jobs
+    for (Job *j : run) {
+      int rc = SALVUS_OK;
+      if (j->chunk_count > 0) {
+        const int64_t R = (int64_t)j->receivers.size() / 3, rows = R * j->c;
+        std::vector<double> tmp((size_t)(rows * j->chunk_count));
+        if (rows) rc = salvus_get_seismograms(j->p, j->chunk_first, j->chunk_count, tmp.data());
+        else rc = salvus_synchronize(j->p);
+        if (rc == SALVUS_OK) {
+          for (int64_t q = 0; q < rows; ++q)
+            std::memcpy(&j->seis[(size_t)(q * j->n_steps + j->chunk_first)], &tmp[(size_t)(q * j->chunk_count)],
+                        sizeof(double) * j->chunk_count);
+          j->steps_done += j->chunk_count;
+        } else {
+          j->error = salvus::last_error();
+        }
+      } else if (j->chunk_count < 0) {
+        rc = SALVUS_E_CUDA;
+      }
+      const bool cancelled = j->cancel;
+      const bool finished = rc != SALVUS_OK || cancelled || j->steps_done >= j->n_steps;
+      if (finished) {
+        release_device(j);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->running.erase(std::find(s->running.begin(), s->running.end(), j));
+        finish_locked(s, j, rc != SALVUS_OK ? SALVUS_JOB_FAILED
+                               : cancelled  ? SALVUS_JOB_CANCELLED
+                                            : SALVUS_JOB_DONE);
+      }
+    }
+  }
+}
+
+Job *find_job(salvus_server *s, int64_t id) {
+  auto it = s->jobs.find(id);
+  return it == s->jobs.end() ? nullptr : it->second.get();
+}
+
+}  // namespace
+
+extern "C" {
+
+int salvus_server_create(int device, int64_t budget, int32_t max_running, int32_t chunk,
+                         salvus_server **out) {
+  if (!out) return salvus::fail(SALVUS_E_INVALID, "null argument");
+  if (budget <= 0 || max_running < 1 || chunk < 1)
+    return salvus::fail(SALVUS_E_INVALID, "budget, max_running and chunk must be positive");
+  if (cudaSetDevice(device) != cudaSuccess)
+    return salvus::fail(SALVUS_E_CUDA, "cannot use device %d", device);
+  auto *s = new salvus_server();
+  s->device = device;
+  s->budget = budget;
+  s->max_running = max_running;
+  s->chunk = chunk;
+  s->sched = std::thread(scheduler_loop, s);
+  s->worker = std::thread(worker_loop, s);
+  *out = s;
+  return SALVUS_OK;
+}
+
+int salvus_server_submit(salvus_server *s, const salvus_job_desc *d, int64_t *job_id) {
+  if (!s || !d || !job_id) return salvus::fail(SALVUS_E_INVALID, "null argument");
+  if (d->n_steps <= 0 || !(d->dt > 0)) return salvus::fail(SALVUS_E_INVALID, "bad dt / n_steps");
+  const salvus_mesh_desc &m = d->mesh;
+  if (m.n_elements <= 0 || m.n_vertices <= 0 || !m.vertices || !m.cells || !m.params)
+    return salvus::fail(SALVUS_E_INVALID, "empty mesh");
+  if (m.shape != SALVUS_QUAD && m.shape != SALVUS_HEX)
+    return salvus::fail(SALVUS_E_UNSUPPORTED, "shape %d not served", m.shape);
+  std::unique_ptr<Job> j(new Job());
+  j->mesh = m;
+  const int dim = m.shape == SALVUS_QUAD ? 2 : 3, nv = m.shape == SALVUS_QUAD ? 4 : 8;
+  const int npar = m.physics == SALVUS_ELASTIC3D ? 3 : 1;
+  j->vertices.assign(m.vertices, m.vertices + m.n_vertices * dim);
+  j->cells.assign(m.cells, m.cells + m.n_elements * nv);
+  j->params.assign(m.params, m.params + (size_t)npar * m.n_elements * nv);
+  if (d->n_sources > 0) j->sources.assign(d->sources, d->sources + d->n_sources);
+  if (d->n_receivers > 0) j->receivers.assign(d->receivers, d->receivers + 3 * d->n_receivers);
+  j->precision = d->precision;
+  j->dt = d->dt;
+  j->n_steps = d->n_steps;
+  j->est_bytes = estimate_bytes(m, d->precision);
+  if (j->est_bytes > s->budget)
+    return salvus::fail(SALVUS_E_OOM, "job needs about %lld bytes; the server budget is %lld",
+                        (long long)j->est_bytes, (long long)s->budget);
+  j->submitted = Clock::now();
+  std::lock_guard<std::mutex> lk(s->mu);
+  j->id = s->next_id++;
+  *job_id = j->id;
+  s->queue.push_back(j.get());
+  s->jobs[j->id] = std::move(j);
+  s->submitted++;
+  s->cv_sched.notify_all();
+  return SALVUS_OK;
+}
+
+int salvus_server_poll(salvus_server *s, int64_t id, int32_t *state, int64_t *steps_done,
+                       int64_t *n_nodes) {
+  if (!s) return salvus::fail(SALVUS_E_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Job *j = find_job(s, id);
+  if (!j) return salvus::fail(SALVUS_E_INVALID, "unknown job %lld", (long long)id);
+  if (state) *state = j->state;
+  if (steps_done) *steps_done = j->steps_done;
+  if (n_nodes) *n_nodes = j->G;
+  if (j->state == SALVUS_JOB_FAILED) salvus::set_error("%s", j->error.c_str());
+  return SALVUS_OK;
+}
+
+int salvus_server_seismograms(salvus_server *s, int64_t id, int64_t first, int64_t count, double *out) {
+  if (!s || !out) return salvus::fail(SALVUS_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Job *j = find_job(s, id);
+  if (!j) return salvus::fail(SALVUS_E_INVALID, "unknown job %lld", (long long)id);
+  if (first < 0 || count < 0 || first + count > j->steps_done)
+    return salvus::fail(SALVUS_E_INVALID, "steps [%lld, %lld) not yet streamed (%lld done)",
+                        (long long)first, (long long)(first + count), (long long)j->steps_done.load());
+  const int64_t rows = (int64_t)j->receivers.size() / 3 * j->c;
+  for (int64_t q = 0; q < rows; ++q)
+    std::memcpy(out + q * count, &j->seis[(size_t)(q * j->n_steps + first)], sizeof(double) * count);
+  return SALVUS_OK;
+}
+
+int salvus_server_wait(salvus_server *s, int64_t id, double timeout_s) {
+  if (!s) return salvus::fail(SALVUS_E_INVALID, "null server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  Job *j = find_job(s, id);
+  if (!j) return salvus::fail(SALVUS_E_INVALID, "unknown job %lld", (long long)id);
+  const bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] {
+    const int st = j->state;
+    return st == SALVUS_JOB_DONE || st == SALVUS_JOB_FAILED || st == SALVUS_JOB_CANCELLED;
+  });
+  if (!ok) return salvus::fail(SALVUS_E_TIMEOUT, "job %lld not finished after %.3f s", (long long)id, timeout_s);
+  if (j->state == SALVUS_JOB_FAILED) return salvus::fail(SALVUS_E_INVALID, "%s", j->error.c_str());
+  return SALVUS_OK;
+}
+
+int salvus_server_cancel(salvus_server *s, int64_t id) {
+  if (!s) return salvus::fail(SALVUS_E_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Job *j = find_job(s, id);
+  if (!j) return salvus::fail(SALVUS_E_INVALID, "unknown job %lld", (long long)id);
+  j->cancel = true;
+  s->cv_sched.notify_all();
+  return SALVUS_OK;
+}
+
+int salvus_server_release(salvus_server *s, int64_t id) {
+  if (!s) return salvus::fail(SALVUS_E_INVALID, "null server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  Job *j = find_job(s, id);
+  if (!j) return salvus::fail(SALVUS_E_INVALID, "unknown job %lld", (long long)id);
+  const int st = j->state;
+  if (st != SALVUS_JOB_DONE && st != SALVUS_JOB_FAILED && st != SALVUS_JOB_CANCELLED)
+    return salvus::fail(SALVUS_E_STATE, "job %lld is still active", (long long)id);
+  s->jobs.erase(id);
+  return SALVUS_OK;
+}
+
+int salvus_server_stats_read(salvus_server *s, salvus_server_stats *o) {
+  if (!s || !o) return salvus::fail(SALVUS_E_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::vector<double> l = s->latencies;
+  std::sort(l.begin(), l.end());
+  auto pct = [&](double q) -> double {
+    if (l.empty()) return 0.0;
+    const size_t k = (size_t)std::min<double>(l.size() - 1, std::ceil(q * l.size()) - 1);
+    return l[k];
+  };
+  std::memset(o, 0, sizeof(*o));
+  o->submitted = s->submitted;
+  o->completed = s->completed;
+  o->failed = s->failed;
+  o->running = (int64_t)s->running.size() + s->n_preparing + (int64_t)s->ready.size();
+  o->queued = (int64_t)s->queue.size();
+  o->p50_latency_s = pct(0.50);
+  o->p99_latency_s = pct(0.99);
+  double sum = 0;
+  for (double x : l) sum += x;
+  o->mean_latency_s = l.empty() ? 0.0 : sum / l.size();
+  o->gll_point_updates = s->updates;
+  o->busy_seconds = s->busy + (s->busy_now ? std::chrono::duration<double>(Clock::now() - s->busy_since).count() : 0.0);
+  o->peak_device_bytes = s->peak_mem;
+  return SALVUS_OK;
+}
+
+int salvus_server_destroy(salvus_server *s) {
+  if (!s) return SALVUS_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    for (auto &kv : s->jobs) kv.second->cancel = true;
+  }
+  s->cv_sched.notify_all();
+  s->cv_work.notify_all();
+  if (s->sched.joinable()) s->sched.join();
+  if (s->worker.joinable()) s->worker.join();
+  cudaSetDevice(s->device);
+  for (auto &kv : s->jobs) release_device(kv.second.get());
+  delete s;
+  return SALVUS_OK;
+}
+
+}  // extern "C"
