@@ -38,6 +38,8 @@ def parse():
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-shots", action="store_true", help="skip the batched-shots leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serving-jobs", type=int, default=24)
     ap.add_argument("--profile-only", action="store_true",
                     help="run a few steps only (for ncu captures); prints no JSON")
     return ap.parse_args()
@@ -179,6 +181,97 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
             "shot_throughput_ratio": batched / plain, "steps": steps,
             "tuning": {"stiffness_shot_lanes": tune[0], "stiffness_elements_per_cta": tune[1],
                        "gather_shot_lanes": tune[2], "gather_nodes_per_cta": tune[3]}}
+
+
+def unit_dt(core, meshgen, kind, order=4):
+    """Critical step of a unit mesh (h = 1, vp_max = 1) for this element
+    family; dt_crit(h, vp) = unit_dt * h / vp (lambda_max scales as (vp/h)^2)."""
+    if kind == "quad":
+        V, C = meshgen.structured_quad(6, 6, 6.0, 6.0)
+        m = core.Mesh(core.QUAD, order, core.ACOUSTIC, V, C, np.ones((1, len(C), 4)))
+    else:
+        V, C = meshgen.structured_hex(4, 4, 4, 4.0, 4.0, 4.0)
+        E = len(C)
+        par = np.stack([np.full((E, 8), 1.0), np.full((E, 8), 1.0), np.full((E, 8), 0.5773)])
+        m = core.Mesh(core.HEX, order, core.ELASTIC3D, V, C, par)
+    return m.critical_dt(iterations=300)
+
+
+def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8):
+    """Config 4 (bounded sample): a seeded stream of n_jobs jobs, half 2-D
+    acoustic quads (edge U{50..400}), half 3-D elastic hexes (edge
+    U{16..48}), order 4, own model and source each, steps U{1000..6000}.
+    First every job runs alone, one after the other (plain form, mesh
+    preparation included); then the same jobs arrive as a Poisson stream at
+    load x the serial service rate and the server runs them."""
+    from salvus_b200 import serving
+    ud = {k: unit_dt(core, meshgen, k) for k in ("quad", "hex")}
+    stream = configs.serving_stream(n_jobs, seed=seed)
+    jobs = []
+    for kind, edge, s, n, _ in stream:
+        cfg = configs.serving_job(kind, edge, s)
+        dt = 0.4 * ud[kind] * cfg["h"] / cfg["vmax"]
+        jobs.append((kind, cfg, dt, n))
+    # serial plain runs
+    t0 = time.perf_counter()
+    serial_updates = 0.0
+    for kind, cfg, dt, n in jobs:
+        m = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                      cfg["params"])
+        p = core.Problem(m, core.FP32, dt=dt)
+        s = cfg["sources"][0]
+        if "moment_tensor" in s:
+            p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                         moment_tensor=s["moment_tensor"])
+        else:
+            p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                         direction=s["direction"])
+        for r in cfg["receivers"]:
+            p.add_receiver(r)
+        p.set_seismogram_capacity(n + 8)
+        p.run(n, core.RUN_PLAIN)
+        p.seismograms()
+        serial_updates += m.n_nodes * n
+        p.close()
+        m.close()
+    serial_s = time.perf_counter() - t0
+    # capacity: all jobs submitted at once
+    srv = serving.Server(budget_bytes=150 * 10**9, max_running=16, chunk_steps=64)
+    t0 = time.perf_counter()
+    ids = [srv.submit(cfg, dt, n) for kind, cfg, dt, n in jobs]
+    for j in ids:
+        srv.wait(j, 3600)
+    burst_s = time.perf_counter() - t0
+    burst_updates = srv.stats()["gll_point_updates"]
+    srv.close()
+    # served stream at `load` times the measured capacity
+    rng = np.random.default_rng(seed + 1)
+    gaps = rng.exponential(burst_s / n_jobs / load, size=n_jobs)
+    srv = serving.Server(budget_bytes=150 * 10**9, max_running=16, chunk_steps=64)
+    t0 = time.perf_counter()
+    ids = []
+    for (kind, cfg, dt, n), gap in zip(jobs, gaps):
+        time.sleep(gap)
+        ids.append(srv.submit(cfg, dt, n))
+    for j in ids:
+        srv.wait(j, 3600)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    return {"workload": f"{n_jobs} jobs: 2-D acoustic quads 50^2-400^2 and 3-D elastic hexes "
+                        f"16^3-48^3, order 4, 1000-6000 steps; latency under Poisson arrivals at "
+                        f"{load:.0%} of the measured capacity (bounded sample of the 2000-job stream)",
+            "p50_latency_s": st["p50_latency_s"], "p99_latency_s": st["p99_latency_s"],
+            "mean_latency_s": st["mean_latency_s"], "completed": st["completed"],
+            "failed": st["failed"], "value": burst_updates / burst_s, "unit": METRIC,
+            "value_form": "all jobs submitted at once; total G*steps / makespan (preparation included)",
+            "makespan_s": burst_s, "stream_updates_per_s": st["gll_point_updates"] / st["busy_seconds"],
+            "stream_wall_s": wall,
+            "serial_value": serial_updates / serial_s, "serial_s": serial_s,
+            "serial_form": "each job alone, one after the other, plain host-launched steps, "
+                           "preparation included",
+            "throughput_ratio": (burst_updates / burst_s) / (serial_updates / serial_s),
+            "peak_device_bytes": st["peak_device_bytes"]}
 
 
 def reference_arm(args, rank, world):
@@ -334,6 +427,10 @@ def main():
     shots = None
     if not args.no_shots:
         shots = shots_leg(core, configs, timed_on, steps=min(args.steps, 300), device=local)
+    serve = None
+    if not args.no_serving and rank == 0 and world == 1:
+        from salvus_b200 import meshgen
+        serve = serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -365,6 +462,7 @@ def main():
             "clocks": ck,
             "cpu_baseline": cpu,
             "shots_batched": shots,
+            "serving": serve,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -9,9 +9,9 @@
 //              jobs' kernels overlap on the device), then collects each
 //              chunk: streams the new seismogram samples to the host and
 //              retires finished jobs, freeing their device memory.
-//   worker     prepares admitted jobs (mesh flattening on the host, device
-//              setup, sources, receivers) while the scheduler keeps running
-//              jobs busy.
+//   workers    (up to 4) prepare admitted jobs (mesh flattening on the host,
+//              device setup, sources, receivers) while the scheduler keeps
+//              running jobs busy.
 // Jobs never share device state, so a job's result does not depend on the
 // mix it ran in.
 #include <cuda_runtime.h>
@@ -103,7 +103,8 @@ struct salvus_server {
   int64_t mem_in_use = 0, peak_mem = 0;
   int n_preparing = 0;
   bool stop = false;
-  std::thread sched, worker;
+  std::thread sched;
+  std::vector<std::thread> workers;  // job preparation pool
   // stats
   std::vector<double> latencies;
   double updates = 0;
@@ -301,7 +302,9 @@ int salvus_server_create(int device, int64_t budget, int32_t max_running, int32_
   s->max_running = max_running;
   s->chunk = chunk;
   s->sched = std::thread(scheduler_loop, s);
-  s->worker = std::thread(worker_loop, s);
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int nw = (int)std::max(1u, std::min(4u, hw / 2));
+  for (int w = 0; w < nw; ++w) s->workers.emplace_back(worker_loop, s);
   *out = s;
   return SALVUS_OK;
 }
@@ -441,7 +444,8 @@ int salvus_server_destroy(salvus_server *s) {
   s->cv_sched.notify_all();
   s->cv_work.notify_all();
   if (s->sched.joinable()) s->sched.join();
-  if (s->worker.joinable()) s->worker.join();
+  for (auto &w : s->workers)
+    if (w.joinable()) w.join();
   cudaSetDevice(s->device);
   for (auto &kv : s->jobs) release_device(kv.second.get());
   delete s;
