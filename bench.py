@@ -71,7 +71,7 @@ def cpu_threads():
         return os.cpu_count() or 1
 
 
-def cpu_leg(args, nel_sample, steps, warm):
+def cpu_leg(args, nel_sample, steps, warm, target_s=10.0):
     """Time the FP64 CPU oracle in reference-faithful mode (per-point Jacobian
     rebuilds, Hexahedra.cpp:600,702) on a bounded sample of the workload."""
     from oracle import pyoracle as po
@@ -86,8 +86,11 @@ def cpu_leg(args, nel_sample, steps, warm):
     for r in cfg["receivers"]:
         o.add_receiver(r)
     dt = 1e-3
-    if warm:
-        o.run(warm, dt)
+    t0 = time.perf_counter()
+    o.run(max(1, warm), dt)  # warm-up, also sizes the sample
+    per_step = (time.perf_counter() - t0) / max(1, warm)
+    if steps is None:  # about target_s of CPU work, 2..200 steps
+        steps = int(min(200, max(2, target_s / max(per_step, 1e-6))))
     t0 = time.perf_counter()
     o.run(steps, dt)
     el = time.perf_counter() - t0
@@ -277,10 +280,12 @@ def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8):
 def reference_arm(args, rank, world):
     if rank != 0:
         return
+    # each step is the full step of a 32^3-element sample of the workload;
+    # the timed steps are sized to about 30 s of CPU work (at most --steps)
     nel_sample = min(args.nel, 32)
-    steps = max(1, min(args.steps, 3))
-    warm = 1 if args.warmup > 0 else 0
-    rate, thr, sample, el = cpu_leg(args, nel_sample, steps, warm)
+    warm = 1
+    rate, thr, sample, el = cpu_leg(args, nel_sample, None, warm, target_s=30.0)
+    steps = int(sample.split(" x ")[1].split(" steps")[0])
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC,
             "n_gpus": args.gpus, "steps": steps, "warmup": warm, "higher_is_better": True,
             "ms_per_step": 1e3 * el / steps, "dtype": "f64", "data": "synthetic",
@@ -434,7 +439,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, thr, sample, _ = cpu_leg(args, min(args.nel, 32), 2, 1)
+        rate, thr, sample, _ = cpu_leg(args, min(args.nel, 32), None, 1)
         cpu = {"value": rate, "unit": METRIC, "cores": thr, "kind": "port", "sample": sample}
 
     if rank == 0:
