@@ -52,6 +52,12 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  *   quad v0(-,-) v1(+,-) v2(+,+) v3(-,+)                  (QuadP1.h:98-108)
  *   hex  v0(-,-,-) v1(-,+,-) v2(+,+,-) v3(+,-,-)
  *        v4(-,-,+) v5(+,-,+) v6(+,+,+) v7(-,+,+)         (HexP1.cpp:86-122)
+ *   tri  v0 -> (-1,-1), v1 -> (1,-1), v2 -> (-1,1), counter-clockwise
+ *                                                          (TriP1.cpp:117-154)
+ *   tet  v0 -> (0,0,0), v1 -> (0,1,0), v2 -> (1,0,0), v3 -> (0,0,1) with
+ *        det[v2-v0; v1-v0; v3-v0] > 0                     (TetP1.cpp:150-205)
+ * Simplices are the P3 mass-lumped elements (12-node triangle, 50-node
+ * tetrahedron; order must be 3); elastic3d runs on hexahedra and tetrahedra. 
  * params are per element, per element vertex (Exodus NAME_0..NAME_k):
  *   acoustic : [1][n_elements][nv]  VP                    (Scalar.cpp:23-25)
  *   elastic3d: [3][n_elements][nv]  RHO, VP, VS  (isotropic form of
@@ -63,13 +69,13 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
 
 typedef struct {
   int32_t shape;   /* enum salvus_shape */
-  int32_t order;   /* polynomial order: quad 1..10, hex 1..6 */
+  int32_t order;   /* polynomial order: quad 1..10, hex 1..6, tri / tet 3 */
   int32_t physics; /* enum salvus_physics */
   int32_t reserved; /* flags: SALVUS_MESH_FP32_ONLY */
   int64_t n_vertices;
   const double *vertices; /* [n_vertices][dim] */
   int64_t n_elements;
-  const int64_t *cells;   /* [n_elements][4 | 8] */
+  const int64_t *cells;   /* [n_elements][nv]: quad 4, hex 8, tri 3, tet 4 */
   const double *params;
 } salvus_mesh_desc;
 
@@ -93,6 +99,20 @@ typedef struct salvus_problem salvus_problem;
 const char *salvus_last_error(void);
 /* Library build string (compile arch, version). */
 const char *salvus_version(void);
+
+/* ---- reference elements ---- */
+/* Nodes, weights and derivative tables of one reference element:
+ * *n_points = P; points [P][dim] reference coordinates; weights [P];
+ * dphi [dim][P][P] with dphi[(k*P + i)*P + q] = d phi_i / d xi_k at point q.
+ * Replaces TensorQuad::GllPointsForOrder / GllIntegrationWeightsForOrder /
+ * setupGradientOperator (TensorQuad.cpp:51-142), the Hexahedra equivalents
+ * (Hexahedra.cpp:75-130, 535-577), Triangle::QuadraturePoints /
+ * QuadratureIntegrationWeight / setupGradientOperator (Triangle.cpp:22-54,
+ * 243-256) and Tetrahedra::QuadraturePoints / QuadratureIntegrationWeights /
+ * setupGradientOperator (Tetrahedra.cpp:64-99, 432-447).  Output pointers may
+ * be NULL.  Needs no GPU. */
+int salvus_element_tables(int32_t shape, int32_t order, int32_t *n_points, double *points,
+                          double *weights, double *dphi);
 
 /* ---- mesh ---- */
 /* Flattens the mesh once: GLL connectivity by topological keys, FP64

@@ -148,6 +148,285 @@ double orc_ricker(double t, double f0, double t0, double amp) {
 }
 
 /* ------------------------------------------------------------------------ */
+/* P3 simplex tables.                                                        */
+/* Nodal basis of the mass-lumped P3 triangle (P3 + cubic bubble x P1, 12
+ * nodes) and tetrahedron (P3 + face bubbles x P2 + interior bubble x P2, 50
+ * nodes): phi_i(x) = sum_m mono_m(x) C[m][i] with C = V^-1, V[q][m] =
+ * mono_m(x_q), exactly as p3ElementPolynomials builds it
+ * (triangle_points_weights_polys.py:62-97, tetrahedra_points_weights_polys.py:55-105),
+ * and the derivative tables are d mono / d xi at the nodes times C
+ * (genP3code, ...:133-160 / :200-225). */
+#define ORC_SP 50
+typedef struct {
+  int P, dim;
+  double x[ORC_SP][3];
+  double w[ORC_SP];
+  double D[3][ORC_SP * ORC_SP]; /* D[k][i*P+q] = d phi_i / d xi_k (x_q) */
+  double C[ORC_SP * ORC_SP];    /* C[m*P+i] */
+} stab_t;
+static stab_t g_stab[2];        /* [0] triangle, [1] tetrahedron */
+static int g_stab_ok[2];
+
+/* value and gradient of a polynomial factor */
+typedef struct { double v, d[3]; } dual_t;
+static dual_t dl_var(double x, int k) { dual_t r = {x, {0, 0, 0}}; r.d[k] = 1; return r; }
+static dual_t dl_const(double c) { dual_t r = {c, {0, 0, 0}}; return r; }
+static dual_t dl_mul(dual_t a, dual_t b) {
+  dual_t r = {a.v * b.v, {0, 0, 0}};
+  for (int k = 0; k < 3; ++k) r.d[k] = a.d[k] * b.v + a.v * b.d[k];
+  return r;
+}
+static dual_t dl_add(dual_t a, dual_t b) {
+  dual_t r = {a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2]}};
+  return r;
+}
+static dual_t dl_scale(dual_t a, double c) {
+  dual_t r = {a.v * c, {a.d[0] * c, a.d[1] * c, a.d[2] * c}};
+  return r;
+}
+static dual_t dl_pow(dual_t a, int e) {
+  dual_t r = dl_const(1);
+  for (int i = 0; i < e; ++i) r = dl_mul(r, a);
+  return r;
+}
+
+/* Monomial list of the triangle generator (triangle_points_weights_polys.py:63-69):
+ * P3 = [1, r, s, rs, r^2, s^2, r^3, s^3, r^2 s, r s^2], then b [r, s] with
+ * b = (-r-s)(s+1)(r+1). */
+static void tri_monomials(const double *x, dual_t *m) {
+  dual_t r = dl_var(x[0], 0), s = dl_var(x[1], 1), one = dl_const(1);
+  dual_t b = dl_mul(dl_mul(dl_add(dl_scale(r, -1), dl_scale(s, -1)), dl_add(s, one)), dl_add(r, one));
+  m[0] = one; m[1] = r; m[2] = s; m[3] = dl_mul(r, s);
+  m[4] = dl_pow(r, 2); m[5] = dl_pow(s, 2); m[6] = dl_pow(r, 3); m[7] = dl_pow(s, 3);
+  m[8] = dl_mul(dl_pow(r, 2), s); m[9] = dl_mul(r, dl_pow(s, 2));
+  m[10] = dl_mul(r, b); m[11] = dl_mul(s, b);
+}
+
+/* Monomial list of the tetrahedron generator (tetrahedra_points_weights_polys.py:55-83). */
+static void tet_monomials(const double *x, dual_t *m) {
+  dual_t r = dl_var(x[0], 0), s = dl_var(x[1], 1), t = dl_var(x[2], 2), one = dl_const(1);
+  dual_t l0 = dl_add(one, dl_scale(dl_add(dl_add(r, s), t), -1)); /* 1 - r - s - t */
+  dual_t b1 = dl_mul(dl_mul(r, s), l0), b2 = dl_mul(dl_mul(r, t), l0), b3 = dl_mul(dl_mul(t, s), l0);
+  dual_t b4 = dl_mul(dl_mul(r, s), t), bt = dl_mul(b4, l0);
+  dual_t rr = dl_add(one, dl_scale(dl_add(r, t), -1)), ss = dl_add(one, dl_scale(dl_add(s, t), -1));
+  int k = 0;
+  /* P3 */
+  m[k++] = one; m[k++] = r; m[k++] = dl_pow(r, 2); m[k++] = dl_pow(r, 3);
+  m[k++] = s; m[k++] = dl_pow(s, 2); m[k++] = dl_pow(s, 3);
+  m[k++] = t; m[k++] = dl_pow(t, 2); m[k++] = dl_pow(t, 3);
+  m[k++] = dl_mul(r, s); m[k++] = dl_mul(dl_pow(r, 2), s); m[k++] = dl_mul(r, dl_pow(s, 2));
+  m[k++] = dl_mul(r, t); m[k++] = dl_mul(dl_pow(r, 2), t); m[k++] = dl_mul(r, dl_pow(t, 2));
+  m[k++] = dl_mul(s, t); m[k++] = dl_mul(dl_pow(s, 2), t); m[k++] = dl_mul(s, dl_pow(t, 2));
+  m[k++] = dl_mul(dl_mul(r, s), t);
+  /* interior bubble x [1, r, s, t, rs, rt, st, r^2, s^2, t^2] */
+  dual_t p1t[10] = {one, r, s, t, dl_mul(r, s), dl_mul(r, t), dl_mul(s, t),
+                    dl_pow(r, 2), dl_pow(s, 2), dl_pow(t, 2)};
+  for (int i = 0; i < 10; ++i) m[k++] = dl_mul(bt, p1t[i]);
+  /* face bubbles x P2 pieces */
+  dual_t f1[5] = {r, s, dl_mul(r, s), dl_pow(r, 2), dl_pow(s, 2)};
+  dual_t f2[5] = {r, t, dl_mul(r, t), dl_pow(r, 2), dl_pow(t, 2)};
+  dual_t f3[5] = {t, s, dl_mul(t, s), dl_pow(t, 2), dl_pow(s, 2)};
+  dual_t f4[5] = {rr, ss, dl_mul(rr, ss), dl_pow(rr, 2), dl_pow(ss, 2)};
+  for (int i = 0; i < 5; ++i) m[k++] = dl_mul(b1, f1[i]);
+  for (int i = 0; i < 5; ++i) m[k++] = dl_mul(b2, f2[i]);
+  for (int i = 0; i < 5; ++i) m[k++] = dl_mul(b3, f3[i]);
+  for (int i = 0; i < 5; ++i) m[k++] = dl_mul(b4, f4[i]);
+}
+
+/* Reference nodes in PETSc closure order (face, edges, vertices) of
+ * p3ReferenceNodes (triangle_points_weights_polys.py:26-47), 4-digit values
+ * as the generator states them; weights of p3QuadratureWeights (:14-24). */
+static void tri_nodes(stab_t *t) {
+  static const double rs[12][2] = {
+      {-0.5853, -0.5853}, {0.1706, -0.5853}, {-0.5853, 0.1706}, {-0.413, -1.0},
+      {0.413, -1.0},      {0.413, -0.413},   {-0.413, 0.413},   {-1.0, 0.413},
+      {-1.0, -0.413},     {-1.0, -1.0},      {1.0, -1.0},       {-1.0, 1.0}};
+  const double s7 = sqrt(7.0);
+  const double ws = 2 * (919 * s7 + 2471) / (124080 * s7 + 330960);
+  const double wa = 2 * (s7 * pow(2 + s7, 4)) / (25280 + 9520 * s7);
+  const double wb = 2 * (147 + 42 * s7) / (400 * s7 + 1280);
+  for (int q = 0; q < 12; ++q) {
+    t->x[q][0] = rs[q][0]; t->x[q][1] = rs[q][1]; t->x[q][2] = 0;
+    t->w[q] = q < 3 ? wb : q < 9 ? wa : ws;
+  }
+}
+
+/* BuildNodesTetrahedraP3 (BuildNodesTetrahedraP3.py:10-313): interior
+ * orbits (gamma, delta), two face orbits per face (beta1, beta2), two points
+ * per edge (alpha), then the corners; the constants and weights (x6 for the
+ * unit-volume normalisation) are those of Chin-Joe-Kong, Mulder and Van
+ * Veldhuizen (1999) as quoted in p3QuadratureWeights
+ * (tetrahedra_points_weights_polys.py:15-45). */
+static void tet_nodes(stab_t *t) {
+  const double beta1 = 0.1972862280257976, beta2 = 0.4256461243139345;
+  const double alpha = 0.2928294047674109, gamma = 0.9503775858394107e-01;
+  const double delta = 0.1252462362578136;
+  static const double O[3] = {0, 0, 0}, X[3] = {1, 0, 0}, Y[3] = {0, 1, 0}, Z[3] = {0, 0, 1};
+  const double *R[4] = {O, X, Y, Z};
+  int k = 0;
+  /* interior A: corner pulled towards the opposite face centroid */
+  for (int c = 0; c < 4; ++c) {
+    for (int m = 0; m < 3; ++m) {
+      double cen = 0;
+      for (int o = 0; o < 4; ++o)
+        if (o != c) cen += R[o][m];
+      t->x[k][m] = (1 - 3 * gamma) * R[c][m] + 3 * gamma * (cen / 3.0);
+    }
+    ++k;
+  }
+  /* interior B: between opposite edge midpoints */
+  static const int pairs[6][4] = {{0, 3, 1, 2}, {0, 1, 2, 3}, {0, 2, 1, 3},
+                                  {1, 2, 0, 3}, {2, 3, 0, 1}, {1, 3, 0, 2}};
+  for (int i = 0; i < 6; ++i, ++k)
+    for (int m = 0; m < 3; ++m) {
+      double a = 0.5 * (R[pairs[i][0]][m] + R[pairs[i][1]][m]);
+      double b = 0.5 * (R[pairs[i][2]][m] + R[pairs[i][3]][m]);
+      t->x[k][m] = (1 - 2 * delta) * a + 2 * delta * b;
+    }
+  /* faces: (O,Y,X) (O,Z,Y) (O,X,Z) (X,Y,Z), beta1 orbit then beta2 orbit */
+  const double *F[4][3] = {{O, Y, X}, {O, Z, Y}, {O, X, Z}, {X, Y, Z}};
+  for (int f = 0; f < 4; ++f)
+    for (int o = 0; o < 2; ++o) {
+      const double beta = o == 0 ? beta1 : beta2;
+      for (int i = 0; i < 3; ++i, ++k)
+        for (int m = 0; m < 3; ++m) {
+          double mid = 0.5 * (F[f][(i + 1) % 3][m] + F[f][(i + 2) % 3][m]);
+          t->x[k][m] = (1 - 2 * beta) * F[f][i][m] + 2 * beta * mid;
+        }
+    }
+  /* edges */
+  const double *Ed[6][2] = {{O, Y}, {Y, X}, {X, O}, {O, Z}, {Z, Y}, {X, Z}};
+  for (int e = 0; e < 6; ++e)
+    for (int o = 0; o < 2; ++o, ++k)
+      for (int m = 0; m < 3; ++m) {
+        double a = o == 0 ? 1 - alpha : alpha;
+        t->x[k][m] = a * Ed[e][0][m] + (1 - a) * Ed[e][1][m];
+      }
+  /* corners v0..v3 = (0,0,0) (0,1,0) (1,0,0) (0,0,1) (TetP1.cpp:247-258 map) */
+  const double *Cn[4] = {O, Y, X, Z};
+  for (int c = 0; c < 4; ++c, ++k)
+    for (int m = 0; m < 3; ++m) t->x[k][m] = Cn[c][m];
+  const double w0 = 0.2143608668049743e-03 * 6, wa = 0.8268179517797114e-03 * 6;
+  const double wb1 = 0.1840177904191860e-02 * 6, wb2 = 0.1831324329245650e-02 * 6;
+  const double wg = 0.7542468904648131e-02 * 6, wd = 0.1360991755970793e-01 * 6;
+  for (int q = 0; q < 50; ++q) {
+    double w;
+    if (q < 4) w = wg;
+    else if (q < 10) w = wd;
+    else if (q < 34) w = ((q - 10) % 6) < 3 ? wb1 : wb2;
+    else if (q < 46) w = wa;
+    else w = w0;
+    t->w[q] = w;
+  }
+}
+
+/* In-place inverse by Gauss-Jordan elimination with partial pivoting
+ * (extended precision). */
+static int invert_ld(int n, long double *A) {
+  long double *I = (long double *)calloc((size_t)n * n, sizeof(long double));
+  if (!I) return -1;
+  for (int i = 0; i < n; ++i) I[i * n + i] = 1;
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < n; ++r)
+      if (fabsl(A[r * n + c]) > fabsl(A[piv * n + c])) piv = r;
+    if (A[piv * n + c] == 0) { free(I); return -1; }
+    if (piv != c)
+      for (int k = 0; k < n; ++k) {
+        long double x = A[c * n + k]; A[c * n + k] = A[piv * n + k]; A[piv * n + k] = x;
+        x = I[c * n + k]; I[c * n + k] = I[piv * n + k]; I[piv * n + k] = x;
+      }
+    long double d = A[c * n + c];
+    for (int k = 0; k < n; ++k) { A[c * n + k] /= d; I[c * n + k] /= d; }
+    for (int r = 0; r < n; ++r) {
+      if (r == c) continue;
+      long double f = A[r * n + c];
+      if (f == 0) continue;
+      for (int k = 0; k < n; ++k) { A[r * n + k] -= f * A[c * n + k]; I[r * n + k] -= f * I[c * n + k]; }
+    }
+  }
+  memcpy(A, I, sizeof(long double) * (size_t)n * n);
+  free(I);
+  return 0;
+}
+
+static void simplex_monomials(int tet, const double *x, dual_t *m) {
+  if (tet) tet_monomials(x, m);
+  else tri_monomials(x, m);
+}
+
+static int build_stab(int tet) {
+  stab_t *t = &g_stab[tet];
+  t->P = tet ? 50 : 12;
+  t->dim = tet ? 3 : 2;
+  const int P = t->P;
+  if (tet) tet_nodes(t);
+  else tri_nodes(t);
+  long double *V = (long double *)malloc(sizeof(long double) * P * P);
+  if (!V) return -1;
+  dual_t m[ORC_SP];
+  for (int q = 0; q < P; ++q) {
+    simplex_monomials(tet, t->x[q], m);
+    for (int j = 0; j < P; ++j) V[q * P + j] = m[j].v;
+  }
+  if (invert_ld(P, V)) { free(V); return -1; }
+  for (int i = 0; i < P * P; ++i) t->C[i] = (double)V[i];
+  for (int q = 0; q < P; ++q) {
+    simplex_monomials(tet, t->x[q], m);
+    for (int k = 0; k < t->dim; ++k)
+      for (int i = 0; i < P; ++i) {
+        long double s = 0;
+        for (int j = 0; j < P; ++j) s += (long double)m[j].d[k] * V[j * P + i];
+        t->D[k][i * P + q] = (double)s;
+      }
+  }
+  free(V);
+  return 0;
+}
+
+__attribute__((constructor)) static void init_simplex_tables(void) {
+  g_stab_ok[0] = build_stab(0) == 0;
+  g_stab_ok[1] = build_stab(1) == 0;
+}
+
+static const stab_t *stab_for(int shape) {
+  int k = shape == ORC_TRI ? 0 : shape == ORC_TET ? 1 : -1;
+  if (k < 0 || !g_stab_ok[k]) return NULL;
+  return &g_stab[k];
+}
+
+int orc_simplex_tables(int shape, double *nodes, double *weights, double *D) {
+  const stab_t *t = stab_for(shape);
+  if (!t) { set_err("no simplex tables for shape %d", shape); return -1; }
+  const int P = t->P;
+  for (int q = 0; q < P; ++q) {
+    if (nodes) for (int m = 0; m < 3; ++m) nodes[q * 3 + m] = t->x[q][m];
+    if (weights) weights[q] = t->w[q];
+  }
+  if (D) for (int k = 0; k < t->dim; ++k) memcpy(D + (size_t)k * P * P, t->D[k], sizeof(double) * P * P);
+  return 0;
+}
+
+int orc_simplex_basis(int shape, const double *ref, double *phi, double *dphi) {
+  const stab_t *t = stab_for(shape);
+  if (!t) { set_err("no simplex tables for shape %d", shape); return -1; }
+  const int P = t->P;
+  dual_t m[ORC_SP];
+  simplex_monomials(shape == ORC_TET, ref, m);
+  for (int i = 0; i < P; ++i) {
+    long double v = 0, d[3] = {0, 0, 0};
+    for (int j = 0; j < P; ++j) {
+      long double c = t->C[j * P + i];
+      v += c * m[j].v;
+      for (int k = 0; k < t->dim; ++k) d[k] += c * m[j].d[k];
+    }
+    if (phi) phi[i] = (double)v;
+    if (dphi) for (int k = 0; k < t->dim; ++k) dphi[i * t->dim + k] = (double)d[k];
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* P1 geometry.                                                              */
 /* Quad vertex signs (QuadP1.h:98-108): v0(-,-) v1(+,-) v2(+,+) v3(-,+).     */
 static const double QS[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
@@ -155,8 +434,26 @@ static const double QS[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
 static const double HS[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1},
                                 {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
 
+/* TriP1::interpolateAtPoint TriP1.cpp:156-171 (reference triangle
+ * (-1,-1) (1,-1) (-1,1)); TetP1::interpolateAtPoint TetP1.cpp:56-71
+ * (v0 -> (0,0,0), v1 -> (0,1,0), v2 -> (1,0,0), v3 -> (0,0,1)). */
+static int shape_dim(int shape) { return shape == ORC_QUAD || shape == ORC_TRI ? 2 : 3; }
+static int shape_nv(int shape) {
+  return shape == ORC_QUAD ? 4 : shape == ORC_HEX ? 8 : shape == ORC_TRI ? 3 : 4;
+}
+static int is_simplex(int shape) { return shape == ORC_TRI || shape == ORC_TET; }
+
 int orc_p1_interpolate(int shape, const double *ref, double *w) {
-  if (shape == ORC_QUAD) {
+  if (shape == ORC_TRI) {
+    w[0] = -ref[0] / 2.0 - ref[1] / 2.0;
+    w[1] = ref[0] / 2.0 + 1.0 / 2.0;
+    w[2] = ref[1] / 2.0 + 1.0 / 2.0;
+  } else if (shape == ORC_TET) {
+    w[0] = -ref[0] - ref[1] - ref[2] + 1;
+    w[1] = ref[1];
+    w[2] = ref[0];
+    w[3] = ref[2];
+  } else if (shape == ORC_QUAD) {
     for (int k = 0; k < 4; ++k)
       w[k] = 0.25 * (1 + QS[k][0] * ref[0]) * (1 + QS[k][1] * ref[1]);
   } else {
@@ -202,6 +499,24 @@ static int inv3(const double J[9], double *det, double *inv) {
  * HexP1.cpp:189-240. */
 int orc_p1_jacobian(int shape, const double *vtx, const double *ref, unsigned flags,
                     double *detJ, double *invJ) {
+  if (shape == ORC_TRI) {
+    /* TriP1::inverseJacobian TriP1.cpp:117-154: rows d/dr = (v1 - v0)/2,
+     * d/ds = (v2 - v0)/2 */
+    double J[4] = {(vtx[2] - vtx[0]) / 2, (vtx[3] - vtx[1]) / 2,
+                   (vtx[4] - vtx[0]) / 2, (vtx[5] - vtx[1]) / 2};
+    return inv2(J, detJ, invJ);
+  }
+  if (shape == ORC_TET) {
+    /* TetP1::inverseJacobian TetP1.cpp:150-205: rows d/dr = v2 - v0,
+     * d/ds = v1 - v0, d/dt = v3 - v0 */
+    double J[9];
+    for (int m = 0; m < 3; ++m) {
+      J[0 + m] = vtx[6 + m] - vtx[m];
+      J[3 + m] = vtx[3 + m] - vtx[m];
+      J[6 + m] = vtx[9 + m] - vtx[m];
+    }
+    return inv3(J, detJ, invJ);
+  }
   if (shape == ORC_QUAD) {
     double J[4] = {0, 0, 0, 0};
     double r = ref[0], s = ref[1];
@@ -241,7 +556,7 @@ int orc_p1_jacobian(int shape, const double *vtx, const double *ref, unsigned fl
 static void p1_map(int shape, const double *vtx, const double *ref, double *x) {
   double w[8];
   orc_p1_interpolate(shape, ref, w);
-  int nv = shape == ORC_QUAD ? 4 : 8, d = shape == ORC_QUAD ? 2 : 3;
+  int nv = shape_nv(shape), d = shape_dim(shape);
   for (int m = 0; m < d; ++m) {
     double s = 0;
     for (int k = 0; k < nv; ++k) s += w[k] * vtx[d * k + m];
@@ -254,6 +569,19 @@ int orc_check_hull(int shape, const double *vtx, const double *x) {
   double det, ref0[3] = {0, 0, 0};
   orc_p1_jacobian(shape, vtx, ref0, 0, &det, NULL);
   if (det <= 0) { set_err("poorly behaved element (detJ <= 0)"); return -1; }
+  if (is_simplex(shape)) {
+    /* Barycentric test of TriP1::checkHull TriP1.cpp:7-37 /
+     * TetP1::checkHull TetP1.cpp:6-49, corrected: the reference's final
+     * "fabs(1-(l1+l2+l3)) < 1e-8" rejection is identically true for
+     * triangles (l3 = 1-l1-l2) and rejects every point of the face opposite
+     * the last vertex for tetrahedra; here all barycentrics >= -1e-12. */
+    double ref[3], w[4];
+    if (orc_inverse_map(shape, vtx, x, ref)) return -1;
+    orc_p1_interpolate(shape, ref, w);
+    for (int k = 0; k < shape_nv(shape); ++k)
+      if (w[k] < -1e-12) return 0;
+    return 1;
+  }
   if (shape == ORC_QUAD) {
     int nneg = 0, npos = 0;
     static const int em[5] = {0, 1, 2, 3, 0};
@@ -288,7 +616,9 @@ int orc_check_hull(int shape, const double *vtx, const double *x) {
  * QuadP1::inverseCoordinateTransform QuadP1.cpp:41-92,
  * HexP1::inverseCoordinateTransform HexP1.cpp:135-187. */
 int orc_inverse_map(int shape, const double *vtx, const double *x, double *ref) {
-  const int d = shape == ORC_QUAD ? 2 : 3;
+  /* affine simplices (TriP1.cpp:39-59, TetP1.cpp:73-102 closed forms) need
+   * a single Newton step from the origin */
+  const int d = shape_dim(shape);
   double sol[3] = {0, 0, 0};
   for (int it = 0;; ++it) {
     double X[3], det, inv[9];
@@ -316,26 +646,41 @@ int orc_inverse_map(int shape, const double *vtx, const double *x, double *ref) 
 typedef struct {
   int shape, dim, n, P, nv;
   double xi[ORC_MAX_N], w[ORC_MAX_N], D[ORC_MAX_N * ORC_MAX_N];
+  const stab_t *sx; /* simplex tables (NULL for tensor elements) */
 } basis_t;
 
 static int basis_init(basis_t *b, int shape, int order) {
   b->shape = shape;
-  b->dim = shape == ORC_QUAD ? 2 : 3;
+  b->dim = shape_dim(shape);
+  b->nv = shape_nv(shape);
   b->n = order + 1;
+  b->sx = NULL;
+  if (is_simplex(shape)) {
+    /* P3 only (Triangle.cpp:25-37, Tetrahedra.cpp:67-84) */
+    if (order != 3) { set_err("simplices are built for order 3 only (got %d)", order); return -1; }
+    b->sx = stab_for(shape);
+    if (!b->sx) { set_err("simplex tables unavailable"); return -1; }
+    b->P = b->sx->P;
+    return 0;
+  }
   b->P = b->dim == 2 ? b->n * b->n : b->n * b->n * b->n;
-  b->nv = shape == ORC_QUAD ? 4 : 8;
   if (b->P > ORC_MAX_P) { set_err("order %d unsupported for this shape", order); return -1; }
   if (orc_gll(order, b->xi, b->w)) return -1;
   return orc_deriv_matrix(order, b->D);
 }
 
 static inline void point_ref(const basis_t *b, int p, double *ref) {
+  if (b->sx) {
+    ref[0] = b->sx->x[p][0]; ref[1] = b->sx->x[p][1]; ref[2] = b->sx->x[p][2];
+    return;
+  }
   int n = b->n;
   ref[0] = b->xi[p % n];
   ref[1] = b->xi[(p / n) % n];
   ref[2] = b->dim == 3 ? b->xi[p / (n * n)] : 0.0;
 }
 static inline double point_w(const basis_t *b, int p) {
+  if (b->sx) return b->sx->w[p];
   int n = b->n;
   double w = b->w[p % n] * b->w[(p / n) % n];
   if (b->dim == 3) w *= b->w[p / (n * n)];
@@ -346,6 +691,19 @@ static inline double point_w(const basis_t *b, int p) {
  * Hexahedra.cpp:611-616. */
 static void ref_gradient(const basis_t *b, const double *u, double *gr /* [P][dim] */) {
   const int n = b->n, d = b->dim;
+  if (b->sx) {
+    /* reference gradient at node q: sum_j dphi_j/dxi_k (x_q) u_j
+     * (Triangle::computeGradient Triangle.cpp:417-439; the tetrahedron's
+     * mGradientPhi_dx of Tetrahedra.cpp:372-383 folds J^-1 into the same sum) */
+    const int P = b->P;
+    for (int q = 0; q < P; ++q)
+      for (int k = 0; k < d; ++k) {
+        double s = 0;
+        for (int j = 0; j < P; ++j) s += b->sx->D[k][j * P + q] * u[j];
+        gr[q * d + k] = s;
+      }
+    return;
+  }
   for (int p = 0; p < b->P; ++p) {
     int r = p % n, s = (p / n) % n, t = p / (n * n);
     double g0 = 0, g1 = 0, g2 = 0;
@@ -399,6 +757,22 @@ static void grad_test_from_geom(const basis_t *b, const double *detJ, const doub
       for (int a = 0; a < d; ++a) s += iJ[a * d + k] * f[p * d + a];
       F[p * d + k] = s * detJ[p];
     }
+  }
+  if (b->sx) {
+    /* out_i = sum_q w_q detJ sum_k dphi_i/dxi_k (x_q) F_k(q)
+     * (Tetrahedra::applyGradTestAndIntegrate Tetrahedra.cpp:248-275,
+     * Triangle::applyGradTestAndIntegrate Triangle.cpp:371-393) */
+    const int P = b->P;
+    for (int i = 0; i < P; ++i) {
+      double s = 0;
+      for (int q = 0; q < P; ++q) {
+        double t = 0;
+        for (int k = 0; k < d; ++k) t += F[q * d + k] * b->sx->D[k][i * P + q];
+        s += b->sx->w[q] * t;
+      }
+      out[i] = s;
+    }
+    return;
   }
   for (int p = 0; p < b->P; ++p) {
     int r = p % n, s = (p / n) % n, t = p / (n * n);
@@ -478,6 +852,10 @@ int orc_element_test(int shape, int order, const double *vtx, unsigned flags,
 }
 
 static void tensor_lagrange(const basis_t *b, const double *ref, double *l, double *dl /* [P][d] or NULL */) {
+  if (b->sx) {
+    orc_simplex_basis(b->shape, ref, l, dl);
+    return;
+  }
   double lr[ORC_MAX_N], ls[ORC_MAX_N], lt[ORC_MAX_N], dr[ORC_MAX_N], ds[ORC_MAX_N], dt[ORC_MAX_N];
   const int n = b->n;
   orc_lagrange(n - 1, ref[0], lr, dr);
@@ -555,6 +933,7 @@ struct orc_problem {
   /* cached per-point data (not used in faithful mode) */
   double *detJ, *invJ, *mat; /* mat: acoustic vp^2 [E][P]; elastic 9 c_ij [E][9][P] */
   double *mi;      /* [G] inverse diagonal mass */
+  double *Ke;      /* triangles: dense element stiffness [E][P][P] */
   double *u, *v, *a, *a_; /* [G][c] */
   int64_t step;
   /* colouring for threaded assembly */
@@ -713,6 +1092,16 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
     invJ = p->invJ + e * P * d * d;
     mat = p->mat + e * P * (p->d.physics == ORC_ACOUSTIC ? 1 : 9);
   }
+  if (b->shape == ORC_TRI) {
+    /* ScalarTri::computeStiffnessTerm ScalarTri.cpp:12-17: K_e u_e */
+    const double *K = p->Ke + e * P * P;
+    for (int i = 0; i < P; ++i) {
+      double s = 0;
+      for (int j = 0; j < P; ++j) s += K[i * P + j] * ue[j];
+      ke[i] = s;
+    }
+    return;
+  }
   if (p->d.physics == ORC_ACOUSTIC) {
     double g[ORC_MAX_P * 3];
     grad_from_geom(b, invJ, ue, g);
@@ -763,9 +1152,9 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
 }
 
 orc_problem *orc_create(const orc_desc *d) {
-  if (!d || (d->shape != ORC_QUAD && d->shape != ORC_HEX)) { set_err("bad shape"); return NULL; }
-  if (d->physics == ORC_ELASTIC3D && d->shape != ORC_HEX) {
-    set_err("elastic 3-D physics needs hexahedra (Elastic3D.cpp:137)");
+  if (!d || d->shape < ORC_QUAD || d->shape > ORC_TET) { set_err("bad shape"); return NULL; }
+  if (d->physics == ORC_ELASTIC3D && d->shape != ORC_HEX && d->shape != ORC_TET) {
+    set_err("elastic 3-D physics needs hexahedra or tetrahedra");
     return NULL;
   }
   orc_problem *p = (orc_problem *)xcalloc(1, sizeof(orc_problem));
@@ -793,7 +1182,9 @@ orc_problem *orc_create(const orc_desc *d) {
     if (!(det > 0)) { set_err("element %lld has detJ <= 0", (long long)e); orc_destroy(p); return NULL; }
   }
   if (number_nodes(p)) { orc_destroy(p); return NULL; }
-  colour_elements(p);
+  /* simplices: vertex valences exceed the 64-colour mask; their threaded
+   * assembly buffers element results and scatters them in element order */
+  if (!is_simplex(d->shape)) colour_elements(p);
   const int nm = d->physics == ORC_ACOUSTIC ? 1 : 9;
   const int faithful = (d->flags & ORC_FAITHFUL_RECOMPUTE) != 0;
   if (!faithful) {
@@ -805,6 +1196,33 @@ orc_problem *orc_create(const orc_desc *d) {
   if (!faithful || d->physics == ORC_ELASTIC3D) {
     p->mat = (double *)xcalloc((size_t)(p->E * P * nm), sizeof(double));
     for (int64_t e = 0; e < p->E; ++e) element_material(p, e, p->mat + e * P * nm, NULL);
+  }
+  if (d->shape == ORC_TRI) {
+    /* Triangle::buildStiffnessMatrix Triangle.cpp:194-241:
+     * K_ij = detJ sum_q w_q vp_q^2 (dphi_i/dx dphi_j/dx + dphi_i/dz dphi_j/dz) */
+    p->Ke = (double *)xcalloc((size_t)(p->E * P * P), sizeof(double));
+    double dx[12 * 12], dz[12 * 12];
+    for (int64_t e = 0; e < p->E; ++e) {
+      double det, iJ[4], ref0[3] = {0, 0, 0}, vp2[12];
+      orc_p1_jacobian(ORC_TRI, p->vtx + e * nv * dim, ref0, 0, &det, iJ);
+      element_material(p, e, vp2, NULL);
+      for (int i = 0; i < P; ++i)
+        for (int q = 0; q < P; ++q) {
+          const double dr = b->sx->D[0][i * P + q], ds = b->sx->D[1][i * P + q];
+          dx[i * P + q] = dr * iJ[0] + ds * iJ[1];
+          dz[i * P + q] = dr * iJ[2] + ds * iJ[3];
+        }
+      double *K = p->Ke + e * P * P;
+      for (int i = 0; i < P; ++i)
+        for (int j = 0; j < P; ++j) {
+          double sx = 0, sz = 0;
+          for (int q = 0; q < P; ++q) {
+            sx += b->sx->w[q] * (vp2[q] * dx[i * P + q] * dx[j * P + q]);
+            sz += b->sx->w[q] * (vp2[q] * dz[i * P + q] * dz[j * P + q]);
+          }
+          K[i * P + j] = det * sx + det * sz;
+        }
+    }
   }
   /* Diagonal mass: Scalar.cpp:34-39 (no rho), Elastic3D.cpp:63-67 (rho);
    * summed in element order then reciprocal (Order2Newmark.cpp:32-66). */
@@ -827,7 +1245,7 @@ orc_problem *orc_create(const orc_desc *d) {
 void orc_destroy(orc_problem *p) {
   if (!p) return;
   free(p->vtx); free(p->par); free(p->conn); free(p->xyz);
-  free(p->detJ); free(p->invJ); free(p->mat); free(p->mi);
+  free(p->detJ); free(p->invJ); free(p->mat); free(p->mi); free(p->Ke);
   free(p->u); free(p->v); free(p->a); free(p->a_);
   free(p->col_off); free(p->col_elems);
   for (int i = 0; i < p->nsrc; ++i) free(p->src[i].wts);
@@ -953,6 +1371,22 @@ static void assemble(orc_problem *p, const double *u, double t, double *a, int w
       for (int q = 0; q < P; ++q)
         for (int k = 0; k < c; ++k) a[cn[q] * c + k] += -ke[q * c + k];
     }
+  } else if (p->ncolours == 0) {
+    double *buf = (double *)xcalloc((size_t)(p->E * P * c), sizeof(double));
+#pragma omp parallel for num_threads(p->d.threads) schedule(static)
+    for (int64_t e = 0; e < p->E; ++e) {
+      double ue[ORC_MAX_P * 3];
+      const int64_t *cn = p->conn + e * P;
+      for (int q = 0; q < P; ++q)
+        for (int k = 0; k < c; ++k) ue[q * c + k] = u[cn[q] * c + k];
+      element_stiffness(p, e, ue, buf + e * P * c);
+    }
+    for (int64_t e = 0; e < p->E; ++e) {
+      const int64_t *cn = p->conn + e * P;
+      for (int q = 0; q < P; ++q)
+        for (int k = 0; k < c; ++k) a[cn[q] * c + k] += -buf[(e * P + q) * c + k];
+    }
+    free(buf);
   } else {
     for (int col = 0; col < p->ncolours; ++col) {
       const int64_t lo = p->col_off[col], hi = p->col_off[col + 1];

@@ -18,7 +18,9 @@
 extern "C" {
 #endif
 
-enum { ORC_QUAD = 0, ORC_HEX = 1 };
+/* ORC_TRI / ORC_TET: the P3 mass-lumped simplices (12-node triangle,
+ * 50-node tetrahedron) of Triangle.cpp / Tetrahedra.cpp, order 3 only. */
+enum { ORC_QUAD = 0, ORC_HEX = 1, ORC_TRI = 2, ORC_TET = 3 };
 enum { ORC_ACOUSTIC = 0, ORC_ELASTIC3D = 1 };
 
 /* Reference quirk switches ("reference-literal" mode).  The default (0) is the
@@ -47,7 +49,9 @@ typedef struct {
   int64_t n_vertices;
   const double *vertices;   /* [n_vertices][dim] */
   int64_t n_elements;
-  const int64_t *cells;     /* [n_elements][4 | 8], PETSc right-hand order */
+  const int64_t *cells;     /* [n_elements][4 | 8 | 3 | 4]: PETSc right-hand
+                               order for quads / hexes, TriP1 / TetP1 vertex
+                               order (positively oriented) for simplices */
   /* Per element, per element-vertex material (ExodusModel NAME_0..NAME_k
    * convention, ExodusModel.cpp:455-470):
    *   acoustic: [1][n_elements][nv] = VP
@@ -66,6 +70,15 @@ int orc_gll(int order, double *points, double *weights);
 int orc_deriv_matrix(int order, double *D /* [n][n], D[i*n+j] = l_j'(xi_i) */);
 int orc_lagrange(int order, double xi, double *l /* [n] */, double *dl /* [n] or NULL */);
 double orc_ricker(double t, double f0, double t0, double amp);
+
+/* ---- P3 simplex tables (restatement of the sympy generators
+ * src/py/pysalvus/code_generation/triangle_points_weights_polys.py and
+ * tetrahedra_points_weights_polys.py + BuildNodesTetrahedraP3.py):
+ * nodes [P][3] (unused coordinates 0), weights [P],
+ * D[k][i][q] = d phi_i / d xi_k at node q (k < dim). ---- */
+int orc_simplex_tables(int shape, double *nodes, double *weights, double *D);
+/* phi_i(ref) [P] and d phi_i / d xi_k (ref) as dphi[i][k] (NULL to skip). */
+int orc_simplex_basis(int shape, const double *ref, double *phi, double *dphi);
 
 /* ---- element level (single element, no mesh) ---- */
 int orc_p1_jacobian(int shape, const double *vtx, const double *ref, unsigned flags,

@@ -11,7 +11,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
-QUAD, HEX = 0, 1
+QUAD, HEX, TRI, TET = 0, 1, 2, 3
 ACOUSTIC, ELASTIC3D = 0, 1
 Q1_Z_NOT_ADVANCED = 1 << 0
 Q2_ELASTIC_SRC_UNSCALED = 1 << 1
@@ -74,8 +74,22 @@ def lib():
                      "orc_element_delta"):
             getattr(L, name).argtypes = [ctypes.c_int, ctypes.c_int, _DP, ctypes.c_uint, _DP, _DP]
         L.orc_element_par.argtypes = [ctypes.c_int, ctypes.c_int, _DP, _DP]
+        L.orc_simplex_tables.argtypes = [ctypes.c_int, _DP, _DP, _DP]
+        L.orc_simplex_basis.argtypes = [ctypes.c_int, _DP, _DP, _DP]
         _LIB = L
     return _LIB
+
+
+def _dim(shape):
+    return 2 if shape in (QUAD, TRI) else 3
+
+
+def _npts(shape, order):
+    if shape == TRI:
+        return 12
+    if shape == TET:
+        return 50
+    return (order + 1) ** _dim(shape)
 
 
 def _p(a):
@@ -111,6 +125,23 @@ def ricker(t, f0, t0, amp):
     return lib().orc_ricker(float(t), float(f0), float(t0), float(amp))
 
 
+def simplex_tables(shape):
+    """(nodes [P][dim], weights [P], D [dim][P][P]) with D[k][i][q] = dphi_i/dxi_k (x_q)."""
+    P, d = _npts(shape, 3), _dim(shape)
+    x, w, D = np.zeros((P, 3)), np.zeros(P), np.zeros((d, P, P))
+    assert lib().orc_simplex_tables(shape, _p(x), _p(w), _p(D)) == 0
+    return x[:, :d], w, D
+
+
+def simplex_basis(shape, ref):
+    P, d = _npts(shape, 3), _dim(shape)
+    r = np.zeros(3)
+    r[:d] = ref
+    phi, dphi = np.zeros(P), np.zeros((P, d))
+    assert lib().orc_simplex_basis(shape, _p(r), _p(phi), _p(dphi)) == 0
+    return phi, dphi
+
+
 def _elem(fn, shape, order, vtx, flags, inp, out_shape):
     vtx, inp = _c(vtx), _c(inp)
     out = np.zeros(out_shape)
@@ -121,31 +152,25 @@ def _elem(fn, shape, order, vtx, flags, inp, out_shape):
 
 
 def element_gradient(shape, order, vtx, u, flags=0):
-    d = 2 if shape == QUAD else 3
-    P = (order + 1) ** d
-    return _elem("orc_element_gradient", shape, order, vtx, flags, u, (P, d))
+    return _elem("orc_element_gradient", shape, order, vtx, flags, u,
+                 (_npts(shape, order), _dim(shape)))
 
 
 def element_grad_test(shape, order, vtx, f, flags=0):
-    d = 2 if shape == QUAD else 3
-    P = (order + 1) ** d
-    return _elem("orc_element_grad_test", shape, order, vtx, flags, f, (P,))
+    return _elem("orc_element_grad_test", shape, order, vtx, flags, f, (_npts(shape, order),))
 
 
 def element_test(shape, order, vtx, f, flags=0):
-    d = 2 if shape == QUAD else 3
-    return _elem("orc_element_test", shape, order, vtx, flags, f, ((order + 1) ** d,))
+    return _elem("orc_element_test", shape, order, vtx, flags, f, (_npts(shape, order),))
 
 
 def element_delta(shape, order, vtx, ref, flags=0):
-    d = 2 if shape == QUAD else 3
-    return _elem("orc_element_delta", shape, order, vtx, flags, ref, ((order + 1) ** d,))
+    return _elem("orc_element_delta", shape, order, vtx, flags, ref, (_npts(shape, order),))
 
 
 def element_par(shape, order, par_vtx):
-    d = 2 if shape == QUAD else 3
     par_vtx = _c(par_vtx)
-    out = np.zeros((order + 1) ** d)
+    out = np.zeros(_npts(shape, order))
     assert lib().orc_element_par(shape, order, _p(par_vtx), _p(out)) == 0
     return out
 
@@ -161,11 +186,11 @@ def inverse_map(shape, vtx, x):
     rc = lib().orc_inverse_map(shape, _p(vtx), _p(x), _p(ref))
     if rc:
         raise RuntimeError(lib().orc_last_error().decode())
-    return ref[: (2 if shape == QUAD else 3)]
+    return ref[: _dim(shape)]
 
 
 def p1_jacobian(shape, vtx, ref, flags=0):
-    d = 2 if shape == QUAD else 3
+    d = _dim(shape)
     vtx, ref3 = _c(vtx), np.zeros(3)
     ref3[:d] = ref
     det, inv = np.zeros(1), np.zeros((d, d))
@@ -189,7 +214,7 @@ class Problem:
         self.h = lib().orc_create(ctypes.byref(d))
         if not self.h:
             raise RuntimeError(lib().orc_last_error().decode())
-        self.dim = 2 if shape == QUAD else 3
+        self.dim = _dim(shape)
         self.G = lib().orc_num_nodes(self.h)
         self.c = lib().orc_num_components(self.h)
         self.nrec = 0

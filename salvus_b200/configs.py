@@ -7,7 +7,7 @@ that tests can run the same physics at reduced size.
 import numpy as np
 
 from . import meshgen
-from .core import ACOUSTIC, ELASTIC3D, HEX, QUAD
+from .core import ACOUSTIC, ELASTIC3D, HEX, QUAD, TET, TRI
 
 
 def standing_wave_2d(nel=40, order=4, L=1.0e4, vp=4000.0):
@@ -122,6 +122,51 @@ def serving_stream(n_jobs, seed=4, quad_edges=(50, 400), hex_edges=(16, 48), ste
         out.append((kind, int(rng.integers(lo, hi + 1)), int(seed * 100003 + k),
                     int(rng.integers(steps[0], steps[1] + 1)), t))
     return out
+
+
+def simplex_tri(nx=448, ny=224, lx=2.0e4, ly=1.0e4, vp=4000.0, std=0.05, corr=1000.0, f0=1.0,
+                n_receivers=16, seed=3):
+    """2-D acoustic P3 triangles: seeded Delaunay mesh of a jittered
+    (nx+1) x (ny+1) point lattice over lx x ly (about 2 nx ny triangles),
+    vp homogeneous times (1 + std GRF), Ricker f0 at the centre, a seeded
+    receiver ring of radius 0.3 ly."""
+    V, C = meshgen.delaunay_tri(nx, ny, lx, ly, seed=seed)
+    h = lx / nx
+    grf = meshgen.gaussian_random_field((ny + 1, nx + 1), h, corr, seed).ravel()
+    vpv = vp * (1.0 + std * grf)
+    par = meshgen.per_element_vertex(vpv, C)[None]
+    center = (lx / 2 + 0.31 * h, ly / 2 - 0.17 * h)
+    return dict(shape=TRI, order=3, physics=ACOUSTIC, vertices=V, cells=C, params=par, L=lx,
+                sources=[dict(location=center, center_freq=f0, time_delay=1.2 / f0, amplitude=1.0,
+                              direction=[1.0])],
+                receivers=meshgen.ring_positions(center, 0.3 * ly, n_receivers, seed))
+
+
+def simplex_tet(n=55, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
+                corr=1000.0, f0=1.0, n_receivers=64, seed=3):
+    """3-D P3 tetrahedra: jittered n^3 lattice over an L cube, 6 tetrahedra
+    per cell (6 n^3 elements; n = 55 gives about 1M), material homogeneous
+    times (1 + std GRF); elastic: seeded moment-tensor Ricker source, acoustic:
+    pressure source; receivers at seeded positions on the top surface."""
+    V, C = meshgen.kuhn_tet(n, n, n, L, L, L, seed=seed)
+    h = L / n
+    grf = meshgen.gaussian_random_field((n + 1,) * 3, h, corr, seed).ravel()
+    pert = 1.0 + std * grf
+    rng = np.random.default_rng(seed)
+    rec_xy = rng.uniform(0.02 * L, 0.98 * L, size=(n_receivers, 2))
+    receivers = np.concatenate([rec_xy, np.full((n_receivers, 1), L)], axis=1)
+    loc = (L / 2 + 0.37 * h, L / 2 - 0.21 * h, L / 2 + 0.13 * h)
+    if physics == ACOUSTIC:
+        par = meshgen.per_element_vertex(vp * pert, C)[None]
+        src = dict(location=loc, center_freq=f0, time_delay=1.2 / f0, amplitude=1.0, direction=[1.0])
+    else:
+        par = np.stack([meshgen.per_element_vertex(rho * pert, C),
+                        meshgen.per_element_vertex(vp * pert, C),
+                        meshgen.per_element_vertex(vs * pert, C)])
+        src = dict(location=loc, center_freq=f0, time_delay=1.2 / f0, amplitude=1.0e13,
+                   moment_tensor=rng.standard_normal(6))
+    return dict(shape=TET, order=3, physics=physics, vertices=V, cells=C, params=par, L=L,
+                sources=[src], receivers=receivers)
 
 
 def oracle_params(cfg):

@@ -56,6 +56,7 @@ class SourceDesc(ctypes.Structure):
 SIGNATURES = [
     ("salvus_last_error", ctypes.c_char_p, []),
     ("salvus_version", ctypes.c_char_p, []),
+    ("salvus_element_tables", ctypes.c_int, [_I32, _I32, ctypes.POINTER(_I32), _DP, _DP, _DP]),
     ("salvus_mesh_create", ctypes.c_int, [ctypes.POINTER(MeshDesc), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("salvus_mesh_destroy", ctypes.c_int, [_VP]),
     ("salvus_mesh_info", ctypes.c_int, [_VP, ctypes.POINTER(_I64), ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
@@ -117,6 +118,18 @@ def _dp(a):
     return a.ctypes.data_as(_DP)
 
 
+def element_tables(shape, order):
+    """(points [P][dim], weights [P], dphi [dim][P][P]) of a reference element,
+    dphi[k][i][q] = d phi_i / d xi_k at point q (no GPU needed)."""
+    dim = 2 if shape in (QUAD, TRI) else 3
+    P = _I32()
+    _check(lib().salvus_element_tables(shape, order, ctypes.byref(P), None, None, None))
+    P = P.value
+    x, w, D = np.zeros((P, dim)), np.zeros(P), np.zeros((dim, P, P))
+    _check(lib().salvus_element_tables(shape, order, None, _dp(x), _dp(w), _dp(D)))
+    return x, w, D
+
+
 class Mesh:
     """Flattened mesh resident on one GPU (DMPlex mesh + Exodus model + the
     per-element precomputation of the reference, done once)."""
@@ -134,7 +147,7 @@ class Mesh:
         G, c, P = _I64(), _I32(), _I32()
         _check(lib().salvus_mesh_info(self.h, ctypes.byref(G), ctypes.byref(c), ctypes.byref(P)))
         self.n_nodes, self.n_components, self.points_per_element = G.value, c.value, P.value
-        self.dim = 2 if shape == QUAD else 3
+        self.dim = 2 if shape in (QUAD, TRI) else 3
         self.n_elements = self._c.shape[0]
 
     def close(self):

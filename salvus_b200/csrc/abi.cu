@@ -19,6 +19,7 @@
 #include "kernels_hex_tma.cuh"
 #include "kernels_hex_v2.cuh"
 #include "kernels_batch.cuh"
+#include "kernels_simplex.cuh"
 #include <algorithm>
 #include <cstdlib>
 #include <type_traits>
@@ -190,9 +191,45 @@ static int acoustic3(const salvus_mesh *m, const real *rec, const real *u, real 
   return launch_acoustic<3, N, real>(m, rec, u, r, s);
 }
 
+// P3 simplices on CUDA cores
+template <typename real>
+static const real *simplex_tables(const salvus_mesh *m) {
+  return sizeof(real) == 4 ? (const real *)m->d_sd32.ptr : (const real *)m->d_sd64.ptr;
+}
+
+template <typename real, int C>
+static int launch_tet(const salvus_mesh *m, const real *rec, const real *u, real *r,
+                      cudaStream_t st) {
+  using S = TetShape<real, C>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(tet_stiffness_kernel<real, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)S::SMEM);
+    attr = true;
+  }
+  tet_stiffness_kernel<real, C><<<blocks_for(m->E, S::EPB), S::THREADS, S::SMEM, st>>>(
+      m->E, rec, m->d_conn.as<int32_t>(), simplex_tables<real>(m), u, r);
+  g_launches++;
+  return check_launch("tetrahedron stiffness");
+}
+
+template <typename real>
+static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, real *r,
+                          cudaStream_t st) {
+  if (m->shape == SALVUS_TRI) {
+    tri_acoustic_kernel<real><<<blocks_for(m->E, 128), 128, 0, st>>>(
+        m->E, rec, m->d_conn.as<int32_t>(), simplex_tables<real>(m), u, r);
+    g_launches++;
+    return check_launch("triangle stiffness");
+  }
+  if (m->physics == SALVUS_ELASTIC3D) return launch_tet<real, 3>(m, rec, u, r, st);
+  return launch_tet<real, 1>(m, rec, u, r, st);
+}
+
 template <typename real>
 static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u, real *r,
                             cudaStream_t st, int *err = nullptr) {
+  if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st);
   if (m->physics == SALVUS_ELASTIC3D) {
     switch (m->order) {
       case 1: return launch_elastic<1, real>(m, rec, u, r, st, err);
@@ -230,8 +267,36 @@ static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u
 
 // ---------------------------------------------------------------------------
 // mesh setup
+template <typename real>
+static int build_simplex_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &sd,
+                                 DeviceBuffer &mass_local) {
+  const int rw = record_words(m->shape, m->physics, sizeof(real) == 8);
+  int rc = out.alloc(sizeof(real) * (size_t)m->E * rw);
+  if (rc) return rc;
+  SimplexTable tab{};
+  for (int q = 0; q < m->P; ++q) {
+    for (int a = 0; a < 3; ++a) tab.x[q][a] = m->basis.nodes[(size_t)q * 3 + a];
+    tab.w[q] = m->basis.sw[q];
+  }
+  simplex_geometry_kernel<real><<<blocks_for(m->E, 128), 128, 0, m->stream>>>(
+      m->E, m->shape, m->physics, m->P, rw, m->d_vtx.as<double>(), m->d_par.as<double>(), tab,
+      out.as<real>(), mass_local.as<double>());
+  g_launches++;
+  if ((rc = check_launch("simplex geometry"))) return rc;
+  std::vector<real> t(m->basis.SD.size());
+  for (size_t i = 0; i < t.size(); ++i) t[i] = (real)m->basis.SD[i];
+  if ((rc = sd.alloc(sizeof(real) * t.size()))) return rc;
+  SALVUS_CUDA(cudaMemcpyAsync(sd.ptr, t.data(), sizeof(real) * t.size(), cudaMemcpyHostToDevice,
+                              m->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(m->stream));
+  return SALVUS_OK;
+}
+
 template <typename real, bool kPack>
 static int build_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &mass_local) {
+  if (is_simplex(m->shape))
+    return build_simplex_records<real>(m, out, sizeof(real) == 4 ? m->d_sd32 : m->d_sd64,
+                                       mass_local);
   const int rw = record_words(m->shape, m->physics, sizeof(real) == 8);
   int rc = out.alloc(sizeof(real) * (size_t)(m->E * m->P) * rw);
   if (rc) return rc;
@@ -729,13 +794,41 @@ const char *salvus_version(void) {
 
 int64_t salvus_launch_count(void) { return g_launches.load(); }
 
+int salvus_element_tables(int32_t shape, int32_t order, int32_t *n_points, double *points,
+                          double *weights, double *dphi) {
+  Basis b;
+  int rc = make_basis(shape, order, &b);
+  if (rc) return rc;
+  const int P = b.P, dim = b.dim;
+  if (n_points) *n_points = P;
+  std::vector<double> phi(P), dp((size_t)P * 3);
+  for (int q = 0; q < P; ++q) {
+    double ref[3];
+    point_ref(b, q, ref);
+    if (points)
+      for (int a = 0; a < dim; ++a) points[(size_t)q * dim + a] = ref[a];
+    if (weights) weights[q] = point_weight(b, q);
+    if (dphi) {
+      if (b.simplex) {
+        for (int k = 0; k < dim; ++k)
+          for (int i = 0; i < P; ++i) dphi[((size_t)k * P + i) * P + q] = b.SD[((size_t)k * P + i) * P + q];
+      } else {
+        basis_at(b, ref, phi.data(), dp.data());
+        for (int k = 0; k < dim; ++k)
+          for (int i = 0; i < P; ++i) dphi[((size_t)k * P + i) * P + q] = dp[(size_t)i * 3 + k];
+      }
+    }
+  }
+  return SALVUS_OK;
+}
+
 int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out) {
   if (!d || !out) return fail(SALVUS_E_INVALID, "null argument");
   *out = nullptr;
-  if (d->shape != SALVUS_QUAD && d->shape != SALVUS_HEX)
-    return fail(SALVUS_E_UNSUPPORTED, "shape %d not supported by the tensor path", d->shape);
-  if (d->physics == SALVUS_ELASTIC3D && d->shape != SALVUS_HEX)
-    return fail(SALVUS_E_UNSUPPORTED, "elastic 3-D physics needs hexahedra (Elastic3D.cpp:137)");
+  if (d->shape < SALVUS_QUAD || d->shape > SALVUS_TET)
+    return fail(SALVUS_E_UNSUPPORTED, "unknown element shape %d", d->shape);
+  if (d->physics == SALVUS_ELASTIC3D && d->shape != SALVUS_HEX && d->shape != SALVUS_TET)
+    return fail(SALVUS_E_UNSUPPORTED, "elastic 3-D physics needs hexahedra or tetrahedra");
   if (d->physics != SALVUS_ACOUSTIC && d->physics != SALVUS_ELASTIC3D)
     return fail(SALVUS_E_INVALID, "unknown physics %d", d->physics);
   if (d->n_elements <= 0 || d->n_vertices <= 0 || !d->vertices || !d->cells || !d->params)
@@ -766,13 +859,16 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
         m->vtx[(size_t)((e * m->nv + k) * m->dim + a)] = d->vertices[vi * m->dim + a];
     }
   for (int64_t e = 0; e < m->E; ++e) {
-    // right-hand rule check (QuadP1::checkHull / HexP1::checkHull)
+    // right-hand rule check (QuadP1::checkHull / HexP1::checkHull): detJ > 0
+    // at every corner (simplices: the constant detJ)
     const double *v = m->vtx.data() + e * m->nv * m->dim;
-    for (int q = 0; q < (m->dim == 2 ? 4 : 8); ++q) {
-      double ref[3];
-      for (int a = 0; a < m->dim; ++a) ref[a] = (m->dim == 2 ? (q >> a) & 1 : (q >> a) & 1) ? 1.0 : -1.0;
+    const int ncheck = is_simplex(m->shape) ? 1 : (m->dim == 2 ? 4 : 8);
+    for (int q = 0; q < ncheck; ++q) {
+      double ref[3] = {0, 0, 0};
+      if (!is_simplex(m->shape))
+        for (int a = 0; a < m->dim; ++a) ref[a] = ((q >> a) & 1) ? 1.0 : -1.0;
       double det;
-      p1_jacobian(m->dim, v, ref, &det, nullptr);
+      p1_jacobian(m->shape, v, ref, &det, nullptr);
       if (!(det > 0))
         return fail(SALVUS_E_INVALID, "element %lld is inverted or degenerate (detJ <= 0)",
                     (long long)e);
@@ -991,27 +1087,23 @@ int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
   src.desc = *s;
   int rc = locate_point(m, s->location, &src.elem, src.ref);
   if (rc) return rc;
-  const int n = m->n, P = m->P, c = p->c;
-  std::vector<double> lr(n), ls(n), lt(n, 1.0), dr(n), ds(n), dt(n, 0.0);
-  lagrange_1d(m->basis, src.ref[0], lr.data(), dr.data());
-  lagrange_1d(m->basis, src.ref[1], ls.data(), ds.data());
-  if (m->dim == 3) lagrange_1d(m->basis, src.ref[2], lt.data(), dt.data());
+  const int P = m->P, c = p->c;
+  // delta-function coefficients phi_q(x_s) / (w_q detJ_q), times w_q detJ_q
+  // by applyTestAndIntegrate (Scalar.cpp:87): phi_q(x_s) per unit force
+  std::vector<double> phi(P), dphi((size_t)P * 3);
+  basis_at(m->basis, src.ref, phi.data(), dphi.data());
   src.wts.assign((size_t)P * c, 0.0);
   if (s->kind == SALVUS_SOURCE_FORCE) {
-    for (int q = 0; q < P; ++q) {
-      const int i = q % n, j = (q / n) % n, k = q / (n * n);
-      const double l = lr[i] * ls[j] * (m->dim == 3 ? lt[k] : 1.0);
-      for (int a = 0; a < c; ++a) src.wts[(size_t)q * c + a] = l * s->comp[a];
-    }
+    for (int q = 0; q < P; ++q)
+      for (int a = 0; a < c; ++a) src.wts[(size_t)q * c + a] = phi[q] * s->comp[a];
   } else {
     double det, iJ[9];
-    p1_jacobian(3, m->vtx.data() + src.elem * 8 * 3, src.ref, &det, iJ);
+    p1_jacobian(m->shape, m->vtx.data() + src.elem * m->nv * 3, src.ref, &det, iJ);
     const double M[3][3] = {{s->comp[0], s->comp[5], s->comp[4]},
                             {s->comp[5], s->comp[1], s->comp[3]},
                             {s->comp[4], s->comp[3], s->comp[2]}};
     for (int q = 0; q < P; ++q) {
-      const int i = q % n, j = (q / n) % n, k = q / (n * n);
-      const double gref[3] = {dr[i] * ls[j] * lt[k], lr[i] * ds[j] * lt[k], lr[i] * ls[j] * dt[k]};
+      const double *gref = &dphi[(size_t)q * 3];
       double gx[3];
       for (int a = 0; a < 3; ++a) gx[a] = iJ[a * 3] * gref[0] + iJ[a * 3 + 1] * gref[1] + iJ[a * 3 + 2] * gref[2];
       for (int a = 0; a < 3; ++a)
@@ -1031,13 +1123,8 @@ int salvus_problem_add_receiver(salvus_problem *p, const double *xyz) {
   for (int a = 0; a < 3; ++a) r.xyz[a] = a < m->dim ? xyz[a] : 0.0;
   int rc = locate_point(m, r.xyz, &r.elem, r.ref);
   if (rc) return rc;
-  const int n = m->n;
-  std::vector<double> lr(n), ls(n), lt(n, 1.0);
-  lagrange_1d(m->basis, r.ref[0], lr.data(), nullptr);
-  lagrange_1d(m->basis, r.ref[1], ls.data(), nullptr);
-  if (m->dim == 3) lagrange_1d(m->basis, r.ref[2], lt.data(), nullptr);
   r.l.resize(m->P);
-  for (int q = 0; q < m->P; ++q) r.l[q] = lr[q % n] * ls[(q / n) % n] * (m->dim == 3 ? lt[q / (n * n)] : 1.0);
+  basis_at(m->basis, r.ref, r.l.data(), nullptr);
   p->recs.push_back(std::move(r));
   p->rec_dirty = true;
   drop_graph(p);

@@ -51,12 +51,16 @@ static void legendre3(int N, double x, double *p, double *dp, double *d2p) {
 // Legendre ODE.  Weights 2 / (N (N+1) P_N(x)^2).  D from the closed form
 // D_ij = P_N(x_i) / (P_N(x_j) (x_i - x_j)), D_00 = -N(N+1)/4, D_NN = -D_00.
 int make_basis(int shape, int order, Basis *b) {
+  if (is_simplex(shape)) return make_simplex_basis(shape, order, b);
+  if (shape != SALVUS_QUAD && shape != SALVUS_HEX)
+    return fail(SALVUS_E_UNSUPPORTED, "unknown element shape %d", shape);
   const int dim = (shape == SALVUS_QUAD) ? 2 : 3;
   const int maxo = dim == 2 ? kMaxQuadOrder : kMaxHexOrder;
   if (order < 1 || order > maxo)
     return fail(SALVUS_E_UNSUPPORTED, "polynomial order %d not supported for %s (1..%d)", order,
                 dim == 2 ? "quad" : "hex", maxo);
   const int N = order, n = N + 1;
+  b->shape = shape; b->simplex = false;
   b->order = N; b->n = n; b->dim = dim;
   b->P = dim == 2 ? n * n : n * n * n;
   b->nv = dim == 2 ? 4 : 8;
@@ -124,12 +128,77 @@ void lagrange_1d(const Basis &b, double x, double *l, double *dl) {
   }
 }
 
+void point_ref(const Basis &b, int p, double *ref) {
+  if (b.simplex) {
+    for (int a = 0; a < 3; ++a) ref[a] = b.nodes[(size_t)p * 3 + a];
+    return;
+  }
+  const int n = b.n;
+  ref[0] = b.xi[p % n];
+  ref[1] = b.xi[(p / n) % n];
+  ref[2] = b.dim == 3 ? b.xi[p / (n * n)] : 0.0;
+}
+
+double point_weight(const Basis &b, int p) {
+  if (b.simplex) return b.sw[p];
+  const int n = b.n;
+  double w = b.w[p % n] * b.w[(p / n) % n];
+  return b.dim == 3 ? w * b.w[p / (n * n)] : w;
+}
+
+void basis_at(const Basis &b, const double *ref, double *phi, double *dphi) {
+  if (b.simplex) {
+    simplex_basis_at(b, ref, phi, dphi);
+    return;
+  }
+  const int n = b.n, P = b.P;
+  std::vector<double> l(3 * n, 1.0), dl(3 * n, 0.0);
+  for (int a = 0; a < b.dim; ++a) lagrange_1d(b, ref[a], &l[a * n], &dl[a * n]);
+  for (int q = 0; q < P; ++q) {
+    const int i = q % n, j = (q / n) % n, k = b.dim == 3 ? q / (n * n) : 0;
+    const double lz = b.dim == 3 ? l[2 * n + k] : 1.0, dz = b.dim == 3 ? dl[2 * n + k] : 0.0;
+    phi[q] = l[i] * l[n + j] * lz;
+    if (dphi) {
+      dphi[q * 3 + 0] = dl[i] * l[n + j] * lz;
+      dphi[q * 3 + 1] = l[i] * dl[n + j] * lz;
+      dphi[q * 3 + 2] = l[i] * l[n + j] * dz;
+    }
+  }
+}
+
 static const double kQuadSign[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
 static const double kHexSign[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1},
                                       {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
 
+static void inverse3(const double *J, double *detJ, double *invJ);
+
 // J[i][k] = dx_k / dxi_i; gradient = invJ * reference gradient.
-void p1_jacobian(int dim, const double *vtx, const double *ref, double *detJ, double *invJ) {
+void p1_jacobian(int shape, const double *vtx, const double *ref, double *detJ, double *invJ) {
+  const int dim = shape_dim(shape);
+  if (shape == SALVUS_TRI) {
+    // reference triangle (-1,-1) (1,-1) (-1,1): rows (v1 - v0)/2, (v2 - v0)/2
+    const double J[4] = {0.5 * (vtx[2] - vtx[0]), 0.5 * (vtx[3] - vtx[1]),
+                         0.5 * (vtx[4] - vtx[0]), 0.5 * (vtx[5] - vtx[1])};
+    const double d = J[0] * J[3] - J[1] * J[2];
+    *detJ = d;
+    if (invJ) {
+      invJ[0] = J[3] / d; invJ[1] = -J[1] / d;
+      invJ[2] = -J[2] / d; invJ[3] = J[0] / d;
+    }
+    return;
+  }
+  if (shape == SALVUS_TET) {
+    // reference tetrahedron v0 (0,0,0) v1 (0,1,0) v2 (1,0,0) v3 (0,0,1):
+    // rows d/dr = v2 - v0, d/ds = v1 - v0, d/dt = v3 - v0
+    double J[9];
+    for (int m = 0; m < 3; ++m) {
+      J[m] = vtx[6 + m] - vtx[m];
+      J[3 + m] = vtx[3 + m] - vtx[m];
+      J[6 + m] = vtx[9 + m] - vtx[m];
+    }
+    inverse3(J, detJ, invJ);
+    return;
+  }
   if (dim == 2) {
     double J[4] = {0, 0, 0, 0};
     for (int k = 0; k < 4; ++k) {
@@ -159,6 +228,10 @@ void p1_jacobian(int dim, const double *vtx, const double *ref, double *detJ, do
       J[6 + m] += d2 * vtx[3 * k + m];
     }
   }
+  inverse3(J, detJ, invJ);
+}
+
+static void inverse3(const double *J, double *detJ, double *invJ) {
   double m00 = J[4] * J[8] - J[5] * J[7], m01 = J[5] * J[6] - J[3] * J[8],
          m02 = J[3] * J[7] - J[4] * J[6];
   double d = J[0] * m00 + J[1] * m01 + J[2] * m02;
@@ -177,24 +250,66 @@ void p1_jacobian(int dim, const double *vtx, const double *ref, double *detJ, do
   }
 }
 
-void p1_map(int dim, const double *vtx, const double *ref, double *x) {
-  const int nv = dim == 2 ? 4 : 8;
-  for (int m = 0; m < dim; ++m) x[m] = 0.0;
-  for (int k = 0; k < nv; ++k) {
-    double wk = dim == 2 ? 0.25 * (1 + kQuadSign[k][0] * ref[0]) * (1 + kQuadSign[k][1] * ref[1])
-                         : 0.125 * (1 + kHexSign[k][0] * ref[0]) * (1 + kHexSign[k][1] * ref[1]) *
-                               (1 + kHexSign[k][2] * ref[2]);
-    for (int m = 0; m < dim; ++m) x[m] += wk * vtx[dim * k + m];
+// Vertex weights of the P1 map: QuadP1.h:98-108, HexP1.cpp:242-298,
+// TriP1::interpolateAtPoint TriP1.cpp:156-171 ([-r/2-s/2, r/2+1/2, s/2+1/2]),
+// TetP1::interpolateAtPoint TetP1.cpp:56-71 ([1-r-s-t, s, r, t]).
+void p1_weights(int shape, const double *ref, double *w) {
+  switch (shape) {
+    case SALVUS_QUAD:
+      for (int k = 0; k < 4; ++k)
+        w[k] = 0.25 * (1 + kQuadSign[k][0] * ref[0]) * (1 + kQuadSign[k][1] * ref[1]);
+      break;
+    case SALVUS_HEX:
+      for (int k = 0; k < 8; ++k)
+        w[k] = 0.125 * (1 + kHexSign[k][0] * ref[0]) * (1 + kHexSign[k][1] * ref[1]) *
+               (1 + kHexSign[k][2] * ref[2]);
+      break;
+    case SALVUS_TRI:
+      w[0] = -0.5 * (ref[0] + ref[1]);
+      w[1] = 0.5 * (ref[0] + 1.0);
+      w[2] = 0.5 * (ref[1] + 1.0);
+      break;
+    default:
+      w[0] = 1.0 - ref[0] - ref[1] - ref[2];
+      w[1] = ref[1];
+      w[2] = ref[0];
+      w[3] = ref[2];
+      break;
   }
+}
+
+void p1_map(int shape, const double *vtx, const double *ref, double *x) {
+  const int dim = shape_dim(shape), nv = shape_nv(shape);
+  double w[8];
+  p1_weights(shape, ref, w);
+  for (int m = 0; m < dim; ++m) x[m] = 0.0;
+  for (int k = 0; k < nv; ++k)
+    for (int m = 0; m < dim; ++m) x[m] += w[k] * vtx[dim * k + m];
 }
 
 // Same inclusion rule as QuadP1::checkHull (QuadP1.cpp:8-39: all edge cross
 // products of one sign, zeros count for both) and HexP1::checkHull
 // (HexP1.cpp:8-84: no outward face normal sees the point).
-int check_hull(int dim, const double *vtx, const double *x) {
+//
+// Simplices: barycentric coordinates of the point all >= -1e-12.  (The
+// reference's TriP1::checkHull / TetP1::checkHull, TriP1.cpp:7-37 /
+// TetP1.cpp:6-49, end with a "fabs(1-(l1+l2+l3)) < 1e-8 -> outside" test that
+// is always true for triangles and rejects a whole face of every
+// tetrahedron; the barycentric part is kept, that test is not.)
+int check_hull(int shape, const double *vtx, const double *x) {
+  const int dim = shape_dim(shape);
   double det, zero[3] = {0, 0, 0};
-  p1_jacobian(dim, vtx, zero, &det, nullptr);
+  p1_jacobian(shape, vtx, zero, &det, nullptr);
   if (!(det > 0)) return fail(SALVUS_E_INVALID, "poorly behaved element (detJ <= 0)");
+  if (is_simplex(shape)) {
+    double ref[3] = {0, 0, 0}, w[4];
+    int rc = inverse_map(shape, vtx, x, ref);
+    if (rc) return rc;
+    p1_weights(shape, ref, w);
+    for (int k = 0; k < shape_nv(shape); ++k)
+      if (w[k] < -1e-12) return 0;
+    return 1;
+  }
   if (dim == 2) {
     int nneg = 0, npos = 0;
     for (int i = 0; i < 4; ++i) {
@@ -222,14 +337,15 @@ int check_hull(int dim, const double *vtx, const double *x) {
 // Newton inverse of the P1 map, iterated to machine precision (the reference
 // stops at a 1e-6 physical residual, which on affine cells is already exact
 // after the first step).
-int inverse_map(int dim, const double *vtx, const double *x, double *ref) {
+int inverse_map(int shape, const double *vtx, const double *x, double *ref) {
+  const int dim = shape_dim(shape);
   double r[3] = {0, 0, 0};
   double prev = INFINITY;
   int stalled = 0;
   for (int it = 0; it < 60; ++it) {
     double X[3] = {0, 0, 0}, det, inv[9];
-    p1_map(dim, vtx, r, X);
-    p1_jacobian(dim, vtx, r, &det, inv);
+    p1_map(shape, vtx, r, X);
+    p1_jacobian(shape, vtx, r, &det, inv);
     double step_norm = 0.0;
     double dr[3] = {0, 0, 0};
     for (int a = 0; a < dim; ++a) {
@@ -250,6 +366,9 @@ int inverse_map(int dim, const double *vtx, const double *x, double *ref) {
 }
 
 int record_words(int shape, int physics, int fp64) {
+  // simplices: one record per element (affine geometry), see kernels_simplex.cuh
+  if (shape == SALVUS_TRI) return 16;                        // G(3) pad s[12]
+  if (shape == SALVUS_TET) return physics == SALVUS_ELASTIC3D ? 112 : 60;
   if (physics == SALVUS_ELASTIC3D) return fp64 ? 11 : 12;  // invJ(9) lambda' mu' [conn]
   if (shape == SALVUS_QUAD) return fp64 ? 3 : 4;          // G00 G01 G11 [conn]
   return fp64 ? 6 : 8;                                    // G(6) [conn pad]

@@ -1,4 +1,5 @@
-// host_mesh.cpp -- one-time flattening of a conforming quad / hex mesh into
+// host_mesh.cpp -- one-time flattening of a conforming quad / hex mesh (and,
+// through flatten_simplex, triangle / tetrahedron meshes) into
 // GLL connectivity and the node -> element-point incidence used by the
 // deterministic assembly.  Semantics of Mesh::setupGlobalDof (Mesh.cpp:361-452:
 // DMPlexCreateSection + spectral closure permutation): nodes on shared
@@ -39,12 +40,44 @@ struct Key4Hash {
 
 }  // namespace
 
+int flatten_simplex(salvus_mesh *m, const int64_t *cells, int64_t n_vertices);
+static int flatten_tensor(salvus_mesh *m, const int64_t *cells, int64_t n_vertices);
+
 int flatten_mesh(salvus_mesh *m, const int64_t *cells, int64_t n_vertices) {
-  const int dim = m->dim, n = m->n, N = n - 1, P = m->P;
+  const int dim = m->dim, P = m->P;
   const int64_t E = m->E;
   if ((double)E * P >= 2147483647.0)
     return fail(SALVUS_E_UNSUPPORTED, "mesh too large: E*P = %lld exceeds int32 incidence",
                 (long long)(E * P));
+  int rc = is_simplex(m->shape) ? flatten_simplex(m, cells, n_vertices)
+                                : flatten_tensor(m, cells, n_vertices);
+  if (rc) return rc;
+  const int64_t G = m->G;
+  // node -> incident element points, ascending element order
+  m->inc_off.assign((size_t)G + 1, 0);
+  for (int64_t i = 0; i < E * P; ++i) m->inc_off[(size_t)m->conn[i] + 1]++;
+  for (int64_t g = 0; g < G; ++g) m->inc_off[g + 1] += m->inc_off[g];
+  m->inc_idx.assign((size_t)(E * P), 0);
+  std::vector<int32_t> fill(m->inc_off.begin(), m->inc_off.end() - 1);
+  for (int64_t i = 0; i < E * P; ++i) m->inc_idx[(size_t)fill[m->conn[i]]++] = (int32_t)i;
+  // node coordinates (P1 map of the element points)
+  m->xyz.assign((size_t)(G * dim), 0.0);
+  for (int64_t e = 0; e < E; ++e) {
+    const double *v = m->vtx.data() + e * m->nv * dim;
+    for (int p = 0; p < P; ++p) {
+      double ref[3], x[3];
+      point_ref(m->basis, p, ref);
+      p1_map(m->shape, v, ref, x);
+      int64_t g = m->conn[(size_t)(e * P + p)];
+      for (int d = 0; d < dim; ++d) m->xyz[(size_t)(g * dim + d)] = x[d];
+    }
+  }
+  return SALVUS_OK;
+}
+
+static int flatten_tensor(salvus_mesh *m, const int64_t *cells, int64_t n_vertices) {
+  const int dim = m->dim, n = m->n, N = n - 1, P = m->P;
+  const int64_t E = m->E;
   m->conn.assign((size_t)(E * P), -1);
   std::vector<int64_t> vtx_id(n_vertices, -1);
   std::unordered_map<uint64_t, int64_t> edges;
@@ -135,26 +168,6 @@ int flatten_mesh(salvus_mesh *m, const int64_t *cells, int64_t n_vertices) {
     }
   }
   m->G = G;
-  // node -> incident element points, ascending element order
-  m->inc_off.assign((size_t)G + 1, 0);
-  for (int64_t i = 0; i < E * P; ++i) m->inc_off[(size_t)m->conn[i] + 1]++;
-  for (int64_t g = 0; g < G; ++g) m->inc_off[g + 1] += m->inc_off[g];
-  m->inc_idx.assign((size_t)(E * P), 0);
-  std::vector<int32_t> fill(m->inc_off.begin(), m->inc_off.end() - 1);
-  for (int64_t i = 0; i < E * P; ++i) m->inc_idx[(size_t)fill[m->conn[i]]++] = (int32_t)i;
-  // node coordinates (P1 map of the GLL points)
-  m->xyz.assign((size_t)(G * dim), 0.0);
-  for (int64_t e = 0; e < E; ++e) {
-    const double *v = m->vtx.data() + e * m->nv * dim;
-    for (int p = 0; p < P; ++p) {
-      double ref[3] = {m->basis.xi[p % n], m->basis.xi[(p / n) % n],
-                       dim == 3 ? m->basis.xi[p / (n * n)] : 0.0};
-      double x[3];
-      p1_map(dim, v, ref, x);
-      int64_t g = m->conn[(size_t)(e * P + p)];
-      for (int d = 0; d < dim; ++d) m->xyz[(size_t)(g * dim + d)] = x[d];
-    }
-  }
   return SALVUS_OK;
 }
 
@@ -176,11 +189,11 @@ int locate_point(const salvus_mesh *m, const double *x, int64_t *elem, double *r
       if (x[d] < lo - pad || x[d] > hi + pad) out = true;
     }
     if (out) continue;
-    int h = check_hull(dim, v, x);
+    int h = check_hull(m->shape, v, x);
     if (h < 0) return h;
     if (h == 1) {
       *elem = e;
-      return inverse_map(dim, v, x, ref);
+      return inverse_map(m->shape, v, x, ref);
     }
   }
   return fail(SALVUS_E_NOT_FOUND, "point (%g, %g, %g) lies outside the mesh", x[0], x[1],

@@ -26,19 +26,41 @@ int fail(int code, const char *fmt, ...);
                             cudaGetErrorString(e_), __FILE__, __LINE__);       \
   } while (0)
 
-// 1-D GLL basis of order N computed from the mathematics in FP64.
+// Reference element of one shape.  Tensor shapes: the 1-D GLL basis of
+// order N (xi, w, D[i*n+j] = l_j'(xi_i)).  Simplices (P3 only): the nodal
+// tables of the mass-lumped 12-node triangle / 50-node tetrahedron.
 struct Basis {
-  int order = 0, n = 0, dim = 0, P = 0, nv = 0;
-  std::vector<double> xi, w, D;  // D[i*n+j] = l_j'(xi_i)
+  int shape = 0, order = 0, n = 0, dim = 0, P = 0, nv = 0;
+  bool simplex = false;
+  std::vector<double> xi, w, D;  // tensor: 1-D GLL nodes, weights, derivative matrix
+  std::vector<double> nodes;     // simplex: [P][3] reference coordinates
+  std::vector<double> sw;        // simplex: [P] quadrature weights
+  std::vector<double> SD;        // simplex: [dim][P][P], SD[(k*P + j)*P + q] = d phi_j/d xi_k (x_q)
+  std::vector<double> C;         // simplex: [P][P] phi_i = sum_m g_m C[m*P + i]
 };
 int make_basis(int shape, int order, Basis *b);
+int make_simplex_basis(int shape, int order, Basis *b);
 void lagrange_1d(const Basis &b, double x, double *l, double *dl);
+// Basis values phi[P] and reference gradients dphi[P][3] (may be null) at a
+// reference point, for any shape.
+void basis_at(const Basis &b, const double *ref, double *phi, double *dphi);
+void simplex_basis_at(const Basis &b, const double *ref, double *phi, double *dphi);
+// Reference coordinates and quadrature weight of element point p.
+void point_ref(const Basis &b, int p, double *ref);
+double point_weight(const Basis &b, int p);
 
-// P1 geometry of one element (vertex signs of QuadP1.h:98-108 / HexP1.cpp).
-void p1_jacobian(int dim, const double *vtx, const double *ref, double *detJ, double *invJ);
-void p1_map(int dim, const double *vtx, const double *ref, double *x);
-int check_hull(int dim, const double *vtx, const double *x);  // 1 in, 0 out, <0 error
-int inverse_map(int dim, const double *vtx, const double *x, double *ref);
+// P1 geometry of one element: vertex signs of QuadP1.h:98-108 / HexP1.cpp,
+// affine maps of TriP1.cpp:117-154 / TetP1.cpp:150-205.
+void p1_jacobian(int shape, const double *vtx, const double *ref, double *detJ, double *invJ);
+void p1_map(int shape, const double *vtx, const double *ref, double *x);
+void p1_weights(int shape, const double *ref, double *w);  // vertex weights [nv]
+int check_hull(int shape, const double *vtx, const double *x);  // 1 in, 0 out, <0 error
+int inverse_map(int shape, const double *vtx, const double *x, double *ref);
+inline int shape_dim(int shape) { return (shape == SALVUS_QUAD || shape == SALVUS_TRI) ? 2 : 3; }
+inline int shape_nv(int shape) {
+  return shape == SALVUS_QUAD ? 4 : shape == SALVUS_HEX ? 8 : shape == SALVUS_TRI ? 3 : 4;
+}
+inline bool is_simplex(int shape) { return shape == SALVUS_TRI || shape == SALVUS_TET; }
 
 struct DeviceBuffer {
   void *ptr = nullptr;
@@ -74,6 +96,7 @@ struct salvus_mesh {
   salvus::DeviceBuffer d_conn, d_inc_off, d_inc_idx, d_vtx, d_par;
   salvus::DeviceBuffer d_mi64, d_mi32;
   salvus::DeviceBuffer d_rec32, d_rec64;  // stiffness records per precision
+  salvus::DeviceBuffer d_sd32, d_sd64;    // simplex derivative tables [dim][P][P]
   cudaStream_t stream = nullptr;
 };
 

@@ -6,6 +6,10 @@ Vertex order inside a cell follows the reference's right-hand (PETSc) rule:
   hex   v0(-,-,-) v1(-,+,-) v2(+,+,-) v3(+,-,-)
         v4(-,-,+) v5(+,-,+) v6(+,+,+) v7(-,+,+)       (HexP1.cpp:86-122)
 
+  tri   v0 -> (-1,-1), v1 -> (1,-1), v2 -> (-1,1), counter-clockwise (TriP1.cpp:117-154)
+  tet   v0 -> (0,0,0), v1 -> (0,1,0), v2 -> (1,0,0), v3 -> (0,0,1), with
+        det[v2-v0; v1-v0; v3-v0] > 0                  (TetP1.cpp:150-205)
+
 Material follows the ExodusModel convention: one value per element vertex
 (NAME_0 .. NAME_k, ExodusModel.cpp:455-470), P1-interpolated to GLL points.
 """
@@ -78,3 +82,66 @@ def ring_positions(center, radius, count, seed):
     phi = rng.uniform(0.0, 2.0 * np.pi)
     th = 2.0 * np.pi * np.arange(count) / count + phi
     return np.stack([center[0] + radius * np.cos(th), center[1] + radius * np.sin(th)], axis=1)
+
+
+def _jittered_lattice(counts, lengths, jitter, rng):
+    """Regular vertex lattice with interior vertices moved by up to
+    jitter x spacing (boundary vertices slide along their faces only)."""
+    axes = [np.linspace(0.0, l, n + 1) for n, l in zip(counts, lengths)]
+    grids = np.meshgrid(*axes[::-1], indexing="ij")[::-1]  # x fastest
+    pts = np.stack([g.ravel() for g in grids], axis=1)
+    h = np.array([l / n for n, l in zip(counts, lengths)])
+    d = rng.uniform(-jitter, jitter, size=pts.shape) * h
+    for k, l in enumerate(lengths):
+        on_edge = (np.abs(pts[:, k]) < 1e-9 * l) | (np.abs(pts[:, k] - l) < 1e-9 * l)
+        d[on_edge, k] = 0.0
+    return pts + d
+
+
+def delaunay_tri(nx, ny, lx, ly, jitter=0.3, seed=3):
+    """Seeded Delaunay triangulation (scipy) of a jittered (nx+1) x (ny+1)
+    point lattice over [0,lx] x [0,ly]: about 2 nx ny triangles, returned
+    counter-clockwise in TriP1 vertex order."""
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    pts = _jittered_lattice((nx, ny), (lx, ly), jitter, rng)
+    tri = Delaunay(pts)
+    cells = tri.simplices.astype(np.int64)
+    v = pts[cells]
+    det = (v[:, 1, 0] - v[:, 0, 0]) * (v[:, 2, 1] - v[:, 0, 1]) - \
+        (v[:, 1, 1] - v[:, 0, 1]) * (v[:, 2, 0] - v[:, 0, 0])
+    neg = det < 0
+    cells[neg, 1], cells[neg, 2] = cells[neg, 2].copy(), cells[neg, 1].copy()
+    keep = np.abs(det) > 1e-12 * (lx * ly / (nx * ny))
+    return pts, np.ascontiguousarray(cells[keep])
+
+
+# Kuhn (Freudenthal) split of a cube into 6 tetrahedra along the main
+# diagonal 0 -> 7 (corner index = i + 2 j + 4 k).
+_KUHN = [(0, 1, 3, 7), (0, 1, 5, 7), (0, 2, 3, 7), (0, 2, 6, 7), (0, 4, 5, 7), (0, 4, 6, 7)]
+
+
+def kuhn_tet(nx, ny, nz, lx, ly, lz, jitter=0.15, seed=3):
+    """Seeded tetrahedral mesh of [0,lx] x [0,ly] x [0,lz]: a jittered vertex
+    lattice whose cells are split into 6 tetrahedra each (no slivers, unlike
+    a Delaunay of random points).  Cells are returned in TetP1 order with
+    positive orientation."""
+    rng = np.random.default_rng(seed)
+    pts = _jittered_lattice((nx, ny, nz), (lx, ly, lz), jitter, rng)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    i, j, k = i.ravel(), j.ravel(), k.ravel()
+
+    def vid(c):
+        return ((k + (c >> 2)) * (ny + 1) + (j + ((c >> 1) & 1))) * (nx + 1) + (i + (c & 1))
+
+    cells = np.concatenate([np.stack([vid(a), vid(b), vid(c), vid(d)], axis=1)
+                            for (a, b, c, d) in _KUHN], axis=0)
+    # interleave so that the 6 tetrahedra of one cube are consecutive
+    cells = cells.reshape(6, -1, 4).transpose(1, 0, 2).reshape(-1, 4).astype(np.int64)
+    v = pts[cells]
+    det = np.einsum("ij,ij->i", v[:, 2] - v[:, 0],
+                    np.cross(v[:, 1] - v[:, 0], v[:, 3] - v[:, 0]))
+    neg = det < 0
+    cells[neg, 1], cells[neg, 2] = cells[neg, 2].copy(), cells[neg, 1].copy()
+    return pts, np.ascontiguousarray(cells)
