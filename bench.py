@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-shots", action="store_true", help="skip the batched-shots leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--no-simplex", action="store_true", help="skip the P3 simplex leg")
     ap.add_argument("--serving-jobs", type=int, default=24)
     ap.add_argument("--profile-only", action="store_true",
                     help="run a few steps only (for ncu captures); prints no JSON")
@@ -184,6 +185,52 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
             "shot_throughput_ratio": batched / plain, "steps": steps,
             "tuning": {"stiffness_shot_lanes": tune[0], "stiffness_elements_per_cta": tune[1],
                        "gather_shot_lanes": tune[2], "gather_nodes_per_cta": tune[3]}}
+
+
+def simplex_leg(core, configs, timed, steps, device=0):
+    """Config 3: P3 simplices in FP32 -- acoustic triangles (Delaunay, ~200k
+    elements over 20 x 10 km) and elastic tetrahedra (~1M elements over a
+    10 km cube), homogeneous + 5 % GRF, Ricker f0 = 1 Hz.  Each is timed as
+    graph-replayed steps; the stiffness kernel is timed per launch."""
+    out = {}
+    for name, cfg in (("tri_acoustic", configs.simplex_tri()),
+                      ("tet_elastic", configs.simplex_tet(physics=core.ELASTIC3D))):
+        mesh = core.Mesh(cfg["shape"], 3, cfg["physics"], cfg["vertices"], cfg["cells"],
+                         cfg["params"], device=device)
+        dt = 0.4 * mesh.critical_dt(iterations=40)
+        p = core.Problem(mesh, core.FP32, dt=dt)
+        for s in cfg["sources"]:
+            if "moment_tensor" in s:
+                p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                             moment_tensor=s["moment_tensor"])
+            else:
+                p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                             direction=s["direction"])
+        for r in cfg["receivers"]:
+            p.add_receiver(r)
+        p.set_seismogram_capacity(steps + 64)
+        p.run(5, core.RUN_GRAPH)
+        p.synchronize()
+        ms = timed(p, lambda: p.run(steps, core.RUN_GRAPH))
+        p.profile(True)
+        p.run(min(steps, 50), core.RUN_PLAIN)
+        prof = p.profile_read()
+        p.profile(False)
+        G, E, P, c = mesh.n_nodes, mesh.n_elements, mesh.points_per_element, mesh.n_components
+        k_ms, k_n = prof.get("stiffness", (0.0, 1))
+        st_ms = k_ms / max(k_n, 1)
+        # useful FLOPs of the factored operator per element: gradient and
+        # divergence contractions, 2 x (dim x P x P) multiply-adds per component
+        dim = mesh.dim
+        flops = E * c * 2 * 2 * dim * P * P
+        out[name] = {"elements": E, "nodes": G, "components": c, "dt": dt, "steps": steps,
+                     "value": G * steps / (ms / 1e3), "unit": METRIC,
+                     "ms_per_step": ms / steps,
+                     "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+                     "stiffness_tflops": flops / (st_ms / 1e3) / 1e12 if st_ms > 0 else None}
+        p.close()
+        mesh.close()
+    return out
 
 
 def unit_dt(core, meshgen, kind, order=4):
@@ -437,6 +484,10 @@ def main():
         from salvus_b200 import meshgen
         serve = serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs)
 
+    simplex = None
+    if not args.no_simplex:
+        simplex = simplex_leg(core, configs, timed_on, steps=min(args.steps, 200), device=local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, thr, sample, _ = cpu_leg(args, min(args.nel, 32), None, 1)
@@ -468,6 +519,7 @@ def main():
             "cpu_baseline": cpu,
             "shots_batched": shots,
             "serving": serve,
+            "simplices": simplex,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -20,6 +20,7 @@
 #include "kernels_hex_v2.cuh"
 #include "kernels_batch.cuh"
 #include "kernels_simplex.cuh"
+#include "kernels_simplex_tc.cuh"
 #include <algorithm>
 #include <cstdlib>
 #include <type_traits>
@@ -213,9 +214,34 @@ static int launch_tet(const salvus_mesh *m, const real *rec, const real *u, real
   return check_launch("tetrahedron stiffness");
 }
 
+// FP32 tetrahedra on the tensor cores (tcgen05, split TF32)
+template <int C>
+static int launch_tet_tc(const salvus_mesh *m, const float *rec, const float *u, float *r,
+                         cudaStream_t st, int *err) {
+  using S = TetTcShape<C>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(tet_tc_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)S::SMEM);
+    attr = true;
+  }
+  const int64_t tiles = (m->E + S::NE - 1) / S::NE;
+  const unsigned grid = (unsigned)(tiles < m->sm_count ? tiles : m->sm_count);
+  tet_tc_kernel<C><<<grid, S::THREADS, S::SMEM, st>>>(
+      m->E, rec, m->d_conn.as<int32_t>(), m->d_tc_tab.as<uint4>(), u, r, err);
+  g_launches++;
+  return check_launch("tetrahedron stiffness (tensor cores)");
+}
+
 template <typename real>
 static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, real *r,
-                          cudaStream_t st) {
+                          cudaStream_t st, int *err) {
+  if constexpr (std::is_same<real, float>::value) {
+    if (m->shape == SALVUS_TET && m->tet_kernel == 0) {
+      if (m->physics == SALVUS_ELASTIC3D) return launch_tet_tc<3>(m, rec, u, r, st, err);
+      return launch_tet_tc<1>(m, rec, u, r, st, err);
+    }
+  }
   if (m->shape == SALVUS_TRI) {
     tri_acoustic_kernel<real><<<blocks_for(m->E, 128), 128, 0, st>>>(
         m->E, rec, m->d_conn.as<int32_t>(), simplex_tables<real>(m), u, r);
@@ -229,7 +255,7 @@ static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, 
 template <typename real>
 static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u, real *r,
                             cudaStream_t st, int *err = nullptr) {
-  if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st);
+  if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st, err);
   if (m->physics == SALVUS_ELASTIC3D) {
     switch (m->order) {
       case 1: return launch_elastic<1, real>(m, rec, u, r, st, err);
@@ -288,6 +314,41 @@ static int build_simplex_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer
   if ((rc = sd.alloc(sizeof(real) * t.size()))) return rc;
   SALVUS_CUDA(cudaMemcpyAsync(sd.ptr, t.data(), sizeof(real) * t.size(), cudaMemcpyHostToDevice,
                               m->stream));
+  if (sizeof(real) == 4 && m->shape == SALVUS_TET) {
+    // tensor-core operand images, K-major no-swizzle core-matrix order, each
+    // as a TF32 hi part and an FP32 remainder:
+    //   B1[kappa = 56 k + q][j] = dphi_j/dxi_k (x_q)   176 x 56
+    //   B2[i][kappa = 56 k + q] = dphi_i/dxi_k (x_q)    64 x 168
+    constexpr int P = 50;
+    constexpr size_t B1 = 176 * 56, B2 = 64 * 168;
+    std::vector<float> img(2 * B1 + 2 * B2, 0.f);
+    auto off = [](int row, int k, int kdim) {
+      return (size_t)(((row >> 3) * (kdim / 4) * 128 + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4) / 4);
+    };
+    auto split = [](double v, float &hi, float &lo) {
+      // nearest TF32 value (round half away from zero on the 13 dropped bits)
+      const float f = (float)v;
+      uint32_t bits;
+      std::memcpy(&bits, &f, 4);
+      bits = (bits + 0x1000u) & 0xFFFFE000u;
+      std::memcpy(&hi, &bits, 4);
+      lo = (float)(v - (double)hi);
+    };
+    for (int k = 0; k < 3; ++k)
+      for (int q = 0; q < P; ++q)
+        for (int j = 0; j < P; ++j) {
+          float hi, lo;
+          split(m->basis.SD[((size_t)k * P + j) * P + q], hi, lo);
+          const int kap = 56 * k + q;
+          img[off(kap, j, 56)] = hi;
+          img[B1 + off(kap, j, 56)] = lo;
+          img[2 * B1 + off(j, kap, 168)] = hi;
+          img[2 * B1 + B2 + off(j, kap, 168)] = lo;
+        }
+    if ((rc = m->d_tc_tab.alloc(sizeof(float) * img.size()))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(m->d_tc_tab.ptr, img.data(), sizeof(float) * img.size(),
+                                cudaMemcpyHostToDevice, m->stream));
+  }
   SALVUS_CUDA(cudaStreamSynchronize(m->stream));
   return SALVUS_OK;
 }
@@ -836,6 +897,12 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
   std::unique_ptr<salvus_mesh> m(new salvus_mesh());
   m->device = device;
   m->fp32_only = (d->reserved & SALVUS_MESH_FP32_ONLY) != 0;
+  {
+    // FP32 tetrahedra: tensor cores by default; SALVUS_TET_KERNEL=cuda selects
+    // the CUDA-core kernel (read when the mesh is created)
+    const char *s = std::getenv("SALVUS_TET_KERNEL");
+    m->tet_kernel = (s && std::strcmp(s, "cuda") == 0) ? 1 : 0;
+  }
   m->shape = d->shape;
   m->order = d->order;
   m->physics = d->physics;
@@ -1217,7 +1284,7 @@ int salvus_problem_get_field(salvus_problem *p, int32_t f, int32_t shot, double 
     SALVUS_CUDA(cudaMemcpyAsync(vals, p->d_stage.ptr, 8 * N, cudaMemcpyDeviceToHost, p->stream));
   }
   SALVUS_CUDA(cudaStreamSynchronize(p->stream));
-  return SALVUS_OK;
+  return device_status(p);
 }
 
 static int single_shot_only(salvus_problem *p) {

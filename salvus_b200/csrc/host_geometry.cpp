@@ -341,7 +341,7 @@ int inverse_map(int shape, const double *vtx, const double *x, double *ref) {
   const int dim = shape_dim(shape);
   double r[3] = {0, 0, 0};
   double prev = INFINITY;
-  int stalled = 0;
+  int stalled = 0, floor_steps = 0;
   for (int it = 0; it < 60; ++it) {
     double X[3] = {0, 0, 0}, det, inv[9];
     p1_map(shape, vtx, r, X);
@@ -354,10 +354,15 @@ int inverse_map(int shape, const double *vtx, const double *x, double *ref) {
     }
     for (int a = 0; a < dim; ++a) r[a] += dr[a];
     // quadratic convergence until the step reaches the rounding floor of the
-    // physical coordinates; stop once it no longer shrinks
+    // physical coordinates; stop once it no longer shrinks, or after three
+    // steps below 1e-10 (steps at the rounding floor fluctuate)
     stalled = (step_norm >= 0.5 * prev) ? stalled + 1 : 0;
     prev = step_norm;
-    if (step_norm < 1e-14 || (step_norm < 1e-10 && stalled >= 2)) {
+    floor_steps = step_norm < 1e-10 ? floor_steps + 1 : 0;
+    // affine simplices: the first Newton step is exact, the second polishes
+    const bool affine_done = is_simplex(shape) && it >= 1;
+    if (step_norm < 1e-14 || (step_norm < 1e-10 && stalled >= 2) || floor_steps >= 3 ||
+        affine_done) {
       for (int a = 0; a < dim; ++a) ref[a] = r[a];
       return SALVUS_OK;
     }
@@ -368,7 +373,7 @@ int inverse_map(int shape, const double *vtx, const double *x, double *ref) {
 int record_words(int shape, int physics, int fp64) {
   // simplices: one record per element (affine geometry), see kernels_simplex.cuh
   if (shape == SALVUS_TRI) return 16;                        // G(3) pad s[12]
-  if (shape == SALVUS_TET) return physics == SALVUS_ELASTIC3D ? 112 : 60;
+  if (shape == SALVUS_TET) return physics == SALVUS_ELASTIC3D ? 120 : 64;
   if (physics == SALVUS_ELASTIC3D) return fp64 ? 11 : 12;  // invJ(9) lambda' mu' [conn]
   if (shape == SALVUS_QUAD) return fp64 ? 3 : 4;          // G00 G01 G11 [conn]
   return fp64 ? 6 : 8;                                    // G(6) [conn pad]

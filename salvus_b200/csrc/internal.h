@@ -97,6 +97,8 @@ struct salvus_mesh {
   salvus::DeviceBuffer d_mi64, d_mi32;
   salvus::DeviceBuffer d_rec32, d_rec64;  // stiffness records per precision
   salvus::DeviceBuffer d_sd32, d_sd64;    // simplex derivative tables [dim][P][P]
+  salvus::DeviceBuffer d_tc_tab;          // tetrahedra: tensor-core operand image (hi | lo)
+  int tet_kernel = 0;                     // FP32 tetrahedra: 0 tensor cores, 1 CUDA cores
   cudaStream_t stream = nullptr;
 };
 

@@ -26,8 +26,11 @@
 //
 // Records (one per element; affine geometry is constant over the element):
 //   triangle acoustic     [G00 G01 G11 0 | s_0 .. s_11]            16 words
-//   tetrahedron acoustic  [G00 G01 G02 G11 G12 G22 0 0 | s_0..s_49 | 0 0]  60
-//   tetrahedron elastic   [invJ (9) 0 0 0 | lw_0..lw_49 | mw_0..mw_49]    112
+//   tetrahedron acoustic  [G00 G01 G02 G11 G12 G22 0 0 | s_0..s_49 | 0 x6]    64
+//   tetrahedron elastic   [invJ (9) 0 x3 | lw_0..lw_49 | 0 0 | mw_0..mw_49 | 0 x6]
+//                                                                            120
+// (padded so that every 8-node run of s / lw / mw starts on 16 bytes and an
+// 8-node run that starts at node 48 stays inside the record)
 // with G = detJ invJ^T invJ (invJ[x_a][xi_b] = d xi_b / d x_a), s_q = w_q vp_q^2,
 // lw_q = w_q detJ lambda_q, mw_q = w_q detJ mu_q.
 #pragma once
@@ -41,8 +44,8 @@ struct SimplexTable {
   double w[50];     // nodal quadrature weights
 };
 
-constexpr int kTriRec = 16, kTetAcRec = 60, kTetElRec = 112;
-constexpr int kTetLambda = 12, kTetMu = 62;
+constexpr int kTriRec = 16, kTetAcRec = 64, kTetElRec = 120;
+constexpr int kTetLambda = 12, kTetMu = 64;
 
 // One thread per element.
 template <typename real>

@@ -1,0 +1,434 @@
+// kernels_simplex_tc.cuh -- FP32 tetrahedron stiffness (P3, 50 nodes) with
+// both dense contractions on the 5th-generation tensor cores (tcgen05, TF32
+// inputs, FP32 accumulation in tensor memory) and a three-term split-precision
+// correction, so the result carries FP32-level accuracy:
+//     x y ~ x_hi y_hi + x_lo y_hi + x_hi y_lo,   x_hi = x rounded to the
+//     nearest TF32 value (low 13 mantissa bits zero), x_lo = x - x_hi (exact).
+//
+// Same arithmetic as tet_stiffness_kernel (Tetrahedra.cpp:235-275 for the
+// acoustic element, Elastic3D.cpp:70-118 for the elastic one); records as in
+// kernels_simplex.cuh.  One CTA per SM walks tiles of elements:
+//
+//   rows     128 rows of a tile: acoustic one element per row (128
+//            elements); elastic (element, component) triplets, 10 elements
+//            per 32-row lane quarter (40 elements, lanes 30-31 of each
+//            quarter idle), so that a warp holds whole elements and can
+//            exchange components with shuffles.
+//   GEMM 1   gradient:  D1[row][k*56 + q] = sum_j u_row[j] dphi_j/dxi_k (x_q)
+//            M = 128, N = 176 (3 directions x 56, padded), K = 56 (7 steps)
+//   pointwise  per node q: physical gradient, stress, reference flux
+//            F_row[k][q] (FP32, CUDA cores), written back to shared memory in
+//            chunks of 8 nodes
+//   GEMM 2   divergence: D2[row][i] = sum_{k,q} F_row[k][q] dphi_i/dxi_k (x_q)
+//            M = 128, N = 64 (50 used), K = 3 x 8 per chunk, 7 chunks
+//
+// The B operands are two constant tables, both K-major, loaded once per CTA
+// (hi and lo parts, 161 KB in all):
+//   B1[kappa][j] = dphi_j/dxi_k (x_q), kappa = 56 k + q   (176 x 56)
+//   B2[i][kappa] = dphi_i/dxi_k (x_q)                      (64 x 168)
+// The tensor core reads shared memory through no-swizzle canonical layouts of
+// 8-row x 16-byte core matrices.  (The MN-major form of B1 would serve GEMM 2
+// without a second table, but an MN-major TF32 B operand in this no-swizzle
+// layout produced no output on sm_100a, so both tables are K-major.)
+//
+// Roles: warps 0-7 gather u, run the pointwise stage (warp group 0 takes the
+// even chunks, group 1 the odd ones, each group with one flux buffer) and
+// write the residual; warp 8 owns the
+// tensor memory and one elected lane issues every MMA in a fixed order, so
+// the accumulation order -- and the result -- is the same on every run.
+// Hand-offs go through mbarriers; every wait is bounded (about a second of
+// clock cycles) and a timeout sets *err and stops the CTA cleanly.
+#pragma once
+
+#include <cstdint>
+
+#include "kernels_hex_tma.cuh"  // smem_addr, mbarrier helpers
+
+namespace salvus {
+
+template <int C>
+struct TetTcShape {
+  static constexpr int P = 50;
+  static constexpr int NE = C == 1 ? 128 : 40;  // elements per tile
+  static constexpr int WORKERS = 256, THREADS = 288;
+  static constexpr int KSTEPS = 7;              // gradient K = 56
+  static constexpr uint32_t B1_SBO = 14 * 128;               // 56 K -> 14 chunks
+  static constexpr uint32_t B1_BYTES = 176 * 56 * 4;         // 39424 per part
+  static constexpr uint32_t B2_SBO = 42 * 128;               // 168 K -> 42 chunks
+  static constexpr uint32_t B2_BYTES = 64 * 168 * 4;         // 43008 per part
+  static constexpr uint32_t A1_SBO = 14 * 128;               // 56 K -> 14 chunks
+  static constexpr uint32_t A1_BYTES = 128 * 56 * 4;         // 28672 per part
+  static constexpr uint32_t A2_SBO = 6 * 128;                // 24 K -> 6 chunks
+  static constexpr uint32_t A2_BYTES = 128 * 24 * 4;         // 12288 per part
+  static constexpr uint32_t OFF_B1 = 0;
+  static constexpr uint32_t OFF_B2 = 2 * B1_BYTES;
+  static constexpr uint32_t TAB_BYTES = 2 * B1_BYTES + 2 * B2_BYTES;  // 164864
+  static constexpr uint32_t OFF_A = TAB_BYTES;               // A1 | A2 x 2 (aliased)
+  static constexpr uint32_t A_REGION = 2 * A1_BYTES;         // 57344 >= 4 A2_BYTES
+  static constexpr uint32_t OFF_BAR = OFF_A + A_REGION;
+  static constexpr uint32_t SMEM = OFF_BAR + 256;
+  static constexpr uint32_t TMEM_COLS = 256;
+  static constexpr uint32_t D2_COL = 192;
+  static constexpr int RW = C == 1 ? 64 : 120;               // record words
+};
+
+namespace tc {
+
+// byte offset of (row, k) in a K-major no-swizzle canonical tile
+__device__ __forceinline__ uint32_t kmajor_off(int row, int k, uint32_t sbo) {
+  return (uint32_t)(row >> 3) * sbo + (uint32_t)(k >> 2) * 128u + (uint32_t)(row & 7) * 16u +
+         (uint32_t)(k & 3) * 4u;
+}
+
+// shared-memory matrix descriptor: no swizzle, version 1 (sm_100)
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: D F32, A/B TF32, A K-major, B K- or MN-major
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, bool b_mn_major) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((b_mn_major ? 1u : 0u) << 16) |
+         ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(dtmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void ld8(uint32_t taddr, float *v) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void ld_wait() {
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// split x into its nearest TF32 value and the exact FP32 remainder
+__device__ __forceinline__ void split(float x, float &hi, float &lo) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  hi = __uint_as_float(h);
+  lo = x - hi;
+}
+
+// Bounded wait: clock-based limit (~1 s); a failure anywhere in the CTA
+// (*flag != 0) ends every later wait at once.  The flag records which wait
+// gave up: 1000 + 100 * role + barrier index (role 0 workers, 1 issuer).
+__device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, volatile int *flag,
+                                     int code) {
+  const long long t0 = clock64();
+  while (true) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (*flag) return false;
+    if (clock64() - t0 > (1ll << 31)) {
+      atomicCAS((int *)flag, 0, code);
+      return false;
+    }
+  }
+}
+
+}  // namespace tc
+
+// Operand table image (host-built): B1 hi, B1 lo, B2 hi, B2 lo, each in
+// K-major canonical order.
+template <int C>
+__global__ void __launch_bounds__(288, 1)
+tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restrict__ conn,
+              const uint4 *__restrict__ table, const float *__restrict__ u, float *__restrict__ r,
+              int *__restrict__ err) {
+  using S = TetTcShape<C>;
+  constexpr int P = S::P, NE = S::NE, RW = S::RW;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + S::OFF_BAR);
+  // bar[0] A1 full (256) | bar[1] GEMM 1 done | bar[2+c] chunk c full (128) |
+  // bar[9+c] chunk c consumed | bar[16] drain
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + S::OFF_BAR + 17 * 8);
+  volatile int *flag = reinterpret_cast<volatile int *>(sm + S::OFF_BAR + 17 * 8 + 4);
+  const uint32_t sbase = smem_addr(sm);
+
+  for (int i = tid; i < (int)(S::TAB_BYTES / 16); i += S::THREADS)
+    reinterpret_cast<uint4 *>(sm)[i] = table[i];
+  if (tid == 0) {
+    mbar_init(&bar[0], S::WORKERS);
+    mbar_init(&bar[1], 1);
+    for (int c = 0; c < 7; ++c) {
+      mbar_init(&bar[2 + c], 128);
+      mbar_init(&bar[9 + c], 1);
+    }
+    mbar_init(&bar[16], 1);
+    *flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(tslot)),
+                 "r"(S::TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *tslot;
+  const int64_t ntiles = (E + NE - 1) / NE;
+
+  if (warp == 8) {
+    // ---------------- MMA issuer ----------------
+    // The whole warp walks the loop (so it stays converged for the warp-wide
+    // instructions at the end); lane 0 issues the MMAs and commits.
+    constexpr uint32_t IG = tc::idesc_tf32(128, 176, false);
+    constexpr uint32_t ID = tc::idesc_tf32(128, 64, false);
+    const uint32_t b1_hi = sbase + S::OFF_B1, b1_lo = b1_hi + S::B1_BYTES;
+    const uint32_t b2_hi = sbase + S::OFF_B2, b2_lo = b2_hi + S::B2_BYTES;
+    const uint32_t a1_hi = sbase + S::OFF_A, a1_lo = a1_hi + S::A1_BYTES;
+    const bool leader = lane == 0;
+    auto wwait = [&](uint64_t *b, uint32_t p, int code) {
+      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
+    };
+    uint32_t it = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+      const uint32_t par = it & 1;
+      if (!wwait(&bar[0], par, 1100)) break;
+      tc::fence_after();
+      if (leader) {
+        for (int s = 0; s < S::KSTEPS; ++s) {
+          const uint32_t ko = (uint32_t)s * 256u;
+          const uint64_t ah = tc::desc(a1_hi + ko, 128, S::A1_SBO);
+          const uint64_t al = tc::desc(a1_lo + ko, 128, S::A1_SBO);
+          const uint64_t bh = tc::desc(b1_hi + ko, 128, S::B1_SBO);
+          const uint64_t bl = tc::desc(b1_lo + ko, 128, S::B1_SBO);
+          tc::mma_tf32(tmem, ah, bh, IG, s > 0);
+          tc::mma_tf32(tmem, al, bh, IG, 1);
+          tc::mma_tf32(tmem, ah, bl, IG, 1);
+        }
+        tc::commit(&bar[1]);
+      }
+      __syncwarp();
+      bool ok = true;
+      for (int c = 0; c < 7; ++c) {
+        if (!wwait(&bar[2 + c], par, 1102 + c)) {
+          ok = false;
+          break;
+        }
+        tc::fence_after();
+        if (leader) {
+          const uint32_t a2_hi = sbase + S::OFF_A + (uint32_t)(c & 1) * 2u * S::A2_BYTES;
+          const uint32_t a2_lo = a2_hi + S::A2_BYTES;
+          for (int k = 0; k < 3; ++k) {
+            const uint64_t ah = tc::desc(a2_hi + (uint32_t)k * 256u, 128, S::A2_SBO);
+            const uint64_t al = tc::desc(a2_lo + (uint32_t)k * 256u, 128, S::A2_SBO);
+            // K = kappa in [56 k + 8 c, 56 k + 8 c + 8): chunk (14 k + 2 c) of B2
+            const uint32_t kg = (uint32_t)(14 * k + 2 * c) * 128u;
+            const uint64_t bh = tc::desc(b2_hi + kg, 128, S::B2_SBO);
+            const uint64_t bl = tc::desc(b2_lo + kg, 128, S::B2_SBO);
+            tc::mma_tf32(tmem + S::D2_COL, ah, bh, ID, (c > 0 || k > 0) ? 1u : 0u);
+            tc::mma_tf32(tmem + S::D2_COL, al, bh, ID, 1);
+            tc::mma_tf32(tmem + S::D2_COL, ah, bl, ID, 1);
+          }
+          tc::commit(&bar[9 + c]);
+        }
+        __syncwarp();
+      }
+      if (!ok) break;
+    }
+    // drain every MMA issued by lane 0 before the memory is released
+    if (leader) {
+      tc::commit(&bar[16]);
+      const long long t0 = clock64();
+      while (!mbar_try_wait(&bar[16], 0) && clock64() - t0 < (1ll << 31)) {
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------- workers ----------------
+    const int wg = warp >> 2, quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    const int slot = C == 1 ? row : quarter * 10 + lane / 3;
+    const int comp = C == 1 ? 0 : lane % 3;
+    const bool row_ok = C == 1 || lane < 30;
+    const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+    unsigned char *a_hi = sm + S::OFF_A, *a_lo = a_hi + S::A1_BYTES;
+    // warp-uniform outcome, so that every lane reaches the .sync.aligned
+    // tensor-memory loads together
+    auto wwait = [&](uint64_t *b, uint32_t p, int code) {
+      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
+    };
+    uint32_t it = 0;
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+      const uint32_t par = it & 1;
+      const int64_t e = tile * NE + slot;
+      const bool ok = row_ok && e < E;
+      const float *rc = rec + (ok ? e : 0) * RW;
+      // element constants: acoustic G (6); elastic invJ (9)
+      float cst[9];
+#pragma unroll
+      for (int a = 0; a < 9; ++a) cst[a] = ok && (C == 3 || a < 6) ? __ldg(rc + a) : 0.f;
+      // gather u: group wg takes j in [28 wg, 28 wg + 28)
+#pragma unroll
+      for (int jc = 0; jc < 7; ++jc) {
+        const int j0 = wg * 28 + jc * 4;
+        float v[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int j = j0 + t;
+          v[t] = 0.f;
+          if (ok && j < P) v[t] = __ldg(u + (int64_t)__ldg(conn + e * P + j) * C + comp);
+        }
+        float4 h, l;
+        tc::split(v[0], h.x, l.x);
+        tc::split(v[1], h.y, l.y);
+        tc::split(v[2], h.z, l.z);
+        tc::split(v[3], h.w, l.w);
+        const uint32_t off = tc::kmajor_off(row, j0, S::A1_SBO);
+        *reinterpret_cast<float4 *>(a_hi + off) = h;
+        *reinterpret_cast<float4 *>(a_lo + off) = l;
+      }
+      tc::fence_before();
+      fence_proxy_async_smem();
+      tc::arrive(&bar[0]);
+      if (!wwait(&bar[1], par, 1001)) break;
+      tc::fence_after();
+      bool good = true;
+      for (int c = wg; c < 7; c += 2) {
+        // this group's flux buffer is free once its previous chunk is consumed
+        if (c >= 2 && !wwait(&bar[9 + c - 2], par, 1009 + c - 2)) {
+          good = false;
+          break;
+        }
+        float gr[3][8];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) tc::ld8(tmem + lane_base + (uint32_t)(k * 56 + 8 * c), gr[k]);
+        tc::ld_wait();
+        float F[3][8];
+        if constexpr (C == 1) {
+          float s[8];
+          const float4 s0 = __ldg(reinterpret_cast<const float4 *>(rc + 8 + 8 * c));
+          const float4 s1 = __ldg(reinterpret_cast<const float4 *>(rc + 12 + 8 * c));
+          s[0] = s0.x; s[1] = s0.y; s[2] = s0.z; s[3] = s0.w;
+          s[4] = s1.x; s[5] = s1.y; s[6] = s1.z; s[7] = s1.w;
+#pragma unroll
+          for (int ql = 0; ql < 8; ++ql) {
+            const bool live = ok && 8 * c + ql < P;
+            const float g0 = gr[0][ql], g1 = gr[1][ql], g2 = gr[2][ql];
+            const float w = live ? s[ql] : 0.f;
+            F[0][ql] = w * (cst[0] * g0 + cst[1] * g1 + cst[2] * g2);
+            F[1][ql] = w * (cst[1] * g0 + cst[3] * g1 + cst[4] * g2);
+            F[2][ql] = w * (cst[2] * g0 + cst[4] * g1 + cst[5] * g2);
+          }
+        } else {
+          float lw[8], mw[8];
+          {
+            const float4 a0 = __ldg(reinterpret_cast<const float4 *>(rc + 12 + 8 * c));
+            const float4 a1 = __ldg(reinterpret_cast<const float4 *>(rc + 16 + 8 * c));
+            const float4 b0 = __ldg(reinterpret_cast<const float4 *>(rc + 64 + 8 * c));
+            const float4 b1 = __ldg(reinterpret_cast<const float4 *>(rc + 68 + 8 * c));
+            lw[0] = a0.x; lw[1] = a0.y; lw[2] = a0.z; lw[3] = a0.w;
+            lw[4] = a1.x; lw[5] = a1.y; lw[6] = a1.z; lw[7] = a1.w;
+            mw[0] = b0.x; mw[1] = b0.y; mw[2] = b0.z; mw[3] = b0.w;
+            mw[4] = b1.x; mw[5] = b1.y; mw[6] = b1.z; mw[7] = b1.w;
+          }
+          const int base = lane - comp;
+#pragma unroll
+          for (int ql = 0; ql < 8; ++ql) {
+            const bool live = ok && 8 * c + ql < P;
+            // physical gradient of this component: g[x] = sum_k invJ[x][k] G[k]
+            float g[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x)
+              g[x] = cst[3 * x] * gr[0][ql] + cst[3 * x + 1] * gr[1][ql] + cst[3 * x + 2] * gr[2][ql];
+            // the element's three rows of the displacement gradient
+            float G[3][3];
+#pragma unroll
+            for (int b = 0; b < 3; ++b)
+#pragma unroll
+              for (int x = 0; x < 3; ++x) G[b][x] = __shfl_sync(0xffffffffu, g[x], base + b);
+            const float tr = G[0][0] + G[1][1] + G[2][2];
+            const float m = live ? mw[ql] : 0.f, l = live ? lw[ql] : 0.f;
+            // sigma[comp][x] = mu (g[x] + G[x][comp]) + lambda tr delta (register selects)
+            float sig[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) {
+              const float gxc = comp == 0 ? G[x][0] : (comp == 1 ? G[x][1] : G[x][2]);
+              sig[x] = m * (g[x] + gxc) + (x == comp ? l * tr : 0.f);
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+              F[k][ql] = cst[k] * sig[0] + cst[3 + k] * sig[1] + cst[6 + k] * sig[2];
+          }
+        }
+        unsigned char *b_hi = sm + S::OFF_A + (uint32_t)(c & 1) * 2u * S::A2_BYTES;
+        unsigned char *b_lo = b_hi + S::A2_BYTES;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int h4 = 0; h4 < 2; ++h4) {
+            float4 h, l;
+            tc::split(F[k][4 * h4 + 0], h.x, l.x);
+            tc::split(F[k][4 * h4 + 1], h.y, l.y);
+            tc::split(F[k][4 * h4 + 2], h.z, l.z);
+            tc::split(F[k][4 * h4 + 3], h.w, l.w);
+            const uint32_t off = tc::kmajor_off(row, 8 * k + 4 * h4, S::A2_SBO);
+            *reinterpret_cast<float4 *>(b_hi + off) = h;
+            *reinterpret_cast<float4 *>(b_lo + off) = l;
+          }
+        fence_proxy_async_smem();
+        tc::arrive(&bar[2 + c]);
+      }
+      if (!good) break;
+      if (!wwait(&bar[15], par, 1015)) break;
+      tc::fence_after();
+      // residual columns 32 wg .. 32 wg + 31 of D2
+      float out[32];
+#pragma unroll
+      for (int g8 = 0; g8 < 4; ++g8)
+        tc::ld8(tmem + lane_base + S::D2_COL + (uint32_t)(32 * wg + 8 * g8), out + 8 * g8);
+      tc::ld_wait();
+      if (ok) {
+#pragma unroll
+        for (int t = 0; t < 32; ++t) {
+          const int i = 32 * wg + t;
+          if (i < P) r[(e * P + i) * C + comp] = -out[t];
+        }
+      }
+    }
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (*flag && tid == 0 && err) atomicExch(err, *flag);
+  if (warp == 8) {
+    __syncwarp();
+    tc::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(S::TMEM_COLS)
+                 : "memory");
+  }
+}
+
+}  // namespace salvus
