@@ -280,32 +280,60 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     auto wwait = [&](uint64_t *b, uint32_t p, int code) {
       return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
     };
+    // Loads are software-pipelined: the next tile's connectivity is fetched
+    // while this tile's GEMMs and pointwise stage run, its u values while this
+    // tile's residual is read out; each chunk's material while the previous
+    // chunk of the group is computed.
+    constexpr int NPRE = C == 1 ? 8 : 16;
+    auto load_chunk = [&](const float *rcp, int c, float *dst) {
+      const float4 *p4 = reinterpret_cast<const float4 *>(rcp);
+      if constexpr (C == 1) {
+        const float4 a = __ldg(p4 + 2 + 2 * c), b = __ldg(p4 + 3 + 2 * c);  // s at 8 + 8 c
+        dst[0] = a.x; dst[1] = a.y; dst[2] = a.z; dst[3] = a.w;
+        dst[4] = b.x; dst[5] = b.y; dst[6] = b.z; dst[7] = b.w;
+      } else {
+        const float4 a = __ldg(p4 + 3 + 2 * c), b = __ldg(p4 + 4 + 2 * c);    // lambda at 12 + 8 c
+        const float4 d = __ldg(p4 + 16 + 2 * c), f = __ldg(p4 + 17 + 2 * c);  // mu at 64 + 8 c
+        dst[0] = a.x; dst[1] = a.y; dst[2] = a.z; dst[3] = a.w;
+        dst[4] = b.x; dst[5] = b.y; dst[6] = b.z; dst[7] = b.w;
+        dst[8] = d.x; dst[9] = d.y; dst[10] = d.z; dst[11] = d.w;
+        dst[12] = f.x; dst[13] = f.y; dst[14] = f.z; dst[15] = f.w;
+      }
+    };
+    int32_t cn[28];
+    float uv[28];
+    {
+      const int64_t e = (int64_t)blockIdx.x * NE + slot;
+      const bool ok = row_ok && e < E && blockIdx.x < ntiles;
+#pragma unroll
+      for (int t = 0; t < 28; ++t) {
+        const int j = wg * 28 + t;
+        cn[t] = ok && j < P ? __ldg(conn + e * P + j) : -1;
+      }
+#pragma unroll
+      for (int t = 0; t < 28; ++t) uv[t] = cn[t] >= 0 ? __ldg(u + (int64_t)cn[t] * C + comp) : 0.f;
+    }
     uint32_t it = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const uint32_t par = it & 1;
       const int64_t e = tile * NE + slot;
       const bool ok = row_ok && e < E;
       const float *rc = rec + (ok ? e : 0) * RW;
-      // element constants: acoustic G (6); elastic invJ (9)
+      // element constants: acoustic G (6); elastic invJ (9); first chunk's material
       float cst[9];
 #pragma unroll
       for (int a = 0; a < 9; ++a) cst[a] = ok && (C == 3 || a < 6) ? __ldg(rc + a) : 0.f;
-      // gather u: group wg takes j in [28 wg, 28 wg + 28)
+      float pre[NPRE];
+      load_chunk(rc, wg, pre);
+      // A1 <- this tile's u (gathered during the previous tile)
 #pragma unroll
       for (int jc = 0; jc < 7; ++jc) {
         const int j0 = wg * 28 + jc * 4;
-        float v[4];
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const int j = j0 + t;
-          v[t] = 0.f;
-          if (ok && j < P) v[t] = __ldg(u + (int64_t)__ldg(conn + e * P + j) * C + comp);
-        }
         float4 h, l;
-        tc::split(v[0], h.x, l.x);
-        tc::split(v[1], h.y, l.y);
-        tc::split(v[2], h.z, l.z);
-        tc::split(v[3], h.w, l.w);
+        tc::split(uv[4 * jc + 0], h.x, l.x);
+        tc::split(uv[4 * jc + 1], h.y, l.y);
+        tc::split(uv[4 * jc + 2], h.z, l.z);
+        tc::split(uv[4 * jc + 3], h.w, l.w);
         const uint32_t off = tc::kmajor_off(row, j0, S::A1_SBO);
         *reinterpret_cast<float4 *>(a_hi + off) = h;
         *reinterpret_cast<float4 *>(a_lo + off) = l;
@@ -313,6 +341,16 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
       tc::fence_before();
       fence_proxy_async_smem();
       tc::arrive(&bar[0]);
+      {
+        const int64_t tn = tile + gridDim.x;
+        const int64_t en = tn * NE + slot;
+        const bool okn = row_ok && tn < ntiles && en < E;
+#pragma unroll
+        for (int t = 0; t < 28; ++t) {
+          const int j = wg * 28 + t;
+          cn[t] = okn && j < P ? __ldg(conn + en * P + j) : -1;
+        }
+      }
       if (!wwait(&bar[1], par, 1001)) break;
       tc::fence_after();
       bool good = true;
@@ -322,17 +360,17 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
           good = false;
           break;
         }
+        float cur[NPRE];
+#pragma unroll
+        for (int x = 0; x < NPRE; ++x) cur[x] = pre[x];
+        if (c + 2 < 7) load_chunk(rc, c + 2, pre);
         float gr[3][8];
 #pragma unroll
         for (int k = 0; k < 3; ++k) tc::ld8(tmem + lane_base + (uint32_t)(k * 56 + 8 * c), gr[k]);
         tc::ld_wait();
         float F[3][8];
         if constexpr (C == 1) {
-          float s[8];
-          const float4 s0 = __ldg(reinterpret_cast<const float4 *>(rc + 8 + 8 * c));
-          const float4 s1 = __ldg(reinterpret_cast<const float4 *>(rc + 12 + 8 * c));
-          s[0] = s0.x; s[1] = s0.y; s[2] = s0.z; s[3] = s0.w;
-          s[4] = s1.x; s[5] = s1.y; s[6] = s1.z; s[7] = s1.w;
+          const float *s = cur;
 #pragma unroll
           for (int ql = 0; ql < 8; ++ql) {
             const bool live = ok && 8 * c + ql < P;
@@ -343,17 +381,7 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
             F[2][ql] = w * (cst[2] * g0 + cst[4] * g1 + cst[5] * g2);
           }
         } else {
-          float lw[8], mw[8];
-          {
-            const float4 a0 = __ldg(reinterpret_cast<const float4 *>(rc + 12 + 8 * c));
-            const float4 a1 = __ldg(reinterpret_cast<const float4 *>(rc + 16 + 8 * c));
-            const float4 b0 = __ldg(reinterpret_cast<const float4 *>(rc + 64 + 8 * c));
-            const float4 b1 = __ldg(reinterpret_cast<const float4 *>(rc + 68 + 8 * c));
-            lw[0] = a0.x; lw[1] = a0.y; lw[2] = a0.z; lw[3] = a0.w;
-            lw[4] = a1.x; lw[5] = a1.y; lw[6] = a1.z; lw[7] = a1.w;
-            mw[0] = b0.x; mw[1] = b0.y; mw[2] = b0.z; mw[3] = b0.w;
-            mw[4] = b1.x; mw[5] = b1.y; mw[6] = b1.z; mw[7] = b1.w;
-          }
+          const float *lw = cur, *mw = cur + 8;
           const int base = lane - comp;
 #pragma unroll
           for (int ql = 0; ql < 8; ++ql) {
@@ -402,6 +430,8 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
         tc::arrive(&bar[2 + c]);
       }
       if (!good) break;
+#pragma unroll
+      for (int t = 0; t < 28; ++t) uv[t] = cn[t] >= 0 ? __ldg(u + (int64_t)cn[t] * C + comp) : 0.f;
       if (!wwait(&bar[15], par, 1015)) break;
       tc::fence_after();
       // residual columns 32 wg .. 32 wg + 31 of D2
