@@ -40,6 +40,10 @@ def parse():
     ap.add_argument("--no-shots", action="store_true", help="skip the batched-shots leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-simplex", action="store_true", help="skip the P3 simplex leg")
+    ap.add_argument("--simplex-only", action="store_true",
+                    help="run only the P3 simplex leg (profiling / quick checks)")
+    ap.add_argument("--tet-n", type=int, default=55,
+                    help="tetrahedral lattice cells per side (6 n^3 elements; 55 -> ~1M)")
     ap.add_argument("--serving-jobs", type=int, default=24)
     ap.add_argument("--profile-only", action="store_true",
                     help="run a few steps only (for ncu captures); prints no JSON")
@@ -187,14 +191,14 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
                        "gather_shot_lanes": tune[2], "gather_nodes_per_cta": tune[3]}}
 
 
-def simplex_leg(core, configs, timed, steps, device=0):
+def simplex_leg(core, configs, timed, steps, device=0, tet_n=55):
     """Config 3: P3 simplices in FP32 -- acoustic triangles (Delaunay, ~200k
     elements over 20 x 10 km) and elastic tetrahedra (~1M elements over a
     10 km cube), homogeneous + 5 % GRF, Ricker f0 = 1 Hz.  Each is timed as
     graph-replayed steps; the stiffness kernel is timed per launch."""
     out = {}
     for name, cfg in (("tri_acoustic", configs.simplex_tri()),
-                      ("tet_elastic", configs.simplex_tet(physics=core.ELASTIC3D))):
+                      ("tet_elastic", configs.simplex_tet(n=tet_n, physics=core.ELASTIC3D))):
         mesh = core.Mesh(cfg["shape"], 3, cfg["physics"], cfg["vertices"], cfg["cells"],
                          cfg["params"], device=device)
         dt = 0.4 * mesh.critical_dt(iterations=40)
@@ -365,6 +369,22 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    if args.simplex_only:
+        def timed_simple(prob, fn):
+            stream = torch.cuda.ExternalStream(prob.stream_handle())
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            return a.elapsed_time(b)
+        out = simplex_leg(core, configs, timed_simple, steps=args.steps, device=local,
+                          tet_n=args.tet_n)
+        if rank == 0:
+            print(json.dumps({"simplices": out}), flush=True)
+        return
+
     cfg = configs.elastic_hex(nel=args.nel, order=args.order)
     mesh = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
                      cfg["params"], device=local)
@@ -486,7 +506,8 @@ def main():
 
     simplex = None
     if not args.no_simplex:
-        simplex = simplex_leg(core, configs, timed_on, steps=min(args.steps, 200), device=local)
+        simplex = simplex_leg(core, configs, timed_on, steps=min(args.steps, 200), device=local,
+                              tet_n=args.tet_n)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -355,11 +355,6 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
       tc::fence_after();
       bool good = true;
       for (int c = wg; c < 7; c += 2) {
-        // this group's flux buffer is free once its previous chunk is consumed
-        if (c >= 2 && !wwait(&bar[9 + c - 2], par, 1009 + c - 2)) {
-          good = false;
-          break;
-        }
         float cur[NPRE];
 #pragma unroll
         for (int x = 0; x < NPRE; ++x) cur[x] = pre[x];
@@ -383,6 +378,8 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
         } else {
           const float *lw = cur, *mw = cur + 8;
           const int base = lane - comp;
+          // lanes of the element's other two components, (comp - 1) and (comp - 2) mod 3
+          const int c1 = comp == 0 ? 2 : comp - 1, c2 = comp == 2 ? 0 : comp + 1;
 #pragma unroll
           for (int ql = 0; ql < 8; ++ql) {
             const bool live = ok && 8 * c + ql < P;
@@ -391,25 +388,36 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
 #pragma unroll
             for (int x = 0; x < 3; ++x)
               g[x] = cst[3 * x] * gr[0][ql] + cst[3 * x + 1] * gr[1][ql] + cst[3 * x + 2] * gr[2][ql];
-            // the element's three rows of the displacement gradient
-            float G[3][3];
-#pragma unroll
-            for (int b = 0; b < 3; ++b)
-#pragma unroll
-              for (int x = 0; x < 3; ++x) G[b][x] = __shfl_sync(0xffffffffu, g[x], base + b);
-            const float tr = G[0][0] + G[1][1] + G[2][2];
+            // column `comp` of the element's displacement gradient and its
+            // trace with four shuffles: in round r each lane sends
+            // g[(comp + r) % 3]; lane b's round-r value is g_b[comp] for the
+            // reader of component (b + r) % 3
+            const float own = comp == 0 ? g[0] : (comp == 1 ? g[1] : g[2]);
+            const float s1 = comp == 0 ? g[1] : (comp == 1 ? g[2] : g[0]);
+            const float s2 = comp == 0 ? g[2] : (comp == 1 ? g[0] : g[1]);
+            const float d1 = __shfl_sync(0xffffffffu, own, base + c1);
+            const float d2 = __shfl_sync(0xffffffffu, own, base + c2);
+            const float v1 = __shfl_sync(0xffffffffu, s1, base + c1);  // g_{c1}[comp]
+            const float v2 = __shfl_sync(0xffffffffu, s2, base + c2);  // g_{c2}[comp]
+            const float tr = own + d1 + d2;
             const float m = live ? mw[ql] : 0.f, l = live ? lw[ql] : 0.f;
-            // sigma[comp][x] = mu (g[x] + G[x][comp]) + lambda tr delta (register selects)
+            // sigma[comp][x] = mu (g[x] + g_x[comp]) + lambda tr delta(x, comp)
+            float gcol[3];
+#pragma unroll
+            for (int x = 0; x < 3; ++x) gcol[x] = x == comp ? own : (x == c1 ? v1 : v2);
             float sig[3];
 #pragma unroll
-            for (int x = 0; x < 3; ++x) {
-              const float gxc = comp == 0 ? G[x][0] : (comp == 1 ? G[x][1] : G[x][2]);
-              sig[x] = m * (g[x] + gxc) + (x == comp ? l * tr : 0.f);
-            }
+            for (int x = 0; x < 3; ++x) sig[x] = m * (g[x] + gcol[x]) + (x == comp ? l * tr : 0.f);
 #pragma unroll
             for (int k = 0; k < 3; ++k)
               F[k][ql] = cst[k] * sig[0] + cst[3 + k] * sig[1] + cst[6 + k] * sig[2];
           }
+        }
+        // this group's flux buffer is free once its previous chunk is consumed
+        // (waited here, after the arithmetic, so the MMAs overlap it)
+        if (c >= 2 && !wwait(&bar[9 + c - 2], par, 1009 + c - 2)) {
+          good = false;
+          break;
         }
         unsigned char *b_hi = sm + S::OFF_A + (uint32_t)(c & 1) * 2u * S::A2_BYTES;
         unsigned char *b_lo = b_hi + S::A2_BYTES;
