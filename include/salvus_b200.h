@@ -53,9 +53,9 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  *   hex  v0(-,-,-) v1(-,+,-) v2(+,+,-) v3(+,-,-)
  *        v4(-,-,+) v5(+,-,+) v6(+,+,+) v7(-,+,+)         (HexP1.cpp:86-122)
  *   tri  v0 -> (-1,-1), v1 -> (1,-1), v2 -> (-1,1), counter-clockwise
- *                                                          (TriP1.cpp:117-154)
+ *                                                          (TriP1.cpp:56-94)
  *   tet  v0 -> (0,0,0), v1 -> (0,1,0), v2 -> (1,0,0), v3 -> (0,0,1) with
- *        det[v2-v0; v1-v0; v3-v0] > 0                     (TetP1.cpp:150-205)
+ *        det[v2-v0; v1-v0; v3-v0] > 0                     (TetP1.cpp:91-150)
  * Simplices are the P3 mass-lumped elements (12-node triangle, 50-node
  * tetrahedron; order must be 3); elastic3d runs on hexahedra and tetrahedra. 
  * params are per element, per element vertex (Exodus NAME_0..NAME_k):
@@ -107,9 +107,9 @@ const char *salvus_version(void);
  * Replaces TensorQuad::GllPointsForOrder / GllIntegrationWeightsForOrder /
  * setupGradientOperator (TensorQuad.cpp:51-142), the Hexahedra equivalents
  * (Hexahedra.cpp:75-130, 535-577), Triangle::QuadraturePoints /
- * QuadratureIntegrationWeight / setupGradientOperator (Triangle.cpp:22-54,
- * 243-256) and Tetrahedra::QuadraturePoints / QuadratureIntegrationWeights /
- * setupGradientOperator (Tetrahedra.cpp:64-99, 432-447).  Output pointers may
+ * QuadratureIntegrationWeight / setupGradientOperator (Triangle.cpp:24-54,
+ * 244-254) and Tetrahedra::QuadraturePoints / QuadratureIntegrationWeights /
+ * setupGradientOperator (Tetrahedra.cpp:66-99, 434-448).  Output pointers may
  * be NULL.  Needs no GPU. */
 int salvus_element_tables(int32_t shape, int32_t order, int32_t *n_points, double *points,
                           double *weights, double *dphi);

@@ -302,7 +302,7 @@ static void tet_nodes(stab_t *t) {
         double a = o == 0 ? 1 - alpha : alpha;
         t->x[k][m] = a * Ed[e][0][m] + (1 - a) * Ed[e][1][m];
       }
-  /* corners v0..v3 = (0,0,0) (0,1,0) (1,0,0) (0,0,1) (TetP1.cpp:247-258 map) */
+  /* corners v0..v3 = (0,0,0) (0,1,0) (1,0,0) (0,0,1) (TetP1.cpp:153-199 map) */
   const double *Cn[4] = {O, Y, X, Z};
   for (int c = 0; c < 4; ++c, ++k)
     for (int m = 0; m < 3; ++m) t->x[k][m] = Cn[c][m];
@@ -434,8 +434,8 @@ static const double QS[4][2] = {{-1, -1}, {1, -1}, {1, 1}, {-1, 1}};
 static const double HS[8][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1},
                                 {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
 
-/* TriP1::interpolateAtPoint TriP1.cpp:156-171 (reference triangle
- * (-1,-1) (1,-1) (-1,1)); TetP1::interpolateAtPoint TetP1.cpp:56-71
+/* TriP1::interpolateAtPoint TriP1.cpp:96-109 (reference triangle
+ * (-1,-1) (1,-1) (-1,1)); TetP1::interpolateAtPoint TetP1.cpp:45-60
  * (v0 -> (0,0,0), v1 -> (0,1,0), v2 -> (1,0,0), v3 -> (0,0,1)). */
 static int shape_dim(int shape) { return shape == ORC_QUAD || shape == ORC_TRI ? 2 : 3; }
 static int shape_nv(int shape) {
@@ -500,14 +500,14 @@ static int inv3(const double J[9], double *det, double *inv) {
 int orc_p1_jacobian(int shape, const double *vtx, const double *ref, unsigned flags,
                     double *detJ, double *invJ) {
   if (shape == ORC_TRI) {
-    /* TriP1::inverseJacobian TriP1.cpp:117-154: rows d/dr = (v1 - v0)/2,
+    /* TriP1::inverseJacobian TriP1.cpp:56-94: rows d/dr = (v1 - v0)/2,
      * d/ds = (v2 - v0)/2 */
     double J[4] = {(vtx[2] - vtx[0]) / 2, (vtx[3] - vtx[1]) / 2,
                    (vtx[4] - vtx[0]) / 2, (vtx[5] - vtx[1]) / 2};
     return inv2(J, detJ, invJ);
   }
   if (shape == ORC_TET) {
-    /* TetP1::inverseJacobian TetP1.cpp:150-205: rows d/dr = v2 - v0,
+    /* TetP1::inverseJacobian TetP1.cpp:91-150: rows d/dr = v2 - v0,
      * d/ds = v1 - v0, d/dt = v3 - v0 */
     double J[9];
     for (int m = 0; m < 3; ++m) {
@@ -570,8 +570,8 @@ int orc_check_hull(int shape, const double *vtx, const double *x) {
   orc_p1_jacobian(shape, vtx, ref0, 0, &det, NULL);
   if (det <= 0) { set_err("poorly behaved element (detJ <= 0)"); return -1; }
   if (is_simplex(shape)) {
-    /* Barycentric test of TriP1::checkHull TriP1.cpp:7-37 /
-     * TetP1::checkHull TetP1.cpp:6-49, corrected: the reference's final
+    /* Barycentric test of TriP1::checkHull TriP1.cpp:6-34 /
+     * TetP1::checkHull TetP1.cpp:6-43, corrected: the reference's final
      * "fabs(1-(l1+l2+l3)) < 1e-8" rejection is identically true for
      * triangles (l3 = 1-l1-l2) and rejects every point of the face opposite
      * the last vertex for tetrahedra; here all barycentrics >= -1e-12. */
@@ -616,7 +616,7 @@ int orc_check_hull(int shape, const double *vtx, const double *x) {
  * QuadP1::inverseCoordinateTransform QuadP1.cpp:41-92,
  * HexP1::inverseCoordinateTransform HexP1.cpp:135-187. */
 int orc_inverse_map(int shape, const double *vtx, const double *x, double *ref) {
-  /* affine simplices (TriP1.cpp:39-59, TetP1.cpp:73-102 closed forms) need
+  /* affine simplices (TriP1.cpp:36-54, TetP1.cpp:62-89 closed forms) need
    * a single Newton step from the origin */
   const int d = shape_dim(shape);
   double sol[3] = {0, 0, 0};
@@ -656,7 +656,7 @@ static int basis_init(basis_t *b, int shape, int order) {
   b->n = order + 1;
   b->sx = NULL;
   if (is_simplex(shape)) {
-    /* P3 only (Triangle.cpp:25-37, Tetrahedra.cpp:67-84) */
+    /* P3 only (Triangle.cpp:24-39, Tetrahedra.cpp:66-84) */
     if (order != 3) { set_err("simplices are built for order 3 only (got %d)", order); return -1; }
     b->sx = stab_for(shape);
     if (!b->sx) { set_err("simplex tables unavailable"); return -1; }
@@ -693,8 +693,8 @@ static void ref_gradient(const basis_t *b, const double *u, double *gr /* [P][di
   const int n = b->n, d = b->dim;
   if (b->sx) {
     /* reference gradient at node q: sum_j dphi_j/dxi_k (x_q) u_j
-     * (Triangle::computeGradient Triangle.cpp:417-439; the tetrahedron's
-     * mGradientPhi_dx of Tetrahedra.cpp:372-383 folds J^-1 into the same sum) */
+     * (Triangle::computeGradient Triangle.cpp:365-385; the tetrahedron's
+     * mGradientPhi_dx of Tetrahedra.cpp:396-407 folds J^-1 into the same sum) */
     const int P = b->P;
     for (int q = 0; q < P; ++q)
       for (int k = 0; k < d; ++k) {
@@ -761,7 +761,7 @@ static void grad_test_from_geom(const basis_t *b, const double *detJ, const doub
   if (b->sx) {
     /* out_i = sum_q w_q detJ sum_k dphi_i/dxi_k (x_q) F_k(q)
      * (Tetrahedra::applyGradTestAndIntegrate Tetrahedra.cpp:248-275,
-     * Triangle::applyGradTestAndIntegrate Triangle.cpp:371-393) */
+     * Triangle::applyGradTestAndIntegrate Triangle.cpp:323-346) */
     const int P = b->P;
     for (int i = 0; i < P; ++i) {
       double s = 0;

@@ -251,8 +251,8 @@ static void inverse3(const double *J, double *detJ, double *invJ) {
 }
 
 // Vertex weights of the P1 map: QuadP1.h:98-108, HexP1.cpp:242-298,
-// TriP1::interpolateAtPoint TriP1.cpp:156-171 ([-r/2-s/2, r/2+1/2, s/2+1/2]),
-// TetP1::interpolateAtPoint TetP1.cpp:56-71 ([1-r-s-t, s, r, t]).
+// TriP1::interpolateAtPoint TriP1.cpp:96-109 ([-r/2-s/2, r/2+1/2, s/2+1/2]),
+// TetP1::interpolateAtPoint TetP1.cpp:45-60 ([1-r-s-t, s, r, t]).
 void p1_weights(int shape, const double *ref, double *w) {
   switch (shape) {
     case SALVUS_QUAD:
@@ -292,8 +292,8 @@ void p1_map(int shape, const double *vtx, const double *ref, double *x) {
 // (HexP1.cpp:8-84: no outward face normal sees the point).
 //
 // Simplices: barycentric coordinates of the point all >= -1e-12.  (The
-// reference's TriP1::checkHull / TetP1::checkHull, TriP1.cpp:7-37 /
-// TetP1.cpp:6-49, end with a "fabs(1-(l1+l2+l3)) < 1e-8 -> outside" test that
+// reference's TriP1::checkHull / TetP1::checkHull, TriP1.cpp:6-34 /
+// TetP1.cpp:6-43, end with a "fabs(1-(l1+l2+l3)) < 1e-8 -> outside" test that
 // is always true for triangles and rejects a whole face of every
 // tetrahedron; the barycentric part is kept, that test is not.)
 int check_hull(int shape, const double *vtx, const double *x) {

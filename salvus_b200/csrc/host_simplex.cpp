@@ -1,7 +1,7 @@
 // host_simplex.cpp -- the P3 mass-lumped simplex reference elements and the
 // flattening of triangle / tetrahedron meshes.
 //
-// Reference elements (Triangle.cpp:22-118, Tetrahedra.cpp:64-147 with the
+// Reference elements (Triangle.cpp:24-107, Tetrahedra.cpp:66-151 with the
 // tables of the sympy generators triangle_points_weights_polys.py and
 // tetrahedra_points_weights_polys.py / BuildNodesTetrahedraP3.py):
 //   triangle     12 nodes: 3 interior, 2 per edge, 3 vertices; space

@@ -50,7 +50,7 @@ void point_ref(const Basis &b, int p, double *ref);
 double point_weight(const Basis &b, int p);
 
 // P1 geometry of one element: vertex signs of QuadP1.h:98-108 / HexP1.cpp,
-// affine maps of TriP1.cpp:117-154 / TetP1.cpp:150-205.
+// affine maps of TriP1.cpp:56-94 / TetP1.cpp:91-150.
 void p1_jacobian(int shape, const double *vtx, const double *ref, double *detJ, double *invJ);
 void p1_map(int shape, const double *vtx, const double *ref, double *x);
 void p1_weights(int shape, const double *ref, double *w);  // vertex weights [nv]

@@ -5,13 +5,13 @@
 // fixed order.
 //
 // Reference arithmetic restated:
-//   geometry   TriP1::inverseJacobian (TriP1.cpp:117-154),
-//              TetP1::inverseJacobian (TetP1.cpp:150-205), material at the
-//              nodes by ParAtIntPts (Triangle.cpp:444-462,
-//              Tetrahedra.cpp:188-200) with the P1 vertex weights of
-//              interpolateAtPoint (TriP1.cpp:156-171, TetP1.cpp:56-71);
-//   mass       applyTestAndIntegrate (Triangle.cpp:395-401,
-//              Tetrahedra.cpp:484-491): w_q detJ (x rho for elastic);
+//   geometry   TriP1::inverseJacobian (TriP1.cpp:56-94),
+//              TetP1::inverseJacobian (TetP1.cpp:91-150), material at the
+//              nodes by ParAtIntPts (Triangle.cpp:408-428,
+//              Tetrahedra.cpp:186-197) with the P1 vertex weights of
+//              interpolateAtPoint (TriP1.cpp:96-109, TetP1.cpp:45-60);
+//   mass       applyTestAndIntegrate (Triangle.cpp:349-355,
+//              Tetrahedra.cpp:486-492): w_q detJ (x rho for elastic);
 //   triangle   ScalarTri::computeStiffnessTerm (ScalarTri.cpp:12-17) applies
 //              the dense K_e of Triangle::buildStiffnessMatrix
 //              (Triangle.cpp:194-241), K_ij = detJ sum_q w_q vp_q^2
@@ -19,7 +19,7 @@
 //              form (reference gradient, metric, divergence) so the record
 //              is 16 words per element instead of 144;
 //   tetrahedron Scalar<Tetrahedra>: computeGradient (Tetrahedra.cpp:235-245)
-//              times vp^2, then applyGradTestAndIntegrate (:248-275);
+//              times vp^2, then applyGradTestAndIntegrate (:248-274);
 //   tet elastic (no reference element): Elastic3D::computeStiffnessTerm
 //              (Elastic3D.cpp:70-118) with the tetrahedron's gradient and
 //              gradient-test operators, isotropic lambda / mu.

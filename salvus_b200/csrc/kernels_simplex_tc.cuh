@@ -5,7 +5,7 @@
 //     x y ~ x_hi y_hi + x_lo y_hi + x_hi y_lo,   x_hi = x rounded to the
 //     nearest TF32 value (low 13 mantissa bits zero), x_lo = x - x_hi (exact).
 //
-// Same arithmetic as tet_stiffness_kernel (Tetrahedra.cpp:235-275 for the
+// Same arithmetic as tet_stiffness_kernel (Tetrahedra.cpp:235-274 for the
 // acoustic element, Elastic3D.cpp:70-118 for the elastic one); records as in
 // kernels_simplex.cuh.  One CTA per SM walks tiles of elements:
 //

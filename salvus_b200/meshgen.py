@@ -6,9 +6,9 @@ Vertex order inside a cell follows the reference's right-hand (PETSc) rule:
   hex   v0(-,-,-) v1(-,+,-) v2(+,+,-) v3(+,-,-)
         v4(-,-,+) v5(+,-,+) v6(+,+,+) v7(-,+,+)       (HexP1.cpp:86-122)
 
-  tri   v0 -> (-1,-1), v1 -> (1,-1), v2 -> (-1,1), counter-clockwise (TriP1.cpp:117-154)
+  tri   v0 -> (-1,-1), v1 -> (1,-1), v2 -> (-1,1), counter-clockwise (TriP1.cpp:56-94)
   tet   v0 -> (0,0,0), v1 -> (0,1,0), v2 -> (1,0,0), v3 -> (0,0,1), with
-        det[v2-v0; v1-v0; v3-v0] > 0                  (TetP1.cpp:150-205)
+        det[v2-v0; v1-v0; v3-v0] > 0                  (TetP1.cpp:91-150)
 
 Material follows the ExodusModel convention: one value per element vertex
 (NAME_0 .. NAME_k, ExodusModel.cpp:455-470), P1-interpolated to GLL points.
