@@ -5,7 +5,11 @@
 //   Scalar<TensorQuad<QuadP1>>                   Quad<Acoustic>
 //   Scalar<Hexahedra<HexP1>>                     Hexahedron<Acoustic>
 //   Elastic3D<Hexahedra<HexP1>>                  Hexahedron<Elastic3D>
-//   Element::Factory("quad"|"hex", {"fluid"|"3delastic"})  (Element.cpp:117-304)
+//   ScalarTri<Scalar<Triangle<TriP1>>>           Triangle<Acoustic>
+//   Scalar<Tetrahedra<TetP1>>                    Tetrahedron<Acoustic>
+//   (no reference element)                       Tetrahedron<Elastic3D>
+//   Element::Factory("quad"|"hex"|"tri"|"tet", {"fluid"|"3delastic"})
+//                                                (Element.cpp:117-304)
 //                                                makeProblem(shape, physics, ...)
 //   Problem / Order2Newmark                      Problem<Element> (= Order2Newmark<Element>)
 //     assembleIntoGlobalDof (Problem.cpp:143-214)    assembleIntoGlobalDof()
@@ -66,6 +70,26 @@ struct Hexahedron {
   static constexpr int max_order = 6;  // Hexahedra.h:14-17 (order7_hex.c missing)
 };
 
+// ---- P3 simplices (Triangle<TriP1>, Tetrahedra<TetP1>; order 3 only) ----
+template <class Physics>
+struct Triangle {
+  static_assert(Physics::physics == SALVUS_ACOUSTIC,
+                "triangles carry acoustic physics (ScalarTri, Element.cpp:202-227)");
+  using physics_type = Physics;
+  static constexpr int shape = SALVUS_TRI;
+  static constexpr int dim = 2;
+  static constexpr int vertices = 3;
+  static constexpr int max_order = 3;  // Triangle.cpp:24-39
+};
+template <class Physics>
+struct Tetrahedron {
+  using physics_type = Physics;
+  static constexpr int shape = SALVUS_TET;
+  static constexpr int dim = 3;
+  static constexpr int vertices = 4;
+  static constexpr int max_order = 3;  // Tetrahedra.cpp:66-84
+};
+
 // ---- sources and receivers ----
 struct Ricker {
   std::array<double, 3> location{0, 0, 0};
@@ -101,9 +125,9 @@ struct Receiver {
 template <class Element>
 class Mesh {
  public:
-  // vertices [n_vertices][dim]; cells [n_elements][4|8] (PETSc right-hand
-  // order); params per element vertex: acoustic VP [E][nv], elastic
-  // RHO, VP, VS [3][E][nv].
+  // vertices [n_vertices][dim]; cells [n_elements][nv] (PETSc right-hand
+  // order for quads / hexes, TriP1 / TetP1 order for simplices); params per
+  // element vertex: acoustic VP [E][nv], elastic RHO, VP, VS [3][E][nv].
   Mesh(int order, const std::vector<double> &vertices, const std::vector<int64_t> &cells,
        const std::vector<double> &params, int device = 0) {
     if (order < 1 || order > Element::max_order)
@@ -231,7 +255,7 @@ template <class Element>
 using Order2Newmark = Problem<Element>;
 
 // String factory in the spirit of Element::Factory (Element.cpp:26-304):
-// shape "quad" | "hex", physics "fluid" | "3delastic".
+// shape "quad" | "hex" | "tri" | "tet", physics "fluid" | "3delastic".
 struct Simulation {
   std::shared_ptr<void> mesh;
   std::unique_ptr<ProblemBase> problem;
@@ -260,6 +284,12 @@ inline Simulation makeProblem(const std::string &shape, const std::string &physi
     return detail::make<Hexahedron<Acoustic>>(order, vertices, cells, params, dt, precision, device);
   if (shape == "hex" && physics == "3delastic")
     return detail::make<Hexahedron<Elastic3D>>(order, vertices, cells, params, dt, precision, device);
+  if (shape == "tri" && physics == "fluid")
+    return detail::make<Triangle<Acoustic>>(order, vertices, cells, params, dt, precision, device);
+  if (shape == "tet" && physics == "fluid")
+    return detail::make<Tetrahedron<Acoustic>>(order, vertices, cells, params, dt, precision, device);
+  if (shape == "tet" && physics == "3delastic")
+    return detail::make<Tetrahedron<Elastic3D>>(order, vertices, cells, params, dt, precision, device);
   throw std::runtime_error("Element type " + shape + " with physics " + physics +
                            " not supported on this path");
 }

@@ -1116,7 +1116,7 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
     return;
   }
   /* elastic 3-D */
-  double ux[ORC_MAX_P], uy[ORC_MAX_P], uz[ORC_MAX_P];
+  double ux[ORC_MAX_P] = {0}, uy[ORC_MAX_P] = {0}, uz[ORC_MAX_P] = {0};
   for (int q = 0; q < P; ++q) { ux[q] = ue[q * 3]; uy[q] = ue[q * 3 + 1]; uz[q] = ue[q * 3 + 2]; }
   double gx[ORC_MAX_P * 3], gy[ORC_MAX_P * 3], gz[ORC_MAX_P * 3];
   grad_from_geom(b, invJ, ux, gx);

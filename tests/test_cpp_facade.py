@@ -58,3 +58,16 @@ def test_facade_matches_python_path(tmp_path):
     s = p.seismograms()
     assert np.abs(s).max() > 0
     assert np.array_equal(np.array(got["hex_elastic"]), s.ravel())
+
+    V, C = meshgen.kuhn_tet(2, 2, 2, 600.0, 600.0, 600.0, jitter=0.0)
+    E = len(C)
+    par = np.stack([np.full((E, 4), x) for x in (2700.0, 6000.0, 3464.0)])
+    m = core.Mesh(core.TET, 3, core.ELASTIC3D, V, C, par)
+    p = core.Problem(m, core.FP32, dt=5e-4)
+    p.add_source((311.0, 287.0, 305.0), 8.0, 0.15, 1e10,
+                 moment_tensor=[1.0, -0.5, 0.3, 0.2, 0.1, -0.4])
+    p.add_receiver((100.0, 500.0, 600.0))
+    p.run(120, core.RUN_GRAPH)
+    s = p.seismograms()
+    assert np.abs(s).max() > 0
+    assert np.array_equal(np.array(got["tet_elastic"]), s.ravel())
