@@ -87,33 +87,52 @@ static int launch_acoustic(const salvus_mesh *m, const real *rec, const real *u,
 }
 
 // FP32 elastic hexahedra: SALVUS_HEX_KERNEL selects the variant
-//   persistent (default) TMA double-buffered persistent CTAs
-//   tma                  one TMA-staged group per CTA
-//   classic              register/shared-memory baseline (also the FP64 path)
+//   v2e5 (default)   column threads, 32-bit shared planes, 128-thread CTAs
+//                    (whole warps: 5 order-4 elements)
+//   v2, v2e10, v2e14 the same kernel with 224 / 256 / 352-thread CTAs
+//   m-suffixed       the same with a resident-CTA register cap
+//   tma, persistent  TMA bulk-copied records (one group per CTA / double-
+//                    buffered persistent CTAs)
+//   v3               cp.async record heads
+//   classic          register/shared-memory baseline (also the FP64 path)
 enum HexVariant {
   HEX_PERSISTENT = 0, HEX_TMA = 1, HEX_CLASSIC = 2, HEX_V2 = 3, HEX_V2_E4 = 4, HEX_V3 = 5,
-  HEX_V3_E4 = 6
+  HEX_V3_E4 = 6, HEX_V2_E10 = 7, HEX_V2_E5 = 8, HEX_V2_E10M4 = 9, HEX_V2_E5M8 = 10,
+  HEX_V2_E14 = 11, HEX_V2_E10M3 = 12, HEX_V2_E8M3 = 13, HEX_V2_E5M6 = 14, HEX_V2_E14M2 = 15
 };
+// Read at every launch (cheap), so a tuning sweep can switch variants
+// within one process.
 static int hex_variant() {
-  static int v = -1;
-  if (v < 0) {
-    const char *s = std::getenv("SALVUS_HEX_KERNEL");
-    v = HEX_V2;
-    if (s && std::strcmp(s, "v3") == 0) v = HEX_V3;
-    if (s && std::strcmp(s, "classic") == 0) v = HEX_CLASSIC;
-    if (s && std::strcmp(s, "tma") == 0) v = HEX_TMA;
-    if (s && std::strcmp(s, "persistent") == 0) v = HEX_PERSISTENT;
-    if (s && std::strcmp(s, "v2") == 0) v = HEX_V2;
-    if (s && std::strcmp(s, "v2e4") == 0) v = HEX_V2_E4;
-    if (s && std::strcmp(s, "v3e4") == 0) v = HEX_V3_E4;
-  }
-  return v;
+  const char *s = std::getenv("SALVUS_HEX_KERNEL");
+  if (!s) return HEX_V2_E5;  // measured fastest (whole 128-thread CTAs, 6 per SM)
+  static const struct { const char *name; int v; } kNames[] = {
+      {"v2", HEX_V2},           {"v3", HEX_V3},         {"classic", HEX_CLASSIC},
+      {"tma", HEX_TMA},         {"persistent", HEX_PERSISTENT}, {"v2e4", HEX_V2_E4},
+      {"v3e4", HEX_V3_E4},      {"v2e10", HEX_V2_E10},  {"v2e5", HEX_V2_E5},
+      {"v2e10m4", HEX_V2_E10M4}, {"v2e5m8", HEX_V2_E5M8}, {"v2e14", HEX_V2_E14},
+      {"v2e10m3", HEX_V2_E10M3}, {"v2e8m3", HEX_V2_E8M3}, {"v2e5m6", HEX_V2_E5M6},
+      {"v2e14m2", HEX_V2_E14M2}};
+  for (const auto &k : kNames)
+    if (std::strcmp(s, k.name) == 0) return k.v;
+  return HEX_V2_E5;
 }
 
-template <int N, int EPB, bool kAsync>
+template <int N, int EPB, bool kAsync, int MINB = 0>
 static int launch_elastic_v2(const salvus_mesh *m, const float *rec, const float *u, float *r,
                              cudaStream_t st) {
   using T = ElasticV2Shape<N, EPB, kAsync>;
+  if constexpr (MINB > 0) {
+    static bool attr_m = false;
+    if (!attr_m) {
+      cudaFuncSetAttribute(elastic_hex_stiffness_v2m_kernel<N, EPB, MINB>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+      attr_m = true;
+    }
+    elastic_hex_stiffness_v2m_kernel<N, EPB, MINB>
+        <<<blocks_for(m->E, EPB), T::THREADS, T::SMEM, st>>>(m->E, rec, u, r, dmatrix<float>(m->basis));
+    g_launches++;
+    return check_launch("elastic stiffness (v2)");
+  }
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(elastic_hex_stiffness_v2_kernel<N, EPB, kAsync>,
@@ -138,6 +157,18 @@ static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, 
     if (var == HEX_V2_E4) return launch_elastic_v2<N, E4, false>(m, rec, u, r, st);
     if (var == HEX_V3) return launch_elastic_v2<N, E8, true>(m, rec, u, r, st);
     if (var == HEX_V3_E4) return launch_elastic_v2<N, E4, true>(m, rec, u, r, st);
+    // element counts that fill whole warps at order 4 (n^2 = 25 threads each)
+    constexpr int E10 = 256 / n2 > 0 ? 256 / n2 : 1, E5 = 128 / n2 > 0 ? 128 / n2 : 1;
+    constexpr int E14 = 352 / n2 > 0 ? 352 / n2 : 1;
+    if (var == HEX_V2_E10) return launch_elastic_v2<N, E10, false>(m, rec, u, r, st);
+    if (var == HEX_V2_E5) return launch_elastic_v2<N, E5, false>(m, rec, u, r, st);
+    if (var == HEX_V2_E10M4) return launch_elastic_v2<N, E10, false, 4>(m, rec, u, r, st);
+    if (var == HEX_V2_E5M8) return launch_elastic_v2<N, E5, false, 8>(m, rec, u, r, st);
+    if (var == HEX_V2_E14) return launch_elastic_v2<N, E14, false>(m, rec, u, r, st);
+    if (var == HEX_V2_E10M3) return launch_elastic_v2<N, E10, false, 3>(m, rec, u, r, st);
+    if (var == HEX_V2_E8M3) return launch_elastic_v2<N, E8, false, 3>(m, rec, u, r, st);
+    if (var == HEX_V2_E5M6) return launch_elastic_v2<N, E5, false, 6>(m, rec, u, r, st);
+    if (var == HEX_V2_E14M2) return launch_elastic_v2<N, E14, false, 2>(m, rec, u, r, st);
     if (var == HEX_TMA && err) {
       using T = ElasticTmaShape<N>;
       static bool attr = false;

@@ -6,7 +6,8 @@
 // along t live in registers; r- and s-direction operands come from shared
 // memory, packed as float4 (x, y, z, pad) so one load serves all three
 // components.  Shared memory per group of EPB elements:
-//   srec [EPB][P][3] float4   48 B records (invJ 9, lambda', mu', conn);
+//   srec [EPB][3][P] float4   48 B records (invJ 9, lambda', mu', conn) in
+//                            the three-plane layout of the global records;
 //                            after a point's record is consumed its slot
 //                            holds (F_r xyz, -) and (F_s xyz, -)
 //   su   [EPB][P]    float4   gathered u (x, y, z, pad); reused to stage the
@@ -109,7 +110,7 @@ __device__ __forceinline__ void elastic_group(float4 *__restrict__ srec, float4 
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const int p = ij + n2 * k;
-      const int node = __float_as_int(erec[p * 3 + 2].w);
+      const int node = __float_as_int(erec[2 * P + p].w);
       ux[k] = __ldg(u + 3 * (int64_t)node + 0);
       uy[k] = __ldg(u + 3 * (int64_t)node + 1);
       uz[k] = __ldg(u + 3 * (int64_t)node + 2);
@@ -123,7 +124,7 @@ __device__ __forceinline__ void elastic_group(float4 *__restrict__ srec, float4 
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const int p = ij + n2 * k;
-      const float4 ra = erec[p * 3 + 0], rb = erec[p * 3 + 1], rc = erec[p * 3 + 2];
+      const float4 ra = erec[p], rb = erec[P + p], rc = erec[2 * P + p];
       const float J[9] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w, rc.x};
       const float lam = rc.y, mu = rc.z;
       float d[3][3];
@@ -162,8 +163,8 @@ __device__ __forceinline__ void elastic_group(float4 *__restrict__ srec, float4 
 #pragma unroll
         for (int b = 0; b < 3; ++b)
           F[c][b] = J[0 * 3 + b] * sig[c][0] + J[1 * 3 + b] * sig[c][1] + J[2 * 3 + b] * sig[c][2];
-      erec[p * 3 + 0] = make_float4(F[0][0], F[1][0], F[2][0], 0.f);
-      erec[p * 3 + 1] = make_float4(F[0][1], F[1][1], F[2][1], 0.f);
+      erec[p] = make_float4(F[0][0], F[1][0], F[2][0], 0.f);
+      erec[P + p] = make_float4(F[0][1], F[1][1], F[2][1], 0.f);
       Ftx[k] = F[0][2]; Fty[k] = F[1][2]; Ftz[k] = F[2][2];
     }
   }
@@ -176,8 +177,8 @@ __device__ __forceinline__ void elastic_group(float4 *__restrict__ srec, float4 
       float ox = 0, oy = 0, oz = 0;
 #pragma unroll
       for (int l = 0; l < n; ++l) {
-        const float4 a = erec[(l + n * j + n2 * k) * 3 + 0];
-        const float4 b = erec[(i + n * l + n2 * k) * 3 + 1];
+        const float4 a = erec[l + n * j + n2 * k];
+        const float4 b = erec[P + i + n * l + n2 * k];
         const float dk = Dm.d[l * n + k];
         ox += DTi[l] * a.x + DTj[l] * b.x + dk * Ftx[l];
         oy += DTi[l] * a.y + DTj[l] * b.y + dk * Fty[l];

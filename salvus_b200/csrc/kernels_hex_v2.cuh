@@ -11,7 +11,9 @@
 //    straddle two elements touches 32 distinct banks on every store;
 //  * connectivity comes from word 11 of each 48-byte record, so no separate
 //    connectivity stream is read; the record's last float4 (J8, lambda', mu',
-//    conn) is fetched first to start the displacement gather early.
+//    conn) is fetched first to start the displacement gather early;
+//  * records are three float4 planes per element ([E][3][P]), so the 32
+//    lanes of a warp load 512 contiguous bytes per instruction.
 #pragma once
 
 #include <cstdint>
@@ -44,10 +46,9 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 template <int N, int EPB_, bool kAsync>
-__global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, kAsync>::THREADS)
-elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
-                                const float *__restrict__ u, float *__restrict__ r,
-                                DMatrix<float> Dm) {
+__device__ __forceinline__ void elastic_hex_v2_body(int64_t E, const float *__restrict__ rec,
+                                                    const float *__restrict__ u,
+                                                    float *__restrict__ r, const DMatrix<float> &Dm) {
   using S = ElasticV2Shape<N, EPB_, kAsync>;
   constexpr int n = S::n, n2 = S::n2, P = S::P, EPB = S::EPB;
   extern __shared__ __align__(16) float smem_v2raw[];
@@ -61,7 +62,7 @@ elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
   const bool ok = le < EPB && e < E;
   float *su = smem_v2 + (size_t)(ok ? le : 0) * S::US;                      // [3][P]
   float *sF = smem_v2 + (size_t)EPB * S::US + (size_t)(ok ? le : 0) * S::FS;  // [3][2][P]
-  const float4 *rq = reinterpret_cast<const float4 *>(rec) + (e * P) * 3;
+  const float4 *rq = reinterpret_cast<const float4 *>(rec) + (e * 3) * P;  // planes [3][P]
 
   float Dri[n], Dsj[n], DTi[n], DTj[n];
 #pragma unroll
@@ -77,13 +78,13 @@ elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const int p = ij + n2 * k;
-      cp_async16(sra + le * P + p, rq + p * 3 + 0);
-      cp_async16(srb + le * P + p, rq + p * 3 + 1);
+      cp_async16(sra + le * P + p, rq + p);
+      cp_async16(srb + le * P + p, rq + P + p);
     }
   }
   if (ok) {
 #pragma unroll
-    for (int k = 0; k < n; ++k) rc[k] = __ldg(rq + (ij + n2 * k) * 3 + 2);
+    for (int k = 0; k < n; ++k) rc[k] = __ldg(rq + 2 * P + ij + n2 * k);
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const int64_t node = __float_as_int(rc[k].w);
@@ -106,8 +107,8 @@ elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const int p = ij + n2 * k;
-      const float4 ra = kAsync ? sra[le * P + p] : __ldg(rq + p * 3 + 0);
-      const float4 rb = kAsync ? srb[le * P + p] : __ldg(rq + p * 3 + 1);
+      const float4 ra = kAsync ? sra[le * P + p] : __ldg(rq + p);
+      const float4 rb = kAsync ? srb[le * P + p] : __ldg(rq + P + p);
       const float J[9] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w, rc[k].x};
       const float lam = rc[k].y, mu = rc[k].z;
       float d[3][3];
@@ -171,6 +172,24 @@ elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
       }
     }
   }
+}
+
+// MINB = 0: the compiler picks the register count for THREADS threads per
+// CTA; MINB > 0 also asks for MINB resident CTAs per SM (register cap).
+template <int N, int EPB_, bool kAsync, int MINB = 0>
+__global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, kAsync>::THREADS)
+elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
+                                const float *__restrict__ u, float *__restrict__ r,
+                                DMatrix<float> Dm) {
+  elastic_hex_v2_body<N, EPB_, kAsync>(E, rec, u, r, Dm);
+}
+
+template <int N, int EPB_, int MINB>
+__global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, false>::THREADS, MINB)
+elastic_hex_stiffness_v2m_kernel(int64_t E, const float *__restrict__ rec,
+                                 const float *__restrict__ u, float *__restrict__ r,
+                                 DMatrix<float> Dm) {
+  elastic_hex_v2_body<N, EPB_, false>(E, rec, u, r, Dm);
 }
 
 }  // namespace salvus

@@ -90,6 +90,10 @@ __device__ __forceinline__ double p1_interp_dev(int dim, const double *vals, con
 // Records:
 //   acoustic : G = w detJ vp^2 invJ^T invJ (symmetric; 3 or 6 words)
 //   elastic  : invJ (row-major [x_a][xi_b], 9 words), lambda w detJ, mu w detJ
+// FP32 elastic records (12 words with connectivity) are stored as three
+// float4 planes per element, [E][3][P] float4: plane 0 = invJ 0-3, plane 1 =
+// invJ 4-7, plane 2 = (invJ 8, lambda', mu', conn), so that consecutive
+// points of one plane are consecutive 16-byte words (contiguous warp loads).
 template <typename real, bool kPackConn>
 __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, int rw,
                                 const double *__restrict__ vtx, const double *__restrict__ par,
@@ -141,10 +145,22 @@ __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, i
     // c11 = rho vp^2, c66 = rho vs^2, c12 = c11 - 2 c66 (Elastic3D.cpp:42-53)
     double mu = rho * vs * vs;
     double lam = rho * vp * vp - 2.0 * mu;
-    for (int a = 0; a < 9; ++a) out[a] = (real)iJ[a];
-    out[9] = (real)(wd * lam);
-    out[10] = (real)(wd * mu);
+    if constexpr (kPackConn) {
+      real w12[12];
+      for (int a = 0; a < 9; ++a) w12[a] = (real)iJ[a];
+      w12[9] = (real)(wd * lam);
+      w12[10] = (real)(wd * mu);
+      const int32_t cn = conn[tid];
+      w12[11] = 0;
+      reinterpret_cast<int32_t *>(w12)[11] = cn;
+      for (int a = 0; a < 12; ++a) rec[((e * 3 + a / 4) * P + p) * 4 + a % 4] = w12[a];
+    } else {
+      for (int a = 0; a < 9; ++a) out[a] = (real)iJ[a];
+      out[9] = (real)(wd * lam);
+      out[10] = (real)(wd * mu);
+    }
     mass_local[tid] = wd * rho;
+    return;
   }
   if (kPackConn) {
     int32_t c = conn[tid];

@@ -130,18 +130,20 @@ struct ElasticShape {
   static constexpr size_t SMEM = sizeof(real) * (size_t)EPB * 9 * P;
 };
 
+// FP32 records: three float4 planes per element ([E][3][P], kernels_setup.cuh)
 __device__ __forceinline__ void load_elastic_rec(const float *__restrict__ rec,
-                                                 const int32_t *__restrict__, int64_t ep,
-                                                 float *J, float *lam, float *mu) {
-  const float4 *q = reinterpret_cast<const float4 *>(rec) + 3 * ep;
-  float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+                                                 const int32_t *__restrict__, int64_t e, int p,
+                                                 int P, float *J, float *lam, float *mu) {
+  const float4 *q = reinterpret_cast<const float4 *>(rec) + e * 3 * P + p;
+  float4 a = __ldg(q), b = __ldg(q + P), c = __ldg(q + 2 * P);
   J[0] = a.x; J[1] = a.y; J[2] = a.z; J[3] = a.w;
   J[4] = b.x; J[5] = b.y; J[6] = b.z; J[7] = b.w;
   J[8] = c.x; *lam = c.y; *mu = c.z;
 }
 __device__ __forceinline__ void load_elastic_rec(const double *__restrict__ rec,
-                                                 const int32_t *__restrict__, int64_t ep,
-                                                 double *J, double *lam, double *mu) {
+                                                 const int32_t *__restrict__, int64_t e, int p,
+                                                 int P, double *J, double *lam, double *mu) {
+  const int64_t ep = e * P + p;
 #pragma unroll
   for (int a = 0; a < 9; ++a) J[a] = rec[ep * 11 + a];
   *lam = rec[ep * 11 + 9];
@@ -194,7 +196,7 @@ elastic_hex_stiffness_kernel(int64_t E, const real *__restrict__ rec,
     for (int k = 0; k < n; ++k) {
       const int p = ij + n2 * k;
       real J[9], lam, mu;
-      load_elastic_rec(rec, conn, e * P + p, J, &lam, &mu);
+      load_elastic_rec(rec, conn, e, p, P, J, &lam, &mu);
       real d[3][3];  // d[c][b]: derivative of u_c along reference direction b
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
