@@ -224,6 +224,24 @@ int salvus_problem_info(const salvus_problem *p, int32_t *n_shots, int32_t *n_re
 int salvus_apply_stiffness_noalloc(const salvus_mesh *mesh, int32_t precision, const void *u,
                                    void *a, void *stream);
 
+/* ---- problem groups: many meshes of uneven size advanced together ----
+ * A group of FP32 single-shot problems of one element class (acoustic quads
+ * or elastic hexahedra of one order, on one device) advances with one launch
+ * per step stage for all members (SALVUS_GROUP_STEP=persistent: one
+ * persistent work-queue launch per step): every CTA runs the single-problem
+ * kernel body on its member's arrays, so each member's result is bitwise the
+ * one it gets alone.  salvus_group_run(g, n) advances
+ * every member n steps (graph-replayed in chunks of 32); it orders itself
+ * after the members' pending work and their later work after it.  Members
+ * stay owned by the caller and must outlive the group; do not advance a
+ * member on its own while a group run is in flight.  No reference
+ * counterpart (the reference steps one mesh per process, Main.cpp:45-66). */
+typedef struct salvus_group salvus_group;
+int salvus_group_create(salvus_problem *const *members, int32_t n_members, salvus_group **out);
+int salvus_group_run(salvus_group *g, int64_t n_steps);
+int salvus_group_synchronize(salvus_group *g);
+int salvus_group_destroy(salvus_group *g);
+
 /* ---- serving: continuous batching of forward-modelling jobs ----
  * No reference counterpart (the reference runs one simulation per process,
  * Main.cpp:10-78).  A server owns one GPU and a device-memory budget.  A

@@ -65,6 +65,10 @@ SIGNATURES = [
     ("salvus_mesh_locate_point", ctypes.c_int, [_VP, _DP, ctypes.POINTER(_I64), _DP]),
     ("salvus_mesh_inverse_mass", ctypes.c_int, [_VP, _DP]),
     ("salvus_mesh_max_eigenvalue", ctypes.c_int, [_VP, _I32, ctypes.c_uint64, _DP]),
+    ("salvus_group_create", ctypes.c_int, [ctypes.POINTER(_VP), _I32, ctypes.POINTER(_VP)]),
+    ("salvus_group_run", ctypes.c_int, [_VP, _I64]),
+    ("salvus_group_synchronize", ctypes.c_int, [_VP]),
+    ("salvus_group_destroy", ctypes.c_int, [_VP]),
     ("salvus_problem_create", ctypes.c_int, [_VP, _I32, _I32, ctypes.POINTER(_VP)]),
     ("salvus_problem_destroy", ctypes.c_int, [_VP]),
     ("salvus_problem_set_dt", ctypes.c_int, [_VP, _D]),
@@ -315,6 +319,36 @@ class Problem:
         _check(lib().salvus_profile_read(self.h, n, names, _dp(ms), cnt.ctypes.data_as(ctypes.POINTER(_I64)),
                                          ctypes.byref(k)))
         return {names[i].decode(): (ms[i], int(cnt[i])) for i in range(k.value)}
+
+
+class Group:
+    """FP32 single-shot problems of one element class (acoustic quads or
+    elastic hexahedra of one order) advanced together, one launch per step
+    stage for all members; each member's result is bitwise its solo result."""
+
+    def __init__(self, problems):
+        self.problems = list(problems)
+        arr = (_VP * len(self.problems))(*[p.h for p in self.problems])
+        h = _VP()
+        _check(lib().salvus_group_create(arr, len(self.problems), ctypes.byref(h)))
+        self.h = h
+
+    def run(self, n_steps):
+        _check(lib().salvus_group_run(self.h, int(n_steps)))
+
+    def synchronize(self):
+        _check(lib().salvus_group_synchronize(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().salvus_group_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def launch_count():

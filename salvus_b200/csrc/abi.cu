@@ -21,6 +21,7 @@
 #include "kernels_batch.cuh"
 #include "kernels_simplex.cuh"
 #include "kernels_simplex_tc.cuh"
+#include "kernels_group.cuh"
 #include <algorithm>
 #include <cstdlib>
 #include <type_traits>
@@ -871,6 +872,248 @@ static int ready(salvus_problem *p) {
   return SALVUS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// problem groups: FP32 single-shot problems of one element class advance with
+// one launch per stage (kernels_group.cuh)
+template <int N>
+static int group_stiffness_t(const salvus_mesh *m0, const GroupSlot *slots, int J, int64_t blocks,
+                             cudaStream_t st) {
+  if (m0->shape == SALVUS_QUAD) {
+    group_quad_acoustic_stiffness<N><<<(unsigned)blocks, AcousticShape<2, N>::THREADS, 0, st>>>(
+        slots, J, dmatrix<float>(m0->basis));
+  } else if constexpr (N <= kMaxHexOrder) {
+    constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
+    using T = ElasticV2Shape<N, EPB, false>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(group_hex_elastic_stiffness<N, EPB>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+      attr = true;
+    }
+    group_hex_elastic_stiffness<N, EPB><<<(unsigned)blocks, T::THREADS, T::SMEM, st>>>(
+        slots, J, dmatrix<float>(m0->basis));
+  }
+  g_launches++;
+  return check_launch("group stiffness");
+}
+
+static int group_stiffness(const salvus_mesh *m0, const GroupSlot *slots, int J, int64_t blocks,
+                           cudaStream_t st) {
+  switch (m0->order) {
+    case 1: return group_stiffness_t<1>(m0, slots, J, blocks, st);
+    case 2: return group_stiffness_t<2>(m0, slots, J, blocks, st);
+    case 3: return group_stiffness_t<3>(m0, slots, J, blocks, st);
+    case 4: return group_stiffness_t<4>(m0, slots, J, blocks, st);
+    case 5: return group_stiffness_t<5>(m0, slots, J, blocks, st);
+    case 6: return group_stiffness_t<6>(m0, slots, J, blocks, st);
+    case 7: return group_stiffness_t<7>(m0, slots, J, blocks, st);
+    case 8: return group_stiffness_t<8>(m0, slots, J, blocks, st);
+    case 9: return group_stiffness_t<9>(m0, slots, J, blocks, st);
+    case 10: return group_stiffness_t<10>(m0, slots, J, blocks, st);
+  }
+  return fail(SALVUS_E_UNSUPPORTED, "no grouped stiffness for order %d", m0->order);
+}
+
+// stiffness CTAs per member (the single-problem kernel's element groups)
+static int64_t group_stiff_blocks(const salvus_mesh *m) {
+  const int n2 = m->n * m->n;
+  if (m->shape == SALVUS_QUAD) {
+    const int P = n2, epb = (256 / P) > 0 ? (256 / P) : 1;  // AcousticShape<2, N>::EPB
+    return (m->E + epb - 1) / epb;
+  }
+  const int epb = 128 / n2 > 0 ? 128 / n2 : 1;  // v2 with 128-thread CTAs
+  return (m->E + epb - 1) / epb;
+}
+
+}  // namespace salvus
+
+struct salvus_group {
+  std::vector<salvus_problem *> members;
+  const salvus_mesh *m0 = nullptr;
+  int c = 1;
+  bool stages = true;  // one launch per stage; SALVUS_GROUP_STEP=persistent: one launch per step
+  std::vector<salvus::GroupSlot> slots;
+  salvus::DeviceBuffer d_slots;
+  int64_t n_stiff = 0, n_gather = 0, n_rec = 0;
+  // persistent single-launch step: work-item queue
+  std::vector<salvus::GroupCounts> counts;
+  std::vector<salvus::GroupWork> work;
+  int64_t total = 0;
+  int grid = 0;
+  salvus::DeviceBuffer d_counts, d_work, d_done, d_sync;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<cudaEvent_t> member_ev;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  int64_t sig[3] = {-1, -1, -1};
+};
+
+namespace salvus {
+
+static int group_upload(salvus::DeviceBuffer &b, const void *src, size_t bytes, cudaStream_t st) {
+  if (b.bytes < bytes) {
+    int rc = b.alloc(bytes);
+    if (rc) return rc;
+  }
+  SALVUS_CUDA(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, st));
+  return SALVUS_OK;
+}
+
+static int group_fill(salvus_group *g) {
+  int64_t bs = 0, bg = 0, br = 0;
+  g->slots.resize(g->members.size());
+  for (size_t k = 0; k < g->members.size(); ++k) {
+    salvus_problem *p = g->members[k];
+    const salvus_mesh *m = p->mesh;
+    int rc = ready(p);
+    if (rc) return rc;
+    GroupSlot &s = g->slots[k];
+    s.rec = m->d_rec32.as<float>();
+    s.conn = m->d_conn.as<int32_t>();
+    s.inc_off = m->d_inc_off.as<int32_t>();
+    s.inc_idx = m->d_inc_idx.as<int32_t>();
+    s.mi = m->d_mi32.as<float>();
+    s.E = m->E;
+    s.G = m->G;
+    s.u = p->d_u.as<float>();
+    s.v = p->d_v.as<float>();
+    s.ap = p->d_ap.as<float>();
+    s.a = p->d_a.as<float>();
+    s.r = p->d_r.as<float>();
+    s.dt = (float)p->dt;
+    s.dtd = p->dt;
+    s.step = p->d_step.as<int64_t>();
+    s.nsrc = (int)p->srcs.size();
+    s.nrec = (int)p->recs.size();
+    s.src_elem = p->d_src_elem.as<int64_t>();
+    s.src_par = p->d_src_par.as<double>();
+    s.src_wts = p->d_src_wts.as<double>();
+    s.rec_elem = p->d_rec_elem.as<int64_t>();
+    s.rec_l = p->d_rec_l.as<double>();
+    s.seis = p->d_seis.as<double>();
+    s.cap = p->seis_cap;
+    s.b_stiff = bs;
+    s.b_gather = bg;
+    s.b_rec = br;
+    bs += group_stiff_blocks(m);
+    bg += (m->G + 255) / 256;
+    br += s.nrec;
+  }
+  g->n_stiff = bs;
+  g->n_gather = bg;
+  g->n_rec = br;
+  int rc = group_upload(g->d_slots, g->slots.data(), sizeof(GroupSlot) * g->slots.size(), g->stream);
+  if (rc) return rc;
+  // work-item queue of the persistent step: every member's stiffness items
+  // (kStiffPer element groups each), then per member source (1), gather items
+  // (kGatherPer CTA-wide node tiles each), receivers (1 each), advance (1)
+  constexpr int kStiffPer = 2, kGatherPer = 8;
+  const int J = (int)g->members.size();
+  const int tile = g->m0->shape == SALVUS_HEX ? 128 : 256;  // CTA width
+  g->counts.assign(J, GroupCounts{0, 0, 0});
+  g->work.clear();
+  auto add = [&](int type, int j, int64_t tiles, int per) -> int32_t {
+    int32_t items = 0;
+    for (int64_t f = 0; f < tiles; f += per, ++items)
+      g->work.push_back(GroupWork{type, j, (int)f, (int)std::min<int64_t>(per, tiles - f)});
+    return items;
+  };
+  for (int j = 0; j < J; ++j)
+    g->counts[j].stiff = add(GI_STIFF, j, group_stiff_blocks(g->members[j]->mesh), kStiffPer);
+  for (int j = 0; j < J; ++j) {
+    add(GI_SRC, j, 1, 1);
+    g->counts[j].gather = add(GI_GATHER, j, (g->members[j]->mesh->G + tile - 1) / tile, kGatherPer);
+    g->counts[j].rec = add(GI_REC, j, (int64_t)g->members[j]->recs.size(), 1);
+    add(GI_ADV, j, 1, 1);
+  }
+  g->total = (int64_t)g->work.size();
+  if ((rc = group_upload(g->d_counts, g->counts.data(), sizeof(GroupCounts) * J, g->stream))) return rc;
+  if ((rc = group_upload(g->d_work, g->work.data(), sizeof(GroupWork) * g->work.size(), g->stream)))
+    return rc;
+  if (g->d_done.bytes < sizeof(int32_t) * 4 * J) {
+    if ((rc = g->d_done.alloc(sizeof(int32_t) * 4 * J))) return rc;
+    SALVUS_CUDA(cudaMemsetAsync(g->d_done.ptr, 0, sizeof(int32_t) * 4 * J, g->stream));
+  }
+  if (!g->d_sync.ptr) {
+    if ((rc = g->d_sync.alloc(sizeof(GroupSync)))) return rc;
+    SALVUS_CUDA(cudaMemsetAsync(g->d_sync.ptr, 0, sizeof(GroupSync), g->stream));
+  }
+  return SALVUS_OK;
+}
+
+template <int N, bool kHex, int C>
+static int group_persistent_t(salvus_group *g) {
+  constexpr int threads = kHex ? 128 : 256;
+  size_t smem = 0;
+  if constexpr (kHex) {
+    constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
+    smem = ElasticV2Shape<N, EPB, false>::SMEM;
+  }
+  auto kern = group_persistent_step<N, kHex, C>;
+  if (g->grid == 0) {
+    if (smem) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 0;
+    SALVUS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+    g->grid = (per_sm > 0 ? per_sm : 1) * g->m0->sm_count;
+  }
+  const int grid = (int)std::min<int64_t>(g->grid, g->total);
+  kern<<<grid, threads, smem, g->stream>>>(
+      g->d_slots.as<GroupSlot>(), g->d_counts.as<GroupCounts>(), (int)g->members.size(),
+      g->d_work.as<GroupWork>(), g->total, g->d_done.as<int32_t>(), g->d_sync.as<GroupSync>(),
+      dmatrix<float>(g->m0->basis), g->m0->P);
+  g_launches++;
+  return check_launch("group persistent step");
+}
+
+static int group_persistent(salvus_group *g) {
+  const salvus_mesh *m = g->m0;
+  if (m->shape == SALVUS_HEX) {
+    switch (m->order) {
+      case 1: return group_persistent_t<1, true, 3>(g);
+      case 2: return group_persistent_t<2, true, 3>(g);
+      case 3: return group_persistent_t<3, true, 3>(g);
+      case 4: return group_persistent_t<4, true, 3>(g);
+      case 5: return group_persistent_t<5, true, 3>(g);
+      case 6: return group_persistent_t<6, true, 3>(g);
+    }
+  } else {
+    switch (m->order) {
+      case 1: return group_persistent_t<1, false, 1>(g);
+      case 2: return group_persistent_t<2, false, 1>(g);
+      case 3: return group_persistent_t<3, false, 1>(g);
+      case 4: return group_persistent_t<4, false, 1>(g);
+      case 5: return group_persistent_t<5, false, 1>(g);
+      case 6: return group_persistent_t<6, false, 1>(g);
+      case 7: return group_persistent_t<7, false, 1>(g);
+      case 8: return group_persistent_t<8, false, 1>(g);
+      case 9: return group_persistent_t<9, false, 1>(g);
+      case 10: return group_persistent_t<10, false, 1>(g);
+    }
+  }
+  return fail(SALVUS_E_UNSUPPORTED, "no grouped step for order %d", m->order);
+}
+
+static int group_step(salvus_group *g) {
+  if (!g->stages) return group_persistent(g);
+  const int J = (int)g->members.size();
+  const int P = g->m0->P;
+  const GroupSlot *slots = g->d_slots.as<GroupSlot>();
+  int rc;
+  if ((rc = group_stiffness(g->m0, slots, J, g->n_stiff, g->stream))) return rc;
+  if (g->c == 1) group_source<1><<<J, 256, 0, g->stream>>>(slots, P);
+  else group_source<3><<<J, 256, 0, g->stream>>>(slots, P);
+  if (g->c == 1) group_gather_update<1><<<(unsigned)g->n_gather, 256, 0, g->stream>>>(slots, J);
+  else group_gather_update<3><<<(unsigned)g->n_gather, 256, 0, g->stream>>>(slots, J);
+  if (g->n_rec > 0) {
+    if (g->c == 1) group_receivers<1><<<(unsigned)g->n_rec, kRecThreads, 0, g->stream>>>(slots, J, P);
+    else group_receivers<3><<<(unsigned)g->n_rec, kRecThreads, 0, g->stream>>>(slots, J, P);
+  }
+  group_advance<<<1, 256, 0, g->stream>>>(slots, J);
+  g_launches += g->n_rec > 0 ? 4 : 3;
+  return check_launch("group step");
+}
+
 }  // namespace salvus
 
 using namespace salvus;
@@ -1507,3 +1750,126 @@ int salvus_profile_read(salvus_problem *p, int32_t max_entries, const char **nam
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// problem groups
+int salvus_group_create(salvus_problem *const *members, int32_t n, salvus_group **out) {
+  if (!members || !out || n < 1) return fail(SALVUS_E_INVALID, "empty group");
+  *out = nullptr;
+  const salvus_mesh *m0 = members[0] ? members[0]->mesh : nullptr;
+  if (!m0) return fail(SALVUS_E_INVALID, "null problem in group");
+  const bool quad_ac = m0->shape == SALVUS_QUAD && m0->physics == SALVUS_ACOUSTIC;
+  const bool hex_el = m0->shape == SALVUS_HEX && m0->physics == SALVUS_ELASTIC3D;
+  if (!quad_ac && !hex_el)
+    return fail(SALVUS_E_UNSUPPORTED, "groups are built for acoustic quads and elastic hexahedra");
+  for (int32_t k = 0; k < n; ++k) {
+    const salvus_problem *p = members[k];
+    if (!p) return fail(SALVUS_E_INVALID, "null problem in group");
+    const salvus_mesh *m = p->mesh;
+    if (p->prec != SALVUS_FP32 || p->shots != 1)
+      return fail(SALVUS_E_UNSUPPORTED, "group members must be FP32 single-shot problems");
+    if (m->shape != m0->shape || m->order != m0->order || m->physics != m0->physics ||
+        m->device != m0->device)
+      return fail(SALVUS_E_INVALID, "group members must share shape, order, physics and device");
+    for (int32_t q = 0; q < k; ++q)
+      if (members[q] == p) return fail(SALVUS_E_INVALID, "problem listed twice in a group");
+  }
+  std::unique_ptr<salvus_group> g(new salvus_group());
+  g->members.assign(members, members + n);
+  g->m0 = m0;
+  g->c = m0->physics == SALVUS_ELASTIC3D ? 3 : 1;
+  {
+    // measured: one launch per stage beats the single persistent work-queue
+    // launch (whose combined kernel runs the latency-bound gather at the
+    // occupancy of its heaviest body), so it is the default
+    const char *s = std::getenv("SALVUS_GROUP_STEP");
+    g->stages = !(s && std::strcmp(s, "persistent") == 0);
+  }
+  SALVUS_CUDA(cudaSetDevice(m0->device));
+  SALVUS_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  SALVUS_CUDA(cudaEventCreateWithFlags(&g->ev, cudaEventDisableTiming));
+  g->member_ev.resize(n, nullptr);
+  for (auto &e : g->member_ev) SALVUS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  *out = g.release();
+  return SALVUS_OK;
+}
+
+int salvus_group_run(salvus_group *g, int64_t n_steps) {
+  if (!g) return fail(SALVUS_E_INVALID, "null group");
+  if (n_steps < 0) return fail(SALVUS_E_INVALID, "negative step count");
+  SALVUS_CUDA(cudaSetDevice(g->m0->device));
+  // order the group after every member's pending work
+  for (size_t k = 0; k < g->members.size(); ++k) {
+    SALVUS_CUDA(cudaEventRecord(g->member_ev[k], g->members[k]->stream));
+    SALVUS_CUDA(cudaStreamWaitEvent(g->stream, g->member_ev[k], 0));
+  }
+  int rc = group_fill(g);
+  if (rc) return rc;
+  const int chunk = 32;
+  const int64_t sig[3] = {g->n_stiff, g->n_gather, g->n_rec};
+  if (g->graph && (sig[0] != g->sig[0] || sig[1] != g->sig[1] || sig[2] != g->sig[2])) {
+    cudaGraphExecDestroy(g->graph);
+    g->graph = nullptr;
+  }
+  if (!g->graph && n_steps >= chunk) {
+    cudaGraph_t graph;
+    SALVUS_CUDA(cudaStreamBeginCapture(g->stream, cudaStreamCaptureModeThreadLocal));
+    int crc = SALVUS_OK;
+    for (int s = 0; s < chunk && crc == SALVUS_OK; ++s) crc = group_step(g);
+    cudaError_t ce = cudaStreamEndCapture(g->stream, &graph);
+    if (crc) return crc;
+    if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&g->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+    g->graph_steps = chunk;
+    for (int a = 0; a < 3; ++a) g->sig[a] = sig[a];
+  }
+  int64_t done = 0;
+  while (g->graph && n_steps - done >= g->graph_steps) {
+    SALVUS_CUDA(cudaGraphLaunch(g->graph, g->stream));
+    g_launches += (int64_t)g->graph_steps * (g->n_rec > 0 ? 4 : 3);
+    done += g->graph_steps;
+  }
+  for (; done < n_steps; ++done)
+    if ((rc = group_step(g))) return rc;
+  for (auto *p : g->members) p->step += n_steps;
+  // members' later work waits for the group
+  SALVUS_CUDA(cudaEventRecord(g->ev, g->stream));
+  for (auto *p : g->members) SALVUS_CUDA(cudaStreamWaitEvent(p->stream, g->ev, 0));
+  return SALVUS_OK;
+}
+
+int salvus_group_synchronize(salvus_group *g) {
+  if (!g) return fail(SALVUS_E_INVALID, "null group");
+  SALVUS_CUDA(cudaSetDevice(g->m0->device));
+  SALVUS_CUDA(cudaStreamSynchronize(g->stream));
+  if (g->d_sync.ptr) {
+    GroupSync s{};
+    SALVUS_CUDA(cudaMemcpy(&s, g->d_sync.ptr, sizeof(s), cudaMemcpyDeviceToHost));
+    if (s.err) return fail(SALVUS_E_TIMEOUT, "a bounded wait of the grouped step gave up; results invalid");
+  }
+  for (auto *p : g->members)
+    if (int rc = device_status(p)) return rc;
+  return SALVUS_OK;
+}
+
+cudaStream_t salvus_group_stream_internal(const salvus_group *g) { return g ? g->stream : nullptr; }
+
+int salvus_group_destroy(salvus_group *g) {
+  if (!g) return SALVUS_OK;
+  cudaSetDevice(g->m0->device);
+  if (g->stream) cudaStreamSynchronize(g->stream);
+  if (g->graph) cudaGraphExecDestroy(g->graph);
+  for (auto e : g->member_ev)
+    if (e) cudaEventDestroy(e);
+  if (g->ev) cudaEventDestroy(g->ev);
+  g->d_slots.release();
+  g->d_counts.release();
+  g->d_work.release();
+  g->d_done.release();
+  g->d_sync.release();
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+  return SALVUS_OK;
+}

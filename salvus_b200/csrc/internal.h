@@ -77,6 +77,9 @@ int record_words(int shape, int physics, int fp64);
 
 }  // namespace salvus
 
+// stream of a problem group (server scheduling)
+cudaStream_t salvus_group_stream_internal(const salvus_group *g);
+
 struct salvus_mesh {
   int device = 0;
   int sm_count = 148;

@@ -46,7 +46,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 template <int N, int EPB_, bool kAsync>
-__device__ __forceinline__ void elastic_hex_v2_body(int64_t E, const float *__restrict__ rec,
+__device__ __forceinline__ void elastic_hex_v2_body(int64_t bid, int64_t E,
+                                                    const float *__restrict__ rec,
                                                     const float *__restrict__ u,
                                                     float *__restrict__ r, const DMatrix<float> &Dm) {
   using S = ElasticV2Shape<N, EPB_, kAsync>;
@@ -58,7 +59,7 @@ __device__ __forceinline__ void elastic_hex_v2_body(int64_t E, const float *__re
   const int t = threadIdx.x;
   const int le = t / n2, ij = t - le * n2;
   const int i = ij % n, j = ij / n;
-  const int64_t e = (int64_t)blockIdx.x * EPB + le;
+  const int64_t e = bid * EPB + le;
   const bool ok = le < EPB && e < E;
   float *su = smem_v2 + (size_t)(ok ? le : 0) * S::US;                      // [3][P]
   float *sF = smem_v2 + (size_t)EPB * S::US + (size_t)(ok ? le : 0) * S::FS;  // [3][2][P]
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, kAsync>::THREADS)
 elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
                                 const float *__restrict__ u, float *__restrict__ r,
                                 DMatrix<float> Dm) {
-  elastic_hex_v2_body<N, EPB_, kAsync>(E, rec, u, r, Dm);
+  elastic_hex_v2_body<N, EPB_, kAsync>(blockIdx.x, E, rec, u, r, Dm);
 }
 
 template <int N, int EPB_, int MINB>
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, false>::THREADS, MINB)
 elastic_hex_stiffness_v2m_kernel(int64_t E, const float *__restrict__ rec,
                                  const float *__restrict__ u, float *__restrict__ r,
                                  DMatrix<float> Dm) {
-  elastic_hex_v2_body<N, EPB_, false>(E, rec, u, r, Dm);
+  elastic_hex_v2_body<N, EPB_, false>(blockIdx.x, E, rec, u, r, Dm);
 }
 
 }  // namespace salvus

@@ -43,12 +43,12 @@ __device__ __forceinline__ void newmark_point(real an, real &ap, real &v, real &
 // mode 0: fused  a = mi * sum(r); Newmark update of (u, v, a_)
 // mode 1: gather a = sum(r)
 template <typename real, int C, int MODE>
-__global__ void gather_kernel(int64_t G, const int32_t *__restrict__ off,
-                              const int32_t *__restrict__ idx, const real *__restrict__ r,
-                              const real *__restrict__ mi, real *__restrict__ u,
-                              real *__restrict__ v, real *__restrict__ ap, real *__restrict__ a,
-                              real dt) {
-  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void gather_body(int64_t g, int64_t G, const int32_t *__restrict__ off,
+                                            const int32_t *__restrict__ idx,
+                                            const real *__restrict__ r,
+                                            const real *__restrict__ mi, real *__restrict__ u,
+                                            real *__restrict__ v, real *__restrict__ ap,
+                                            real *__restrict__ a, real dt) {
   if (g >= G) return;
   // Newmark operands first: they do not depend on the gather, so their loads
   // overlap the dependent index -> residual chain below.
@@ -106,6 +106,16 @@ __global__ void gather_kernel(int64_t G, const int32_t *__restrict__ off,
   }
 }
 
+template <typename real, int C, int MODE>
+__global__ void gather_kernel(int64_t G, const int32_t *__restrict__ off,
+                              const int32_t *__restrict__ idx, const real *__restrict__ r,
+                              const real *__restrict__ mi, real *__restrict__ u,
+                              real *__restrict__ v, real *__restrict__ ap, real *__restrict__ a,
+                              real dt) {
+  gather_body<real, C, MODE>((int64_t)blockIdx.x * blockDim.x + threadIdx.x, G, off, idx, r, mi, u,
+                             v, ap, a, dt);
+}
+
 template <typename real, int C>
 __global__ void inverse_mass_kernel(int64_t G, const real *__restrict__ mi, real *__restrict__ a) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -134,9 +144,11 @@ __device__ __forceinline__ double ricker_dev(double t, double f0, double t0, dou
 // Sources in attach order, one CTA; adds w_{p,c} * stf(t_n) into the
 // element-local residual of the source element.  src_par = [f0, t0, amp].
 template <typename real, int C>
-__global__ void source_kernel(int nsrc, int P, const int64_t *__restrict__ elem,
-                              const double *__restrict__ par, const double *__restrict__ wts,
-                              const int64_t *__restrict__ step, double dt, real *__restrict__ r) {
+__device__ __forceinline__ void source_body(int nsrc, int P, const int64_t *__restrict__ elem,
+                                            const double *__restrict__ par,
+                                            const double *__restrict__ wts,
+                                            const int64_t *__restrict__ step, double dt,
+                                            real *__restrict__ r) {
   const double t = (double)(*step) * dt;
   for (int s = 0; s < nsrc; ++s) {
     const double stf = ricker_dev(t, par[3 * s], par[3 * s + 1], par[3 * s + 2]);
@@ -147,23 +159,34 @@ __global__ void source_kernel(int nsrc, int P, const int64_t *__restrict__ elem,
   }
 }
 
+template <typename real, int C>
+__global__ void source_kernel(int nsrc, int P, const int64_t *__restrict__ elem,
+                              const double *__restrict__ par, const double *__restrict__ wts,
+                              const int64_t *__restrict__ step, double dt, real *__restrict__ r) {
+  source_body<real, C>(nsrc, P, elem, par, wts, step, dt, r);
+}
+
 // Receivers: one CTA per receiver, one thread per element point (strided);
 // each thread keeps a Kahan-compensated FP64 partial per component, then a
 // fixed-order tree combines the partials (deterministic).
 // seis[(rec*C + c)*cap + step % cap] = sum_p l_p u_p.
 constexpr int kRecThreads = 128;
 template <typename real, int C>
-__global__ void __launch_bounds__(kRecThreads)
-receiver_kernel(int P, const int64_t *__restrict__ elem, const double *__restrict__ lw,
-                const int32_t *__restrict__ conn, const real *__restrict__ u,
-                double *__restrict__ seis, int64_t cap, const int64_t *__restrict__ step) {
+__device__ __forceinline__ void receiver_body(int rc, int P, const int64_t *__restrict__ elem,
+                                              const double *__restrict__ lw,
+                                              const int32_t *__restrict__ conn,
+                                              const real *__restrict__ u,
+                                              double *__restrict__ seis, int64_t cap,
+                                              const int64_t *__restrict__ step) {
   __shared__ double part[C][kRecThreads];
-  const int rc = blockIdx.x, t = threadIdx.x;
+  // CTAs wider than kRecThreads (grouped persistent steps) keep their extra
+  // threads idle here but in every barrier
+  const int t = threadIdx.x;
   const int64_t e = elem[rc];
   double s[C], comp[C];
 #pragma unroll
   for (int c = 0; c < C; ++c) s[c] = comp[c] = 0.0;
-  for (int p = t; p < P; p += kRecThreads) {
+  for (int p = t; p < P && t < kRecThreads; p += kRecThreads) {
     const double l = lw[(int64_t)rc * P + p];
     const int64_t node = conn[e * P + p];
 #pragma unroll
@@ -174,8 +197,9 @@ receiver_kernel(int P, const int64_t *__restrict__ elem, const double *__restric
       s[c] = tt;
     }
   }
+  if (t < kRecThreads)
 #pragma unroll
-  for (int c = 0; c < C; ++c) part[c][t] = s[c];
+    for (int c = 0; c < C; ++c) part[c][t] = s[c];
   __syncthreads();
   for (int o = kRecThreads / 2; o > 0; o >>= 1) {
     if (t < o)
@@ -184,6 +208,14 @@ receiver_kernel(int P, const int64_t *__restrict__ elem, const double *__restric
     __syncthreads();
   }
   if (t < C) seis[((int64_t)rc * C + t) * cap + (*step % cap)] = part[t][0];
+}
+
+template <typename real, int C>
+__global__ void __launch_bounds__(kRecThreads)
+receiver_kernel(int P, const int64_t *__restrict__ elem, const double *__restrict__ lw,
+                const int32_t *__restrict__ conn, const real *__restrict__ u,
+                double *__restrict__ seis, int64_t cap, const int64_t *__restrict__ step) {
+  receiver_body<real, C>(blockIdx.x, P, elem, lw, conn, u, seis, cap, step);
 }
 
 // Advances the device step counter (one thread), after every kernel of the

@@ -63,10 +63,15 @@ __device__ __forceinline__ void load_acoustic_rec(const double *__restrict__ rec
   *node = conn[ep];
 }
 
+// bid: element-group index (the CTA index of a single-mesh launch; grouped
+// multi-mesh launches pass the CTA's index within its mesh).
 template <int DIM, int N, typename real>
-__global__ void __launch_bounds__(AcousticShape<DIM, N>::THREADS)
-acoustic_stiffness_kernel(int64_t E, const real *__restrict__ rec, const int32_t *__restrict__ conn,
-                          const real *__restrict__ u, real *__restrict__ r, DMatrix<real> Dm) {
+__device__ __forceinline__ void acoustic_stiffness_body(int64_t bid, int64_t E,
+                                                        const real *__restrict__ rec,
+                                                        const int32_t *__restrict__ conn,
+                                                        const real *__restrict__ u,
+                                                        real *__restrict__ r,
+                                                        const DMatrix<real> &Dm) {
   using S = AcousticShape<DIM, N>;
   constexpr int n = S::n, P = S::P, EPB = S::EPB, n2 = n * n;
   __shared__ real sD[n * n];
@@ -75,7 +80,7 @@ acoustic_stiffness_kernel(int64_t E, const real *__restrict__ rec, const int32_t
   const int t = threadIdx.x;
   const int le = t / P, p = t - le * P;
   if (t < n * n) sD[t] = Dm.d[t];
-  const int64_t e = (int64_t)blockIdx.x * EPB + le;
+  const int64_t e = bid * EPB + le;
   const bool ok = le < EPB && e < E;
   real g[S::NG];
   int32_t node = 0;
@@ -114,6 +119,13 @@ acoustic_stiffness_kernel(int64_t E, const real *__restrict__ rec, const int32_t
     }
     r[e * P + p] = -out;
   }
+}
+
+template <int DIM, int N, typename real>
+__global__ void __launch_bounds__(AcousticShape<DIM, N>::THREADS)
+acoustic_stiffness_kernel(int64_t E, const real *__restrict__ rec, const int32_t *__restrict__ conn,
+                          const real *__restrict__ u, real *__restrict__ r, DMatrix<real> Dm) {
+  acoustic_stiffness_body<DIM, N, real>(blockIdx.x, E, rec, conn, u, r, Dm);
 }
 
 // ---------------------------------------------------------------------------
