@@ -137,6 +137,12 @@ int salvus_mesh_connectivity(const salvus_mesh *mesh, int64_t *conn);
  * used by attachSource / attachReceiver.  Works on host-only meshes. */
 int salvus_mesh_locate_point(const salvus_mesh *mesh, const double *xyz, int64_t *element,
                              double *ref);
+/* Nodes on the outer boundary of the mesh (on element faces -- edges in
+ * 2-D -- that belong to one element), ascending global ids; nodes may be NULL
+ * to query the count: the point set Mesh::setupTopology collects from the
+ * side sets and their closures (Mesh.cpp:286-312) when every side of the
+ * mesh is in a side set. */
+int salvus_mesh_boundary_nodes(const salvus_mesh *mesh, int64_t *count, int64_t *nodes);
 /* Diagonal inverse mass [G] in FP64 (VecReciprocal, Order2Newmark.cpp:52). */
 int salvus_mesh_inverse_mass(const salvus_mesh *mesh, double *mi);
 /* Estimate lambda_max(M^-1 K) by power iteration on the GPU (FP64);
@@ -161,6 +167,12 @@ int salvus_problem_add_source(salvus_problem *p, const salvus_source *src);
  * taken after every step (FP64 sum of Lagrange-weighted nodes). */
 int salvus_problem_add_receiver(salvus_problem *p, const double *xyz);
 /* Capacity of the on-device seismogram ring, in steps (default 4096). */
+/* Homogeneous Dirichlet boundary (HomogeneousDirichlet.cpp:14-79): every
+ * element point on one of the listed global nodes has its stiffness row
+ * zeroed (the source term still acts there), as the reference's
+ * HomogeneousDirichlet mixin does for the DOFs on boundary vertices, edges and
+ * faces of its elements.  n = 0 clears.  Not for shot-batched problems. */
+int salvus_problem_set_dirichlet(salvus_problem *p, int64_t n, const int64_t *nodes);
 int salvus_problem_set_seismogram_capacity(salvus_problem *p, int64_t steps);
 /* Host <-> device field copies, [G][c] FP64 for one shot
  * (Problem::insertElementalFieldIntoMesh Problem.cpp:286-300,

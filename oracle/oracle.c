@@ -934,6 +934,7 @@ struct orc_problem {
   double *detJ, *invJ, *mat; /* mat: acoustic vp^2 [E][P]; elastic 9 c_ij [E][9][P] */
   double *mi;      /* [G] inverse diagonal mass */
   double *Ke;      /* triangles: dense element stiffness [E][P][P] */
+  char *dirichlet; /* [G] node flags (NULL: none) */
   double *u, *v, *a, *a_; /* [G][c] */
   int64_t step;
   /* colouring for threaded assembly */
@@ -1245,7 +1246,7 @@ orc_problem *orc_create(const orc_desc *d) {
 void orc_destroy(orc_problem *p) {
   if (!p) return;
   free(p->vtx); free(p->par); free(p->conn); free(p->xyz);
-  free(p->detJ); free(p->invJ); free(p->mat); free(p->mi); free(p->Ke);
+  free(p->detJ); free(p->invJ); free(p->mat); free(p->mi); free(p->Ke); free(p->dirichlet);
   free(p->u); free(p->v); free(p->a); free(p->a_);
   free(p->col_off); free(p->col_elems);
   for (int i = 0; i < p->nsrc; ++i) free(p->src[i].wts);
@@ -1357,6 +1358,27 @@ int orc_inverse_mass(const orc_problem *p, double *mi) {
   return 0;
 }
 
+int orc_set_dirichlet(orc_problem *p, int64_t n, const int64_t *nodes) {
+  free(p->dirichlet);
+  p->dirichlet = NULL;
+  if (n <= 0) return 0;
+  p->dirichlet = (char *)xcalloc((size_t)p->G, 1);
+  for (int64_t k = 0; k < n; ++k) {
+    if (nodes[k] < 0 || nodes[k] >= p->G) { set_err("node out of range"); return -1; }
+    p->dirichlet[nodes[k]] = 1;
+  }
+  return 0;
+}
+
+/* HomogeneousDirichlet::computeStiffnessTerm (HomogeneousDirichlet.cpp:65-73) */
+static void zero_dirichlet_rows(const orc_problem *p, int64_t e, double *ke) {
+  if (!p->dirichlet) return;
+  const int P = p->b.P, c = p->c;
+  for (int q = 0; q < P; ++q)
+    if (p->dirichlet[p->conn[e * P + q]])
+      for (int k = 0; k < c; ++k) ke[q * c + k] = 0.0;
+}
+
 /* a = f(t) - K u, assembled.  Problem::assembleIntoGlobalDof Problem.cpp:143-214. */
 static void assemble(orc_problem *p, const double *u, double t, double *a, int with_src) {
   const int P = p->b.P, c = p->c;
@@ -1368,6 +1390,7 @@ static void assemble(orc_problem *p, const double *u, double t, double *a, int w
       for (int q = 0; q < P; ++q)
         for (int k = 0; k < c; ++k) ue[q * c + k] = u[cn[q] * c + k];
       element_stiffness(p, e, ue, ke);
+      zero_dirichlet_rows(p, e, ke);
       for (int q = 0; q < P; ++q)
         for (int k = 0; k < c; ++k) a[cn[q] * c + k] += -ke[q * c + k];
     }
@@ -1380,6 +1403,7 @@ static void assemble(orc_problem *p, const double *u, double t, double *a, int w
       for (int q = 0; q < P; ++q)
         for (int k = 0; k < c; ++k) ue[q * c + k] = u[cn[q] * c + k];
       element_stiffness(p, e, ue, buf + e * P * c);
+      zero_dirichlet_rows(p, e, buf + e * P * c);
     }
     for (int64_t e = 0; e < p->E; ++e) {
       const int64_t *cn = p->conn + e * P;
@@ -1398,6 +1422,7 @@ static void assemble(orc_problem *p, const double *u, double t, double *a, int w
         for (int q = 0; q < P; ++q)
           for (int k = 0; k < c; ++k) ue[q * c + k] = u[cn[q] * c + k];
         element_stiffness(p, e, ue, ke);
+        zero_dirichlet_rows(p, e, ke);
         for (int q = 0; q < P; ++q)
           for (int k = 0; k < c; ++k) a[cn[q] * c + k] += -ke[q * c + k];
       }

@@ -113,6 +113,9 @@ int orc_node_coords(const orc_problem *p, double *xyz /* [G][dim] */);
 int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double amp,
                    int kind, const double *comp);
 int orc_add_receiver(orc_problem *p, const double *x);
+/* Homogeneous Dirichlet (HomogeneousDirichlet.cpp:65-73): zero the element
+ * stiffness rows of every element point on these nodes (oracle numbering). */
+int orc_set_dirichlet(orc_problem *p, int64_t n, const int64_t *nodes);
 /* which: 0 = u, 1 = v.  Arrays are [G][c]. */
 int orc_set_field(orc_problem *p, int which, const double *vals);
 int orc_get_field(const orc_problem *p, int which, double *vals);

@@ -51,6 +51,7 @@ def lib():
         L.orc_node_coords.argtypes = [ctypes.c_void_p, _DP]
         L.orc_add_source.argtypes = [ctypes.c_void_p, _DP, _D, _D, _D, ctypes.c_int, _DP]
         L.orc_add_receiver.argtypes = [ctypes.c_void_p, _DP]
+        L.orc_set_dirichlet.argtypes = [ctypes.c_void_p, _I64, ctypes.POINTER(_I64)]
         L.orc_set_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
         L.orc_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
         L.orc_inverse_mass.argtypes = [ctypes.c_void_p, _DP]
@@ -246,6 +247,10 @@ class Problem:
             raise RuntimeError(lib().orc_last_error().decode())
         self.nrec += 1
         return rc
+
+    def set_dirichlet(self, nodes):
+        nodes = np.ascontiguousarray(nodes, dtype=np.int64)
+        assert lib().orc_set_dirichlet(self.h, len(nodes), nodes.ctypes.data_as(ctypes.POINTER(_I64))) == 0
 
     def set_field(self, which, vals):
         vals = _c(vals).reshape(self.G, self.c)

@@ -64,6 +64,8 @@ SIGNATURES = [
     ("salvus_mesh_connectivity", ctypes.c_int, [_VP, ctypes.POINTER(_I64)]),
     ("salvus_mesh_locate_point", ctypes.c_int, [_VP, _DP, ctypes.POINTER(_I64), _DP]),
     ("salvus_mesh_inverse_mass", ctypes.c_int, [_VP, _DP]),
+    ("salvus_mesh_boundary_nodes", ctypes.c_int, [_VP, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
+    ("salvus_problem_set_dirichlet", ctypes.c_int, [_VP, _I64, ctypes.POINTER(_I64)]),
     ("salvus_mesh_max_eigenvalue", ctypes.c_int, [_VP, _I32, ctypes.c_uint64, _DP]),
     ("salvus_group_create", ctypes.c_int, [ctypes.POINTER(_VP), _I32, ctypes.POINTER(_VP)]),
     ("salvus_group_run", ctypes.c_int, [_VP, _I64]),
@@ -183,6 +185,15 @@ class Mesh:
         _check(lib().salvus_mesh_locate_point(self.h, _dp(x), ctypes.byref(e), _dp(r)))
         return e.value, r[: self.dim]
 
+    def boundary_nodes(self):
+        """Global ids of the nodes on the outer boundary (ascending)."""
+        n = _I64()
+        _check(lib().salvus_mesh_boundary_nodes(self.h, ctypes.byref(n), None))
+        out = np.zeros(n.value, dtype=np.int64)
+        _check(lib().salvus_mesh_boundary_nodes(self.h, ctypes.byref(n),
+                                                out.ctypes.data_as(ctypes.POINTER(_I64))))
+        return out
+
     def inverse_mass(self):
         m = np.zeros(self.n_nodes)
         _check(lib().salvus_mesh_inverse_mass(self.h, _dp(m)))
@@ -248,6 +259,12 @@ class Problem:
         x[: len(location)] = location
         _check(lib().salvus_problem_add_receiver(self.h, _dp(x)))
         self.n_receivers += 1
+
+    def set_dirichlet(self, nodes):
+        """Homogeneous Dirichlet on these global nodes (HomogeneousDirichlet)."""
+        nodes = np.ascontiguousarray(nodes, dtype=np.int64)
+        _check(lib().salvus_problem_set_dirichlet(self.h, len(nodes),
+                                                  nodes.ctypes.data_as(ctypes.POINTER(_I64))))
 
     def set_seismogram_capacity(self, steps):
         _check(lib().salvus_problem_set_seismogram_capacity(self.h, int(steps)))

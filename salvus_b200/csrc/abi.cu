@@ -30,6 +30,7 @@ namespace salvus {
 const char *last_error();
 int flatten_mesh(salvus_mesh *m, const int64_t *cells, int64_t n_vertices);
 int locate_point(const salvus_mesh *m, const double *x, int64_t *elem, double *ref);
+int boundary_nodes(const salvus_mesh *m, std::vector<int64_t> &out);
 
 static std::atomic<int64_t> g_launches{0};
 
@@ -525,6 +526,15 @@ static void drop_graph(salvus_problem *p) {
 }
 
 template <typename real, int C>
+static int launch_dirichlet(salvus_problem *p) {
+  if (p->n_dir_pts == 0) return SALVUS_OK;
+  dirichlet_zero_kernel<real, C><<<blocks_for(p->n_dir_pts, 256), 256, 0, p->stream>>>(
+      p->n_dir_pts, p->d_dir_pts.as<int32_t>(), F<real>(p->d_r));
+  g_launches++;
+  return check_launch("dirichlet");
+}
+
+template <typename real, int C>
 static int launch_sources(salvus_problem *p) {
   if (p->srcs.empty()) return SALVUS_OK;
   ProfScope ps(p, K_SRC);
@@ -570,6 +580,7 @@ static int step_fused_t(salvus_problem *p) {
                                        p->d_err.as<int>())))
       return rc;
   }
+  if ((rc = launch_dirichlet<real, C>(p))) return rc;
   if ((rc = launch_sources<real, C>(p))) return rc;
   {
     ProfScope ps(p, K_UPDATE);
@@ -792,6 +803,7 @@ static int assemble_t(salvus_problem *p) {
                                        p->d_err.as<int>())))
       return rc;
   }
+  if ((rc = launch_dirichlet<real, C>(p))) return rc;
   if ((rc = launch_sources<real, C>(p))) return rc;
   ProfScope ps(p, K_GATHER);
   gather_kernel<real, C, 1><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(
@@ -1768,6 +1780,8 @@ int salvus_group_create(salvus_problem *const *members, int32_t n, salvus_group 
     const salvus_mesh *m = p->mesh;
     if (p->prec != SALVUS_FP32 || p->shots != 1)
       return fail(SALVUS_E_UNSUPPORTED, "group members must be FP32 single-shot problems");
+    if (p->n_dir_pts > 0)
+      return fail(SALVUS_E_UNSUPPORTED, "group members cannot carry Dirichlet boundaries");
     if (m->shape != m0->shape || m->order != m0->order || m->physics != m0->physics ||
         m->device != m0->device)
       return fail(SALVUS_E_INVALID, "group members must share shape, order, physics and device");
@@ -1871,5 +1885,45 @@ int salvus_group_destroy(salvus_group *g) {
   g->d_sync.release();
   if (g->stream) cudaStreamDestroy(g->stream);
   delete g;
+  return SALVUS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// homogeneous Dirichlet boundaries
+int salvus_mesh_boundary_nodes(const salvus_mesh *m, int64_t *count, int64_t *nodes) {
+  if (!m || !count) return fail(SALVUS_E_INVALID, "null argument");
+  std::vector<int64_t> b;
+  int rc = boundary_nodes(m, b);
+  if (rc) return rc;
+  if (nodes) std::memcpy(nodes, b.data(), sizeof(int64_t) * b.size());
+  *count = (int64_t)b.size();
+  return SALVUS_OK;
+}
+
+int salvus_problem_set_dirichlet(salvus_problem *p, int64_t n, const int64_t *nodes) {
+  if (!p || (n > 0 && !nodes) || n < 0) return fail(SALVUS_E_INVALID, "bad arguments");
+  const salvus_mesh *m = p->mesh;
+  if (p->shots > 1)
+    return fail(SALVUS_E_UNSUPPORTED, "Dirichlet boundaries are not built for shot-batched problems");
+  std::vector<char> flag((size_t)m->G, 0);
+  for (int64_t k = 0; k < n; ++k) {
+    if (nodes[k] < 0 || nodes[k] >= m->G) return fail(SALVUS_E_INVALID, "node %lld out of range",
+                                                      (long long)nodes[k]);
+    flag[(size_t)nodes[k]] = 1;
+  }
+  // every element point on a flagged node, ascending (element, point)
+  std::vector<int32_t> pts;
+  for (int64_t i = 0; i < m->E * m->P; ++i)
+    if (flag[(size_t)m->conn[(size_t)i]]) pts.push_back((int32_t)i);
+  SALVUS_CUDA(cudaSetDevice(m->device));
+  if (!pts.empty()) {
+    int rc = p->d_dir_pts.alloc(sizeof(int32_t) * pts.size());
+    if (rc) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_dir_pts.ptr, pts.data(), sizeof(int32_t) * pts.size(),
+                                cudaMemcpyHostToDevice, p->stream));
+    SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  }
+  p->n_dir_pts = (int64_t)pts.size();
+  drop_graph(p);
   return SALVUS_OK;
 }

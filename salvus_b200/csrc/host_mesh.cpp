@@ -9,6 +9,7 @@
 // Shared entities are keyed topologically by global vertex ids, so the
 // numbering needs no coordinates and no tolerances.
 #include <algorithm>
+#include <cmath>
 #include <array>
 #include <cstring>
 #include <unordered_map>
@@ -198,6 +199,85 @@ int locate_point(const salvus_mesh *m, const double *x, int64_t *elem, double *r
   }
   return fail(SALVUS_E_NOT_FOUND, "point (%g, %g, %g) lies outside the mesh", x[0], x[1],
               dim == 3 ? x[2] : 0.0);
+}
+
+// Nodes on the outer boundary: element faces (edges in 2-D) that belong to a
+// single element, keyed by their sorted global vertex ids; a point lies on a
+// face when its P1 weights vanish on every vertex off the face.
+int boundary_nodes(const salvus_mesh *m, std::vector<int64_t> &out) {
+  const int nv = m->nv, P = m->P, dim = m->dim;
+  // faces of the reference element as vertex lists
+  std::vector<std::vector<int>> faces;
+  if (is_simplex(m->shape)) {
+    for (int opp = 0; opp < nv; ++opp) {
+      std::vector<int> f;
+      for (int v = 0; v < nv; ++v)
+        if (v != opp) f.push_back(v);
+      faces.push_back(f);
+    }
+  } else {
+    // vertex v lies on face (d, side) when its reference coordinate d is side
+    std::vector<std::array<double, 3>> vref(nv);
+    for (int v = 0; v < nv; ++v) {
+      // the vertex is the point where its own P1 weight is 1: probe corners
+      for (int c = 0; c < (1 << dim); ++c) {
+        double ref[3] = {0, 0, 0}, w[8];
+        for (int d = 0; d < dim; ++d) ref[d] = ((c >> d) & 1) ? 1.0 : -1.0;
+        p1_weights(m->shape, ref, w);
+        if (w[v] > 0.5) vref[v] = {ref[0], ref[1], ref[2]};
+      }
+    }
+    for (int d = 0; d < dim; ++d)
+      for (double side : {-1.0, 1.0}) {
+        std::vector<int> f;
+        for (int v = 0; v < nv; ++v)
+          if (vref[v][d] == side) f.push_back(v);
+        faces.push_back(f);
+      }
+  }
+  // local points of each face
+  std::vector<std::vector<int>> face_pts(faces.size());
+  for (size_t f = 0; f < faces.size(); ++f)
+    for (int q = 0; q < P; ++q) {
+      double ref[3], w[8];
+      point_ref(m->basis, q, ref);
+      p1_weights(m->shape, ref, w);
+      bool on = true;
+      for (int v = 0; v < nv && on; ++v)
+        if (std::find(faces[f].begin(), faces[f].end(), v) == faces[f].end() &&
+            std::fabs(w[v]) > 1e-12)
+          on = false;
+      if (on) face_pts[f].push_back(q);
+    }
+  // count faces by sorted global vertex keys (vertex ids read back from the
+  // connectivity of the element's vertex points)
+  std::vector<int> vpt(nv, -1);
+  for (int v = 0; v < nv; ++v)
+    for (int q = 0; q < P; ++q) {
+      double ref[3], w[8];
+      point_ref(m->basis, q, ref);
+      p1_weights(m->shape, ref, w);
+      if (std::fabs(w[v] - 1.0) < 1e-12) vpt[v] = q;
+    }
+  std::unordered_map<Key4, int, Key4Hash> count;
+  count.reserve((size_t)(m->E * faces.size()));
+  auto key_of = [&](int64_t e, const std::vector<int> &f) {
+    Key4 k{{-1, -1, -1, -1}};
+    for (size_t a = 0; a < f.size(); ++a) k.v[a] = m->conn[(size_t)(e * P + vpt[f[a]])];
+    std::sort(k.v.begin(), k.v.begin() + f.size());
+    return k;
+  };
+  for (int64_t e = 0; e < m->E; ++e)
+    for (auto &f : faces) count[key_of(e, f)]++;
+  std::vector<char> flag((size_t)m->G, 0);
+  for (int64_t e = 0; e < m->E; ++e)
+    for (size_t f = 0; f < faces.size(); ++f)
+      if (count[key_of(e, faces[f])] == 1)
+        for (int q : face_pts[f]) flag[(size_t)m->conn[(size_t)(e * P + q)]] = 1;
+  out.clear();
+  for (int64_t g = 0; g < m->G; ++g)
+    if (flag[(size_t)g]) out.push_back(g);
+  return SALVUS_OK;
 }
 
 }  // namespace salvus

@@ -118,6 +118,10 @@ struct salvus_problem {
   salvus::DeviceBuffer d_step;   // int64 device step counter
   salvus::DeviceBuffer d_stage;  // FP64 staging for host field copies
   salvus::DeviceBuffer d_err;    // int: device-side error word (bounded waits)
+  // homogeneous Dirichlet: element-local points (e*P + p) whose stiffness
+  // rows are zeroed
+  salvus::DeviceBuffer d_dir_pts;
+  int64_t n_dir_pts = 0;
   // sources (host mirror + device)
   struct Src {
     salvus_source desc;

@@ -116,6 +116,18 @@ __global__ void gather_kernel(int64_t G, const int32_t *__restrict__ off,
                              v, ap, a, dt);
 }
 
+// Homogeneous Dirichlet (HomogeneousDirichlet.cpp:65-73): zero the stiffness
+// rows of the listed element-local points (before sources are added).
+template <typename real, int C>
+__global__ void dirichlet_zero_kernel(int64_t n, const int32_t *__restrict__ pts,
+                                      real *__restrict__ r) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t ep = pts[i];
+#pragma unroll
+  for (int c = 0; c < C; ++c) r[ep * C + c] = real(0);
+}
+
 template <typename real, int C>
 __global__ void inverse_mass_kernel(int64_t G, const real *__restrict__ mi, real *__restrict__ a) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -212,3 +212,29 @@ def test_oracle_tet_elastic_energy_and_rigid_motion():
     dt = sc.oracle_dt(cfg, 0.3)
     p.run(50, dt)
     assert abs(p.energy() / e0 - 1) < 0.05
+
+
+@pytest.mark.parametrize("which", ["quad", "hex", "tri", "tet"])
+def test_boundary_nodes(which):
+    """Outer-boundary nodes: exactly the nodes on the box surface."""
+    if which == "quad":
+        V, C = meshgen.structured_quad(6, 5, 6e3, 5e3)
+        m = core.Mesh(core.QUAD, 4, core.ACOUSTIC, V, C, np.full((1, len(C), 4), 3e3), device=-1)
+        L = np.array([6e3, 5e3])
+    elif which == "hex":
+        V, C = meshgen.structured_hex(3, 4, 2, 3e3, 4e3, 2e3)
+        m = core.Mesh(core.HEX, 3, core.ACOUSTIC, V, C, np.full((1, len(C), 8), 3e3), device=-1)
+        L = np.array([3e3, 4e3, 2e3])
+    elif which == "tri":
+        cfg = sc.small_tri()
+        m = core.Mesh(core.TRI, 3, core.ACOUSTIC, cfg["vertices"], cfg["cells"], cfg["params"], device=-1)
+        L = np.array([2e4, 1e4])
+    else:
+        cfg = sc.small_tet(core.ACOUSTIC)
+        m = core.Mesh(core.TET, 3, core.ACOUSTIC, cfg["vertices"], cfg["cells"], cfg["params"], device=-1)
+        L = np.array([1e4] * 3)
+    X = m.node_coords()
+    tol = 1e-9 * L.max()
+    on_box = np.any((np.abs(X) < tol) | (np.abs(X - L) < tol), axis=1)
+    b = m.boundary_nodes()
+    assert np.array_equal(np.sort(b), np.flatnonzero(on_box))
