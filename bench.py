@@ -40,6 +40,11 @@ def parse():
     ap.add_argument("--no-shots", action="store_true", help="skip the batched-shots leg")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-simplex", action="store_true", help="skip the P3 simplex leg")
+    ap.add_argument("--no-elastic2d", action="store_true", help="skip the 2-D elastic quad leg")
+    ap.add_argument("--elastic2d-only", action="store_true",
+                    help="run only the 2-D elastic quad leg (profiling)")
+    ap.add_argument("--e2d-nel", type=int, default=720,
+                    help="2-D elastic leg: nel x nel quads (default 720, ~8.3M nodes)")
     ap.add_argument("--simplex-only", action="store_true",
                     help="run only the P3 simplex leg (profiling / quick checks)")
     ap.add_argument("--tet-n", type=int, default=55,
@@ -237,6 +242,53 @@ def simplex_leg(core, configs, timed, steps, device=0, tet_n=55):
     return out
 
 
+def elastic2d_leg(core, configs, timed, steps, device=0, nel=720, peak=None):
+    """2-D elastic quads (Elastic2D physics, SURVEY next row): FP32, order 4,
+    nel^2 distorted-free structured quads over 10 x 10 km, 5 % GRF, weak VTI
+    anisotropy, moment-tensor + force Ricker sources, 16 receivers.  Timed as
+    graph-replayed steps; the stiffness kernel per launch against HBM."""
+    cfg = configs.elastic_2d(nel=nel, order=4)
+    mesh = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                     cfg["params"], device=device)
+    dt = 0.4 * mesh.critical_dt(iterations=40)
+    p = core.Problem(mesh, core.FP32, dt=dt)
+    for s in cfg["sources"]:
+        if "moment_tensor" in s:
+            p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                         moment_tensor=s["moment_tensor"])
+        else:
+            p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                         direction=s["direction"])
+    for r in cfg["receivers"]:
+        p.add_receiver(r)
+    p.set_seismogram_capacity(steps + 64)
+    p.run(5, core.RUN_GRAPH)
+    p.synchronize()
+    ms = timed(p, lambda: p.run(steps, core.RUN_GRAPH))
+    p.profile(True)
+    p.run(min(steps, 50), core.RUN_PLAIN)
+    prof = p.profile_read()
+    p.profile(False)
+    G, E, P = mesh.n_nodes, mesh.n_elements, mesh.points_per_element
+    k_ms, k_n = prof.get("stiffness", (0.0, 1))
+    st_ms = k_ms / max(k_n, 1)
+    # algorithmic bytes per stiffness launch: per point 32 B record (invJ 4,
+    # C11 C13 C33 C55 x w detJ) + 4 B connectivity + 8 B residual write, plus
+    # the compulsory u read of 8 B per node
+    b_stiff = E * P * (32 + 4 + 8) + G * 8
+    ach = b_stiff / (st_ms / 1e3) / 1e9 if st_ms > 0 else None
+    out = {"elements": E, "nodes": G, "components": 2, "dt": dt, "steps": steps,
+           "value": G * steps / (ms / 1e3), "unit": METRIC, "ms_per_step": ms / steps,
+           "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
+           "roofline": {"bound": "hbm", "kernel": "elastic2d_stiffness", "achieved": ach,
+                        "peak": peak, "unit": "GB/s",
+                        "frac": (ach / peak) if (ach and peak) else None,
+                        "algorithmic_bytes": b_stiff}}
+    p.close()
+    mesh.close()
+    return out
+
+
 def unit_dt(core, meshgen, kind, order=4):
     """Critical step of a unit mesh (h = 1, vp_max = 1) for this element
     family; dt_crit(h, vp) = unit_dt * h / vp (lambda_max scales as (vp/h)^2)."""
@@ -369,7 +421,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    if args.simplex_only:
+    if args.simplex_only or args.elastic2d_only:
         def timed_simple(prob, fn):
             stream = torch.cuda.ExternalStream(prob.stream_handle())
             torch.cuda.synchronize()
@@ -379,10 +431,16 @@ def main():
             b.record(stream)
             torch.cuda.synchronize()
             return a.elapsed_time(b)
-        out = simplex_leg(core, configs, timed_simple, steps=args.steps, device=local,
-                          tet_n=args.tet_n)
+        if args.elastic2d_only:
+            peaks = measured_peaks()
+            out = {"elastic2d": elastic2d_leg(core, configs, timed_simple, steps=args.steps,
+                                              device=local, nel=args.e2d_nel,
+                                              peak=peaks["hbm_gbs"] if peaks else 6650.0)}
+        else:
+            out = {"simplices": simplex_leg(core, configs, timed_simple, steps=args.steps,
+                                            device=local, tet_n=args.tet_n)}
         if rank == 0:
-            print(json.dumps({"simplices": out}), flush=True)
+            print(json.dumps(out), flush=True)
         return
 
     cfg = configs.elastic_hex(nel=args.nel, order=args.order)
@@ -509,6 +567,11 @@ def main():
         simplex = simplex_leg(core, configs, timed_on, steps=min(args.steps, 200), device=local,
                               tet_n=args.tet_n)
 
+    e2d = None
+    if not args.no_elastic2d:
+        e2d = elastic2d_leg(core, configs, timed_on, steps=min(args.steps, 300), device=local,
+                            nel=args.e2d_nel, peak=peak)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         rate, thr, sample, _ = cpu_leg(args, min(args.nel, 32), None, 1)
@@ -541,6 +604,7 @@ def main():
             "shots_batched": shots,
             "serving": serve,
             "simplices": simplex,
+            "elastic2d": e2d,
         }
         print(json.dumps(line), flush=True)
     if dist:

@@ -39,7 +39,7 @@ extern "C" {
 #define SALVUS_E_NOT_FOUND (-8)   /* source / receiver outside the mesh */
 
 enum salvus_shape { SALVUS_QUAD = 0, SALVUS_HEX = 1, SALVUS_TRI = 2, SALVUS_TET = 3 };
-enum salvus_physics { SALVUS_ACOUSTIC = 0, SALVUS_ELASTIC3D = 1 };
+enum salvus_physics { SALVUS_ACOUSTIC = 0, SALVUS_ELASTIC3D = 1, SALVUS_ELASTIC2D = 2 };
 enum salvus_precision { SALVUS_FP32 = 0, SALVUS_FP64 = 1 };
 enum salvus_field { SALVUS_FIELD_U = 0, SALVUS_FIELD_V = 1, SALVUS_FIELD_A = 2,
                     SALVUS_FIELD_A_PREV = 3 };
@@ -57,11 +57,14 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  *   tet  v0 -> (0,0,0), v1 -> (0,1,0), v2 -> (1,0,0), v3 -> (0,0,1) with
  *        det[v2-v0; v1-v0; v3-v0] > 0                     (TetP1.cpp:91-150)
  * Simplices are the P3 mass-lumped elements (12-node triangle, 50-node
- * tetrahedron; order must be 3); elastic3d runs on hexahedra and tetrahedra. 
+ * tetrahedron; order must be 3); elastic3d runs on hexahedra and tetrahedra,
+ * elastic2d on quadrilaterals.
  * params are per element, per element vertex (Exodus NAME_0..NAME_k):
  *   acoustic : [1][n_elements][nv]  VP                    (Scalar.cpp:23-25)
  *   elastic3d: [3][n_elements][nv]  RHO, VP, VS  (isotropic form of
- *              Elastic3D.cpp:33-54 with VPV=VPH=VP, VSV=VSH=VS, ETA=1) */
+ *              Elastic3D.cpp:33-54 with VPV=VPH=VP, VSV=VSH=VS, ETA=1)
+ *   elastic2d: [5][n_elements][4]   RHO, C11, C13, C33, C55
+ *              (Elastic2D.cpp:29-37; fields ux, uy) */
 /* salvus_mesh_desc.flags: build only the FP32 stiffness records (halves the
  * per-mesh geometry memory; FP64 problems and the FP64 eigenvalue estimate
  * are then unavailable on that mesh). */
@@ -80,9 +83,11 @@ typedef struct {
 } salvus_mesh_desc;
 
 /* One Ricker point source (Ricker::fire, Ricker.cpp:27-33; Source.h:75).
- * FORCE: comp[0..c-1] is the direction (c = 1 acoustic, 3 elastic).
+ * FORCE: comp[0..c-1] is the direction (c = 1 acoustic, 2 elastic 2-D,
+ * 3 elastic 3-D).
  * MOMENT_TENSOR (elastic only, no reference counterpart): comp = [Mxx, Myy,
- * Mzz, Myz, Mxz, Mxy]; nodal force f_{i,a} = sum_b M_ab dphi_i/dx_b (x_s). */
+ * Mzz, Myz, Mxz, Mxy] in 3-D, [Mxx, Myy, Mxy] in 2-D; nodal force
+ * f_{i,a} = sum_b M_ab dphi_i/dx_b (x_s). */
 typedef struct {
   double location[3];
   double center_freq;

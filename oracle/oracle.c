@@ -1040,8 +1040,16 @@ static void colour_elements(orc_problem *p) {
   free(fill); free(col); free(mask);
 }
 
+/* Material words per GLL point: acoustic vp^2; elastic 3-D 9 c_ij;
+ * elastic 2-D c11 c13 c33 c55. */
+static int mat_words(int physics) {
+  return physics == ORC_ACOUSTIC ? 1 : (physics == ORC_ELASTIC2D ? 4 : 9);
+}
+
 /* Material at GLL points of element e: acoustic vp^2 (Scalar.cpp:45);
- * elastic c_ij (Elastic3D.cpp:42-53, c11 c12 c13 c22 c23 c33 c44 c55 c66). */
+ * elastic c_ij (Elastic3D.cpp:42-53, c11 c12 c13 c22 c23 c33 c44 c55 c66);
+ * elastic 2-D C11 C13 C33 C55 (Elastic2D.cpp:57-60; its c13 / c23 slots stay
+ * zero, Elastic2D.cpp:16-21,55-56). */
 static void element_material(const orc_problem *p, int64_t e, double *m, double *rho) {
   const basis_t *b = &p->b;
   const int P = b->P, nv = b->nv;
@@ -1051,6 +1059,11 @@ static void element_material(const orc_problem *p, int64_t e, double *m, double 
   if (p->d.physics == ORC_ACOUSTIC) {
     for (int q = 0; q < P; ++q) m[q] = pow(tmp[0][q], 2);
     if (rho) for (int q = 0; q < P; ++q) rho[q] = 1.0;
+  } else if (p->d.physics == ORC_ELASTIC2D) {
+    for (int q = 0; q < P; ++q) {
+      for (int k = 0; k < 4; ++k) m[k * P + q] = tmp[k + 1][q];
+      if (rho) rho[q] = tmp[0][q];
+    }
   } else {
     for (int q = 0; q < P; ++q) {
       double r = tmp[0][q], vpv = tmp[1][q], vph = tmp[2][q], vsv = tmp[3][q], vsh = tmp[4][q],
@@ -1080,8 +1093,9 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
   if (faithful) {
     element_geometry(b, vtx, fl, detJ_l, invJ_l);
     detJ = detJ_l; invJ = invJ_l;
-    if (p->d.physics == ORC_ACOUSTIC) {
-      /* Scalar::computeStress re-interpolates VP every call (Scalar.cpp:45) */
+    if (p->d.physics != ORC_ELASTIC3D) {
+      /* Scalar::computeStress / Elastic2D::computeStress re-interpolate the
+       * material every call (Scalar.cpp:45, Elastic2D.cpp:57-60) */
       element_material(p, e, mat_l, NULL);
       mat = mat_l;
     } else {
@@ -1091,7 +1105,7 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
   } else {
     detJ = p->detJ + e * P;
     invJ = p->invJ + e * P * d * d;
-    mat = p->mat + e * P * (p->d.physics == ORC_ACOUSTIC ? 1 : 9);
+    mat = p->mat + e * P * mat_words(p->d.physics);
   }
   if (b->shape == ORC_TRI) {
     /* ScalarTri::computeStiffnessTerm ScalarTri.cpp:12-17: K_e u_e */
@@ -1114,6 +1128,37 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
       if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l); /* Hexahedra.cpp:702 */
       grad_test_from_geom(b, detJ, invJ, g, ke);
     }
+    return;
+  }
+  if (p->d.physics == ORC_ELASTIC2D) {
+    /* Elastic2D::computeStiffnessTerm Elastic2D.cpp:84-107: strain
+     * (ux_x, ux_y, uy_x, uy_y), stress Elastic2D.cpp:62-78 */
+    double ux[ORC_MAX_P] = {0}, uy[ORC_MAX_P] = {0}, gx[ORC_MAX_P * 2], gy[ORC_MAX_P * 2];
+    for (int q = 0; q < P; ++q) { ux[q] = ue[q * 2]; uy[q] = ue[q * 2 + 1]; }
+    grad_from_geom(b, invJ, ux, gx);
+    if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+    grad_from_geom(b, invJ, uy, gy);
+    double fx[ORC_MAX_P * 2], fy[ORC_MAX_P * 2];
+    for (int q = 0; q < P; ++q) {
+      const double exx = gx[q * 2 + 0], eyy = gy[q * 2 + 1];
+      const double exy = gx[q * 2 + 1] + gy[q * 2 + 0];
+      const double c11 = mat[0 * P + q], c13 = mat[1 * P + q], c33 = mat[2 * P + q],
+                   c55 = mat[3 * P + q];
+      const double sxx = c11 * exx + c13 * eyy, syy = c13 * exx + c33 * eyy, sxy = c55 * exy;
+      fx[q * 2 + 0] = sxx; fx[q * 2 + 1] = sxy;
+      fy[q * 2 + 0] = sxy; fy[q * 2 + 1] = syy;
+    }
+    double kx[ORC_MAX_P], ky[ORC_MAX_P];
+    if (fl & ORC_Q3_QUAD_INVJ_AT_OUTPUT) {
+      grad_test_quad_literal(b, vtx, fl, detJ, fx, kx);
+      grad_test_quad_literal(b, vtx, fl, detJ, fy, ky);
+    } else {
+      if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+      grad_test_from_geom(b, detJ, invJ, fx, kx);
+      if (faithful) element_geometry(b, vtx, fl, detJ_l, invJ_l);
+      grad_test_from_geom(b, detJ, invJ, fy, ky);
+    }
+    for (int q = 0; q < P; ++q) { ke[q * 2] = kx[q]; ke[q * 2 + 1] = ky[q]; }
     return;
   }
   /* elastic 3-D */
@@ -1158,14 +1203,19 @@ orc_problem *orc_create(const orc_desc *d) {
     set_err("elastic 3-D physics needs hexahedra or tetrahedra");
     return NULL;
   }
+  if (d->physics == ORC_ELASTIC2D && d->shape != ORC_QUAD) {
+    set_err("elastic 2-D physics needs quadrilaterals");
+    return NULL;
+  }
+  if (d->physics < ORC_ACOUSTIC || d->physics > ORC_ELASTIC2D) { set_err("bad physics"); return NULL; }
   orc_problem *p = (orc_problem *)xcalloc(1, sizeof(orc_problem));
   p->d = *d;
   if (p->d.threads < 1) p->d.threads = 1;
   if (basis_init(&p->b, d->shape, d->order)) { free(p); return NULL; }
   const basis_t *b = &p->b;
   const int dim = b->dim, nv = b->nv, P = b->P;
-  p->c = d->physics == ORC_ACOUSTIC ? 1 : 3;
-  p->npar = d->physics == ORC_ACOUSTIC ? 1 : 6;
+  p->c = d->physics == ORC_ACOUSTIC ? 1 : (d->physics == ORC_ELASTIC2D ? 2 : 3);
+  p->npar = d->physics == ORC_ACOUSTIC ? 1 : (d->physics == ORC_ELASTIC2D ? 5 : 6);
   p->E = d->n_elements;
   p->vtx = (double *)xcalloc((size_t)(p->E * nv * dim), sizeof(double));
   for (int64_t e = 0; e < p->E; ++e)
@@ -1186,7 +1236,7 @@ orc_problem *orc_create(const orc_desc *d) {
   /* simplices: vertex valences exceed the 64-colour mask; their threaded
    * assembly buffers element results and scatters them in element order */
   if (!is_simplex(d->shape)) colour_elements(p);
-  const int nm = d->physics == ORC_ACOUSTIC ? 1 : 9;
+  const int nm = mat_words(d->physics);
   const int faithful = (d->flags & ORC_FAITHFUL_RECOMPUTE) != 0;
   if (!faithful) {
     p->detJ = (double *)xcalloc((size_t)(p->E * P), sizeof(double));
@@ -1283,7 +1333,7 @@ int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double
                    int kind, const double *comp) {
   const basis_t *b = &p->b;
   const int P = b->P, c = p->c, d = b->dim;
-  if (kind == 1 && p->d.physics != ORC_ELASTIC3D) { set_err("moment tensor needs elastic physics"); return -1; }
+  if (kind == 1 && p->d.physics == ORC_ACOUSTIC) { set_err("moment tensor needs elastic physics"); return -1; }
   double ref[3] = {0, 0, 0};
   int64_t e = locate(p, x, ref);
   if (e < 0) return -1;
@@ -1306,22 +1356,30 @@ int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double
       for (int a = 0; a < c; ++a)
         s->wts[q * c + a] = (scale ? integ[q] : delta[q]) * comp[a];
   } else {
-    /* moment tensor: f_{q,a} = sum_b M_ab dphi_q/dx_b (x_s) */
+    /* moment tensor: f_{q,a} = sum_b M_ab dphi_q/dx_b (x_s);
+     * 3-D comp = [Mxx Myy Mzz Myz Mxz Mxy], 2-D comp = [Mxx Myy Mxy] */
     double l[ORC_MAX_P], dl[ORC_MAX_P * 3], det, iJ[9];
     tensor_lagrange(b, ref, l, dl);
     orc_p1_jacobian(b->shape, vtx, ref, p->d.flags, &det, iJ);
-    const double M[3][3] = {{comp[0], comp[5], comp[4]},
-                            {comp[5], comp[1], comp[3]},
-                            {comp[4], comp[3], comp[2]}};
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (d == 2) {
+      M[0][0] = comp[0]; M[1][1] = comp[1]; M[0][1] = M[1][0] = comp[2];
+    } else {
+      M[0][0] = comp[0]; M[1][1] = comp[1]; M[2][2] = comp[2];
+      M[1][2] = M[2][1] = comp[3]; M[0][2] = M[2][0] = comp[4]; M[0][1] = M[1][0] = comp[5];
+    }
     for (int q = 0; q < P; ++q) {
-      double gx[3];
-      for (int a = 0; a < 3; ++a) {
+      double gx[3] = {0, 0, 0};
+      for (int a = 0; a < d; ++a) {
         double sacc = 0;
-        for (int k = 0; k < 3; ++k) sacc += iJ[a * 3 + k] * dl[q * 3 + k];
+        for (int k = 0; k < d; ++k) sacc += iJ[a * d + k] * dl[q * d + k];
         gx[a] = sacc;
       }
-      for (int a = 0; a < 3; ++a)
-        s->wts[q * 3 + a] = M[a][0] * gx[0] + M[a][1] * gx[1] + M[a][2] * gx[2];
+      for (int a = 0; a < d; ++a) {
+        double f = 0;
+        for (int k = 0; k < d; ++k) f += M[a][k] * gx[k];
+        s->wts[q * d + a] = f;
+      }
     }
   }
   return p->nsrc++;
@@ -1454,14 +1512,15 @@ int orc_run(orc_problem *p, int64_t nsteps, double dt, double *seis) {
   const int64_t G = p->G;
   const double acl = 0.5 * dt, dsp = 0.5 * dt * dt;
   /* components advanced by takeTimeStep: Order2Newmark.cpp:93-96 lists
-   * {"ax","ay","ax","a"}; corrected mode advances each component once. */
+   * {"ax","ay","ax","a"} (2-D and 3-D elastic: x twice, z never);
+   * corrected mode advances each component once. */
   int comps[4], ncomp = 0;
   if (c == 1) {
     comps[ncomp++] = 0;
   } else if (p->d.flags & ORC_Q1_Z_NOT_ADVANCED) {
     comps[ncomp++] = 0; comps[ncomp++] = 1; comps[ncomp++] = 0;
   } else {
-    comps[ncomp++] = 0; comps[ncomp++] = 1; comps[ncomp++] = 2;
+    for (int k = 0; k < c; ++k) comps[ncomp++] = k;
   }
   for (int64_t n = 0; n < nsteps; ++n) {
     const double t = (double)p->step * dt; /* integer step count (quirk Q11) */

@@ -21,7 +21,8 @@ extern "C" {
 /* ORC_TRI / ORC_TET: the P3 mass-lumped simplices (12-node triangle,
  * 50-node tetrahedron) of Triangle.cpp / Tetrahedra.cpp, order 3 only. */
 enum { ORC_QUAD = 0, ORC_HEX = 1, ORC_TRI = 2, ORC_TET = 3 };
-enum { ORC_ACOUSTIC = 0, ORC_ELASTIC3D = 1 };
+/* ORC_ELASTIC2D: Elastic2D on quads (Elastic2D.cpp:29-127). */
+enum { ORC_ACOUSTIC = 0, ORC_ELASTIC3D = 1, ORC_ELASTIC2D = 2 };
 
 /* Reference quirk switches ("reference-literal" mode).  The default (0) is the
  * corrected physics that the GPU path is checked against. */
@@ -55,7 +56,8 @@ typedef struct {
   /* Per element, per element-vertex material (ExodusModel NAME_0..NAME_k
    * convention, ExodusModel.cpp:455-470):
    *   acoustic: [1][n_elements][nv] = VP
-   *   elastic : [6][n_elements][nv] = RHO, VPV, VPH, VSV, VSH, ETA */
+   *   elastic : [6][n_elements][nv] = RHO, VPV, VPH, VSV, VSH, ETA
+   *   elastic2d: [5][n_elements][nv] = RHO, C11, C13, C33, C55 */
   const double *params;
   unsigned flags;
   int threads;              /* OpenMP threads for element loops (>=1) */
@@ -109,7 +111,8 @@ int64_t orc_num_nodes(const orc_problem *p);
 int orc_num_components(const orc_problem *p);
 int orc_node_coords(const orc_problem *p, double *xyz /* [G][dim] */);
 /* kind 0: force, comp = direction [c]; kind 1: moment tensor
- * comp = [Mxx, Myy, Mzz, Myz, Mxz, Mxy]. Returns source index or <0. */
+ * comp = [Mxx, Myy, Mzz, Myz, Mxz, Mxy] (3-D) or [Mxx, Myy, Mxy] (2-D).
+ * Returns source index or <0. */
 int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double amp,
                    int kind, const double *comp);
 int orc_add_receiver(orc_problem *p, const double *x);

@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
 QUAD, HEX, TRI, TET = 0, 1, 2, 3
-ACOUSTIC, ELASTIC3D = 0, 1
+ACOUSTIC, ELASTIC3D, ELASTIC2D = 0, 1, 2
 Q1_Z_NOT_ADVANCED = 1 << 0
 Q2_ELASTIC_SRC_UNSCALED = 1 << 1
 Q3_QUAD_INVJ_AT_OUTPUT = 1 << 2

@@ -7,7 +7,7 @@ that tests can run the same physics at reduced size.
 import numpy as np
 
 from . import meshgen
-from .core import ACOUSTIC, ELASTIC3D, HEX, QUAD, TET, TRI
+from .core import ACOUSTIC, ELASTIC2D, ELASTIC3D, HEX, QUAD, TET, TRI
 
 
 def standing_wave_2d(nel=40, order=4, L=1.0e4, vp=4000.0):
@@ -124,6 +124,40 @@ def serving_stream(n_jobs, seed=4, quad_edges=(50, 400), hex_edges=(16, 48), ste
     return out
 
 
+def elastic_2d(nel=200, order=4, L=1.0e4, vp=4000.0, vs=2300.0, rho=2500.0, eps=0.1, std=0.05,
+               corr=800.0, f0=2.0, n_receivers=16, jitter=0.0, seed=5):
+    """2-D elastic quads (Elastic2D physics) on an L x L square: Gaussian
+    random-field perturbation of vp, vs and rho, weak VTI anisotropy
+    C11 = (1 + 2 eps) C33, C33 = rho vp^2, C55 = rho vs^2, C13 = C33 - 2 C55;
+    a seeded moment-tensor source and a vertical force near the centre,
+    receivers on a seeded ring.  jitter moves interior vertices by up to
+    jitter * h (general quadrilaterals)."""
+    V, C = meshgen.structured_quad(nel, nel, L, L)
+    h = L / nel
+    rng = np.random.default_rng(seed)
+    if jitter > 0:
+        inner = np.all((V > 0.5 * h) & (V < L - 0.5 * h), axis=1)
+        V = V.copy()
+        V[inner] += rng.uniform(-jitter * h, jitter * h, size=(inner.sum(), 2))
+    grf = meshgen.gaussian_random_field((nel + 1, nel + 1), h, corr, seed).ravel()
+    pert = 1.0 + std * grf
+    rv, pv, sv = rho * pert, vp * pert, vs * pert
+    c33 = rv * pv * pv
+    c55 = rv * sv * sv
+    c11 = (1.0 + 2.0 * eps) * c33
+    c13 = c33 - 2.0 * c55
+    params = np.stack([meshgen.per_element_vertex(x, C) for x in (rv, c11, c13, c33, c55)])
+    center = (L / 2 + 0.31 * h, L / 2 - 0.17 * h)
+    mt = rng.standard_normal(3)
+    return dict(shape=QUAD, order=order, physics=ELASTIC2D, vertices=V, cells=C, params=params,
+                L=L, vp=vp, vs=vs,
+                sources=[dict(location=center, center_freq=f0, time_delay=1.2 / f0, amplitude=1.0e10,
+                              moment_tensor=mt),
+                         dict(location=(L / 2 - 1.3 * h, L / 2 + 0.6 * h), center_freq=f0,
+                              time_delay=1.4 / f0, amplitude=1.0e9, direction=[0.0, 1.0])],
+                receivers=meshgen.ring_positions((L / 2, L / 2), 0.3 * L, n_receivers, seed))
+
+
 def simplex_tri(nx=448, ny=224, lx=2.0e4, ly=1.0e4, vp=4000.0, std=0.05, corr=1000.0, f0=1.0,
                 n_receivers=16, seed=3):
     """2-D acoustic P3 triangles: seeded Delaunay mesh of a jittered
@@ -172,7 +206,7 @@ def simplex_tet(n=55, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700
 def oracle_params(cfg):
     """Parameter array in the oracle's layout (elastic: RHO VPV VPH VSV VSH ETA)."""
     p = cfg["params"]
-    if cfg["physics"] == ACOUSTIC:
+    if cfg["physics"] in (ACOUSTIC, ELASTIC2D):
         return p
     rho, vp, vs = p
     return np.stack([rho, vp, vp, vs, vs, np.ones_like(rho)])

@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsalvus_b200.so")
 
 QUAD, HEX, TRI, TET = 0, 1, 2, 3
-ACOUSTIC, ELASTIC3D = 0, 1
+ACOUSTIC, ELASTIC3D, ELASTIC2D = 0, 1, 2
 FP32, FP64 = 0, 1
 FIELD_U, FIELD_V, FIELD_A, FIELD_A_PREV = 0, 1, 2, 3
 FORCE, MOMENT_TENSOR = 0, 1
@@ -247,7 +247,8 @@ class Problem:
         s.shot = shot
         if moment_tensor is not None:
             s.kind = MOMENT_TENSOR
-            s.comp[:] = list(moment_tensor)
+            mt = [float(x) for x in moment_tensor]
+            s.comp[:] = mt + [0.0] * (6 - len(mt))
         else:
             s.kind = FORCE
             d = [1.0] if direction is None else list(np.atleast_1d(direction))

@@ -22,6 +22,7 @@
 #include "kernels_simplex.cuh"
 #include "kernels_simplex_tc.cuh"
 #include "kernels_group.cuh"
+#include "kernels_elastic2d.cuh"
 #include <algorithm>
 #include <cstdlib>
 #include <type_traits>
@@ -73,6 +74,18 @@ static int check_launch(const char *what) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(SALVUS_E_CUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
   return SALVUS_OK;
+}
+
+// Calls fn(std::integral_constant<int, C>) for the field's component count
+// (1 acoustic, 2 elastic 2-D, 3 elastic 3-D).
+template <typename Fn>
+static int by_components(int c, Fn &&fn) {
+  switch (c) {
+    case 1: return fn(std::integral_constant<int, 1>{});
+    case 2: return fn(std::integral_constant<int, 2>{});
+    case 3: return fn(std::integral_constant<int, 3>{});
+  }
+  return fail(SALVUS_E_UNSUPPORTED, "no kernels for %d field components", c);
 }
 
 // ---------------------------------------------------------------------------
@@ -218,6 +231,13 @@ static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, 
 
 template <int N, typename real>
 static int acoustic2(const salvus_mesh *m, const real *rec, const real *u, real *r, cudaStream_t s) {
+  if (m->physics == SALVUS_ELASTIC2D) {
+    using S = Elastic2DShape<N>;
+    elastic2d_stiffness_kernel<N, real, 2, 0><<<blocks_for(m->E, S::EPB), S::THREADS, 0, s>>>(
+        m->E, nullptr, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
+    g_launches++;
+    return check_launch("elastic 2-D stiffness");
+  }
   return launch_acoustic<2, N, real>(m, rec, u, r, s);
 }
 template <int N, typename real>
@@ -789,8 +809,10 @@ static int step_batched(salvus_problem *p) {
 
 static int step_fused(salvus_problem *p) {
   if (p->shots > 1) return step_batched(p);
-  if (p->prec == SALVUS_FP32) return p->c == 1 ? step_fused_t<float, 1>(p) : step_fused_t<float, 3>(p);
-  return p->c == 1 ? step_fused_t<double, 1>(p) : step_fused_t<double, 3>(p);
+  return by_components(p->c, [&](auto cc) {
+    constexpr int C = decltype(cc)::value;
+    return p->prec == SALVUS_FP32 ? step_fused_t<float, C>(p) : step_fused_t<double, C>(p);
+  });
 }
 
 template <typename real, int C>
@@ -844,16 +866,13 @@ static int apply_stiffness_into_t(const salvus_mesh *m, const real *rec, const r
                                   real *scratch, cudaStream_t st) {
   int rc = launch_stiffness<real>(m, rec, u, scratch, st, nullptr);
   if (rc) return rc;
-  if (m->c == 1)
-    gather_kernel<real, 1, 1><<<blocks_for(m->G, 256), 256, 0, st>>>(
+  return by_components(m->c, [&](auto cc) {
+    gather_kernel<real, decltype(cc)::value, 1><<<blocks_for(m->G, 256), 256, 0, st>>>(
         m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), scratch, nullptr, nullptr,
         nullptr, nullptr, a, (real)0);
-  else
-    gather_kernel<real, 3, 1><<<blocks_for(m->G, 256), 256, 0, st>>>(
-        m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), scratch, nullptr, nullptr,
-        nullptr, nullptr, a, (real)0);
-  g_launches++;
-  return check_launch("allocation-free gather");
+    g_launches++;
+    return check_launch("allocation-free gather");
+  });
 }
 
 int apply_stiffness_into(const salvus_mesh *m, int precision, const void *u, void *a,
@@ -1176,7 +1195,10 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
     return fail(SALVUS_E_UNSUPPORTED, "unknown element shape %d", d->shape);
   if (d->physics == SALVUS_ELASTIC3D && d->shape != SALVUS_HEX && d->shape != SALVUS_TET)
     return fail(SALVUS_E_UNSUPPORTED, "elastic 3-D physics needs hexahedra or tetrahedra");
-  if (d->physics != SALVUS_ACOUSTIC && d->physics != SALVUS_ELASTIC3D)
+  if (d->physics == SALVUS_ELASTIC2D && d->shape != SALVUS_QUAD)
+    return fail(SALVUS_E_UNSUPPORTED, "elastic 2-D physics needs quadrilaterals");
+  if (d->physics != SALVUS_ACOUSTIC && d->physics != SALVUS_ELASTIC3D &&
+      d->physics != SALVUS_ELASTIC2D)
     return fail(SALVUS_E_INVALID, "unknown physics %d", d->physics);
   if (d->n_elements <= 0 || d->n_vertices <= 0 || !d->vertices || !d->cells || !d->params)
     return fail(SALVUS_E_INVALID, "empty mesh");
@@ -1198,8 +1220,8 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
   m->nv = m->basis.nv;
   m->n = m->basis.n;
   m->P = m->basis.P;
-  m->c = d->physics == SALVUS_ELASTIC3D ? 3 : 1;
-  m->npar = d->physics == SALVUS_ELASTIC3D ? 3 : 1;
+  m->c = physics_components(d->physics);
+  m->npar = physics_params(d->physics);
   m->E = d->n_elements;
   m->vtx.resize((size_t)(m->E * m->nv * m->dim));
   for (int64_t e = 0; e < m->E; ++e)
@@ -1327,22 +1349,16 @@ int salvus_mesh_max_eigenvalue(salvus_mesh *m, int32_t iters, uint64_t seed, dou
                                        m->stream)))
       return rc;
     // y = -gather(r) = K x ; then M^-1
-    if (m->c == 1)
-      gather_kernel<double, 1, 1><<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
+    by_components(m->c, [&](auto cc) {
+      constexpr int C = decltype(cc)::value;
+      gather_kernel<double, C, 1><<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
           m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), r.as<double>(), nullptr,
           nullptr, nullptr, nullptr, y.as<double>(), 0.0);
-    else
-      gather_kernel<double, 3, 1><<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
-          m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), r.as<double>(), nullptr,
-          nullptr, nullptr, nullptr, y.as<double>(), 0.0);
-    g_launches++;
-    if (m->c == 1)
-      inverse_mass_kernel<double, 1><<<blocks_for(N, 256), 256, 0, m->stream>>>(
+      inverse_mass_kernel<double, C><<<blocks_for(N, 256), 256, 0, m->stream>>>(
           m->G, m->d_mi64.as<double>(), y.as<double>());
-    else
-      inverse_mass_kernel<double, 3><<<blocks_for(N, 256), 256, 0, m->stream>>>(
-          m->G, m->d_mi64.as<double>(), y.as<double>());
-    g_launches++;
+      return SALVUS_OK;
+    });
+    g_launches += 2;
     scale_kernel<double><<<blocks_for(N, 256), 256, 0, m->stream>>>(N, y.as<double>(), -1.0);
     g_launches++;
     double xy, xx, yy;
@@ -1432,7 +1448,7 @@ int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
   const salvus_mesh *m = p->mesh;
   if (s->shot < 0 || s->shot >= p->shots)
     return fail(SALVUS_E_INVALID, "shot index %d out of range", s->shot);
-  if (s->kind == SALVUS_SOURCE_MOMENT_TENSOR && m->physics != SALVUS_ELASTIC3D)
+  if (s->kind == SALVUS_SOURCE_MOMENT_TENSOR && m->physics == SALVUS_ACOUSTIC)
     return fail(SALVUS_E_INVALID, "moment-tensor sources need elastic physics");
   if (s->kind != SALVUS_SOURCE_FORCE && s->kind != SALVUS_SOURCE_MOMENT_TENSOR)
     return fail(SALVUS_E_INVALID, "unknown source kind %d", s->kind);
@@ -1450,17 +1466,28 @@ int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
     for (int q = 0; q < P; ++q)
       for (int a = 0; a < c; ++a) src.wts[(size_t)q * c + a] = phi[q] * s->comp[a];
   } else {
+    // 3-D comp = [Mxx Myy Mzz Myz Mxz Mxy]; 2-D comp = [Mxx Myy Mxy]
+    const int d = m->dim;
     double det, iJ[9];
-    p1_jacobian(m->shape, m->vtx.data() + src.elem * m->nv * 3, src.ref, &det, iJ);
-    const double M[3][3] = {{s->comp[0], s->comp[5], s->comp[4]},
-                            {s->comp[5], s->comp[1], s->comp[3]},
-                            {s->comp[4], s->comp[3], s->comp[2]}};
+    p1_jacobian(m->shape, m->vtx.data() + src.elem * m->nv * d, src.ref, &det, iJ);
+    double M[3][3] = {{s->comp[0], s->comp[5], s->comp[4]},
+                      {s->comp[5], s->comp[1], s->comp[3]},
+                      {s->comp[4], s->comp[3], s->comp[2]}};
+    if (d == 2) {
+      M[0][0] = s->comp[0];
+      M[1][1] = s->comp[1];
+      M[0][1] = M[1][0] = s->comp[2];
+    }
     for (int q = 0; q < P; ++q) {
       const double *gref = &dphi[(size_t)q * 3];
-      double gx[3];
-      for (int a = 0; a < 3; ++a) gx[a] = iJ[a * 3] * gref[0] + iJ[a * 3 + 1] * gref[1] + iJ[a * 3 + 2] * gref[2];
-      for (int a = 0; a < 3; ++a)
-        src.wts[(size_t)q * 3 + a] = M[a][0] * gx[0] + M[a][1] * gx[1] + M[a][2] * gx[2];
+      double gx[3] = {0, 0, 0};
+      for (int a = 0; a < d; ++a)
+        for (int k = 0; k < d; ++k) gx[a] += iJ[a * d + k] * gref[k];
+      for (int a = 0; a < d; ++a) {
+        double f = 0;
+        for (int k = 0; k < d; ++k) f += M[a][k] * gx[k];
+        src.wts[(size_t)q * d + a] = f;
+      }
     }
   }
   p->srcs.push_back(std::move(src));
@@ -1586,8 +1613,10 @@ int salvus_assemble(salvus_problem *p) {
   rc = ready(p);
   if (rc) return rc;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
-  if (p->prec == SALVUS_FP32) return p->c == 1 ? assemble_t<float, 1>(p) : assemble_t<float, 3>(p);
-  return p->c == 1 ? assemble_t<double, 1>(p) : assemble_t<double, 3>(p);
+  return by_components(p->c, [&](auto cc) {
+    constexpr int C = decltype(cc)::value;
+    return p->prec == SALVUS_FP32 ? assemble_t<float, C>(p) : assemble_t<double, C>(p);
+  });
 }
 
 int salvus_apply_inverse_mass(salvus_problem *p) {
@@ -1596,8 +1625,10 @@ int salvus_apply_inverse_mass(salvus_problem *p) {
   rc = ready(p);
   if (rc) return rc;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
-  if (p->prec == SALVUS_FP32) return p->c == 1 ? minv_t<float, 1>(p) : minv_t<float, 3>(p);
-  return p->c == 1 ? minv_t<double, 1>(p) : minv_t<double, 3>(p);
+  return by_components(p->c, [&](auto cc) {
+    constexpr int C = decltype(cc)::value;
+    return p->prec == SALVUS_FP32 ? minv_t<float, C>(p) : minv_t<double, C>(p);
+  });
 }
 
 int salvus_take_time_step(salvus_problem *p) {
@@ -1606,8 +1637,10 @@ int salvus_take_time_step(salvus_problem *p) {
   rc = ready(p);
   if (rc) return rc;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
-  if (p->prec == SALVUS_FP32) rc = p->c == 1 ? newmark_t<float, 1>(p) : newmark_t<float, 3>(p);
-  else rc = p->c == 1 ? newmark_t<double, 1>(p) : newmark_t<double, 3>(p);
+  rc = by_components(p->c, [&](auto cc) {
+    constexpr int C = decltype(cc)::value;
+    return p->prec == SALVUS_FP32 ? newmark_t<float, C>(p) : newmark_t<double, C>(p);
+  });
   if (rc == SALVUS_OK) p->step++;
   return rc;
 }

@@ -61,6 +61,13 @@ inline int shape_nv(int shape) {
   return shape == SALVUS_QUAD ? 4 : shape == SALVUS_HEX ? 8 : shape == SALVUS_TRI ? 3 : 4;
 }
 inline bool is_simplex(int shape) { return shape == SALVUS_TRI || shape == SALVUS_TET; }
+// field components per node and material parameters per element vertex
+inline int physics_components(int physics) {
+  return physics == SALVUS_ELASTIC3D ? 3 : (physics == SALVUS_ELASTIC2D ? 2 : 1);
+}
+inline int physics_params(int physics) {
+  return physics == SALVUS_ELASTIC3D ? 3 : (physics == SALVUS_ELASTIC2D ? 5 : 1);
+}
 
 struct DeviceBuffer {
   void *ptr = nullptr;

@@ -113,6 +113,24 @@ __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, i
   p1_jac_dev(dim, v, ref, &detJ, iJ);
   const double wd = wq * detJ;
   real *out = rec + tid * rw;
+  if (physics == 2) {
+    // elastic 2-D quads: RHO, C11, C13, C33, C55 at the point (Elastic2D.cpp:29-37,
+    // 57-60); record invJ (4 words) and C * w detJ (4 words), FP32 as two
+    // float4 planes [E][2][P] (kernels_elastic2d.cuh), FP64 as [E][P][8]
+    double cp[5];
+    for (int k = 0; k < 5; ++k) {
+      double vals[4];
+      for (int a = 0; a < 4; ++a) vals[a] = par[((int64_t)k * E + e) * 4 + a];
+      cp[k] = p1_interp_dev(2, vals, ref);
+    }
+    double w8[8] = {iJ[0], iJ[1], iJ[2], iJ[3], wd * cp[1], wd * cp[2], wd * cp[3], wd * cp[4]};
+    for (int a = 0; a < 8; ++a) {
+      if constexpr (kPackConn) rec[((e * 2 + a / 4) * P + p) * 4 + a % 4] = (real)w8[a];
+      else out[a] = (real)w8[a];
+    }
+    mass_local[tid] = wd * cp[0];  // Elastic2D mass: rho (Elastic2D.cpp:45-50)
+    return;
+  }
   if (physics == 0) {
     double vals[8];
     for (int a = 0; a < nv; ++a) vals[a] = par[e * nv + a];

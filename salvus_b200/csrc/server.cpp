@@ -68,7 +68,7 @@ int64_t estimate_bytes(const salvus_mesh_desc &d, int precision) {
   const int dim = d.shape == SALVUS_QUAD ? 2 : 3;
   const int64_t n = d.order + 1;
   const int64_t P = dim == 2 ? n * n : n * n * n;
-  const int64_t c = d.physics == SALVUS_ELASTIC3D ? 3 : 1;
+  const int64_t c = salvus::physics_components(d.physics);
   const int64_t E = d.n_elements;
   int64_t G = E;
   for (int k = 0; k < dim; ++k) G *= d.order;
@@ -320,7 +320,7 @@ int salvus_server_submit(salvus_server *s, const salvus_job_desc *d, int64_t *jo
   std::unique_ptr<Job> j(new Job());
   j->mesh = m;
   const int dim = m.shape == SALVUS_QUAD ? 2 : 3, nv = m.shape == SALVUS_QUAD ? 4 : 8;
-  const int npar = m.physics == SALVUS_ELASTIC3D ? 3 : 1;
+  const int npar = salvus::physics_params(m.physics);
   j->vertices.assign(m.vertices, m.vertices + m.n_vertices * dim);
   j->cells.assign(m.cells, m.cells + m.n_elements * nv);
   j->params.assign(m.params, m.params + (size_t)npar * m.n_elements * nv);

@@ -88,3 +88,21 @@ def test_tet_acoustic_dirichlet_tensor_cores():
     # rounding (Vandermonde inverse), unlike the tensor Lagrange factors
     assert np.abs(s_g[0]).max() <= 1e-12 * np.abs(s_g[1:]).max()
     assert sc.rel_l2(s_g[1:], s_o[1:]) <= 1e-4
+
+
+@pytest.mark.parametrize("precision,tol", [(core.FP64, 1e-10), (core.FP32, 1e-4)])
+def test_elastic2d_dirichlet(precision, tol):
+    """HomogeneousDirichlet<Elastic2D<TensorQuad<QuadP1>>> (HomogeneousDirichlet.cpp:118-121)"""
+    cfg = configs.elastic_2d(nel=12, order=4, n_receivers=6)
+    dt = oracle_dt(cfg)
+    mesh, prob, orc, idx = build_pair(cfg, precision, dt)
+    b = with_dirichlet(mesh, prob, orc, idx)
+    n = 600
+    prob.set_seismogram_capacity(n)
+    prob.run(n)
+    s_o = orc.run(n, dt)
+    assert np.abs(s_o).max() > 0
+    assert rel_l2(prob.seismograms(), s_o) <= tol
+    u = prob.get_field("u")
+    assert np.abs(u[b]).max() == 0.0
+    assert rel_l2(u, orc.get_field("u")[idx]) <= tol
