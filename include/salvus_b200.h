@@ -39,7 +39,8 @@ extern "C" {
 #define SALVUS_E_NOT_FOUND (-8)   /* source / receiver outside the mesh */
 
 enum salvus_shape { SALVUS_QUAD = 0, SALVUS_HEX = 1, SALVUS_TRI = 2, SALVUS_TET = 3 };
-enum salvus_physics { SALVUS_ACOUSTIC = 0, SALVUS_ELASTIC3D = 1, SALVUS_ELASTIC2D = 2 };
+enum salvus_physics { SALVUS_ACOUSTIC = 0, SALVUS_ELASTIC3D = 1, SALVUS_ELASTIC2D = 2,
+                      SALVUS_COUPLED2D = 3 };
 enum salvus_precision { SALVUS_FP32 = 0, SALVUS_FP64 = 1 };
 enum salvus_field { SALVUS_FIELD_U = 0, SALVUS_FIELD_V = 1, SALVUS_FIELD_A = 2,
                     SALVUS_FIELD_A_PREV = 3 };
@@ -64,7 +65,16 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  *   elastic3d: [3][n_elements][nv]  RHO, VP, VS  (isotropic form of
  *              Elastic3D.cpp:33-54 with VPV=VPH=VP, VSV=VSH=VS, ETA=1)
  *   elastic2d: [5][n_elements][4]   RHO, C11, C13, C33, C55
- *              (Elastic2D.cpp:29-37; fields ux, uy) */
+ *              (Elastic2D.cpp:29-37; fields ux, uy)
+ *   coupled2d: [7][n_elements][4]   FLUID, VP, RHO, C11, C13, C33, C55:
+ *              quadrilaterals of both kinds in one mesh, FLUID = 1 (same at
+ *              all four vertices) marks a fluid element (Scalar physics on
+ *              VP; RHO feeds the coupling), 0 a solid one (Elastic2D); fields
+ *              per node [u, ux, uy].  Neighbours of the other kind couple
+ *              through the ElasticToAcoustic2D / AcousticToElastic2D surface
+ *              integrals (ElasticToAcoustic.cpp:17-41,
+ *              AcousticToElastic2D.cpp:18-60) and share the reference's
+ *              single summed mass (Order2Newmark.cpp:38-52). */
 /* salvus_mesh_desc.flags: build only the FP32 stiffness records (halves the
  * per-mesh geometry memory; FP64 problems and the FP64 eigenvalue estimate
  * are then unavailable on that mesh). */
@@ -84,9 +94,11 @@ typedef struct {
 
 /* One Ricker point source (Ricker::fire, Ricker.cpp:27-33; Source.h:75).
  * FORCE: comp[0..c-1] is the direction (c = 1 acoustic, 2 elastic 2-D,
- * 3 elastic 3-D).
+ * 3 elastic 3-D; coupled2d: [fluid, x, y], of which the owning element's
+ * components act).
  * MOMENT_TENSOR (elastic only, no reference counterpart): comp = [Mxx, Myy,
- * Mzz, Myz, Mxz, Mxy] in 3-D, [Mxx, Myy, Mxy] in 2-D; nodal force
+ * Mzz, Myz, Mxz, Mxy] in 3-D, [Mxx, Myy, Mxy] in 2-D (solid elements of
+ * coupled2d meshes only); nodal force
  * f_{i,a} = sum_b M_ab dphi_i/dx_b (x_s). */
 typedef struct {
   double location[3];

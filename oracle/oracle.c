@@ -921,6 +921,15 @@ typedef struct {
   double *l; /* [P] Lagrange weights */
 } rec_t;
 
+/* One edge point of a fluid-solid coupling surface integral. kind 0: fluid
+ * element point, a_u += cx vx + cy vy; kind 1: solid element point,
+ * a_ux += cx v, a_uy += cy v (v: the fluid velocity field). */
+typedef struct {
+  int64_t e;
+  int q, kind;
+  double cx, cy;
+} cpl_t;
+
 struct orc_problem {
   orc_desc d;
   basis_t b;
@@ -932,9 +941,12 @@ struct orc_problem {
   double *xyz;     /* [G][dim] */
   /* cached per-point data (not used in faithful mode) */
   double *detJ, *invJ, *mat; /* mat: acoustic vp^2 [E][P]; elastic 9 c_ij [E][9][P] */
-  double *mi;      /* [G] inverse diagonal mass */
+  double *mi;      /* [G][c] inverse diagonal mass per component (0: none) */
   double *Ke;      /* triangles: dense element stiffness [E][P][P] */
   char *dirichlet; /* [G] node flags (NULL: none) */
+  char *fluid;     /* coupled meshes: [E] 1 for fluid elements */
+  cpl_t *cpl;      /* coupled meshes: edge-point coupling terms, element order */
+  int64_t ncpl;
   double *u, *v, *a, *a_; /* [G][c] */
   int64_t step;
   /* colouring for threaded assembly */
@@ -1043,7 +1055,15 @@ static void colour_elements(orc_problem *p) {
 /* Material words per GLL point: acoustic vp^2; elastic 3-D 9 c_ij;
  * elastic 2-D c11 c13 c33 c55. */
 static int mat_words(int physics) {
-  return physics == ORC_ACOUSTIC ? 1 : (physics == ORC_ELASTIC2D ? 4 : 9);
+  return physics == ORC_ACOUSTIC ? 1 : (physics == ORC_ELASTIC3D ? 9 : 4);
+}
+
+/* Physics of element e: coupled meshes hold fluid (Scalar) and solid
+ * (Elastic2D) elements, chosen per element by the model's fluid flag
+ * (ExodusModel::getElementType ExodusModel.cpp:473-520). */
+static int elem_physics(const orc_problem *p, int64_t e) {
+  if (p->d.physics != ORC_COUPLED2D) return p->d.physics;
+  return p->fluid[e] ? ORC_ACOUSTIC : ORC_ELASTIC2D;
 }
 
 /* Material at GLL points of element e: acoustic vp^2 (Scalar.cpp:45);
@@ -1053,10 +1073,22 @@ static int mat_words(int physics) {
 static void element_material(const orc_problem *p, int64_t e, double *m, double *rho) {
   const basis_t *b = &p->b;
   const int P = b->P, nv = b->nv;
-  double tmp[6][ORC_MAX_P];
+  double tmp[8][ORC_MAX_P];
   for (int k = 0; k < p->npar; ++k)
     orc_element_par(b->shape, b->n - 1, p->par + ((size_t)k * p->E + e) * nv, tmp[k]);
-  if (p->d.physics == ORC_ACOUSTIC) {
+  if (p->d.physics == ORC_COUPLED2D) {
+    /* FLUID VP RHO C11 C13 C33 C55 */
+    for (int q = 0; q < P; ++q) {
+      if (p->fluid[e]) {
+        m[q] = pow(tmp[1][q], 2);
+        for (int k = 1; k < 4; ++k) m[k * P + q] = 0.0;
+        if (rho) rho[q] = 1.0;
+      } else {
+        for (int k = 0; k < 4; ++k) m[k * P + q] = tmp[k + 3][q];
+        if (rho) rho[q] = tmp[2][q];
+      }
+    }
+  } else if (p->d.physics == ORC_ACOUSTIC) {
     for (int q = 0; q < P; ++q) m[q] = pow(tmp[0][q], 2);
     if (rho) for (int q = 0; q < P; ++q) rho[q] = 1.0;
   } else if (p->d.physics == ORC_ELASTIC2D) {
@@ -1082,7 +1114,8 @@ static void element_material(const orc_problem *p, int64_t e, double *m, double 
 /* Element stiffness K_e u_e, [P][c] in and out.
  * Scalar::computeStiffnessTerm Scalar.cpp:58-71 / computeStress :42-55;
  * Elastic3D::computeStiffnessTerm Elastic3D.cpp:70-103 / computeStress :106-118. */
-static void element_stiffness(const orc_problem *p, int64_t e, const double *ue, double *ke) {
+static void element_stiffness_phys(const orc_problem *p, int64_t e, int phys, const double *ue,
+                                   double *ke) {
   const basis_t *b = &p->b;
   const int P = b->P, d = b->dim;
   const unsigned fl = p->d.flags;
@@ -1117,7 +1150,7 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
     }
     return;
   }
-  if (p->d.physics == ORC_ACOUSTIC) {
+  if (phys == ORC_ACOUSTIC) {
     double g[ORC_MAX_P * 3];
     grad_from_geom(b, invJ, ue, g);
     for (int q = 0; q < P; ++q)
@@ -1130,7 +1163,7 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
     }
     return;
   }
-  if (p->d.physics == ORC_ELASTIC2D) {
+  if (phys == ORC_ELASTIC2D) {
     /* Elastic2D::computeStiffnessTerm Elastic2D.cpp:84-107: strain
      * (ux_x, ux_y, uy_x, uy_y), stress Elastic2D.cpp:62-78 */
     double ux[ORC_MAX_P] = {0}, uy[ORC_MAX_P] = {0}, gx[ORC_MAX_P * 2], gy[ORC_MAX_P * 2];
@@ -1197,17 +1230,127 @@ static void element_stiffness(const orc_problem *p, int64_t e, const double *ue,
   for (int q = 0; q < P; ++q) { ke[q * 3] = kx[q]; ke[q * 3 + 1] = ky[q]; ke[q * 3 + 2] = kz[q]; }
 }
 
+/* Coupled meshes: the element's own physics on its components of [u, ux, uy]
+ * (fluid: u; solid: ux, uy); the others stay zero. */
+static void element_stiffness(const orc_problem *p, int64_t e, const double *ue, double *ke) {
+  if (p->d.physics != ORC_COUPLED2D) {
+    element_stiffness_phys(p, e, p->d.physics, ue, ke);
+    return;
+  }
+  const int P = p->b.P;
+  double us[ORC_MAX_P * 2] = {0}, ks[ORC_MAX_P * 2];
+  for (int i = 0; i < P * 3; ++i) ke[i] = 0.0;
+  if (p->fluid[e]) {
+    for (int q = 0; q < P; ++q) us[q] = ue[q * 3];
+    element_stiffness_phys(p, e, ORC_ACOUSTIC, us, ks);
+    for (int q = 0; q < P; ++q) ke[q * 3] = ks[q];
+  } else {
+    for (int q = 0; q < P; ++q) { us[q * 2] = ue[q * 3 + 1]; us[q * 2 + 1] = ue[q * 3 + 2]; }
+    element_stiffness_phys(p, e, ORC_ELASTIC2D, us, ks);
+    for (int q = 0; q < P; ++q) { ke[q * 3 + 1] = ks[q * 2]; ke[q * 3 + 2] = ks[q * 2 + 1]; }
+  }
+}
+
+typedef struct { int64_t a, b, e; int i; } edge_t;
+static int edge_cmp(const void *x, const void *y) {
+  const edge_t *p = (const edge_t *)x, *q = (const edge_t *)y;
+  if (p->a != q->a) return p->a < q->a ? -1 : 1;
+  if (p->b != q->b) return p->b < q->b ? -1 : 1;
+  return p->e < q->e ? -1 : (p->e > q->e);
+}
+
+/* Coupling surface integrals of the fluid-solid interface, per element in
+ * element order, per local edge i (vertex i -> i+1, TensorQuad.cpp:476-516:
+ * edge "Jacobian" |v_{i+1} - v_i| / 2, GLL weights along the edge, outward
+ * normal (dy, -dx) / |.| of TensorQuad::getEdgeNormal TensorQuad.cpp:400-418).
+ * Elements couple when an edge neighbour has the other physics
+ * (Mesh::CouplingFields Mesh.cpp:480-503 via TotalCouplingFields).
+ *   fluid element (ElasticToAcoustic.cpp:17-41): a_u += int phi (v_s . n_f)
+ *     on every edge with a neighbour (K3: solid neighbours only; K4: times
+ *     vp^2 at the point, the natural boundary term of int vp^2 grad . grad);
+ *   solid element (AcousticToElastic2D.cpp:18-60): a_ux, a_uy -= rho0 int
+ *     phi v on edges with a fluid neighbour, rho0 = mean vertex RHO of that
+ *     neighbour (AcousticToElastic2D.cpp:33-46); K2: -rho0 int phi v n_f,a
+ *     = rho0 int phi v n_s,a. */
+static void build_coupling(orc_problem *p) {
+  const int n = p->b.n, E4 = (int)(p->E * 4);
+  edge_t *ed = (edge_t *)xcalloc((size_t)E4, sizeof(edge_t));
+  for (int64_t e = 0; e < p->E; ++e)
+    for (int i = 0; i < 4; ++i) {
+      int64_t va = p->d.cells[e * 4 + i], vb = p->d.cells[e * 4 + (i + 1) % 4];
+      edge_t *x = &ed[e * 4 + i];
+      x->a = va < vb ? va : vb; x->b = va < vb ? vb : va; x->e = e; x->i = i;
+    }
+  qsort(ed, (size_t)E4, sizeof(edge_t), edge_cmp);
+  int64_t *nbr = (int64_t *)xcalloc((size_t)E4, sizeof(int64_t));
+  for (int k = 0; k < E4; ++k) nbr[ed[k].e * 4 + ed[k].i] = -1;
+  for (int k = 0; k + 1 < E4; ++k)
+    if (ed[k].a == ed[k + 1].a && ed[k].b == ed[k + 1].b) {
+      nbr[ed[k].e * 4 + ed[k].i] = ed[k + 1].e;
+      nbr[ed[k + 1].e * 4 + ed[k + 1].i] = ed[k].e;
+    }
+  free(ed);
+  const unsigned fl = p->d.flags;
+  p->cpl = (cpl_t *)xcalloc((size_t)E4 * n, sizeof(cpl_t));
+  p->ncpl = 0;
+  for (int64_t e = 0; e < p->E; ++e) {
+    const int fe = p->fluid[e];
+    int has_other = 0;
+    for (int i = 0; i < 4; ++i) {
+      int64_t f = nbr[e * 4 + i];
+      if (f >= 0 && p->fluid[f] != fe) has_other = 1;
+    }
+    if (!has_other) continue;
+    for (int i = 0; i < 4; ++i) {
+      const int64_t f = nbr[e * 4 + i];
+      if (f < 0) continue;
+      if (p->fluid[f] == fe && !(fe && !(fl & ORC_K3_INTERFACE_EDGES))) continue;
+      const double *v0 = p->vtx + (e * 4 + i) * 2, *v1 = p->vtx + (e * 4 + (i + 1) % 4) * 2;
+      const double dx = v1[0] - v0[0], dy = v1[1] - v0[1];
+      const double len = sqrt(dx * dx + dy * dy);
+      const double d = len / 2.0, nx = dy / len, ny = -dx / len;
+      double rho0 = 0.0, vp[ORC_MAX_P];
+      if (fe) orc_element_par(ORC_QUAD, n - 1, p->par + ((size_t)1 * p->E + e) * 4, vp);
+      if (!fe) {
+        for (int a = 0; a < 4; ++a) rho0 += p->par[((size_t)2 * p->E + f) * 4 + a];
+        rho0 /= 4;
+      }
+      for (int j = 0; j < n; ++j) {
+        int q;
+        switch (i) {
+          case 0: q = j; break;
+          case 1: q = (n - 1) + n * j; break;
+          case 2: q = n * n - 1 - j; break;
+          default: q = n * (n - 1) - n * j; break;
+        }
+        cpl_t *c = &p->cpl[p->ncpl++];
+        c->e = e; c->q = q; c->kind = fe ? 0 : 1;
+        const double wd = p->b.w[j] * d;
+        if (fe) {
+          const double s2 = (fl & ORC_K4_FLUID_VP2) ? vp[q] * vp[q] : 1.0;
+          c->cx = s2 * wd * nx; c->cy = s2 * wd * ny;
+        } else if (fl & ORC_K2_SOLID_NORMAL) {
+          c->cx = rho0 * wd * nx; c->cy = rho0 * wd * ny;
+        } else {
+          c->cx = -rho0 * wd; c->cy = -rho0 * wd;
+        }
+      }
+    }
+  }
+  free(nbr);
+}
+
 orc_problem *orc_create(const orc_desc *d) {
   if (!d || d->shape < ORC_QUAD || d->shape > ORC_TET) { set_err("bad shape"); return NULL; }
   if (d->physics == ORC_ELASTIC3D && d->shape != ORC_HEX && d->shape != ORC_TET) {
     set_err("elastic 3-D physics needs hexahedra or tetrahedra");
     return NULL;
   }
-  if (d->physics == ORC_ELASTIC2D && d->shape != ORC_QUAD) {
-    set_err("elastic 2-D physics needs quadrilaterals");
+  if ((d->physics == ORC_ELASTIC2D || d->physics == ORC_COUPLED2D) && d->shape != ORC_QUAD) {
+    set_err("2-D elastic and coupled physics need quadrilaterals");
     return NULL;
   }
-  if (d->physics < ORC_ACOUSTIC || d->physics > ORC_ELASTIC2D) { set_err("bad physics"); return NULL; }
+  if (d->physics < ORC_ACOUSTIC || d->physics > ORC_COUPLED2D) { set_err("bad physics"); return NULL; }
   orc_problem *p = (orc_problem *)xcalloc(1, sizeof(orc_problem));
   p->d = *d;
   if (p->d.threads < 1) p->d.threads = 1;
@@ -1215,7 +1358,8 @@ orc_problem *orc_create(const orc_desc *d) {
   const basis_t *b = &p->b;
   const int dim = b->dim, nv = b->nv, P = b->P;
   p->c = d->physics == ORC_ACOUSTIC ? 1 : (d->physics == ORC_ELASTIC2D ? 2 : 3);
-  p->npar = d->physics == ORC_ACOUSTIC ? 1 : (d->physics == ORC_ELASTIC2D ? 5 : 6);
+  p->npar = d->physics == ORC_ACOUSTIC ? 1 : (d->physics == ORC_ELASTIC2D ? 5 :
+            (d->physics == ORC_COUPLED2D ? 7 : 6));
   p->E = d->n_elements;
   p->vtx = (double *)xcalloc((size_t)(p->E * nv * dim), sizeof(double));
   for (int64_t e = 0; e < p->E; ++e)
@@ -1226,6 +1370,19 @@ orc_problem *orc_create(const orc_desc *d) {
     }
   p->par = (double *)xcalloc((size_t)(p->npar * p->E * nv), sizeof(double));
   memcpy(p->par, d->params, sizeof(double) * (size_t)(p->npar * p->E * nv));
+  if (d->physics == ORC_COUPLED2D) {
+    p->fluid = (char *)xcalloc((size_t)p->E, 1);
+    for (int64_t e = 0; e < p->E; ++e) {
+      const double f0 = p->par[e * nv];
+      for (int a = 0; a < nv; ++a)
+        if (p->par[e * nv + a] != f0 || (f0 != 0.0 && f0 != 1.0)) {
+          set_err("element %lld: fluid flag must be 0 or 1 at every vertex", (long long)e);
+          orc_destroy(p);
+          return NULL;
+        }
+      p->fluid[e] = f0 == 1.0;
+    }
+  }
   /* element sanity (checkHull's right-hand-rule check) */
   for (int64_t e = 0; e < p->E; ++e) {
     double det, ref0[3] = {0, 0, 0};
@@ -1245,6 +1402,7 @@ orc_problem *orc_create(const orc_desc *d) {
       element_geometry(b, p->vtx + e * nv * dim, d->flags, p->detJ + e * P, p->invJ + e * P * dim * dim);
   }
   if (!faithful || d->physics == ORC_ELASTIC3D) {
+    /* (coupled meshes keep 4 words for fluid and solid elements alike) */
     p->mat = (double *)xcalloc((size_t)(p->E * P * nm), sizeof(double));
     for (int64_t e = 0; e < p->E; ++e) element_material(p, e, p->mat + e * P * nm, NULL);
   }
@@ -1277,14 +1435,25 @@ orc_problem *orc_create(const orc_desc *d) {
   }
   /* Diagonal mass: Scalar.cpp:34-39 (no rho), Elastic3D.cpp:63-67 (rho);
    * summed in element order then reciprocal (Order2Newmark.cpp:32-66). */
-  p->mi = (double *)xcalloc((size_t)p->G, sizeof(double));
+  /* One mass summed over every element, shared by all components
+   * (Order2Newmark.cpp:38-52); K1 on coupled meshes: fluid elements add to
+   * u's mass only, solid elements to ux's and uy's. */
+  const int cc = p->c;
+  p->mi = (double *)xcalloc((size_t)(p->G * cc), sizeof(double));
   for (int64_t e = 0; e < p->E; ++e) {
     double m[9 * ORC_MAX_P], rho[ORC_MAX_P], me[ORC_MAX_P];
     element_material(p, e, m, rho);
     orc_element_test(b->shape, b->n - 1, p->vtx + e * nv * dim, d->flags, rho, me);
-    for (int q = 0; q < P; ++q) p->mi[p->conn[e * P + q]] += me[q];
+    int k0 = 0, k1 = cc;
+    if (d->physics == ORC_COUPLED2D && (d->flags & ORC_K1_SPLIT_MASS)) {
+      k0 = p->fluid[e] ? 0 : 1;
+      k1 = p->fluid[e] ? 1 : 3;
+    }
+    for (int q = 0; q < P; ++q)
+      for (int k = k0; k < k1; ++k) p->mi[p->conn[e * P + q] * cc + k] += me[q];
   }
-  for (int64_t g = 0; g < p->G; ++g) p->mi[g] = 1.0 / p->mi[g];
+  for (int64_t i = 0; i < p->G * cc; ++i) p->mi[i] = p->mi[i] > 0 ? 1.0 / p->mi[i] : 0.0;
+  if (d->physics == ORC_COUPLED2D) build_coupling(p);
   size_t nf = (size_t)(p->G * p->c);
   p->u = (double *)xcalloc(nf, sizeof(double));
   p->v = (double *)xcalloc(nf, sizeof(double));
@@ -1297,6 +1466,7 @@ void orc_destroy(orc_problem *p) {
   if (!p) return;
   free(p->vtx); free(p->par); free(p->conn); free(p->xyz);
   free(p->detJ); free(p->invJ); free(p->mat); free(p->mi); free(p->Ke); free(p->dirichlet);
+  free(p->fluid); free(p->cpl);
   free(p->u); free(p->v); free(p->a); free(p->a_);
   free(p->col_off); free(p->col_elems);
   for (int i = 0; i < p->nsrc; ++i) free(p->src[i].wts);
@@ -1337,6 +1507,13 @@ int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double
   double ref[3] = {0, 0, 0};
   int64_t e = locate(p, x, ref);
   if (e < 0) return -1;
+  /* components this element's physics pushes: coupled fluid u, solid ux uy */
+  int k0 = 0, k1 = c;
+  if (p->d.physics == ORC_COUPLED2D) {
+    k0 = p->fluid[e] ? 0 : 1;
+    k1 = p->fluid[e] ? 1 : 3;
+    if (kind == 1 && p->fluid[e]) { set_err("moment tensor source in a fluid element"); return -1; }
+  }
   p->src = (src_t *)realloc(p->src, sizeof(src_t) * (size_t)(p->nsrc + 1));
   src_t *s = &p->src[p->nsrc];
   s->elem = e; s->f0 = f0; s->t0 = t0; s->amp = amp;
@@ -1353,7 +1530,7 @@ int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double
     int scale = !(p->d.physics == ORC_ELASTIC3D && (p->d.flags & ORC_Q2_ELASTIC_SRC_UNSCALED));
     if (scale) orc_element_test(b->shape, b->n - 1, vtx, p->d.flags, delta, integ);
     for (int q = 0; q < P; ++q)
-      for (int a = 0; a < c; ++a)
+      for (int a = k0; a < k1; ++a)
         s->wts[q * c + a] = (scale ? integ[q] : delta[q]) * comp[a];
   } else {
     /* moment tensor: f_{q,a} = sum_b M_ab dphi_q/dx_b (x_s);
@@ -1378,7 +1555,7 @@ int orc_add_source(orc_problem *p, const double *x, double f0, double t0, double
       for (int a = 0; a < d; ++a) {
         double f = 0;
         for (int k = 0; k < d; ++k) f += M[a][k] * gx[k];
-        s->wts[q * d + a] = f;
+        s->wts[q * c + k0 + a] = f;
       }
     }
   }
@@ -1412,7 +1589,12 @@ int orc_get_field(const orc_problem *p, int which, double *vals) {
 }
 
 int orc_inverse_mass(const orc_problem *p, double *mi) {
-  memcpy(mi, p->mi, sizeof(double) * (size_t)p->G);
+  for (int64_t g = 0; g < p->G; ++g) mi[g] = p->mi[g * p->c];
+  return 0;
+}
+
+int orc_inverse_mass_c(const orc_problem *p, double *mi) {
+  memcpy(mi, p->mi, sizeof(double) * (size_t)(p->G * p->c));
   return 0;
 }
 
@@ -1486,6 +1668,19 @@ static void assemble(orc_problem *p, const double *u, double t, double *a, int w
       }
     }
   }
+  if (with_src && p->ncpl) {
+    /* computeSurfaceIntegral (Problem.cpp:191-198) with the velocity field */
+    for (int64_t i = 0; i < p->ncpl; ++i) {
+      const cpl_t *k = &p->cpl[i];
+      const int64_t g = p->conn[k->e * P + k->q];
+      if (k->kind == 0) {
+        a[g * 3] += k->cx * p->v[g * 3 + 1] + k->cy * p->v[g * 3 + 2];
+      } else {
+        a[g * 3 + 1] += k->cx * p->v[g * 3];
+        a[g * 3 + 2] += k->cy * p->v[g * 3];
+      }
+    }
+  }
   if (with_src) {
     /* computeSourceTerm at time t (Problem.cpp:196; Scalar.cpp:79-88;
      * Elastic3D.cpp:126-133), sources in attach order. */
@@ -1499,11 +1694,16 @@ static void assemble(orc_problem *p, const double *u, double t, double *a, int w
   }
 }
 
+int orc_apply_stiffness(orc_problem *p, const double *u, double *ku) {
+  assemble(p, u, 0.0, ku, 0);
+  return 0;
+}
+
 int orc_acceleration(orc_problem *p, double t, double *a) {
   assemble(p, p->u, t, a, 1);
   const int c = p->c;
   for (int64_t g = 0; g < p->G; ++g)
-    for (int k = 0; k < c; ++k) a[g * c + k] *= p->mi[g];
+    for (int k = 0; k < c; ++k) a[g * c + k] *= p->mi[g * c + k];
   return 0;
 }
 
@@ -1517,6 +1717,8 @@ int orc_run(orc_problem *p, int64_t nsteps, double dt, double *seis) {
   int comps[4], ncomp = 0;
   if (c == 1) {
     comps[ncomp++] = 0;
+  } else if ((p->d.flags & ORC_Q1_Z_NOT_ADVANCED) && p->d.physics == ORC_COUPLED2D) {
+    comps[ncomp++] = 1; comps[ncomp++] = 2; comps[ncomp++] = 1; comps[ncomp++] = 0;
   } else if (p->d.flags & ORC_Q1_Z_NOT_ADVANCED) {
     comps[ncomp++] = 0; comps[ncomp++] = 1; comps[ncomp++] = 0;
   } else {
@@ -1527,7 +1729,7 @@ int orc_run(orc_problem *p, int64_t nsteps, double dt, double *seis) {
     assemble(p, p->u, t, p->a, 1);
     /* applyInverseMassMatrix Order2Newmark.cpp:68-83 */
     for (int64_t g = 0; g < G; ++g)
-      for (int k = 0; k < c; ++k) p->a[g * c + k] *= p->mi[g];
+      for (int k = 0; k < c; ++k) p->a[g * c + k] *= p->mi[g * c + k];
     /* takeTimeStep Order2Newmark.cpp:85-114 (VecAXPBYPCZ twice + VecCopy) */
     for (int ci = 0; ci < ncomp; ++ci) {
       const int k = comps[ci];
@@ -1578,9 +1780,10 @@ double orc_max_eigenvalue(orc_problem *p, int iters, uint64_t seed) {
     for (int64_t g = 0; g < p->G; ++g)
       for (int k = 0; k < c; ++k) {
         int64_t i = g * c + k;
-        y[i] = -y[i] * p->mi[g];
-        num += y[i] * y[i] / p->mi[g];
-        den += x[i] * y[i] / p->mi[g];
+        if (p->mi[i] == 0.0) { y[i] = 0.0; continue; }
+        y[i] = -y[i] * p->mi[i];
+        num += y[i] * y[i] / p->mi[i];
+        den += x[i] * y[i] / p->mi[i];
       }
     lam = num / den;
     double nrm = 0;
@@ -1600,7 +1803,7 @@ double orc_energy(orc_problem *p) {
   for (int64_t g = 0; g < p->G; ++g)
     for (int k = 0; k < c; ++k) {
       int64_t i = g * c + k;
-      ek += 0.5 * p->v[i] * p->v[i] / p->mi[g];
+      if (p->mi[i] != 0.0) ek += 0.5 * p->v[i] * p->v[i] / p->mi[i];
       ep += -0.5 * p->u[i] * ku[i];
     }
   free(ku);

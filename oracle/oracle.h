@@ -21,8 +21,13 @@ extern "C" {
 /* ORC_TRI / ORC_TET: the P3 mass-lumped simplices (12-node triangle,
  * 50-node tetrahedron) of Triangle.cpp / Tetrahedra.cpp, order 3 only. */
 enum { ORC_QUAD = 0, ORC_HEX = 1, ORC_TRI = 2, ORC_TET = 3 };
-/* ORC_ELASTIC2D: Elastic2D on quads (Elastic2D.cpp:29-127). */
-enum { ORC_ACOUSTIC = 0, ORC_ELASTIC3D = 1, ORC_ELASTIC2D = 2 };
+/* ORC_ELASTIC2D: Elastic2D on quads (Elastic2D.cpp:29-127).
+ * ORC_COUPLED2D: quads of both kinds in one mesh, fluid (Scalar) and solid
+ * (Elastic2D) per element, coupled across shared edges by the
+ * ElasticToAcoustic2D / AcousticToElastic2D surface integrals
+ * (ElasticToAcoustic.cpp:26-41, AcousticToElastic2D.cpp:48-60); fields per
+ * node [u, ux, uy]. */
+enum { ORC_ACOUSTIC = 0, ORC_ELASTIC3D = 1, ORC_ELASTIC2D = 2, ORC_COUPLED2D = 3 };
 
 /* Reference quirk switches ("reference-literal" mode).  The default (0) is the
  * corrected physics that the GPU path is checked against. */
@@ -41,6 +46,23 @@ enum {
    * the Jacobian and re-interpolate material at every GLL point every call
    * (reference operation count; used for the faithful CPU timing). */
   ORC_FAITHFUL_RECOMPUTE = 1u << 4,
+  /* Fluid-solid coupling (ORC_COUPLED2D).  The default restates the
+   * reference's coupling exactly; these switches make it consistent, one
+   * defect at a time (the consistent velocity-coupled scheme is unstable
+   * under the explicit Newmark step, see the oracle tests):
+   * K1: Order2Newmark.cpp:38-52 sums every element's mass (fluid 1, solid
+   *     rho) into one "mi" shared by u, ux and uy; K1 keeps the fluid mass
+   *     for u and the solid mass for ux, uy. */
+  ORC_K1_SPLIT_MASS = 1u << 5,
+  /* K2: AcousticToElastic2D.cpp:53-58 adds -rho0 int(phi v) to both ax and
+   *     ay; K2 multiplies by the fluid's outward normal component. */
+  ORC_K2_SOLID_NORMAL = 1u << 6,
+  /* K3: ElasticToAcoustic.cpp:17-22 couples a fluid element on every edge
+   *     with a neighbour, fluid neighbours included; K3 keeps solid ones. */
+  ORC_K3_INTERFACE_EDGES = 1u << 7,
+  /* K4: ElasticToAcoustic.cpp:33-37 integrates v_s . n without the vp^2 of
+   *     the fluid's natural boundary term (Scalar.cpp:42-55); K4 adds it. */
+  ORC_K4_FLUID_VP2 = 1u << 8,
 };
 
 typedef struct {
@@ -57,7 +79,10 @@ typedef struct {
    * convention, ExodusModel.cpp:455-470):
    *   acoustic: [1][n_elements][nv] = VP
    *   elastic : [6][n_elements][nv] = RHO, VPV, VPH, VSV, VSH, ETA
-   *   elastic2d: [5][n_elements][nv] = RHO, C11, C13, C33, C55 */
+   *   elastic2d: [5][n_elements][nv] = RHO, C11, C13, C33, C55
+   *   coupled2d: [7][n_elements][nv] = FLUID (1 fluid, 0 solid), VP, RHO,
+   *              C11, C13, C33, C55 (fluid elements use VP and RHO, solid
+   *              elements RHO and C..) */
   const double *params;
   unsigned flags;
   int threads;              /* OpenMP threads for element loops (>=1) */
@@ -123,6 +148,11 @@ int orc_set_dirichlet(orc_problem *p, int64_t n, const int64_t *nodes);
 int orc_set_field(orc_problem *p, int which, const double *vals);
 int orc_get_field(const orc_problem *p, int which, double *vals);
 int orc_inverse_mass(const orc_problem *p, double *mi /* [G] */);
+/* Per-component inverse mass [G][c] (coupled meshes: fluid u and solid ux,
+ * uy carry separate masses; 0 where a component has no mass). */
+int orc_inverse_mass_c(const orc_problem *p, double *mi);
+/* -K u (no sources, no coupling) for a given u [G][c]. */
+int orc_apply_stiffness(orc_problem *p, const double *u, double *ku);
 /* Advance nsteps (Main.cpp:45-66 loop body).  seis may be NULL, else
  * [n_receivers][c][nsteps] of u sampled after each step. */
 int orc_run(orc_problem *p, int64_t nsteps, double dt, double *seis);

@@ -12,12 +12,17 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
 QUAD, HEX, TRI, TET = 0, 1, 2, 3
-ACOUSTIC, ELASTIC3D, ELASTIC2D = 0, 1, 2
+ACOUSTIC, ELASTIC3D, ELASTIC2D, COUPLED2D = 0, 1, 2, 3
 Q1_Z_NOT_ADVANCED = 1 << 0
 Q2_ELASTIC_SRC_UNSCALED = 1 << 1
 Q3_QUAD_INVJ_AT_OUTPUT = 1 << 2
 Q17_QUAD_SWAPPED_JAC = 1 << 3
 FAITHFUL_RECOMPUTE = 1 << 4
+K1_SPLIT_MASS = 1 << 5
+K2_SOLID_NORMAL = 1 << 6
+K3_INTERFACE_EDGES = 1 << 7
+K4_FLUID_VP2 = 1 << 8
+COUPLING_CONSISTENT = K1_SPLIT_MASS | K2_SOLID_NORMAL | K3_INTERFACE_EDGES | K4_FLUID_VP2
 LITERAL = Q1_Z_NOT_ADVANCED | Q2_ELASTIC_SRC_UNSCALED | Q3_QUAD_INVJ_AT_OUTPUT | Q17_QUAD_SWAPPED_JAC
 
 _D = ctypes.c_double
@@ -55,6 +60,8 @@ def lib():
         L.orc_set_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
         L.orc_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, _DP]
         L.orc_inverse_mass.argtypes = [ctypes.c_void_p, _DP]
+        L.orc_inverse_mass_c.argtypes = [ctypes.c_void_p, _DP]
+        L.orc_apply_stiffness.argtypes = [ctypes.c_void_p, _DP, _DP]
         L.orc_run.argtypes = [ctypes.c_void_p, _I64, _D, _DP]
         L.orc_acceleration.argtypes = [ctypes.c_void_p, _D, _DP]
         L.orc_max_eigenvalue.restype = _D
@@ -264,6 +271,18 @@ class Problem:
     def inverse_mass(self):
         out = np.zeros(self.G)
         lib().orc_inverse_mass(self.h, _p(out))
+        return out
+
+    def inverse_mass_components(self):
+        out = np.zeros((self.G, self.c))
+        lib().orc_inverse_mass_c(self.h, _p(out))
+        return out
+
+    def apply_stiffness(self, u):
+        """-K u (no sources, no coupling terms)."""
+        u = _c(u).reshape(self.G, self.c)
+        out = np.zeros((self.G, self.c))
+        lib().orc_apply_stiffness(self.h, _p(u), _p(out))
         return out
 
     def acceleration(self, t):

@@ -7,7 +7,7 @@ that tests can run the same physics at reduced size.
 import numpy as np
 
 from . import meshgen
-from .core import ACOUSTIC, ELASTIC2D, ELASTIC3D, HEX, QUAD, TET, TRI
+from .core import ACOUSTIC, COUPLED2D, ELASTIC2D, ELASTIC3D, HEX, QUAD, TET, TRI
 
 
 def standing_wave_2d(nel=40, order=4, L=1.0e4, vp=4000.0):
@@ -158,6 +158,41 @@ def elastic_2d(nel=200, order=4, L=1.0e4, vp=4000.0, vs=2300.0, rho=2500.0, eps=
                 receivers=meshgen.ring_positions((L / 2, L / 2), 0.3 * L, n_receivers, seed))
 
 
+def coupled_2d(nel=40, order=4, L=1.0e4, depth=0.4, vp_f=1500.0, rho_f=1000.0, vp=4000.0,
+               vs=2300.0, rho=2600.0, std=0.05, corr=800.0, f0=2.0, n_receivers=16, seed=6):
+    """2-D fluid over solid (ocean over crust) on nel x nel quads of an L x L
+    square: elements whose centre lies in the top `depth` fraction are fluid
+    (homogeneous vp_f, rho_f), the rest solid (isotropic elastic, 5 % GRF).
+    params [7][E][4] = FLUID, VP, RHO, C11, C13, C33, C55.  A moment-tensor
+    source in the solid, a pressure source in the fluid, receivers on a ring
+    crossing the interface.  Fields per node [u (fluid), ux, uy]."""
+    V, C = meshgen.structured_quad(nel, nel, L, L)
+    h = L / nel
+    grf = meshgen.gaussian_random_field((nel + 1, nel + 1), h, corr, seed).ravel()
+    pert = 1.0 + std * grf
+    rv, pv, sv = rho * pert, vp * pert, vs * pert
+    c33 = rv * pv * pv
+    c55 = rv * sv * sv
+    c13 = c33 - 2.0 * c55
+    ctr = V[C].mean(axis=1)
+    fluid = (ctr[:, 1] > (1.0 - depth) * L).astype(np.float64)
+    fl = fluid[:, None] * np.ones((1, 4))
+    pe = lambda x: meshgen.per_element_vertex(x, C)
+    rho_e = np.where(fl > 0, rho_f, pe(rv))
+    params = np.stack([fl, np.full_like(fl, vp_f), rho_e, pe(c33), pe(c13), pe(c33), pe(c55)])
+    rng = np.random.default_rng(seed)
+    y_if = (1.0 - depth) * L
+    return dict(shape=QUAD, order=order, physics=COUPLED2D, vertices=V, cells=C, params=params,
+                L=L, interface_y=y_if,
+                sources=[dict(location=(L / 2 + 0.31 * h, 0.5 * y_if + 0.13 * h), center_freq=f0,
+                              time_delay=1.2 / f0, amplitude=1.0e10,
+                              moment_tensor=rng.standard_normal(3)),
+                         dict(location=(0.3 * L + 0.2 * h, y_if + 0.5 * depth * L + 0.4 * h),
+                              center_freq=f0, time_delay=1.5 / f0, amplitude=1.0e4,
+                              direction=[1.0, 0.0, 0.0])],
+                receivers=meshgen.ring_positions((L / 2, y_if), 0.25 * L, n_receivers, seed))
+
+
 def simplex_tri(nx=448, ny=224, lx=2.0e4, ly=1.0e4, vp=4000.0, std=0.05, corr=1000.0, f0=1.0,
                 n_receivers=16, seed=3):
     """2-D acoustic P3 triangles: seeded Delaunay mesh of a jittered
@@ -206,7 +241,7 @@ def simplex_tet(n=55, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700
 def oracle_params(cfg):
     """Parameter array in the oracle's layout (elastic: RHO VPV VPH VSV VSH ETA)."""
     p = cfg["params"]
-    if cfg["physics"] in (ACOUSTIC, ELASTIC2D):
+    if cfg["physics"] in (ACOUSTIC, ELASTIC2D, COUPLED2D):
         return p
     rho, vp, vs = p
     return np.stack([rho, vp, vp, vs, vs, np.ones_like(rho)])

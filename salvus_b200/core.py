@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsalvus_b200.so")
 
 QUAD, HEX, TRI, TET = 0, 1, 2, 3
-ACOUSTIC, ELASTIC3D, ELASTIC2D = 0, 1, 2
+ACOUSTIC, ELASTIC3D, ELASTIC2D, COUPLED2D = 0, 1, 2, 3
 FP32, FP64 = 0, 1
 FIELD_U, FIELD_V, FIELD_A, FIELD_A_PREV = 0, 1, 2, 3
 FORCE, MOMENT_TENSOR = 0, 1

@@ -32,6 +32,7 @@ const char *last_error();
 int flatten_mesh(salvus_mesh *m, const int64_t *cells, int64_t n_vertices);
 int locate_point(const salvus_mesh *m, const double *x, int64_t *elem, double *ref);
 int boundary_nodes(const salvus_mesh *m, std::vector<int64_t> &out);
+int setup_coupled(salvus_mesh *m, const int64_t *cells);
 
 static std::atomic<int64_t> g_launches{0};
 
@@ -231,6 +232,28 @@ static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, 
 
 template <int N, typename real>
 static int acoustic2(const salvus_mesh *m, const real *rec, const real *u, real *r, cudaStream_t s) {
+  if (m->physics == SALVUS_COUPLED2D) {
+    // fluid elements (u) then solid elements (ux, uy), class-compact records
+    const int64_t Ef = m->n_fluid, Es = m->E - m->n_fluid;
+    const int32_t *el = m->d_elist.as<int32_t>();
+    if (Ef > 0) {
+      using S = AcousticShape<2, N>;
+      acoustic_list_kernel<N, real><<<blocks_for(Ef, S::EPB), S::THREADS, 0, s>>>(
+          Ef, el, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
+      g_launches++;
+      int rc = check_launch("fluid stiffness");
+      if (rc) return rc;
+    }
+    if (Es > 0) {
+      using S = Elastic2DShape<N>;
+      const real *rs = rec + Ef * m->P * (sizeof(real) == 4 ? 4 : 3);
+      elastic2d_stiffness_kernel<N, real, 3, 1><<<blocks_for(Es, S::EPB), S::THREADS, 0, s>>>(
+          Es, el + Ef, rs, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
+      g_launches++;
+      return check_launch("solid stiffness");
+    }
+    return SALVUS_OK;
+  }
   if (m->physics == SALVUS_ELASTIC2D) {
     using S = Elastic2DShape<N>;
     elastic2d_stiffness_kernel<N, real, 2, 0><<<blocks_for(m->E, S::EPB), S::THREADS, 0, s>>>(
@@ -422,7 +445,8 @@ static int build_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &mass_l
   const int64_t total = m->E * m->P;
   geometry_kernel<real, kPack><<<blocks_for(total, 128), 128, 0, m->stream>>>(
       m->E, m->dim, m->n, m->P, m->physics, rw, m->d_vtx.as<double>(), m->d_par.as<double>(),
-      m->d_conn.as<int32_t>(), gll, out.as<real>(), mass_local.as<double>());
+      m->d_conn.as<int32_t>(), gll, out.as<real>(), mass_local.as<double>(),
+      m->d_cls_k.as<int32_t>(), m->n_fluid);
   g_launches++;
   return check_launch("geometry");
 }
@@ -450,6 +474,29 @@ static int mesh_setup_device(salvus_mesh *m) {
                               cudaMemcpyHostToDevice, m->stream));
   SALVUS_CUDA(cudaMemcpyAsync(m->d_par.ptr, m->par.data(), sizeof(double) * m->par.size(),
                               cudaMemcpyHostToDevice, m->stream));
+  if (m->physics == SALVUS_COUPLED2D) {
+    const size_t nc = (size_t)m->n_cpl;
+    std::vector<float> c32(m->cpl_coef.begin(), m->cpl_coef.end());
+    if ((rc = m->d_elist.alloc(sizeof(int32_t) * m->E)) ||
+        (rc = m->d_cls_k.alloc(sizeof(int32_t) * m->E)) ||
+        (rc = m->d_cpl_pts.alloc(sizeof(int32_t) * 2 * nc)) ||
+        (rc = m->d_cpl32.alloc(sizeof(float) * 2 * nc)) ||
+        (rc = m->d_cpl64.alloc(sizeof(double) * 2 * nc)))
+      return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(m->d_elist.ptr, m->elist.data(), sizeof(int32_t) * m->E,
+                                cudaMemcpyHostToDevice, m->stream));
+    SALVUS_CUDA(cudaMemcpyAsync(m->d_cls_k.ptr, m->cls_k.data(), sizeof(int32_t) * m->E,
+                                cudaMemcpyHostToDevice, m->stream));
+    if (nc) {
+      SALVUS_CUDA(cudaMemcpyAsync(m->d_cpl_pts.ptr, m->cpl_pts.data(), sizeof(int32_t) * 2 * nc,
+                                  cudaMemcpyHostToDevice, m->stream));
+      SALVUS_CUDA(cudaMemcpyAsync(m->d_cpl32.ptr, c32.data(), sizeof(float) * 2 * nc,
+                                  cudaMemcpyHostToDevice, m->stream));
+      SALVUS_CUDA(cudaMemcpyAsync(m->d_cpl64.ptr, m->cpl_coef.data(), sizeof(double) * 2 * nc,
+                                  cudaMemcpyHostToDevice, m->stream));
+    }
+    SALVUS_CUDA(cudaStreamSynchronize(m->stream));
+  }
   DeviceBuffer mass_local;
   if ((rc = mass_local.alloc(sizeof(double) * EP))) return rc;
   if ((rc = build_records<float, true>(m, m->d_rec32, mass_local))) return rc;
@@ -545,6 +592,18 @@ static void drop_graph(salvus_problem *p) {
   p->graph_steps = 0;
 }
 
+// fluid-solid coupling integrals (meshes of fluid and solid quadrilaterals)
+template <typename real>
+static int launch_coupling(salvus_problem *p) {
+  const salvus_mesh *m = p->mesh;
+  if (m->physics != SALVUS_COUPLED2D || m->n_cpl == 0) return SALVUS_OK;
+  const real *coef = sizeof(real) == 4 ? (const real *)m->d_cpl32.ptr : (const real *)m->d_cpl64.ptr;
+  coupling_kernel<real><<<blocks_for(m->n_cpl, 256), 256, 0, p->stream>>>(
+      m->n_cpl_fluid, m->n_cpl, m->d_cpl_pts.as<int32_t>(), coef, F<real>(p->d_v), F<real>(p->d_r));
+  g_launches++;
+  return check_launch("coupling");
+}
+
 template <typename real, int C>
 static int launch_dirichlet(salvus_problem *p) {
   if (p->n_dir_pts == 0) return SALVUS_OK;
@@ -601,6 +660,7 @@ static int step_fused_t(salvus_problem *p) {
       return rc;
   }
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
+  if ((rc = launch_coupling<real>(p))) return rc;
   if ((rc = launch_sources<real, C>(p))) return rc;
   {
     ProfScope ps(p, K_UPDATE);
@@ -826,6 +886,7 @@ static int assemble_t(salvus_problem *p) {
       return rc;
   }
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
+  if ((rc = launch_coupling<real>(p))) return rc;
   if ((rc = launch_sources<real, C>(p))) return rc;
   ProfScope ps(p, K_GATHER);
   gather_kernel<real, C, 1><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(
@@ -1195,10 +1256,9 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
     return fail(SALVUS_E_UNSUPPORTED, "unknown element shape %d", d->shape);
   if (d->physics == SALVUS_ELASTIC3D && d->shape != SALVUS_HEX && d->shape != SALVUS_TET)
     return fail(SALVUS_E_UNSUPPORTED, "elastic 3-D physics needs hexahedra or tetrahedra");
-  if (d->physics == SALVUS_ELASTIC2D && d->shape != SALVUS_QUAD)
-    return fail(SALVUS_E_UNSUPPORTED, "elastic 2-D physics needs quadrilaterals");
-  if (d->physics != SALVUS_ACOUSTIC && d->physics != SALVUS_ELASTIC3D &&
-      d->physics != SALVUS_ELASTIC2D)
+  if ((d->physics == SALVUS_ELASTIC2D || d->physics == SALVUS_COUPLED2D) && d->shape != SALVUS_QUAD)
+    return fail(SALVUS_E_UNSUPPORTED, "elastic 2-D and coupled physics need quadrilaterals");
+  if (d->physics < SALVUS_ACOUSTIC || d->physics > SALVUS_COUPLED2D)
     return fail(SALVUS_E_INVALID, "unknown physics %d", d->physics);
   if (d->n_elements <= 0 || d->n_vertices <= 0 || !d->vertices || !d->cells || !d->params)
     return fail(SALVUS_E_INVALID, "empty mesh");
@@ -1254,6 +1314,7 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
   for (size_t i = 0; i < npar_total; ++i)
     if (!std::isfinite(m->par[i])) return fail(SALVUS_E_INVALID, "non-finite material parameter");
   if ((rc = flatten_mesh(m.get(), d->cells, d->n_vertices))) return rc;
+  if (m->physics == SALVUS_COUPLED2D && (rc = setup_coupled(m.get(), d->cells))) return rc;
   if (device >= 0) {
     if ((rc = mesh_setup_device(m.get()))) return rc;
   } else {
@@ -1385,7 +1446,8 @@ int salvus_problem_create(salvus_mesh *m, int32_t precision, int32_t n_shots, sa
   if (n_shots < 1) return fail(SALVUS_E_INVALID, "n_shots must be >= 1");
   if (precision == SALVUS_FP64 && m->fp32_only)
     return fail(SALVUS_E_STATE, "mesh was created with SALVUS_MESH_FP32_ONLY");
-  if (n_shots > 1 && (precision != SALVUS_FP32 || m->shape != SALVUS_QUAD || m->order > 6))
+  if (n_shots > 1 && (precision != SALVUS_FP32 || m->shape != SALVUS_QUAD ||
+                      m->physics != SALVUS_ACOUSTIC || m->order > 6))
     return fail(SALVUS_E_UNSUPPORTED,
                 "shot batching is built for FP32 acoustic quads of order 1..6 (got shape %d, "
                 "order %d, precision %d)", m->shape, m->order, precision);
@@ -1457,6 +1519,16 @@ int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
   int rc = locate_point(m, s->location, &src.elem, src.ref);
   if (rc) return rc;
   const int P = m->P, c = p->c;
+  // components the owning element pushes: all, or on meshes of fluid and
+  // solid elements u (fluid) / ux, uy (solid)
+  int k0 = 0, k1 = c;
+  if (m->physics == SALVUS_COUPLED2D) {
+    const bool fl = m->par[(size_t)src.elem * 4] == 1.0;
+    k0 = fl ? 0 : 1;
+    k1 = fl ? 1 : 3;
+    if (fl && s->kind == SALVUS_SOURCE_MOMENT_TENSOR)
+      return fail(SALVUS_E_INVALID, "moment-tensor source inside a fluid element");
+  }
   // delta-function coefficients phi_q(x_s) / (w_q detJ_q), times w_q detJ_q
   // by applyTestAndIntegrate (Scalar.cpp:87): phi_q(x_s) per unit force
   std::vector<double> phi(P), dphi((size_t)P * 3);
@@ -1464,7 +1536,7 @@ int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
   src.wts.assign((size_t)P * c, 0.0);
   if (s->kind == SALVUS_SOURCE_FORCE) {
     for (int q = 0; q < P; ++q)
-      for (int a = 0; a < c; ++a) src.wts[(size_t)q * c + a] = phi[q] * s->comp[a];
+      for (int a = k0; a < k1; ++a) src.wts[(size_t)q * c + a] = phi[q] * s->comp[a];
   } else {
     // 3-D comp = [Mxx Myy Mzz Myz Mxz Mxy]; 2-D comp = [Mxx Myy Mxy]
     const int d = m->dim;
@@ -1486,7 +1558,7 @@ int salvus_problem_add_source(salvus_problem *p, const salvus_source *s) {
       for (int a = 0; a < d; ++a) {
         double f = 0;
         for (int k = 0; k < d; ++k) f += M[a][k] * gx[k];
-        src.wts[(size_t)q * d + a] = f;
+        src.wts[(size_t)q * c + k0 + a] = f;
       }
     }
   }

@@ -376,6 +376,7 @@ int record_words(int shape, int physics, int fp64) {
   if (shape == SALVUS_TET) return physics == SALVUS_ELASTIC3D ? 120 : 64;
   if (physics == SALVUS_ELASTIC3D) return fp64 ? 11 : 12;  // invJ(9) lambda' mu' [conn]
   if (physics == SALVUS_ELASTIC2D) return 8;                // invJ(4) C11' C13' C33' C55'
+  if (physics == SALVUS_COUPLED2D) return 8;                // per class: fluid 4 | 3, solid 8
   if (shape == SALVUS_QUAD) return fp64 ? 3 : 4;          // G00 G01 G11 [conn]
   return fp64 ? 6 : 8;                                    // G(6) [conn pad]
 }

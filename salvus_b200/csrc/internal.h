@@ -63,10 +63,12 @@ inline int shape_nv(int shape) {
 inline bool is_simplex(int shape) { return shape == SALVUS_TRI || shape == SALVUS_TET; }
 // field components per node and material parameters per element vertex
 inline int physics_components(int physics) {
-  return physics == SALVUS_ELASTIC3D ? 3 : (physics == SALVUS_ELASTIC2D ? 2 : 1);
+  return (physics == SALVUS_ELASTIC3D || physics == SALVUS_COUPLED2D) ? 3
+                                                                      : (physics == SALVUS_ELASTIC2D ? 2 : 1);
 }
 inline int physics_params(int physics) {
-  return physics == SALVUS_ELASTIC3D ? 3 : (physics == SALVUS_ELASTIC2D ? 5 : 1);
+  return physics == SALVUS_ELASTIC3D ? 3
+         : physics == SALVUS_ELASTIC2D ? 5 : physics == SALVUS_COUPLED2D ? 7 : 1;
 }
 
 struct DeviceBuffer {
@@ -102,12 +104,20 @@ struct salvus_mesh {
   std::vector<int32_t> inc_off;   // [G+1]   node -> incident element points
   std::vector<int32_t> inc_idx;   // [E*P]   e*P + p, sorted by element
   std::vector<double> mi;         // [G] inverse mass (FP64, host copy)
+  // meshes of fluid and solid quadrilaterals (SALVUS_COUPLED2D)
+  int64_t n_fluid = 0;            // fluid elements; they come first in elist
+  std::vector<int32_t> elist;     // [E] fluid elements ascending, then solid ones
+  std::vector<int32_t> cls_k;     // [E] index of each element within its class
+  std::vector<int32_t> cpl_pts;   // [n_cpl][2] coupled element point e*P + p, its node
+  std::vector<double> cpl_coef;   // [n_cpl][2] coupling coefficients (cx, cy)
+  int64_t n_cpl = 0, n_cpl_fluid = 0;  // fluid points first
   // device
   salvus::DeviceBuffer d_conn, d_inc_off, d_inc_idx, d_vtx, d_par;
   salvus::DeviceBuffer d_mi64, d_mi32;
   salvus::DeviceBuffer d_rec32, d_rec64;  // stiffness records per precision
   salvus::DeviceBuffer d_sd32, d_sd64;    // simplex derivative tables [dim][P][P]
   salvus::DeviceBuffer d_tc_tab;          // tetrahedra: tensor-core operand image (hi | lo)
+  salvus::DeviceBuffer d_elist, d_cls_k, d_cpl_pts, d_cpl32, d_cpl64;
   int tet_kernel = 0;                     // FP32 tetrahedra: 0 tensor cores, 1 CUDA cores
   cudaStream_t stream = nullptr;
 };

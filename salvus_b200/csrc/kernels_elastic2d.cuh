@@ -118,6 +118,10 @@ __device__ __forceinline__ void elastic2d_body(int64_t bid, int64_t nE,
     }
     r[(e * P + p) * C + OFF] = -ox;
     r[(e * P + p) * C + OFF + 1] = -oy;
+    // components of other element classes (meshes of fluid and solid elements)
+#pragma unroll
+    for (int c = 0; c < C; ++c)
+      if (c < OFF || c > OFF + 1) r[(e * P + p) * C + c] = real(0);
   }
 }
 

@@ -94,11 +94,15 @@ __device__ __forceinline__ double p1_interp_dev(int dim, const double *vals, con
 // float4 planes per element, [E][3][P] float4: plane 0 = invJ 0-3, plane 1 =
 // invJ 4-7, plane 2 = (invJ 8, lambda', mu', conn), so that consecutive
 // points of one plane are consecutive 16-byte words (contiguous warp loads).
+// Meshes of fluid and solid quadrilaterals (physics 3): records are stored per
+// class, fluid elements first ([Ef] acoustic quad records) then solid ones
+// (elastic 2-D records); cls_k[e] is the element's index within its class.
 template <typename real, bool kPackConn>
 __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, int rw,
                                 const double *__restrict__ vtx, const double *__restrict__ par,
                                 const int32_t *__restrict__ conn, GllTable gll,
-                                real *__restrict__ rec, double *__restrict__ mass_local) {
+                                real *__restrict__ rec, double *__restrict__ mass_local,
+                                const int32_t *__restrict__ cls_k = nullptr, int64_t Ef = 0) {
   int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= E * P) return;
   const int64_t e = tid / P;
@@ -113,6 +117,41 @@ __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, i
   p1_jac_dev(dim, v, ref, &detJ, iJ);
   const double wd = wq * detJ;
   real *out = rec + tid * rw;
+  if (physics == 3) {
+    // FLUID VP RHO C11 C13 C33 C55 per element vertex
+    auto at = [&](int k) {
+      double vals[4];
+      for (int a = 0; a < 4; ++a) vals[a] = par[((int64_t)k * E + e) * 4 + a];
+      return p1_interp_dev(2, vals, ref);
+    };
+    const int64_t k = cls_k[e];
+    if (par[e * 4] == 1.0) {
+      const double vp = at(1), sc = wd * vp * vp;
+      const double g3[3] = {sc * (iJ[0] * iJ[0] + iJ[2] * iJ[2]),
+                            sc * (iJ[0] * iJ[1] + iJ[2] * iJ[3]),
+                            sc * (iJ[1] * iJ[1] + iJ[3] * iJ[3])};
+      if constexpr (kPackConn) {
+        real *o = rec + (k * P + p) * 4;
+        for (int a = 0; a < 3; ++a) o[a] = (real)g3[a];
+        reinterpret_cast<int32_t *>(o)[3] = conn[tid];
+      } else {
+        real *o = rec + (k * P + p) * 3;
+        for (int a = 0; a < 3; ++a) o[a] = (real)g3[a];
+      }
+      mass_local[tid] = wd;  // Scalar mass (Scalar.cpp:34-39)
+    } else {
+      const double w8[8] = {iJ[0], iJ[1], iJ[2], iJ[3],
+                            wd * at(3), wd * at(4), wd * at(5), wd * at(6)};
+      for (int a = 0; a < 8; ++a) {
+        if constexpr (kPackConn)
+          rec[Ef * P * 4 + ((k * 2 + a / 4) * P + p) * 4 + a % 4] = (real)w8[a];
+        else
+          rec[Ef * P * 3 + (k * P + p) * 8 + a] = (real)w8[a];
+      }
+      mass_local[tid] = wd * at(2);  // Elastic2D mass: rho (Elastic2D.cpp:45-50)
+    }
+    return;
+  }
   if (physics == 2) {
     // elastic 2-D quads: RHO, C11, C13, C33, C55 at the point (Elastic2D.cpp:29-37,
     // 57-60); record invJ (4 words) and C * w detJ (4 words), FP32 as two

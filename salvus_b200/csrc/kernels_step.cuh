@@ -128,6 +128,30 @@ __global__ void dirichlet_zero_kernel(int64_t n, const int32_t *__restrict__ pts
   for (int c = 0; c < C; ++c) r[ep * C + c] = real(0);
 }
 
+// Fluid-solid coupling surface integrals on meshes of fluid and solid quads
+// (ElasticToAcoustic.cpp:26-41, AcousticToElastic2D.cpp:48-60), fields
+// [u, ux, uy]: one thread per coupled element point with its coefficients
+// summed over the element's coupled edges; the first n_fluid points belong to
+// fluid elements (u += cx vx + cy vy), the rest to solid elements
+// (ux += cx v, uy += cy v).  Runs after the stiffness (and Dirichlet zeroing)
+// and before the sources, on the velocity field.
+template <typename real>
+__global__ void coupling_kernel(int64_t n_fluid, int64_t n, const int32_t *__restrict__ pts,
+                                const real *__restrict__ coef, const real *__restrict__ v,
+                                real *__restrict__ r) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t ep = pts[2 * i], g = pts[2 * i + 1];
+  const real cx = coef[2 * i], cy = coef[2 * i + 1];
+  if (i < n_fluid) {
+    r[ep * 3] += cx * v[g * 3 + 1] + cy * v[g * 3 + 2];
+  } else {
+    const real vf = v[g * 3];
+    r[ep * 3 + 1] += cx * vf;
+    r[ep * 3 + 2] += cy * vf;
+  }
+}
+
 template <typename real, int C>
 __global__ void inverse_mass_kernel(int64_t G, const real *__restrict__ mi, real *__restrict__ a) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -37,16 +37,18 @@ struct AcousticShape {
   static constexpr int NG = DIM == 2 ? 3 : 6;
 };
 
+// rk: record index of the point, ce: its connectivity index (equal unless the
+// element comes from a list with class-compact records)
 template <int DIM>
 __device__ __forceinline__ void load_acoustic_rec(const float *__restrict__ rec,
-                                                  const int32_t *__restrict__, int64_t ep,
-                                                  float *g, int32_t *node) {
+                                                  const int32_t *__restrict__, int64_t rk,
+                                                  int64_t, float *g, int32_t *node) {
   if (DIM == 2) {
-    float4 a = __ldg(reinterpret_cast<const float4 *>(rec) + ep);
+    float4 a = __ldg(reinterpret_cast<const float4 *>(rec) + rk);
     g[0] = a.x; g[1] = a.y; g[2] = a.z;
     *node = __float_as_int(a.w);
   } else {
-    const float4 *q = reinterpret_cast<const float4 *>(rec) + 2 * ep;
+    const float4 *q = reinterpret_cast<const float4 *>(rec) + 2 * rk;
     float4 a = __ldg(q), b = __ldg(q + 1);
     g[0] = a.x; g[1] = a.y; g[2] = a.z; g[3] = a.w; g[4] = b.x; g[5] = b.y;
     *node = __float_as_int(b.z);
@@ -55,23 +57,28 @@ __device__ __forceinline__ void load_acoustic_rec(const float *__restrict__ rec,
 
 template <int DIM>
 __device__ __forceinline__ void load_acoustic_rec(const double *__restrict__ rec,
-                                                  const int32_t *__restrict__ conn, int64_t ep,
-                                                  double *g, int32_t *node) {
+                                                  const int32_t *__restrict__ conn, int64_t rk,
+                                                  int64_t ce, double *g, int32_t *node) {
   constexpr int NG = DIM == 2 ? 3 : 6;
 #pragma unroll
-  for (int a = 0; a < NG; ++a) g[a] = rec[ep * NG + a];
-  *node = conn[ep];
+  for (int a = 0; a < NG; ++a) g[a] = rec[rk * NG + a];
+  *node = conn[ce];
 }
 
 // bid: element-group index (the CTA index of a single-mesh launch; grouped
 // multi-mesh launches pass the CTA's index within its mesh).
-template <int DIM, int N, typename real>
+// C > 1: nodes carry C field components and this element class owns the
+// first (meshes of fluid and solid elements); the residual's other
+// components of the element's points are written as zero.  kList: the
+// group's k-th element is mesh element elist[k], with record k.
+template <int DIM, int N, typename real, int C = 1, bool kList = false>
 __device__ __forceinline__ void acoustic_stiffness_body(int64_t bid, int64_t E,
                                                         const real *__restrict__ rec,
                                                         const int32_t *__restrict__ conn,
                                                         const real *__restrict__ u,
                                                         real *__restrict__ r,
-                                                        const DMatrix<real> &Dm) {
+                                                        const DMatrix<real> &Dm,
+                                                        const int32_t *__restrict__ elist = nullptr) {
   using S = AcousticShape<DIM, N>;
   constexpr int n = S::n, P = S::P, EPB = S::EPB, n2 = n * n;
   __shared__ real sD[n * n];
@@ -80,13 +87,15 @@ __device__ __forceinline__ void acoustic_stiffness_body(int64_t bid, int64_t E,
   const int t = threadIdx.x;
   const int le = t / P, p = t - le * P;
   if (t < n * n) sD[t] = Dm.d[t];
-  const int64_t e = bid * EPB + le;
-  const bool ok = le < EPB && e < E;
+  const int64_t k_ = bid * EPB + le;
+  const bool ok = le < EPB && k_ < E;
+  int64_t e = k_;
   real g[S::NG];
   int32_t node = 0;
   if (ok) {
-    load_acoustic_rec<DIM>(rec, conn, e * P + p, g, &node);
-    su[le][p] = u[node];
+    if constexpr (kList) e = elist[k_];
+    load_acoustic_rec<DIM>(rec, conn, k_ * P + p, e * P + p, g, &node);
+    su[le][p] = u[(int64_t)node * C];
   }
   __syncthreads();
   const int i = p % n, j = (p / n) % n, k = DIM == 3 ? p / n2 : 0;
@@ -117,7 +126,9 @@ __device__ __forceinline__ void acoustic_stiffness_body(int64_t bid, int64_t E,
       out += sD[l * n + j] * sF[le][1][i + n * l + n2 * k];
       if (DIM == 3) out += sD[l * n + k] * sF[le][DIM - 1][i + n * j + n2 * l];
     }
-    r[e * P + p] = -out;
+    r[(e * P + p) * C] = -out;
+#pragma unroll
+    for (int c = 1; c < C; ++c) r[(e * P + p) * C + c] = real(0);
   }
 }
 
@@ -126,6 +137,16 @@ __global__ void __launch_bounds__(AcousticShape<DIM, N>::THREADS)
 acoustic_stiffness_kernel(int64_t E, const real *__restrict__ rec, const int32_t *__restrict__ conn,
                           const real *__restrict__ u, real *__restrict__ r, DMatrix<real> Dm) {
   acoustic_stiffness_body<DIM, N, real>(blockIdx.x, E, rec, conn, u, r, Dm);
+}
+
+// fluid elements of a mesh that also holds solid elements: nodes carry
+// [u, ux, uy], the listed elements own u
+template <int N, typename real>
+__global__ void __launch_bounds__(AcousticShape<2, N>::THREADS)
+acoustic_list_kernel(int64_t nE, const int32_t *__restrict__ elist, const real *__restrict__ rec,
+                     const int32_t *__restrict__ conn, const real *__restrict__ u,
+                     real *__restrict__ r, DMatrix<real> Dm) {
+  acoustic_stiffness_body<2, N, real, 3, true>(blockIdx.x, nE, rec, conn, u, r, Dm, elist);
 }
 
 // ---------------------------------------------------------------------------
