@@ -8,7 +8,10 @@
 //   ScalarTri<Scalar<Triangle<TriP1>>>           Triangle<Acoustic>
 //   Scalar<Tetrahedra<TetP1>>                    Tetrahedron<Acoustic>
 //   (no reference element)                       Tetrahedron<Elastic3D>
-//   Element::Factory("quad"|"hex"|"tri"|"tet", {"fluid"|"3delastic"})
+//   Elastic2D<TensorQuad<QuadP1>>                Quad<Elastic2D>
+//   Scalar / Elastic2D quads of one mesh with    Quad<FluidSolid2D>
+//     ElasticToAcoustic2D / AcousticToElastic2D
+//   Element::Factory("quad"|"hex"|"tri"|"tet", {"fluid"|"2delastic"|"3delastic"})
 //                                                (Element.cpp:117-304)
 //                                                makeProblem(shape, physics, ...)
 //   Problem / Order2Newmark                      Problem<Element> (= Order2Newmark<Element>)
@@ -49,12 +52,26 @@ struct Elastic3D {  // Elastic3D<...>, Elastic3D.cpp
   static constexpr int components = 3;
   static constexpr const char *name = "3delastic";
 };
+struct Elastic2D {  // Elastic2D<...>, Elastic2D.cpp
+  static constexpr int physics = SALVUS_ELASTIC2D;
+  static constexpr int components = 2;
+  static constexpr const char *name = "2delastic";
+};
+// fluid and solid quadrilaterals in one mesh, element class from the FLUID
+// parameter, coupled through ElasticToAcoustic2D / AcousticToElastic2D;
+// fields [u, ux, uy]
+struct FluidSolid2D {
+  static constexpr int physics = SALVUS_COUPLED2D;
+  static constexpr int components = 3;
+  static constexpr const char *name = "fluid,2delastic";
+};
 
 // ---- element shapes (TensorQuad<QuadP1>, Hexahedra<HexP1>) ----
 template <class Physics>
 struct Quad {
-  static_assert(Physics::physics == SALVUS_ACOUSTIC,
-                "quads carry acoustic physics here (2-D elastic is not part of this path)");
+  static_assert(Physics::physics == SALVUS_ACOUSTIC || Physics::physics == SALVUS_ELASTIC2D ||
+                    Physics::physics == SALVUS_COUPLED2D,
+                "quads carry acoustic, 2-D elastic or coupled fluid-solid physics");
   using physics_type = Physics;
   static constexpr int shape = SALVUS_QUAD;
   static constexpr int dim = 2;
@@ -95,7 +112,7 @@ struct Ricker {
   std::array<double, 3> location{0, 0, 0};
   double center_freq = 1.0, time_delay = 1.0, amplitude = 1.0;
   std::vector<double> direction{1.0};      // force direction (c components)
-  std::vector<double> moment_tensor;       // Mxx Myy Mzz Myz Mxz Mxy (elastic only)
+  std::vector<double> moment_tensor;       // Mxx Myy Mzz Myz Mxz Mxy, or Mxx Myy Mxy in 2-D
   int shot = 0;
   salvus_source desc() const {
     salvus_source s{};
@@ -105,9 +122,10 @@ struct Ricker {
     s.amplitude = amplitude;
     s.shot = shot;
     if (!moment_tensor.empty()) {
-      if (moment_tensor.size() != 6) throw std::runtime_error("moment tensor needs 6 components");
+      if (moment_tensor.size() != 6 && moment_tensor.size() != 3)
+        throw std::runtime_error("moment tensor needs 6 (3-D) or 3 (2-D) components");
       s.kind = SALVUS_SOURCE_MOMENT_TENSOR;
-      for (int a = 0; a < 6; ++a) s.comp[a] = moment_tensor[a];
+      for (size_t a = 0; a < moment_tensor.size(); ++a) s.comp[a] = moment_tensor[a];
     } else {
       s.kind = SALVUS_SOURCE_FORCE;
       for (size_t a = 0; a < direction.size() && a < 6; ++a) s.comp[a] = direction[a];
@@ -127,7 +145,9 @@ class Mesh {
  public:
   // vertices [n_vertices][dim]; cells [n_elements][nv] (PETSc right-hand
   // order for quads / hexes, TriP1 / TetP1 order for simplices); params per
-  // element vertex: acoustic VP [E][nv], elastic RHO, VP, VS [3][E][nv].
+  // element vertex: acoustic VP [E][nv], elastic RHO, VP, VS [3][E][nv],
+  // 2-D elastic RHO, C11, C13, C33, C55 [5][E][4], fluid-solid FLUID, VP,
+  // RHO, C11, C13, C33, C55 [7][E][4].
   Mesh(int order, const std::vector<double> &vertices, const std::vector<int64_t> &cells,
        const std::vector<double> &params, int device = 0) {
     if (order < 1 || order > Element::max_order)
@@ -156,6 +176,14 @@ class Mesh {
     std::vector<double> x((size_t)nodes_ * Element::dim);
     check(salvus_mesh_node_coords(mesh_.get(), x.data()));
     return x;
+  }
+  // nodes of the outer boundary (for HomogeneousDirichlet on every side)
+  std::vector<int64_t> boundaryNodes() const {
+    int64_t n = 0;
+    check(salvus_mesh_boundary_nodes(mesh_.get(), &n, nullptr));
+    std::vector<int64_t> out((size_t)n);
+    if (n) check(salvus_mesh_boundary_nodes(mesh_.get(), &n, out.data()));
+    return out;
   }
   double criticalDt(int iterations = 200) const {
     double lam = 0;
@@ -189,6 +217,8 @@ class ProblemBase {
   virtual std::vector<double> seismograms() = 0;
   virtual std::vector<double> getField(const std::string &name) = 0;
   virtual void setField(const std::string &name, const std::vector<double> &v) = 0;
+  // HomogeneousDirichlet (HomogeneousDirichlet.cpp:14-78) on these nodes
+  virtual void setDirichlet(const std::vector<int64_t> &nodes) = 0;
 };
 
 // Order2Newmark over one element type (Order2Newmark.h:6-26).
@@ -208,6 +238,9 @@ class Problem : public ProblemBase {
   void addReceiver(const Receiver &r) override {
     check(salvus_problem_add_receiver(p_.get(), r.location.data()));
     ++receivers_;
+  }
+  void setDirichlet(const std::vector<int64_t> &nodes) override {
+    check(salvus_problem_set_dirichlet(p_.get(), (int64_t)nodes.size(), nodes.data()));
   }
   void assembleIntoGlobalDof() override { check(salvus_assemble(p_.get())); }
   void applyInverseMassMatrix() override { check(salvus_apply_inverse_mass(p_.get())); }
@@ -255,7 +288,8 @@ template <class Element>
 using Order2Newmark = Problem<Element>;
 
 // String factory in the spirit of Element::Factory (Element.cpp:26-304):
-// shape "quad" | "hex" | "tri" | "tet", physics "fluid" | "3delastic".
+// shape "quad" | "hex" | "tri" | "tet", physics "fluid" | "2delastic" |
+// "3delastic" | "fluid,2delastic" (quads of both kinds in one mesh).
 struct Simulation {
   std::shared_ptr<void> mesh;
   std::unique_ptr<ProblemBase> problem;
@@ -280,6 +314,10 @@ inline Simulation makeProblem(const std::string &shape, const std::string &physi
                               int precision = SALVUS_FP32, int device = 0) {
   if (shape == "quad" && physics == "fluid")
     return detail::make<Quad<Acoustic>>(order, vertices, cells, params, dt, precision, device);
+  if (shape == "quad" && physics == "2delastic")
+    return detail::make<Quad<Elastic2D>>(order, vertices, cells, params, dt, precision, device);
+  if (shape == "quad" && physics == "fluid,2delastic")
+    return detail::make<Quad<FluidSolid2D>>(order, vertices, cells, params, dt, precision, device);
   if (shape == "hex" && physics == "fluid")
     return detail::make<Hexahedron<Acoustic>>(order, vertices, cells, params, dt, precision, device);
   if (shape == "hex" && physics == "3delastic")

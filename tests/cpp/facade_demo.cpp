@@ -1,7 +1,7 @@
 // Drives the C++ plugin facade the way the reference's Main.cpp:45-66 drives
 // its Problem: assembleIntoGlobalDof -> applyInverseMassMatrix ->
-// takeTimeStep, for Quad<Acoustic>, Hexahedron<Elastic3D> and
-// Tetrahedron<Elastic3D>, and prints
+// takeTimeStep, for Quad<Acoustic>, Hexahedron<Elastic3D>,
+// Tetrahedron<Elastic3D> and Quad<FluidSolid2D> (with Dirichlet sides), and prints
 // the seismograms as JSON for comparison with the Python path.
 #include <cstdio>
 #include <vector>
@@ -112,7 +112,30 @@ int main() {
     sim.problem->addSource(src);
     Receiver r; r.location = {100.0, 500.0, 600.0}; sim.problem->addReceiver(r);
     sim.problem->run(120, true);
-    print("tet_elastic", sim.problem->seismograms(), true);
+    print("tet_elastic", sim.problem->seismograms(), false);
+  }
+  {  // fluid over solid quads (Quad<FluidSolid2D>) with Dirichlet sides
+    std::vector<double> v; std::vector<int64_t> c;
+    quad_mesh(8, 1e4, v, c);
+    const size_t E = c.size() / 4;
+    std::vector<double> par(7 * E * 4);
+    for (size_t e = 0; e < E; ++e) {
+      const bool fluid = e / 8 >= 5;  // top three element rows
+      const double vals[7] = {fluid ? 1.0 : 0.0, 1500.0, fluid ? 1000.0 : 2600.0,
+                              4.16e10, 1.408e10, 4.16e10, 1.376e10};
+      for (int k = 0; k < 7; ++k)
+        for (int a = 0; a < 4; ++a) par[(k * E + e) * 4 + a] = vals[k];
+    }
+    Mesh<Quad<FluidSolid2D>> mesh(4, v, c, par);
+    Order2Newmark<Quad<FluidSolid2D>> problem(mesh, 4e-3);
+    problem.setDirichlet(mesh.boundaryNodes());
+    Ricker src; src.location = {5123.0, 3987.0, 0.0}; src.center_freq = 4.0; src.time_delay = 0.3;
+    src.amplitude = 1e10; src.moment_tensor = {1.0, -0.5, 0.3};
+    problem.addSource(src);
+    Receiver r1; r1.location = {4000.0, 7500.0, 0.0}; problem.addReceiver(r1);
+    Receiver r2; r2.location = {6000.0, 2500.0, 0.0}; problem.addReceiver(r2);
+    problem.run(200, true);
+    print("fluid_solid", problem.seismograms(), true);
   }
   std::printf("}\n");
   return 0;

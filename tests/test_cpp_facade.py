@@ -71,3 +71,21 @@ def test_facade_matches_python_path(tmp_path):
     s = p.seismograms()
     assert np.abs(s).max() > 0
     assert np.array_equal(np.array(got["tet_elastic"]), s.ravel())
+
+    # fluid over solid quads with Dirichlet sides, graph replay
+    V, C = meshgen.structured_quad(8, 8, 1e4, 1e4)
+    E = len(C)
+    fluid = (np.arange(E) // 8 >= 5).astype(np.float64)
+    vals = [fluid, np.full(E, 1500.0), np.where(fluid > 0, 1000.0, 2600.0), np.full(E, 4.16e10),
+            np.full(E, 1.408e10), np.full(E, 4.16e10), np.full(E, 1.376e10)]
+    par = np.stack([np.repeat(x[:, None], 4, axis=1) for x in vals])
+    m = core.Mesh(core.QUAD, 4, core.COUPLED2D, V, C, par)
+    p = core.Problem(m, core.FP32, dt=4e-3)
+    p.set_dirichlet(m.boundary_nodes())
+    p.add_source((5123.0, 3987.0), 4.0, 0.3, 1e10, moment_tensor=[1.0, -0.5, 0.3])
+    p.add_receiver((4000.0, 7500.0))
+    p.add_receiver((6000.0, 2500.0))
+    p.run(200, core.RUN_GRAPH)
+    s = p.seismograms()
+    assert np.abs(s[0, 0]).max() > 0 and np.abs(s[1, 1:]).max() > 0
+    assert np.array_equal(np.array(got["fluid_solid"]), s.ravel())
