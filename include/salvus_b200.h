@@ -338,6 +338,39 @@ int salvus_profile_read(salvus_problem *p, int32_t max_entries, const char **nam
 /* Total kernel launches issued by this library in this process. */
 int64_t salvus_launch_count(void);
 
+/* ---- Exodus II meshes and models (no reference-side library needed) ----
+ * Reads the NetCDF classic containers (CDF-1, 64-bit-offset CDF-2) that the
+ * Exodus library writes, with the Exodus II names the reference reads:
+ * Mesh::read (Mesh.cpp:53-86, DMPlexCreateExodusFromFile) and
+ * ExodusModel::read (ExodusModel.cpp:37-81): coordinates, element blocks
+ * (QUAD4 / HEX8 / TRI3 / TET4, one type), elemental variables of the first
+ * time step, side sets.  Cells come back 0-based in this library's vertex
+ * orders (HEX8 bottom face reversed, TET4 n0 n2 n1 n3).  NetCDF-4 (HDF5)
+ * files are rejected (SALVUS_E_UNSUPPORTED). */
+typedef struct salvus_exodus salvus_exodus;
+int salvus_exodus_open(const char *path, salvus_exodus **out);
+int salvus_exodus_close(salvus_exodus *file);
+int salvus_exodus_info(const salvus_exodus *file, int32_t *shape, int32_t *dim,
+                       int64_t *n_vertices, int64_t *n_elements, int32_t *n_elem_vars,
+                       int32_t *n_side_sets);
+/* vertices [n_vertices][dim], cells [n_elements][nv] (either may be NULL) */
+int salvus_exodus_mesh(const salvus_exodus *file, double *vertices, int64_t *cells);
+int salvus_exodus_variable_name(const salvus_exodus *file, int32_t i, char *buf, int32_t len);
+/* elemental variable by name, [n_elements] */
+int salvus_exodus_variable(const salvus_exodus *file, const char *name, double *vals);
+/* salvus_mesh_desc params for a physics from the per-vertex variables NAME_<i>
+ * (ExodusModel::getElementalMaterialParameterAtVertex ExodusModel.cpp:422-470,
+ * VP <-> VPV fallback): acoustic VP; elastic3d RHO, VP, VS (VPH / VSH / ETA,
+ * when present, must equal VPV / VSV / 1); elastic2d RHO C11 C13 C33 C55;
+ * coupled2d the "fluid" flag then VP RHO C11 C13 C33 C55 (absent names 0). */
+int salvus_exodus_params(const salvus_exodus *file, int32_t physics, double *params);
+int salvus_exodus_side_set_name(const salvus_exodus *file, int32_t i, char *buf, int32_t len);
+/* Global nodes of a mesh built from this file that lie on the named side set
+ * (Mesh::setupTopology's "Face Sets", Mesh.cpp:286-312): count first (nodes
+ * NULL), then the ascending list.  For salvus_problem_set_dirichlet. */
+int salvus_exodus_side_set_nodes(const salvus_exodus *file, const salvus_mesh *mesh,
+                                 const char *name, int64_t *count, int64_t *nodes);
+
 #ifdef __cplusplus
 }
 #endif

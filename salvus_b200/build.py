@@ -14,7 +14,8 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libsalvus_b200.so")
 
 SOURCES = ["abi.cu", "noalloc.cu", "server.cpp", "host_geometry.cpp", "host_mesh.cpp",
-           "host_simplex.cpp", "host_coupling.cpp"]
+           "host_simplex.cpp", "host_coupling.cpp",
+           "host_exodus.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
          "-Xptxas", "-O3", "-ccbin", "/usr/bin/g++"]

@@ -66,6 +66,18 @@ SIGNATURES = [
     ("salvus_mesh_inverse_mass", ctypes.c_int, [_VP, _DP]),
     ("salvus_mesh_boundary_nodes", ctypes.c_int, [_VP, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     ("salvus_problem_set_dirichlet", ctypes.c_int, [_VP, _I64, ctypes.POINTER(_I64)]),
+    ("salvus_exodus_open", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
+    ("salvus_exodus_close", ctypes.c_int, [_VP]),
+    ("salvus_exodus_info", ctypes.c_int, [_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
+                                          ctypes.POINTER(_I64), ctypes.POINTER(_I64),
+                                          ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    ("salvus_exodus_mesh", ctypes.c_int, [_VP, _DP, ctypes.POINTER(_I64)]),
+    ("salvus_exodus_variable_name", ctypes.c_int, [_VP, _I32, ctypes.c_char_p, _I32]),
+    ("salvus_exodus_variable", ctypes.c_int, [_VP, ctypes.c_char_p, _DP]),
+    ("salvus_exodus_params", ctypes.c_int, [_VP, _I32, _DP]),
+    ("salvus_exodus_side_set_name", ctypes.c_int, [_VP, _I32, ctypes.c_char_p, _I32]),
+    ("salvus_exodus_side_set_nodes", ctypes.c_int, [_VP, _VP, ctypes.c_char_p,
+                                                    ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     ("salvus_mesh_max_eigenvalue", ctypes.c_int, [_VP, _I32, ctypes.c_uint64, _DP]),
     ("salvus_group_create", ctypes.c_int, [ctypes.POINTER(_VP), _I32, ctypes.POINTER(_VP)]),
     ("salvus_group_run", ctypes.c_int, [_VP, _I64]),
