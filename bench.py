@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-simplex", action="store_true", help="skip the P3 simplex leg")
     ap.add_argument("--no-elastic2d", action="store_true", help="skip the 2-D elastic quad leg")
+    ap.add_argument("--profile-leg", default=None,
+                    choices=["quad", "elastic2d", "coupled", "tri", "tet", "shots", "group"],
+                    help="set up one workload and run --steps plain steps (for ncu captures)")
     ap.add_argument("--elastic2d-only", action="store_true",
                     help="run only the 2-D elastic quad leg (profiling)")
     ap.add_argument("--e2d-nel", type=int, default=720,
@@ -289,6 +292,54 @@ def elastic2d_leg(core, configs, timed, steps, device=0, nel=720, peak=None):
     return out
 
 
+def profile_leg(core, configs, name, steps, device=0):
+    """One workload at a capture-friendly size (inputs larger than L2, a few
+    GB at most), `steps` host-launched plain steps, nothing timed: the command
+    that ncu captures.  quad: 1000^2 acoustic quads N=4; elastic2d / coupled:
+    720^2 quads N=4; tri: 1400 x 700 x 2 P3 triangles; tet: 40^3 x 6 elastic
+    P3 tetrahedra; shots: 200^2 quads x 256 shots; group: 12 acoustic quad
+    meshes of 100^2..320^2 in one problem group."""
+    def populate(p, cfg, shots=False):
+        for s in cfg.get("sources", []):
+            kw = ({"moment_tensor": s["moment_tensor"]} if "moment_tensor" in s
+                  else {"direction": s["direction"]})
+            if shots:
+                kw["shot"] = s["shot"]
+            p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"], **kw)
+        for r in cfg.get("receivers", []):
+            p.add_receiver(r)
+        p.set_seismogram_capacity(steps + 8)
+
+    def build(cfg, **kw):
+        return core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"],
+                         cfg["cells"], cfg["params"], device=device, **kw)
+
+    if name == "group":
+        probs = []
+        for k, edge in enumerate(range(100, 340, 20)):
+            cfg = configs.ricker_2d(nel=edge, order=4, n_receivers=4, seed=k)
+            m = build(cfg)
+            p = core.Problem(m, core.FP32, dt=1e-4)
+            populate(p, cfg)
+            probs.append((m, p))
+        g = core.Group([p for _, p in probs])
+        g.run(steps)
+        g.synchronize()
+        return
+    cfg = {"quad": lambda: configs.ricker_2d(nel=1000, order=4),
+           "elastic2d": lambda: configs.elastic_2d(nel=720, order=4),
+           "coupled": lambda: configs.coupled_2d(nel=720, order=4),
+           "tri": lambda: configs.simplex_tri(nx=1400, ny=700),
+           "tet": lambda: configs.simplex_tet(n=40, physics=core.ELASTIC3D),
+           "shots": lambda: configs.batched_quad(nel=200, order=4, n_shots=256)}[name]()
+    mesh = build(cfg)
+    shots = name == "shots"
+    p = core.Problem(mesh, core.FP32, dt=1e-4, n_shots=256 if shots else 1)
+    populate(p, cfg, shots)
+    p.run(steps, core.RUN_PLAIN)
+    p.synchronize()
+
+
 def unit_dt(core, meshgen, kind, order=4):
     """Critical step of a unit mesh (h = 1, vp_max = 1) for this element
     family; dt_crit(h, vp) = unit_dt * h / vp (lambda_max scales as (vp/h)^2)."""
@@ -420,6 +471,10 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    if args.profile_leg:
+        profile_leg(core, configs, args.profile_leg, args.steps, device=local)
+        return
 
     if args.simplex_only or args.elastic2d_only:
         def timed_simple(prob, fn):

@@ -21,8 +21,9 @@
 #include "kernels_batch.cuh"
 #include "kernels_simplex.cuh"
 #include "kernels_simplex_tc.cuh"
-#include "kernels_group.cuh"
 #include "kernels_elastic2d.cuh"
+#include "kernels_quad_col.cuh"
+#include "kernels_group.cuh"
 #include <algorithm>
 #include <cstdlib>
 #include <type_traits>
@@ -230,8 +231,52 @@ static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, 
   return check_launch("elastic stiffness");
 }
 
+// Quadrilateral stiffness: column-threaded kernels (kernels_quad_col.cuh) by
+// default; SALVUS_QUAD_KERNEL=point selects the point-threaded ones (read at
+// every launch).
+static bool quad_point_kernels() {
+  const char *v = std::getenv("SALVUS_QUAD_KERNEL");
+  return v && std::strcmp(v, "point") == 0;
+}
 template <int N, typename real>
 static int acoustic2(const salvus_mesh *m, const real *rec, const real *u, real *r, cudaStream_t s) {
+  // (FP64 elastic columns of order 9-10 exceed the register file: point kernels)
+  if (!quad_point_kernels() && (sizeof(real) == 4 || N <= 8)) {
+    constexpr int EPB = quad_col_epb<N>();
+    using S = QuadColShape<N, EPB>;
+    const DMatrix<real> D = dmatrix<real>(m->basis);
+    const int32_t *cn = m->d_conn.as<int32_t>();
+    if (m->physics == SALVUS_ACOUSTIC) {
+      acoustic_quad_col_kernel<N, EPB, real><<<blocks_for(m->E, EPB), S::THREADS, 0, s>>>(
+          m->E, rec, cn, u, r, D);
+      g_launches++;
+      return check_launch("acoustic quad stiffness");
+    }
+    if (m->physics == SALVUS_ELASTIC2D) {
+      elastic2d_col_kernel<N, EPB, real, 2, 0><<<blocks_for(m->E, EPB), S::THREADS, 0, s>>>(
+          m->E, nullptr, rec, cn, u, r, D);
+      g_launches++;
+      return check_launch("elastic 2-D stiffness");
+    }
+    // fluid elements (u) then solid elements (ux, uy), class-compact records
+    const int64_t Ef = m->n_fluid, Es = m->E - m->n_fluid;
+    const int32_t *el = m->d_elist.as<int32_t>();
+    if (Ef > 0) {
+      acoustic_quad_col_list_kernel<N, EPB, real><<<blocks_for(Ef, EPB), S::THREADS, 0, s>>>(
+          Ef, el, rec, cn, u, r, D);
+      g_launches++;
+      int rc = check_launch("fluid stiffness");
+      if (rc) return rc;
+    }
+    if (Es > 0) {
+      const real *rs = rec + Ef * m->P * (sizeof(real) == 4 ? 4 : 3);
+      elastic2d_col_kernel<N, EPB, real, 3, 1><<<blocks_for(Es, EPB), S::THREADS, 0, s>>>(
+          Es, el + Ef, rs, cn, u, r, D);
+      g_launches++;
+      return check_launch("solid stiffness");
+    }
+    return SALVUS_OK;
+  }
   if (m->physics == SALVUS_COUPLED2D) {
     // fluid elements (u) then solid elements (ux, uy), class-compact records
     const int64_t Ef = m->n_fluid, Es = m->E - m->n_fluid;
@@ -255,11 +300,25 @@ static int acoustic2(const salvus_mesh *m, const real *rec, const real *u, real 
     return SALVUS_OK;
   }
   if (m->physics == SALVUS_ELASTIC2D) {
-    using S = Elastic2DShape<N>;
-    elastic2d_stiffness_kernel<N, real, 2, 0><<<blocks_for(m->E, S::EPB), S::THREADS, 0, s>>>(
-        m->E, nullptr, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
-    g_launches++;
-    return check_launch("elastic 2-D stiffness");
+    // CTA shape: SALVUS_E2D_EPB elements per CTA (read at every launch; 0 or
+    // unset: as many as fit 256 threads)
+    const char *ev = std::getenv("SALVUS_E2D_EPB");
+    const int epb = ev ? std::atoi(ev) : 0;
+    auto go = [&](auto tag) {
+      constexpr int EPB = decltype(tag)::value;
+      using S = Elastic2DShape<N, EPB>;
+      elastic2d_stiffness_kernel<N, real, 2, 0, EPB><<<blocks_for(m->E, S::EPB), S::THREADS, 0, s>>>(
+          m->E, nullptr, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
+      g_launches++;
+      return check_launch("elastic 2-D stiffness");
+    };
+    switch (epb) {
+      case 2: return go(std::integral_constant<int, 2>{});
+      case 4: return go(std::integral_constant<int, 4>{});
+      case 5: return go(std::integral_constant<int, 5>{});
+      case 8: return go(std::integral_constant<int, 8>{});
+      default: return go(std::integral_constant<int, 0>{});
+    }
   }
   return launch_acoustic<2, N, real>(m, rec, u, r, s);
 }
@@ -971,8 +1030,8 @@ template <int N>
 static int group_stiffness_t(const salvus_mesh *m0, const GroupSlot *slots, int J, int64_t blocks,
                              cudaStream_t st) {
   if (m0->shape == SALVUS_QUAD) {
-    group_quad_acoustic_stiffness<N><<<(unsigned)blocks, AcousticShape<2, N>::THREADS, 0, st>>>(
-        slots, J, dmatrix<float>(m0->basis));
+    group_quad_acoustic_stiffness<N><<<(unsigned)blocks, QuadColShape<N, quad_col_epb<N>()>::THREADS,
+                                        0, st>>>(slots, J, dmatrix<float>(m0->basis));
   } else if constexpr (N <= kMaxHexOrder) {
     constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
     using T = ElasticV2Shape<N, EPB, false>;
@@ -1010,7 +1069,7 @@ static int group_stiffness(const salvus_mesh *m0, const GroupSlot *slots, int J,
 static int64_t group_stiff_blocks(const salvus_mesh *m) {
   const int n2 = m->n * m->n;
   if (m->shape == SALVUS_QUAD) {
-    const int P = n2, epb = (256 / P) > 0 ? (256 / P) : 1;  // AcousticShape<2, N>::EPB
+    const int epb = 128 / m->n > 0 ? 128 / m->n : 1;  // quad_col_epb<N>()
     return (m->E + epb - 1) / epb;
   }
   const int epb = 128 / n2 > 0 ? 128 / n2 : 1;  // v2 with 128-thread CTAs
@@ -1102,7 +1161,7 @@ static int group_fill(salvus_group *g) {
   // (kGatherPer CTA-wide node tiles each), receivers (1 each), advance (1)
   constexpr int kStiffPer = 2, kGatherPer = 8;
   const int J = (int)g->members.size();
-  const int tile = g->m0->shape == SALVUS_HEX ? 128 : 256;  // CTA width
+  const int tile = 128;  // CTA width of the persistent kernel
   g->counts.assign(J, GroupCounts{0, 0, 0});
   g->work.clear();
   auto add = [&](int type, int j, int64_t tiles, int per) -> int32_t {
@@ -1136,7 +1195,7 @@ static int group_fill(salvus_group *g) {
 
 template <int N, bool kHex, int C>
 static int group_persistent_t(salvus_group *g) {
-  constexpr int threads = kHex ? 128 : 256;
+  constexpr int threads = 128;
   size_t smem = 0;
   if constexpr (kHex) {
     constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;

@@ -103,7 +103,23 @@ batched_gather_update_kernel(int64_t G, int S, const int32_t *__restrict__ off,
   const float uo = u[i], wo = w[i], m = __ldg(mi + g);
   const int32_t q0 = __ldg(off + g), q1 = __ldg(off + g + 1);
   float acc = 0.f;
-  for (int32_t q = q0; q < q1; ++q) acc += __ldg(r + (int64_t)__ldg(idx + q) * S + s);
+  const int cnt = q1 - q0;
+  constexpr int kFast = 4;  // quadrilateral valence bound
+  if (cnt <= kFast) {
+    // all incidence indices first, then all residual loads in flight at
+    // once; summed in ascending element order as in the general loop
+    int32_t ep[kFast];
+#pragma unroll
+    for (int q = 0; q < kFast; ++q) ep[q] = q < cnt ? __ldg(idx + q0 + q) : 0;
+    float rv[kFast];
+#pragma unroll
+    for (int q = 0; q < kFast; ++q) rv[q] = q < cnt ? __ldg(r + (int64_t)ep[q] * S + s) : 0.f;
+#pragma unroll
+    for (int q = 0; q < kFast; ++q)
+      if (q < cnt) acc += rv[q];
+  } else {
+    for (int32_t q = q0; q < q1; ++q) acc += __ldg(r + (int64_t)__ldg(idx + q) * S + s);
+  }
   const float wn = wo + dt * (acc * m);
   w[i] = wn;
   u[i] = uo + dt * wn;

@@ -24,11 +24,12 @@
 
 namespace salvus {
 
-template <int N>
+// EPB_ = 0: as many elements as fit 256 threads
+template <int N, int EPB_ = 0>
 struct Elastic2DShape {
   static constexpr int n = N + 1;
   static constexpr int P = n * n;
-  static constexpr int EPB = (256 / P) > 0 ? (256 / P) : 1;
+  static constexpr int EPB = EPB_ > 0 ? EPB_ : ((256 / P) > 0 ? (256 / P) : 1);
   static constexpr int THREADS = ((EPB * P + 31) / 32) * 32;
 };
 
@@ -57,14 +58,14 @@ __device__ __forceinline__ void load_elastic2d_rec(const double *__restrict__ re
 // bid: element-group index.  nE elements are processed (the mesh's, or the
 // list's length); record k of the group's k-th element, residual and
 // connectivity of mesh element elist[k] (k itself without a list).
-template <int N, typename real, int C, int OFF>
+template <int N, typename real, int C, int OFF, int EPB_ = 0>
 __device__ __forceinline__ void elastic2d_body(int64_t bid, int64_t nE,
                                                const int32_t *__restrict__ elist,
                                                const real *__restrict__ rec,
                                                const int32_t *__restrict__ conn,
                                                const real *__restrict__ u, real *__restrict__ r,
                                                const DMatrix<real> &Dm) {
-  using S = Elastic2DShape<N>;
+  using S = Elastic2DShape<N, EPB_>;
   constexpr int n = S::n, P = S::P, EPB = S::EPB;
   __shared__ real sD[n * n];
   __shared__ real su[EPB][2][P];
@@ -125,12 +126,12 @@ __device__ __forceinline__ void elastic2d_body(int64_t bid, int64_t nE,
   }
 }
 
-template <int N, typename real, int C, int OFF>
-__global__ void __launch_bounds__(Elastic2DShape<N>::THREADS)
+template <int N, typename real, int C, int OFF, int EPB_ = 0>
+__global__ void __launch_bounds__(Elastic2DShape<N, EPB_>::THREADS)
 elastic2d_stiffness_kernel(int64_t nE, const int32_t *__restrict__ elist,
                            const real *__restrict__ rec, const int32_t *__restrict__ conn,
                            const real *__restrict__ u, real *__restrict__ r, DMatrix<real> Dm) {
-  elastic2d_body<N, real, C, OFF>(blockIdx.x, nE, elist, rec, conn, u, r, Dm);
+  elastic2d_body<N, real, C, OFF, EPB_>(blockIdx.x, nE, elist, rec, conn, u, r, Dm);
 }
 
 }  // namespace salvus

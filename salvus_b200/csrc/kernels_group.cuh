@@ -60,11 +60,12 @@ __device__ __forceinline__ int group_member(const GroupSlot *__restrict__ slots,
 }
 
 template <int N>
-__global__ void __launch_bounds__(AcousticShape<2, N>::THREADS)
+__global__ void __launch_bounds__(QuadColShape<N, quad_col_epb<N>()>::THREADS)
 group_quad_acoustic_stiffness(const GroupSlot *__restrict__ slots, int J, DMatrix<float> Dm) {
   const int s = group_member<&GroupSlot::b_stiff>(slots, J);
   const GroupSlot &m = slots[s];
-  acoustic_stiffness_body<2, N, float>(blockIdx.x - m.b_stiff, m.E, m.rec, m.conn, m.u, m.r, Dm);
+  acoustic_quad_col_body<N, quad_col_epb<N>(), float>(blockIdx.x - m.b_stiff, m.E, m.rec, m.conn,
+                                                       m.u, m.r, Dm);
 }
 
 template <int N, int EPB>
@@ -139,7 +140,7 @@ struct GroupWork {
 };
 
 template <int N, bool kHex, int C>
-__global__ void __launch_bounds__(kHex ? 128 : 256)
+__global__ void __launch_bounds__(128)
 group_persistent_step(const GroupSlot *__restrict__ slots, const GroupCounts *__restrict__ counts,
                       int J, const GroupWork *__restrict__ work, int64_t total,
                       int32_t *__restrict__ done /* [J][4] */, GroupSync *__restrict__ sync,
@@ -183,7 +184,7 @@ group_persistent_step(const GroupSlot *__restrict__ slots, const GroupCounts *__
           if constexpr (kHex)
             elastic_hex_v2_body<N, EPB, false>(b, m.E, m.rec, m.u, m.r, Dm);
           else
-            acoustic_stiffness_body<2, N, float>(b, m.E, m.rec, m.conn, m.u, m.r, Dm);
+            acoustic_quad_col_body<N, quad_col_epb<N>(), float>(b, m.E, m.rec, m.conn, m.u, m.r, Dm);
           __syncthreads();
         }
         break;
