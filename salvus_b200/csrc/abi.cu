@@ -21,6 +21,7 @@
 #include "kernels_batch.cuh"
 #include "kernels_simplex.cuh"
 #include "kernels_simplex_tc.cuh"
+#include "kernels_tri_tc.cuh"
 #include "kernels_elastic2d.cuh"
 #include "kernels_quad_col.cuh"
 #include "kernels_group.cuh"
@@ -368,10 +369,30 @@ static int launch_tet_tc(const salvus_mesh *m, const float *rec, const float *u,
   return check_launch("tetrahedron stiffness (tensor cores)");
 }
 
+static int launch_tri_tc(const salvus_mesh *m, const float *rec, const float *u, float *r,
+                         cudaStream_t st, int *err) {
+  using S = TriTcShape;
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaFuncSetAttribute(tri_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+    SALVUS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tri_tc_kernel, S::THREADS,
+                                                              S::SMEM));
+    if (per_sm < 1) per_sm = 1;
+  }
+  const int64_t tiles = (m->E + S::NE - 1) / S::NE;
+  const int64_t slots = (int64_t)per_sm * m->sm_count;
+  const unsigned grid = (unsigned)(tiles < slots ? tiles : slots);
+  tri_tc_kernel<<<grid, S::THREADS, S::SMEM, st>>>(m->E, rec, m->d_conn.as<int32_t>(),
+                                                   m->d_tc_tab.as<uint4>(), u, r, err);
+  g_launches++;
+  return check_launch("triangle stiffness (tensor cores)");
+}
+
 template <typename real>
 static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, real *r,
                           cudaStream_t st, int *err) {
   if constexpr (std::is_same<real, float>::value) {
+    if (m->shape == SALVUS_TRI && m->tri_kernel == 0) return launch_tri_tc(m, rec, u, r, st, err);
     if (m->shape == SALVUS_TET && m->tet_kernel == 0) {
       if (m->physics == SALVUS_ELASTIC3D) return launch_tet_tc<3>(m, rec, u, r, st, err);
       return launch_tet_tc<1>(m, rec, u, r, st, err);
@@ -449,6 +470,38 @@ static int build_simplex_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer
   if ((rc = sd.alloc(sizeof(real) * t.size()))) return rc;
   SALVUS_CUDA(cudaMemcpyAsync(sd.ptr, t.data(), sizeof(real) * t.size(), cudaMemcpyHostToDevice,
                               m->stream));
+  if (sizeof(real) == 4 && m->shape == SALVUS_TRI) {
+    // tensor-core operand images (kernels_tri_tc.cuh), K-major no-swizzle
+    // core-matrix order, TF32 hi part and FP32 remainder, zero padding:
+    //   B1[kappa = 16 k + q][j] = dphi_j/dxi_k (x_q)   32 x 16
+    //   B2[i][kappa = 16 k + q] = dphi_i/dxi_k (x_q)    16 x 32
+    constexpr int P = 12;
+    constexpr size_t B = 32 * 16;
+    std::vector<float> img(4 * B, 0.f);
+    auto off = [](int row, int k, int kdim) {
+      return (size_t)(((row >> 3) * (kdim / 4) * 128 + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4) / 4);
+    };
+    for (int k = 0; k < 2; ++k)
+      for (int q = 0; q < P; ++q)
+        for (int j = 0; j < P; ++j) {
+          const double v = m->basis.SD[((size_t)k * P + j) * P + q];
+          const float f = (float)v;
+          uint32_t bits;
+          std::memcpy(&bits, &f, 4);
+          bits = (bits + 0x1000u) & 0xFFFFE000u;  // nearest TF32 (ties away from zero)
+          float hi, lo;
+          std::memcpy(&hi, &bits, 4);
+          lo = (float)(v - (double)hi);
+          const int kap = 16 * k + q;
+          img[off(kap, j, 16)] = hi;
+          img[B + off(kap, j, 16)] = lo;
+          img[2 * B + off(j, kap, 32)] = hi;
+          img[3 * B + off(j, kap, 32)] = lo;
+        }
+    if ((rc = m->d_tc_tab.alloc(sizeof(float) * img.size()))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(m->d_tc_tab.ptr, img.data(), sizeof(float) * img.size(),
+                                cudaMemcpyHostToDevice, m->stream));
+  }
   if (sizeof(real) == 4 && m->shape == SALVUS_TET) {
     // tensor-core operand images, K-major no-swizzle core-matrix order, each
     // as a TF32 hi part and an FP32 remainder:
@@ -1329,6 +1382,10 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
     // the CUDA-core kernel (read when the mesh is created)
     const char *s = std::getenv("SALVUS_TET_KERNEL");
     m->tet_kernel = (s && std::strcmp(s, "cuda") == 0) ? 1 : 0;
+    // FP32 triangles: SALVUS_TRI_KERNEL=tc selects the tensor-core kernel,
+    // anything else the CUDA-core one (read when the mesh is created)
+    const char *t = std::getenv("SALVUS_TRI_KERNEL");
+    m->tri_kernel = (t && std::strcmp(t, "tc") == 0) ? 0 : 1;
   }
   m->shape = d->shape;
   m->order = d->order;

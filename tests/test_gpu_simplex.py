@@ -7,7 +7,7 @@ FP32 GPU vs FP64 oracle seismogram rel-L2 <= 1e-4 (the stated FP32 target).
 import numpy as np
 import pytest
 
-from salvus_b200 import core
+from salvus_b200 import configs, core
 
 import simplex_cases as sc
 
@@ -118,6 +118,30 @@ def test_tensor_core_kernel_matches_cuda_cores(physics, n, monkeypatch):
         mesh.close()
     # split-TF32 products drop the lo x lo term and round the lo parts to TF32:
     # a few 1e-7 per product, about 1e-6 relative on the assembled residual
+    assert sc.rel_l2(out["tc"], out["fp64"]) <= 5e-6
+    assert sc.rel_l2(out["cuda"], out["fp64"]) <= 2e-6
+    assert sc.rel_l2(out["tc"], out["cuda"]) <= 6e-6
+
+
+def test_triangle_tensor_core_kernel_matches_cuda_cores(monkeypatch):
+    """FP32 triangles: the optional tcgen05 kernel (SALVUS_TRI_KERNEL=tc,
+    split-TF32 contractions, several tiles per CTA) against the default
+    CUDA-core FP32 kernel, both against the FP64 kernel, on one assemble of a
+    random field."""
+    cfg = configs.simplex_tri(nx=120, ny=60, n_receivers=4, seed=7)
+    out = {}
+    for name, kern, prec in (("tc", "tc", core.FP32), ("cuda", "cuda", core.FP32),
+                             ("fp64", "cuda", core.FP64)):
+        monkeypatch.setenv("SALVUS_TRI_KERNEL", kern)
+        mesh = core.Mesh(cfg["shape"], 3, cfg["physics"], cfg["vertices"], cfg["cells"],
+                         cfg["params"])
+        prob = core.Problem(mesh, prec, dt=1e-3)
+        rng = np.random.default_rng(5)
+        prob.set_field("u", rng.standard_normal((mesh.n_nodes, 1)))
+        prob.assembleIntoGlobalDof()
+        out[name] = prob.get_field("a")
+        prob.close()
+        mesh.close()
     assert sc.rel_l2(out["tc"], out["fp64"]) <= 5e-6
     assert sc.rel_l2(out["cuda"], out["fp64"]) <= 2e-6
     assert sc.rel_l2(out["tc"], out["cuda"]) <= 6e-6
