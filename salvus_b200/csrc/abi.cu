@@ -789,12 +789,13 @@ static int step_fused_t(salvus_problem *p) {
 // ---------------------------------------------------------------------------
 // shot-batched step (FP32 acoustic quads)
 struct BatchCfg {
-  int sc, epc;
+  int sc, epc, npt;  // shot lanes, elements / node groups per CTA, nodes per thread
 };
-static const BatchCfg kStiffCfg[] = {{32, 1}, {32, 2}, {32, 4}, {64, 1}, {64, 2},
-                                     {128, 1}, {128, 2}, {256, 1}};
-static const BatchCfg kGatherCfg[] = {{32, 4}, {32, 8}, {64, 2}, {64, 4}, {128, 1},
-                                      {128, 2}, {256, 1}};
+static const BatchCfg kStiffCfg[] = {{32, 1, 1}, {32, 2, 1}, {32, 4, 1}, {64, 1, 1},
+                                     {64, 2, 1}, {128, 1, 1}, {128, 2, 1}, {256, 1, 1}};
+static const BatchCfg kGatherCfg[] = {{32, 4, 1},  {32, 8, 1}, {64, 2, 1}, {64, 4, 1},
+                                      {128, 1, 1}, {128, 2, 1}, {256, 1, 1}, {32, 4, 2},
+                                      {64, 2, 2},  {128, 1, 2}, {128, 1, 4}, {256, 1, 2}};
 constexpr int kNumStiffCfg = sizeof(kStiffCfg) / sizeof(kStiffCfg[0]);
 constexpr int kNumGatherCfg = sizeof(kGatherCfg) / sizeof(kGatherCfg[0]);
 
@@ -836,11 +837,11 @@ static int batched_stiffness(const salvus_problem *p, int cfg, cudaStream_t st) 
   return fail(SALVUS_E_UNSUPPORTED, "batched quads support orders 1..6");
 }
 
-template <int SC, int NPB>
+template <int SC, int NPB, int NPT = 1>
 static void launch_bg(const salvus_problem *p, cudaStream_t st) {
   const salvus_mesh *m = p->mesh;
-  dim3 grid((unsigned)((m->G + NPB - 1) / NPB), (unsigned)(p->shots_pad / SC));
-  batched_gather_update_kernel<SC, NPB><<<grid, SC * NPB, 0, st>>>(
+  dim3 grid((unsigned)((m->G + NPB * NPT - 1) / (NPB * NPT)), (unsigned)(p->shots_pad / SC));
+  batched_gather_update_kernel<SC, NPB, NPT><<<grid, SC * NPB, 0, st>>>(
       m->G, p->shots_pad, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(),
       F<float>(p->d_r), m->d_mi32.as<float>(), F<float>(p->d_u), F<float>(p->d_v), (float)p->dt);
 }
@@ -854,6 +855,11 @@ static int batched_gather(const salvus_problem *p, int cfg, cudaStream_t st) {
     case 4: launch_bg<128, 1>(p, st); break;
     case 5: launch_bg<128, 2>(p, st); break;
     case 6: launch_bg<256, 1>(p, st); break;
+    case 7: launch_bg<32, 4, 2>(p, st); break;
+    case 8: launch_bg<64, 2, 2>(p, st); break;
+    case 9: launch_bg<128, 1, 2>(p, st); break;
+    case 10: launch_bg<128, 1, 4>(p, st); break;
+    case 11: launch_bg<256, 1, 2>(p, st); break;
     default: return fail(SALVUS_E_INVALID, "bad gather config %d", cfg);
   }
   g_launches++;
@@ -1910,7 +1916,7 @@ int salvus_problem_autotune(salvus_problem *p, int32_t *stiff_shot_lanes, int32_
   if (stiff_shot_lanes) *stiff_shot_lanes = kStiffCfg[p->tune_stiff].sc;
   if (stiff_elements) *stiff_elements = kStiffCfg[p->tune_stiff].epc;
   if (gather_shot_lanes) *gather_shot_lanes = kGatherCfg[p->tune_gather].sc;
-  if (gather_nodes) *gather_nodes = kGatherCfg[p->tune_gather].epc;
+  if (gather_nodes) *gather_nodes = kGatherCfg[p->tune_gather].epc * kGatherCfg[p->tune_gather].npt;
   return SALVUS_OK;
 }
 

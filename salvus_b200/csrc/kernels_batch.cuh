@@ -87,42 +87,66 @@ __global__ void batched_source_kernel(int S, int P, const int32_t *__restrict__ 
   }
 }
 
-// Node gather + inverse mass + half-step-velocity update, thread = (node,
-// shot).  CTA = NPB nodes x SC shots.
-template <int SC, int NPB>
+// Node gather + inverse mass + half-step-velocity update, thread = (NPT
+// consecutive nodes, shot).  CTA = NPB node groups x SC shots.  The NPT
+// nodes' dependent load chains (offsets -> incidence -> residual) are issued
+// side by side so that more bytes are in flight per thread; the per-node
+// arithmetic and summation order do not depend on NPT.
+template <int SC, int NPB, int NPT>
 __global__ void __launch_bounds__(SC *NPB)
 batched_gather_update_kernel(int64_t G, int S, const int32_t *__restrict__ off,
                              const int32_t *__restrict__ idx, const float *__restrict__ r,
                              const float *__restrict__ mi, float *__restrict__ u,
                              float *__restrict__ w, float dt) {
   const int ny = threadIdx.x / SC, lane = threadIdx.x - ny * SC;
-  const int64_t g = (int64_t)blockIdx.x * NPB + ny;
+  const int64_t g0 = ((int64_t)blockIdx.x * NPB + ny) * NPT;
   const int s = blockIdx.y * SC + lane;
-  if (g >= G || s >= S) return;
-  const int64_t i = g * S + s;
-  const float uo = u[i], wo = w[i], m = __ldg(mi + g);
-  const int32_t q0 = __ldg(off + g), q1 = __ldg(off + g + 1);
-  float acc = 0.f;
-  const int cnt = q1 - q0;
+  if (g0 >= G || s >= S) return;
   constexpr int kFast = 4;  // quadrilateral valence bound
-  if (cnt <= kFast) {
-    // all incidence indices first, then all residual loads in flight at
-    // once; summed in ascending element order as in the general loop
-    int32_t ep[kFast];
+  float uo[NPT], wo[NPT], m[NPT];
+  int32_t q0[NPT], cnt[NPT];
 #pragma unroll
-    for (int q = 0; q < kFast; ++q) ep[q] = q < cnt ? __ldg(idx + q0 + q) : 0;
-    float rv[kFast];
+  for (int k = 0; k < NPT; ++k) {
+    const int64_t g = g0 + k;
+    const bool live = g < G;
+    const int64_t i = g * S + s;
+    uo[k] = live ? u[i] : 0.f;
+    wo[k] = live ? w[i] : 0.f;
+    m[k] = live ? __ldg(mi + g) : 0.f;
+    q0[k] = live ? __ldg(off + g) : 0;
+    cnt[k] = live ? __ldg(off + g + 1) - q0[k] : 0;
+  }
+  // all incidence indices first, then all residual loads in flight at once
+  int32_t ep[NPT][kFast];
 #pragma unroll
-    for (int q = 0; q < kFast; ++q) rv[q] = q < cnt ? __ldg(r + (int64_t)ep[q] * S + s) : 0.f;
+  for (int k = 0; k < NPT; ++k)
+#pragma unroll
+    for (int q = 0; q < kFast; ++q) ep[k][q] = q < cnt[k] ? __ldg(idx + q0[k] + q) : 0;
+  float rv[NPT][kFast];
+#pragma unroll
+  for (int k = 0; k < NPT; ++k)
 #pragma unroll
     for (int q = 0; q < kFast; ++q)
-      if (q < cnt) acc += rv[q];
-  } else {
-    for (int32_t q = q0; q < q1; ++q) acc += __ldg(r + (int64_t)__ldg(idx + q) * S + s);
+      rv[k][q] = q < cnt[k] ? __ldg(r + (int64_t)ep[k][q] * S + s) : 0.f;
+#pragma unroll
+  for (int k = 0; k < NPT; ++k) {
+    const int64_t g = g0 + k;
+    if (g >= G) break;
+    // summed in ascending element order
+    float acc = 0.f;
+    if (cnt[k] <= kFast) {
+#pragma unroll
+      for (int q = 0; q < kFast; ++q)
+        if (q < cnt[k]) acc += rv[k][q];
+    } else {
+      for (int32_t q = q0[k]; q < q0[k] + cnt[k]; ++q)
+        acc += __ldg(r + (int64_t)__ldg(idx + q) * S + s);
+    }
+    const float wn = wo[k] + dt * (acc * m[k]);
+    const int64_t i = g * S + s;
+    w[i] = wn;
+    u[i] = uo[k] + dt * wn;
   }
-  const float wn = wo + dt * (acc * m);
-  w[i] = wn;
-  u[i] = uo + dt * wn;
 }
 
 // Receivers of every shot: block = receiver, thread = shot; FP64 Kahan over
