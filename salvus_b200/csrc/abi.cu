@@ -10,6 +10,7 @@
 #include <cstring>
 #include <memory>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -1612,6 +1613,10 @@ int salvus_problem_destroy(salvus_problem *p) {
     cudaEventDestroy(e.a);
     cudaEventDestroy(e.b);
   }
+  for (int b = 0; b < 2; ++b) {
+    if (p->h_pin[b]) cudaFreeHost(p->h_pin[b]);
+    if (p->pin_ev[b]) cudaEventDestroy(p->pin_ev[b]);
+  }
   cudaStream_t s = p->stream;
   delete p;
   if (s) cudaStreamDestroy(s);
@@ -1713,6 +1718,77 @@ int salvus_problem_set_seismogram_capacity(salvus_problem *p, int64_t steps) {
   return SALVUS_OK;
 }
 
+// Host <-> device copies of whole fields through two pinned bounce chunks:
+// the host copy into (out of) one chunk overlaps the DMA of the other, which
+// runs at pinned-memory speed instead of the staged pageable path.  Small
+// copies go directly.
+static constexpr size_t kPinChunk = size_t(16) << 20;
+// host copy of one chunk, split over a few threads (one thread's memcpy is
+// slower than the DMA it feeds)
+static void par_memcpy(void *dst, const void *src, size_t n) {
+  constexpr int kThreads = 4;
+  const size_t part = (n / kThreads + 63) & ~size_t(63);
+  std::thread th[kThreads - 1];
+  int used = 0;
+  for (int t = 1; t < kThreads && (size_t)t * part < n; ++t, ++used) {
+    const size_t o = (size_t)t * part, m = std::min(part, n - o);
+    th[t - 1] = std::thread([=] { std::memcpy((char *)dst + o, (const char *)src + o, m); });
+  }
+  std::memcpy(dst, src, std::min(part, n));
+  for (int t = 0; t < used; ++t) th[t].join();
+}
+static int pin_ready(salvus_problem *p) {
+  for (int b = 0; b < 2; ++b) {
+    if (!p->h_pin[b]) SALVUS_CUDA(cudaMallocHost(&p->h_pin[b], kPinChunk));
+    if (!p->pin_ev[b]) SALVUS_CUDA(cudaEventCreateWithFlags(&p->pin_ev[b], cudaEventDisableTiming));
+  }
+  return SALVUS_OK;
+}
+static int copy_h2d(salvus_problem *p, void *dst, const void *src, size_t bytes) {
+  if (bytes < 2 * kPinChunk) {
+    SALVUS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, p->stream));
+    return SALVUS_OK;
+  }
+  int rc = pin_ready(p);
+  if (rc) return rc;
+  size_t off = 0;
+  for (int k = 0; off < bytes; ++k) {
+    const int b = k & 1;
+    const size_t n = std::min(kPinChunk, bytes - off);
+    if (k >= 2) SALVUS_CUDA(cudaEventSynchronize(p->pin_ev[b]));  // chunk free again
+    par_memcpy(p->h_pin[b], (const char *)src + off, n);
+    SALVUS_CUDA(cudaMemcpyAsync((char *)dst + off, p->h_pin[b], n, cudaMemcpyHostToDevice, p->stream));
+    SALVUS_CUDA(cudaEventRecord(p->pin_ev[b], p->stream));
+    off += n;
+  }
+  return SALVUS_OK;
+}
+static int copy_d2h(salvus_problem *p, void *dst, const void *src, size_t bytes) {
+  if (bytes < 2 * kPinChunk) {
+    SALVUS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, p->stream));
+    return SALVUS_OK;
+  }
+  int rc = pin_ready(p);
+  if (rc) return rc;
+  const size_t nchunks = (bytes + kPinChunk - 1) / kPinChunk;
+  auto issue = [&](size_t k) -> int {
+    const size_t off = k * kPinChunk, n = std::min(kPinChunk, bytes - off);
+    SALVUS_CUDA(cudaMemcpyAsync(p->h_pin[k & 1], (const char *)src + off, n, cudaMemcpyDeviceToHost,
+                                p->stream));
+    SALVUS_CUDA(cudaEventRecord(p->pin_ev[k & 1], p->stream));
+    return SALVUS_OK;
+  };
+  if ((rc = issue(0))) return rc;
+  for (size_t k = 0; k < nchunks; ++k) {
+    // chunk (k + 1) & 1 was drained to the host in the previous iteration
+    if (k + 1 < nchunks && (rc = issue(k + 1))) return rc;
+    SALVUS_CUDA(cudaEventSynchronize(p->pin_ev[k & 1]));
+    const size_t off = k * kPinChunk, n = std::min(kPinChunk, bytes - off);
+    par_memcpy((char *)dst + off, p->h_pin[k & 1], n);
+  }
+  return SALVUS_OK;
+}
+
 static salvus::DeviceBuffer *field_buffer(salvus_problem *p, int32_t f) {
   switch (f) {
     case SALVUS_FIELD_U: return &p->d_u;
@@ -1757,12 +1833,13 @@ int salvus_problem_set_field(salvus_problem *p, int32_t f, int32_t shot, const d
   const size_t N = (size_t)p->mesh->G * p->c;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
   if (p->prec == SALVUS_FP64) {
-    SALVUS_CUDA(cudaMemcpyAsync(b->ptr, vals, 8 * N, cudaMemcpyHostToDevice, p->stream));
+    int rc = copy_h2d(p, b->ptr, vals, 8 * N);
+    if (rc) return rc;
   } else {
     // FP64 host array -> FP64 staging on the device -> FP32 field
     int rc;
     if (p->d_stage.bytes < 8 * N && (rc = p->d_stage.alloc(8 * N))) return rc;
-    SALVUS_CUDA(cudaMemcpyAsync(p->d_stage.ptr, vals, 8 * N, cudaMemcpyHostToDevice, p->stream));
+    if ((rc = copy_h2d(p, p->d_stage.ptr, vals, 8 * N))) return rc;
     convert_kernel<double, float><<<blocks_for((int64_t)N, 256), 256, 0, p->stream>>>(
         (int64_t)N, p->d_stage.as<double>(), b->as<float>());
     g_launches++;
@@ -1780,7 +1857,8 @@ int salvus_problem_get_field(salvus_problem *p, int32_t f, int32_t shot, double 
   const size_t N = (size_t)p->mesh->G * p->c;
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
   if (p->prec == SALVUS_FP64) {
-    SALVUS_CUDA(cudaMemcpyAsync(vals, b->ptr, 8 * N, cudaMemcpyDeviceToHost, p->stream));
+    int rc = copy_d2h(p, vals, b->ptr, 8 * N);
+    if (rc) return rc;
   } else {
     int rc;
     if (p->d_stage.bytes < 8 * N && (rc = p->d_stage.alloc(8 * N))) return rc;
@@ -1788,7 +1866,7 @@ int salvus_problem_get_field(salvus_problem *p, int32_t f, int32_t shot, double 
         (int64_t)N, b->as<float>(), p->d_stage.as<double>());
     g_launches++;
     if ((rc = check_launch("convert"))) return rc;
-    SALVUS_CUDA(cudaMemcpyAsync(vals, p->d_stage.ptr, 8 * N, cudaMemcpyDeviceToHost, p->stream));
+    if ((rc = copy_d2h(p, vals, p->d_stage.ptr, 8 * N))) return rc;
   }
   SALVUS_CUDA(cudaStreamSynchronize(p->stream));
   return device_status(p);

@@ -135,6 +135,10 @@ struct salvus_problem {
   salvus::DeviceBuffer d_u, d_v, d_a, d_ap, d_r;
   salvus::DeviceBuffer d_step;   // int64 device step counter
   salvus::DeviceBuffer d_stage;  // FP64 staging for host field copies
+  // pinned host bounce buffers for field copies (two chunks, allocated on
+  // the first large copy) and the events that guard their reuse
+  void *h_pin[2] = {nullptr, nullptr};
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   salvus::DeviceBuffer d_err;    // int: device-side error word (bounded waits)
   // homogeneous Dirichlet: element-local points (e*P + p) whose stiffness
   // rows are zeroed

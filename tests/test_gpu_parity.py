@@ -204,3 +204,24 @@ def test_errors_are_loud():
     p.step()
     with pytest.raises(core.SalvusError):
         p.seismograms(0, 5)  # only one step held
+
+
+@pytest.mark.parametrize("precision", [core.FP64, core.FP32])
+def test_large_field_round_trip(precision):
+    """Fields larger than the pinned bounce chunks (4.2 M nodes x 3 x 8 B =
+    100 MB) round-trip through set_field / get_field: exactly in FP64, as the
+    FP32 rounding of the input in FP32."""
+    cfg = configs.elastic_hex(nel=40, order=4, n_receivers=1)
+    mesh = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                     cfg["params"])
+    prob = core.Problem(mesh, precision, dt=1e-3)
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((mesh.n_nodes, 3))
+    assert x.nbytes > 64 << 20
+    for name in ("u", "v"):
+        prob.set_field(name, x)
+        y = prob.get_field(name)
+        want = x if precision == core.FP64 else x.astype(np.float32).astype(np.float64)
+        assert np.array_equal(y, want)
+    prob.close()
+    mesh.close()
