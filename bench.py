@@ -100,7 +100,8 @@ def cpu_leg(args, nel_sample, steps, warm, target_s=10.0):
         o.add_receiver(r)
     dt = 1e-3
     t0 = time.perf_counter()
-    o.run(max(1, warm), dt)  # warm-up, also sizes the sample
+    if warm > 0:
+        o.run(warm, dt)  # warm-up, also sizes the sample
     per_step = (time.perf_counter() - t0) / max(1, warm)
     if steps is None:  # about target_s of CPU work, 2..200 steps
         steps = int(min(200, max(2, target_s / max(per_step, 1e-6))))
@@ -434,15 +435,21 @@ def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8):
 def reference_arm(args, rank, world):
     if rank != 0:
         return
-    # each step is the full step of a 32^3-element sample of the workload;
-    # the timed steps are sized to about 30 s of CPU work (at most --steps)
-    nel_sample = min(args.nel, 32)
-    warm = 1
-    rate, thr, sample, el = cpu_leg(args, nel_sample, None, warm, target_s=30.0)
-    steps = int(sample.split(" x ")[1].split(" steps")[0])
+    # Exactly --warmup + --steps steps, each the full step of a bounded
+    # sample of the workload: the 32^3-element sample when that keeps the
+    # whole run near two minutes, else a smaller cube sized to that budget.
+    from oracle import pyoracle as po  # noqa: F401  (fails loudly if the oracle is not built)
+    K, W = max(1, args.steps), max(1, args.warmup)
+    nel = min(args.nel, 32)
+    _, _, _, el = cpu_leg(args, nel, 1, 0)
+    per_step = el
+    budget = 120.0
+    if (K + W) * per_step > budget:
+        nel = max(6, int(nel * (budget / ((K + W) * per_step)) ** (1.0 / 3.0)))
+    rate, thr, sample, el = cpu_leg(args, nel, K, W)
     line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC,
-            "n_gpus": args.gpus, "steps": steps, "warmup": warm, "higher_is_better": True,
-            "ms_per_step": 1e3 * el / steps, "dtype": "f64", "data": "synthetic",
+            "n_gpus": args.gpus, "steps": K, "warmup": W, "higher_is_better": True,
+            "ms_per_step": 1e3 * el / K, "dtype": "f64", "data": "synthetic",
             "scaling": "weak", "vs_baseline": None,
             "config": workload(args),
             "cpu_baseline": {"value": rate, "unit": METRIC, "cores": thr, "kind": "port",
@@ -451,7 +458,7 @@ def reference_arm(args, rank, world):
                     "d2h_bytes_per_step": 0},
             "note": "the reference needs PETSc/Eigen/HDF5/Exodus (absent); its CPU path is "
                     "timed through the oracle port, which restates it and keeps its per-point "
-                    "Jacobian rebuild cost"}
+                    "Jacobian rebuild cost; each step is one full step of the sample mesh"}
     print(json.dumps(line), flush=True)
 
 
