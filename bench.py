@@ -63,6 +63,24 @@ def env_rank():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def max_over_ranks(x, dist=None, device="cuda"):
+    """The largest of each rank's x (every rank gets it); x itself without a
+    process group.  Replicas time the same work, so the job's time is the
+    slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(nodes, steps, ms, world):
+    """Whole-job GLL-point updates/s of `world` replicas that each advanced
+    `nodes` nodes `steps` steps, from the max-over-ranks time in ms."""
+    return world * nodes * steps / (ms / 1e3)
+
+
 def workload(args):
     return {"workload": f"elastic3d hex {args.nel}^3 order {args.order}, 64 receivers, "
                         f"moment-tensor Ricker, GRF model",
@@ -543,12 +561,7 @@ def main():
         b.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms = a.elapsed_time(b)
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(a.elapsed_time(b), dist, "cuda")
 
     def timed(fn):
         return timed_on(p, fn)
@@ -562,12 +575,12 @@ def main():
     ms = timed(lambda: p.run(args.steps, core.RUN_GRAPH))
     launches = core.launch_count() - l0
     ck = clocks.stop()
-    value = world * G * args.steps / (ms / 1e3)
+    value = replica_rate(G, args.steps, ms, world)
 
     # plain form: one host launch sequence per step
     kp = min(args.steps, 200)
     ms_plain = timed(lambda: p.run(kp, core.RUN_PLAIN))
-    plain = world * G * kp / (ms_plain / 1e3)
+    plain = replica_rate(G, kp, ms_plain, world)
 
     # per-kernel device time (events around each launch, plain form)
     p.profile(True)
@@ -612,7 +625,7 @@ def main():
         seis_holder["s"] = p2.seismograms(0, args.steps)
 
     ms_e2e = timed_on(p2, e2e_job)
-    e2e = world * G * args.steps / (ms_e2e / 1e3)
+    e2e = replica_rate(G, args.steps, ms_e2e, world)
     h2d = 2 * G * 3 * 8 / args.steps
     d2h = len(cfg["receivers"]) * 3 * 8
 
