@@ -338,6 +338,14 @@ int salvus_profile_read(salvus_problem *p, int32_t max_entries, const char **nam
 /* Total kernel launches issued by this library in this process. */
 int64_t salvus_launch_count(void);
 
+/* Energy of the current state, 1/2 v^T M v (kinetic) and 1/2 u^T K u
+ * (strain, with Dirichlet rows zeroed), each summed in FP64 with Kahan
+ * compensation on the GPU and over the CTA partials in a fixed order, so the
+ * result is the same on every run.  No counterpart in the reference: a
+ * conservation diagnostic (the explicit Newmark step keeps it bounded
+ * without sources).  Single-shot problems only.  Synchronous. */
+int salvus_problem_energy(salvus_problem *problem, double *kinetic, double *strain);
+
 /* ---- Exodus II meshes and models (no reference-side library needed) ----
  * Reads the NetCDF classic containers (CDF-1, 64-bit-offset CDF-2) that the
  * Exodus library writes, with the Exodus II names the reference reads:

@@ -66,6 +66,7 @@ SIGNATURES = [
     ("salvus_mesh_inverse_mass", ctypes.c_int, [_VP, _DP]),
     ("salvus_mesh_boundary_nodes", ctypes.c_int, [_VP, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
     ("salvus_problem_set_dirichlet", ctypes.c_int, [_VP, _I64, ctypes.POINTER(_I64)]),
+    ("salvus_problem_energy", ctypes.c_int, [_VP, _DP, _DP]),
     ("salvus_exodus_open", ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
     ("salvus_exodus_close", ctypes.c_int, [_VP]),
     ("salvus_exodus_info", ctypes.c_int, [_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I32),
@@ -278,6 +279,12 @@ class Problem:
         nodes = np.ascontiguousarray(nodes, dtype=np.int64)
         _check(lib().salvus_problem_set_dirichlet(self.h, len(nodes),
                                                   nodes.ctypes.data_as(ctypes.POINTER(_I64))))
+
+    def energy(self):
+        """(kinetic, strain) energy of the current state, FP64 compensated sums."""
+        k, e = ctypes.c_double(), ctypes.c_double()
+        _check(lib().salvus_problem_energy(self.h, ctypes.byref(k), ctypes.byref(e)))
+        return k.value, e.value
 
     def set_seismogram_capacity(self, steps):
         _check(lib().salvus_problem_set_seismogram_capacity(self.h, int(steps)))

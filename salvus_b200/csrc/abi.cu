@@ -1971,6 +1971,65 @@ int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
   return SALVUS_OK;
 }
 
+// Energy of the current state: -K u into a scratch field (stiffness and
+// Dirichlet zeroing, then the gather), then the compensated FP64 sums.
+extern "C++" {
+template <typename real, int C>
+static int energy_t(salvus_problem *p, double *kinetic, double *strain) {
+  const salvus_mesh *m = p->mesh;
+  const size_t N = (size_t)m->G * C;
+  int rc;
+  if (p->d_escr.bytes < N * sizeof(real) && (rc = p->d_escr.alloc(N * sizeof(real)))) return rc;
+  constexpr int kBlocks = 1024;
+  if (p->d_epart.bytes < 2 * kBlocks * sizeof(double) &&
+      (rc = p->d_epart.alloc(2 * kBlocks * sizeof(double))))
+    return rc;
+  if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
+                                   p->d_err.as<int>())))
+    return rc;
+  if ((rc = launch_dirichlet<real, C>(p))) return rc;
+  gather_kernel<real, C, 1><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(
+      m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), F<real>(p->d_r), nullptr,
+      nullptr, nullptr, nullptr, p->d_escr.as<real>(), (real)0);
+  g_launches++;
+  if ((rc = check_launch("energy gather"))) return rc;
+  energy_kernel<real, C><<<kBlocks, 256, 0, p->stream>>>(
+      m->G, F<real>(p->d_u), F<real>(p->d_v), p->d_escr.as<real>(), m->d_mi64.as<double>(),
+      p->d_epart.as<double>());
+  g_launches++;
+  if ((rc = check_launch("energy"))) return rc;
+  std::vector<double> h(2 * kBlocks);
+  SALVUS_CUDA(cudaMemcpyAsync(h.data(), p->d_epart.ptr, sizeof(double) * h.size(),
+                              cudaMemcpyDeviceToHost, p->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  // Kahan over the block partials, in block order
+  double sk = 0, ck = 0, ss = 0, cs = 0;
+  for (int b = 0; b < kBlocks; ++b) {
+    const double yk = h[2 * b] - ck, tk = sk + yk;
+    ck = (tk - sk) - yk;
+    sk = tk;
+    const double ys = h[2 * b + 1] - cs, ts = ss + ys;
+    cs = (ts - ss) - ys;
+    ss = ts;
+  }
+  if (kinetic) *kinetic = sk;
+  if (strain) *strain = ss;
+  return device_status(p);
+}
+}  // extern "C++"
+
+int salvus_problem_energy(salvus_problem *p, double *kinetic, double *strain) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  if (p->shots > 1)
+    return fail(SALVUS_E_UNSUPPORTED, "energy is computed for single-shot problems");
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  return by_components(p->c, [&](auto cc) {
+    constexpr int C = decltype(cc)::value;
+    return p->prec == SALVUS_FP32 ? energy_t<float, C>(p, kinetic, strain)
+                                  : energy_t<double, C>(p, kinetic, strain);
+  });
+}
+
 int salvus_synchronize(salvus_problem *p) {
   if (!p) return fail(SALVUS_E_INVALID, "null problem");
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));

@@ -135,6 +135,7 @@ struct salvus_problem {
   salvus::DeviceBuffer d_u, d_v, d_a, d_ap, d_r;
   salvus::DeviceBuffer d_step;   // int64 device step counter
   salvus::DeviceBuffer d_stage;  // FP64 staging for host field copies
+  salvus::DeviceBuffer d_escr, d_epart;  // energy: -K u scratch, block partials
   // pinned host bounce buffers for field copies (two chunks, allocated on
   // the first large copy) and the events that guard their reuse
   void *h_pin[2] = {nullptr, nullptr};

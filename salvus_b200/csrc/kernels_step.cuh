@@ -279,6 +279,52 @@ __global__ void dot_kernel(int64_t N, int C, const real *__restrict__ x, const r
   if (threadIdx.x == 0) partial[blockIdx.x] = sh[0];
 }
 
+// Energy 1/2 v^T M v and 1/2 u^T K u with FP64 compensated (Kahan) sums:
+// each thread accumulates its grid-stride share of the nodes with a running
+// compensation, the CTA adds the threads' sums in a fixed tree order, and
+// partial[2 * block] / [2 * block + 1] (kinetic, strain) are summed on the
+// host in block order -- the same bits on every run for a given grid.
+// ku = -K u (the gathered stiffness action); M = 1 / mi per node, nodes
+// without mass (mi = 0) carry none.
+template <typename real, int C>
+__global__ void __launch_bounds__(256)
+energy_kernel(int64_t G, const real *__restrict__ u, const real *__restrict__ v,
+              const real *__restrict__ ku, const double *__restrict__ mi,
+              double *__restrict__ partial) {
+  __shared__ double sk[256], ss[256];
+  double ek = 0.0, ck = 0.0, es = 0.0, cs = 0.0;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    const double m = mi[g] != 0.0 ? 1.0 / mi[g] : 0.0;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      const double vv = (double)v[g * C + c], uu = (double)u[g * C + c];
+      const double yk = 0.5 * m * vv * vv - ck;
+      const double tk = ek + yk;
+      ck = (tk - ek) - yk;
+      ek = tk;
+      const double ys = -0.5 * uu * (double)ku[g * C + c] - cs;
+      const double ts = es + ys;
+      cs = (ts - es) - ys;
+      es = ts;
+    }
+  }
+  sk[threadIdx.x] = ek;
+  ss[threadIdx.x] = es;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      sk[threadIdx.x] += sk[threadIdx.x + o];
+      ss[threadIdx.x] += ss[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = sk[0];
+    partial[2 * blockIdx.x + 1] = ss[0];
+  }
+}
+
 template <typename A, typename B>
 __global__ void convert_kernel(int64_t N, const A *__restrict__ a, B *__restrict__ b) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
