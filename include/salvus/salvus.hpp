@@ -219,6 +219,8 @@ class ProblemBase {
   virtual void setField(const std::string &name, const std::vector<double> &v) = 0;
   // HomogeneousDirichlet (HomogeneousDirichlet.cpp:14-78) on these nodes
   virtual void setDirichlet(const std::vector<int64_t> &nodes) = 0;
+  // {kinetic, strain} energy of the current state (FP64 compensated sums)
+  virtual std::array<double, 2> energy() = 0;
 };
 
 // Order2Newmark over one element type (Order2Newmark.h:6-26).
@@ -238,6 +240,11 @@ class Problem : public ProblemBase {
   void addReceiver(const Receiver &r) override {
     check(salvus_problem_add_receiver(p_.get(), r.location.data()));
     ++receivers_;
+  }
+  std::array<double, 2> energy() override {
+    std::array<double, 2> e{0, 0};
+    check(salvus_problem_energy(p_.get(), &e[0], &e[1]));
+    return e;
   }
   void setDirichlet(const std::vector<int64_t> &nodes) override {
     check(salvus_problem_set_dirichlet(p_.get(), (int64_t)nodes.size(), nodes.data()));
