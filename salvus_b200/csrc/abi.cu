@@ -400,8 +400,12 @@ static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, 
     }
   }
   if (m->shape == SALVUS_TRI) {
-    tri_acoustic_kernel<real><<<blocks_for(m->E, 128), 128, 0, st>>>(
-        m->E, rec, m->d_conn.as<int32_t>(), simplex_tables<real>(m), u, r);
+    if (m->tri_kernel == 2)
+      tri_acoustic_kernel<real><<<blocks_for(m->E, 128), 128, 0, st>>>(
+          m->E, rec, m->d_conn.as<int32_t>(), simplex_tables<real>(m), u, r);
+    else
+      tri_acoustic_const_kernel<real><<<blocks_for(m->E, 128), 128, 0, st>>>(
+          m->E, rec, m->d_conn.as<int32_t>(), u, r);
     g_launches++;
     return check_launch("triangle stiffness");
   }
@@ -471,6 +475,16 @@ static int build_simplex_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer
   if ((rc = sd.alloc(sizeof(real) * t.size()))) return rc;
   SALVUS_CUDA(cudaMemcpyAsync(sd.ptr, t.data(), sizeof(real) * t.size(), cudaMemcpyHostToDevice,
                               m->stream));
+  if (m->shape == SALVUS_TRI) {
+    // the reference triangle's table, identical for every mesh: constant
+    // memory of this device (tri_acoustic_const_kernel)
+    if (sizeof(real) == 4)
+      SALVUS_CUDA(cudaMemcpyToSymbolAsync(c_tri_sd32, t.data(), sizeof(real) * t.size(), 0,
+                                          cudaMemcpyHostToDevice, m->stream));
+    else
+      SALVUS_CUDA(cudaMemcpyToSymbolAsync(c_tri_sd64, t.data(), sizeof(real) * t.size(), 0,
+                                          cudaMemcpyHostToDevice, m->stream));
+  }
   if (sizeof(real) == 4 && m->shape == SALVUS_TRI) {
     // tensor-core operand images (kernels_tri_tc.cuh), K-major no-swizzle
     // core-matrix order, TF32 hi part and FP32 remainder, zero padding:
@@ -1389,10 +1403,11 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
     // the CUDA-core kernel (read when the mesh is created)
     const char *s = std::getenv("SALVUS_TET_KERNEL");
     m->tet_kernel = (s && std::strcmp(s, "cuda") == 0) ? 1 : 0;
-    // FP32 triangles: SALVUS_TRI_KERNEL=tc selects the tensor-core kernel,
-    // anything else the CUDA-core one (read when the mesh is created)
+    // triangles: CUDA cores with the derivative table in constant memory by
+    // default; SALVUS_TRI_KERNEL=tc selects the tensor-core kernel (FP32),
+    // =shared the shared-memory-table kernel (read when the mesh is created)
     const char *t = std::getenv("SALVUS_TRI_KERNEL");
-    m->tri_kernel = (t && std::strcmp(t, "tc") == 0) ? 0 : 1;
+    m->tri_kernel = (t && std::strcmp(t, "tc") == 0) ? 0 : (t && std::strcmp(t, "shared") == 0) ? 2 : 1;
   }
   m->shape = d->shape;
   m->order = d->order;

@@ -119,7 +119,7 @@ struct salvus_mesh {
   salvus::DeviceBuffer d_tc_tab;          // tetrahedra: tensor-core operand image (hi | lo)
   salvus::DeviceBuffer d_elist, d_cls_k, d_cpl_pts, d_cpl32, d_cpl64;
   int tet_kernel = 0;                     // FP32 tetrahedra: 0 tensor cores, 1 CUDA cores
-  int tri_kernel = 1;                     // FP32 triangles: 0 tensor cores, 1 CUDA cores
+  int tri_kernel = 1;                     // triangles: 0 tensor cores (FP32), 1 constant-table, 2 shared-table
   cudaStream_t stream = nullptr;
 };
 

@@ -172,6 +172,83 @@ tri_acoustic_kernel(int64_t E, const real *__restrict__ rec, const int32_t *__re
   for (int i = 0; i < P; ++i) r[e * P + i] = -acc[i];
 }
 
+// The triangle's derivative table (2 x 12 x 12, the same for every mesh) in
+// constant memory: with the loops fully unrolled every table entry is a
+// compile-time constant-bank operand of its FMA, so the contractions issue
+// no shared-memory loads at all (the shared-table kernel above is L1-bound).
+__constant__ float c_tri_sd32[2 * 12 * 12];
+__constant__ double c_tri_sd64[2 * 12 * 12];
+template <typename real>
+__device__ __forceinline__ real tri_sd(int i) {
+  if constexpr (sizeof(real) == 4) return c_tri_sd32[i];
+  else return c_tri_sd64[i];
+}
+
+// Same arithmetic and summation order as tri_acoustic_kernel.
+template <typename real>
+__global__ void __launch_bounds__(128)
+tri_acoustic_const_kernel(int64_t E, const real *__restrict__ rec,
+                          const int32_t *__restrict__ conn, const real *__restrict__ u,
+                          real *__restrict__ r) {
+  constexpr int P = 12;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= E) return;
+  // the element's record, connectivity and residual as 16-byte words
+  // (record 64 B, connectivity 48 B, residual 48 B per FP32 element)
+  real rc[kTriRec];
+  int32_t cn[P];
+  if constexpr (sizeof(real) == 4) {
+    const float4 *r4 = reinterpret_cast<const float4 *>(rec + e * kTriRec);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const float4 x = __ldg(r4 + v);
+      rc[4 * v] = x.x; rc[4 * v + 1] = x.y; rc[4 * v + 2] = x.z; rc[4 * v + 3] = x.w;
+    }
+    const int4 *c4 = reinterpret_cast<const int4 *>(conn + e * P);
+#pragma unroll
+    for (int v = 0; v < 3; ++v) {
+      const int4 x = __ldg(c4 + v);
+      cn[4 * v] = x.x; cn[4 * v + 1] = x.y; cn[4 * v + 2] = x.z; cn[4 * v + 3] = x.w;
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < kTriRec; ++a) rc[a] = rec[e * kTriRec + a];
+#pragma unroll
+    for (int j = 0; j < P; ++j) cn[j] = conn[e * P + j];
+  }
+  const real g00 = rc[0], g01 = rc[1], g11 = rc[2];
+  real ue[P], acc[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    ue[j] = u[cn[j]];
+    acc[j] = 0;
+  }
+#pragma unroll
+  for (int q = 0; q < P; ++q) {
+    real a0 = 0, a1 = 0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      a0 += tri_sd<real>(j * P + q) * ue[j];
+      a1 += tri_sd<real>(P * P + j * P + q) * ue[j];
+    }
+    const real s = rc[4 + q];
+    const real f0 = s * (g00 * a0 + g01 * a1);
+    const real f1 = s * (g01 * a0 + g11 * a1);
+#pragma unroll
+    for (int i = 0; i < P; ++i)
+      acc[i] += tri_sd<real>(i * P + q) * f0 + tri_sd<real>(P * P + i * P + q) * f1;
+  }
+  if constexpr (sizeof(real) == 4) {
+    float4 *o4 = reinterpret_cast<float4 *>(r + e * P);
+#pragma unroll
+    for (int v = 0; v < 3; ++v)
+      o4[v] = make_float4(-acc[4 * v], -acc[4 * v + 1], -acc[4 * v + 2], -acc[4 * v + 3]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < P; ++i) r[e * P + i] = -acc[i];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Tetrahedron (acoustic C = 1, elastic C = 3) on CUDA cores: one thread per
 // element node, EPB elements per CTA.  The derivative table is held twice in
