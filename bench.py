@@ -265,8 +265,8 @@ def simplex_leg(core, configs, timed, steps, device=0, tet_n=55):
 
 
 def elastic2d_leg(core, configs, timed, steps, device=0, nel=720, peak=None):
-    """2-D elastic quads (Elastic2D physics, SURVEY next row): FP32, order 4,
-    nel^2 distorted-free structured quads over 10 x 10 km, 5 % GRF, weak VTI
+    """2-D elastic quads (Elastic2D physics): FP32, order 4,
+    nel^2 undistorted structured quads over 10 x 10 km, 5 % GRF, weak VTI
     anisotropy, moment-tensor + force Ricker sources, 16 receivers.  Timed as
     graph-replayed steps; the stiffness kernel per launch against HBM."""
     cfg = configs.elastic_2d(nel=nel, order=4)
