@@ -165,3 +165,32 @@ def test_invalid_meshes_rejected():
     m = core.Mesh(core.QUAD, 4, core.ACOUSTIC, V, C, par, device=-1)
     with pytest.raises(core.SalvusError):
         core.Problem(m)
+
+
+def test_invalid_physics_meshes_rejected():
+    """2-D elastic and fluid-solid physics need quadrilaterals; the fluid flag
+    must be 0 or 1 and the same at all four vertices of an element."""
+    V, C = meshgen.structured_quad(3, 3, 3.0, 3.0)
+    E = len(C)
+    with pytest.raises(core.SalvusError):
+        Vh, Ch = meshgen.structured_hex(1, 1, 1, 1.0, 1.0, 1.0)
+        core.Mesh(core.HEX, 2, core.ELASTIC2D, Vh, Ch, np.ones((5, 1, 8)), device=-1)
+    Vt, Ct = meshgen.delaunay_tri(3, 3, 3.0, 3.0, seed=1)
+    with pytest.raises(core.SalvusError):
+        core.Mesh(core.TRI, 3, core.COUPLED2D, Vt, Ct, np.ones((7, len(Ct), 3)), device=-1)
+    par = np.ones((7, E, 4))
+    par[0] = 0.0
+    par[0][4] = 1.0
+    m = core.Mesh(core.QUAD, 3, core.COUPLED2D, V, C, par, device=-1)  # one fluid element
+    assert m.n_components == 3
+    m.close()
+    half = par.copy()
+    half[0][2] = 0.5
+    with pytest.raises(core.SalvusError, match="FLUID"):
+        core.Mesh(core.QUAD, 3, core.COUPLED2D, V, C, half, device=-1)
+    mixed = par.copy()
+    mixed[0][3, 1] = 1.0
+    with pytest.raises(core.SalvusError, match="FLUID"):
+        core.Mesh(core.QUAD, 3, core.COUPLED2D, V, C, mixed, device=-1)
+    with pytest.raises(core.SalvusError):
+        core.Mesh(core.QUAD, 3, 7, V, C, par, device=-1)
