@@ -257,7 +257,9 @@ int salvus_apply_stiffness_noalloc(const salvus_mesh *mesh, int32_t precision, c
  * A group of FP32 single-shot problems of one element class (acoustic quads
  * or elastic hexahedra of one order, on one device) advances with one launch
  * per step stage for all members (SALVUS_GROUP_STEP=persistent: one
- * persistent work-queue launch per step): every CTA runs the single-problem
+ * persistent work-queue launch per step; SALVUS_GROUP_STEP=partitioned: one
+ * cooperative launch per step, each member on its own range of resident
+ * CTAs): every CTA runs the single-problem
  * kernel body on its member's arrays, so each member's result is bitwise the
  * one it gets alone.  salvus_group_run(g, n) advances
  * every member n steps (graph-replayed in chunks of 32); it orders itself

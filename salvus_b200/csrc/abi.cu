@@ -1156,7 +1156,11 @@ struct salvus_group {
   std::vector<salvus_problem *> members;
   const salvus_mesh *m0 = nullptr;
   int c = 1;
-  bool stages = true;  // one launch per stage; SALVUS_GROUP_STEP=persistent: one launch per step
+  bool stages = true;  // one launch per stage; SALVUS_GROUP_STEP=persistent: one queue launch per step
+  bool partitioned = false;  // SALVUS_GROUP_STEP=partitioned: one cooperative launch per step
+  std::vector<salvus::GroupPart> parts;
+  salvus::DeviceBuffer d_parts, d_bars;
+  int coop_slots = 0;  // co-resident CTAs of the partitioned kernel
   std::vector<salvus::GroupSlot> slots;
   salvus::DeviceBuffer d_slots;
   int64_t n_stiff = 0, n_gather = 0, n_rec = 0;
@@ -1184,6 +1188,8 @@ static int group_upload(salvus::DeviceBuffer &b, const void *src, size_t bytes, 
   SALVUS_CUDA(cudaMemcpyAsync(b.ptr, src, bytes, cudaMemcpyHostToDevice, st));
   return SALVUS_OK;
 }
+
+static int group_partitioned(salvus_group *g, bool launch);
 
 static int group_fill(salvus_group *g) {
   int64_t bs = 0, bg = 0, br = 0;
@@ -1264,6 +1270,8 @@ static int group_fill(salvus_group *g) {
     if ((rc = g->d_sync.alloc(sizeof(GroupSync)))) return rc;
     SALVUS_CUDA(cudaMemsetAsync(g->d_sync.ptr, 0, sizeof(GroupSync), g->stream));
   }
+  // the partitioned step's CTA ranges and counters (allocated here, before any capture)
+  if (g->partitioned) return group_partitioned(g, false);
   return SALVUS_OK;
 }
 
@@ -1319,7 +1327,106 @@ static int group_persistent(salvus_group *g) {
   return fail(SALVUS_E_UNSUPPORTED, "no grouped step for order %d", m->order);
 }
 
+// launch=false: size the member CTA ranges (once) and allocate their counters;
+// launch=true: one cooperative launch of the step
+template <int N, bool kHex, int C>
+static int group_partitioned_t(salvus_group *g, bool launch) {
+  constexpr int threads = 128;
+  size_t smem = 0;
+  if constexpr (kHex) {
+    constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
+    smem = ElasticV2Shape<N, EPB, false>::SMEM;
+  }
+  auto kern = group_partitioned_step<N, kHex, C>;
+  const int J = (int)g->members.size();
+  if (!launch) {
+    if (g->coop_slots == 0) {
+      if (smem) SALVUS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      int per_sm = 0;
+      SALVUS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem));
+      g->coop_slots = (per_sm > 0 ? per_sm : 1) * g->m0->sm_count;
+    }
+    if (g->parts.size() == (size_t)J) return SALVUS_OK;
+    // CTAs per member in proportion to its work (element points + nodes), at least one
+    if (J > g->coop_slots)
+      return fail(SALVUS_E_UNSUPPORTED, "%d members exceed the %d co-resident CTAs", J, g->coop_slots);
+    const int tile = 128;
+    std::vector<double> w(J);
+    double wsum = 0;
+    for (int j = 0; j < J; ++j) {
+      const salvus_mesh *m = g->members[j]->mesh;
+      w[j] = (double)m->E * m->P + (double)m->G;
+      wsum += w[j];
+    }
+    std::vector<GroupPart> parts(J);
+    const int spare = g->coop_slots - J;
+    int first = 0;
+    for (int j = 0; j < J; ++j) {
+      const salvus_mesh *m = g->members[j]->mesh;
+      GroupPart &pt = parts[j];
+      pt.cta_first = first;
+      pt.cta_count = 1 + (int)std::floor((double)spare * w[j] / wsum);
+      pt.n_stiff = (int32_t)group_stiff_blocks(m);
+      pt.n_gather = (int32_t)((m->G + tile - 1) / tile);
+      first += pt.cta_count;
+    }
+    int rc = group_upload(g->d_parts, parts.data(), sizeof(GroupPart) * J, g->stream);
+    if (rc) return rc;
+    if ((rc = g->d_bars.alloc(sizeof(GroupBar) * J))) return rc;
+    SALVUS_CUDA(cudaMemsetAsync(g->d_bars.ptr, 0, sizeof(GroupBar) * J, g->stream));
+    g->parts = std::move(parts);
+    return SALVUS_OK;
+  }
+  if (g->parts.size() != (size_t)J) return fail(SALVUS_E_INVALID, "partitioned group not set up");
+  const int grid = g->parts.back().cta_first + g->parts.back().cta_count;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = g->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  SALVUS_CUDA(cudaLaunchKernelEx(&cfg, kern, (const GroupSlot *)g->d_slots.as<GroupSlot>(),
+                                 (const GroupPart *)g->d_parts.as<GroupPart>(), J,
+                                 g->d_bars.as<GroupBar>(), g->d_sync.as<GroupSync>(),
+                                 dmatrix<float>(g->m0->basis), g->m0->P));
+  g_launches++;
+  return check_launch("group partitioned step");
+}
+
+static int group_partitioned(salvus_group *g, bool launch) {
+  const salvus_mesh *m = g->m0;
+  if (m->shape == SALVUS_HEX) {
+    switch (m->order) {
+      case 1: return group_partitioned_t<1, true, 3>(g, launch);
+      case 2: return group_partitioned_t<2, true, 3>(g, launch);
+      case 3: return group_partitioned_t<3, true, 3>(g, launch);
+      case 4: return group_partitioned_t<4, true, 3>(g, launch);
+      case 5: return group_partitioned_t<5, true, 3>(g, launch);
+      case 6: return group_partitioned_t<6, true, 3>(g, launch);
+    }
+  } else {
+    switch (m->order) {
+      case 1: return group_partitioned_t<1, false, 1>(g, launch);
+      case 2: return group_partitioned_t<2, false, 1>(g, launch);
+      case 3: return group_partitioned_t<3, false, 1>(g, launch);
+      case 4: return group_partitioned_t<4, false, 1>(g, launch);
+      case 5: return group_partitioned_t<5, false, 1>(g, launch);
+      case 6: return group_partitioned_t<6, false, 1>(g, launch);
+      case 7: return group_partitioned_t<7, false, 1>(g, launch);
+      case 8: return group_partitioned_t<8, false, 1>(g, launch);
+      case 9: return group_partitioned_t<9, false, 1>(g, launch);
+      case 10: return group_partitioned_t<10, false, 1>(g, launch);
+    }
+  }
+  return fail(SALVUS_E_UNSUPPORTED, "no grouped step for order %d", m->order);
+}
+
 static int group_step(salvus_group *g) {
+  if (g->partitioned) return group_partitioned(g, true);
   if (!g->stages) return group_persistent(g);
   const int J = (int)g->members.size();
   const int P = g->m0->P;
@@ -2172,11 +2279,13 @@ int salvus_group_create(salvus_problem *const *members, int32_t n, salvus_group 
   g->m0 = m0;
   g->c = m0->physics == SALVUS_ELASTIC3D ? 3 : 1;
   {
-    // measured: one launch per stage beats the single persistent work-queue
-    // launch (whose combined kernel runs the latency-bound gather at the
-    // occupancy of its heaviest body), so it is the default
+    // measured: one launch per stage beats both single-launch forms (the
+    // work-queue and the member-partitioned kernel, whose combined bodies
+    // run the latency-bound gather at the occupancy of the heaviest body),
+    // so it is the default
     const char *s = std::getenv("SALVUS_GROUP_STEP");
-    g->stages = !(s && std::strcmp(s, "persistent") == 0);
+    g->partitioned = s && std::strcmp(s, "partitioned") == 0;
+    g->stages = !(s && (std::strcmp(s, "persistent") == 0 || g->partitioned));
   }
   SALVUS_CUDA(cudaSetDevice(m0->device));
   SALVUS_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
@@ -2221,7 +2330,7 @@ int salvus_group_run(salvus_group *g, int64_t n_steps) {
   int64_t done = 0;
   while (g->graph && n_steps - done >= g->graph_steps) {
     SALVUS_CUDA(cudaGraphLaunch(g->graph, g->stream));
-    g_launches += (int64_t)g->graph_steps * (g->n_rec > 0 ? 4 : 3);
+    g_launches += (int64_t)g->graph_steps * (g->stages ? (g->n_rec > 0 ? 5 : 4) : 1);
     done += g->graph_steps;
   }
   for (; done < n_steps; ++done)

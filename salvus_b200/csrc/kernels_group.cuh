@@ -193,11 +193,11 @@ group_persistent_step(const GroupSlot *__restrict__ slots, const GroupCounts *__
         break;
       case GI_GATHER:
         for (int b = w.first; b < w.first + w.count; ++b)
-          gather_body<float, C, 0>((int64_t)b * blockDim.x + t, m.G, m.inc_off, m.inc_idx, m.r, m.mi,
+          gather_body<float, C, 0, true>((int64_t)b * blockDim.x + t, m.G, m.inc_off, m.inc_idx, m.r, m.mi,
                                    m.u, m.v, m.ap, m.a, m.dt);
         break;
       case GI_REC:
-        receiver_body<float, C>(w.first, P, m.rec_elem, m.rec_l, m.conn, m.u, m.seis, m.cap, m.step);
+        receiver_body<float, C, true>(w.first, P, m.rec_elem, m.rec_l, m.conn, m.u, m.seis, m.cap, m.step);
         break;
       default:
         if (t == 0) *m.step += 1;
@@ -222,6 +222,110 @@ group_persistent_step(const GroupSlot *__restrict__ slots, const GroupCounts *__
     if (t == 0) {
       sync->head = 0ull;
       sync->finished = 0u;
+      __threadfence();
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// member-partitioned single-launch step
+//
+// group_partitioned_step: ONE cooperative launch per step.  Every member owns
+// a contiguous range of co-resident CTAs (sized to its share of the group's
+// work) and runs its whole step inside that range: stiffness tiles
+// round-robin over its CTAs; the member's first CTA, once all of them are
+// through the stiffness, adds the sources; after a flag every CTA takes its
+// gather tiles; after all gathers the receivers are spread over the CTAs;
+// the first CTA then advances the step.  A CTA only ever waits (bounded) for
+// CTAs of its own member, so members never hold each other up, and the
+// cooperative launch guarantees that all CTAs are resident.
+struct GroupPart {
+  int32_t cta_first, cta_count;  // the member's CTAs
+  int32_t n_stiff, n_gather;     // element groups, 128-node gather tiles
+};
+struct GroupBar {  // per member; the member's last CTA out zeroes it
+  int32_t stiff_done, src_done, gather_done, rec_done, out;
+};
+
+template <int N, bool kHex, int C>
+__global__ void __launch_bounds__(128, kHex ? 5 : 8)
+group_partitioned_step(const GroupSlot *__restrict__ slots, const GroupPart *__restrict__ parts,
+                       int J, GroupBar *__restrict__ bars, GroupSync *__restrict__ sync,
+                       DMatrix<float> Dm, int P) {
+  constexpr int n2 = (N + 1) * (N + 1);
+  constexpr int EPB = kHex ? (128 / n2 > 0 ? 128 / n2 : 1) : 1;
+  __shared__ int s_ok;
+  const int t = threadIdx.x;
+  // member of this CTA (cta_first ascending)
+  int lo = 0, hi = J - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (parts[mid].cta_first <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const GroupPart pt = parts[lo];
+  const GroupSlot &m = slots[lo];
+  GroupBar *gb = bars + lo;
+  const int b = (int)blockIdx.x - pt.cta_first, nb = pt.cta_count;
+  auto member_wait = [&](const int32_t *c, int32_t target) {
+    if (t == 0) s_ok = group_wait(c, target, sync);
+    __syncthreads();
+    return s_ok != 0;
+  };
+  auto arrive = [&](int32_t *c) {
+    __syncthreads();
+    if (t == 0) {
+      __threadfence();
+      atomicAdd(c, 1);
+    }
+  };
+  // stiffness
+  for (int k = b; k < pt.n_stiff; k += nb) {
+    if constexpr (kHex)
+      elastic_hex_v2_body<N, EPB, false>(k, m.E, m.rec, m.u, m.r, Dm);
+    else
+      acoustic_quad_col_body<N, quad_col_epb<N>(), float>(k, m.E, m.rec, m.conn, m.u, m.r, Dm);
+    __syncthreads();
+  }
+  arrive(&gb->stiff_done);
+  bool ok = true;
+  if (b == 0) {
+    ok = member_wait(&gb->stiff_done, nb);
+    if (ok && m.nsrc > 0)
+      source_body<float, C>(m.nsrc, P, m.src_elem, m.src_par, m.src_wts, m.step, m.dtd, m.r);
+    __syncthreads();
+    if (t == 0) {
+      __threadfence();
+      atomicExch(&gb->src_done, 1);
+    }
+  }
+  ok = ok && member_wait(&gb->src_done, 1);
+  // gather and update
+  if (ok)
+    for (int k = b; k < pt.n_gather; k += nb)
+      gather_body<float, C, 0, true>((int64_t)k * 128 + t, m.G, m.inc_off, m.inc_idx, m.r, m.mi,
+                                     m.u, m.v, m.ap, m.a, m.dt);
+  arrive(&gb->gather_done);
+  ok = ok && member_wait(&gb->gather_done, nb);
+  // receivers
+  if (ok)
+    for (int k = b; k < m.nrec; k += nb)
+      receiver_body<float, C, true>(k, P, m.rec_elem, m.rec_l, m.conn, m.u, m.seis, m.cap, m.step);
+  arrive(&gb->rec_done);
+  if (b == 0) {
+    ok = ok && member_wait(&gb->rec_done, nb);
+    if (ok && t == 0) *m.step += 1;
+  }
+  // the member's last CTA out resets its counters for the next launch
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    if (atomicAdd(&gb->out, 1) == nb - 1) {
+      gb->stiff_done = 0;
+      gb->src_done = 0;
+      gb->gather_done = 0;
+      gb->rec_done = 0;
+      gb->out = 0;
       __threadfence();
     }
   }

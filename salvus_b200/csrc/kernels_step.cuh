@@ -42,7 +42,9 @@ __device__ __forceinline__ void newmark_point(real an, real &ap, real &v, real &
 
 // mode 0: fused  a = mi * sum(r); Newmark update of (u, v, a_)
 // mode 1: gather a = sum(r)
-template <typename real, int C, int MODE>
+// kInKernelR: r was written earlier in the same launch (fused group steps)
+// and is read with coherent loads (ld.global.ca), not ld.global.nc.
+template <typename real, int C, int MODE, bool kInKernelR = false>
 __device__ __forceinline__ void gather_body(int64_t g, int64_t G, const int32_t *__restrict__ off,
                                             const int32_t *__restrict__ idx,
                                             const real *__restrict__ r,
@@ -76,7 +78,10 @@ __device__ __forceinline__ void gather_body(int64_t g, int64_t G, const int32_t 
 #pragma unroll
     for (int q = 0; q < kFast; ++q)
 #pragma unroll
-      for (int c = 0; c < C; ++c) rv[q][c] = q < cnt ? r[(int64_t)ep[q] * C + c] : real(0);
+      for (int c = 0; c < C; ++c) {
+        const real *rp = r + (int64_t)ep[q] * C + c;
+        rv[q][c] = q < cnt ? (kInKernelR ? __ldca(rp) : *rp) : real(0);
+      }
     // ascending element order, as in the general loop
 #pragma unroll
     for (int q = 0; q < kFast; ++q)
@@ -88,7 +93,7 @@ __device__ __forceinline__ void gather_body(int64_t g, int64_t G, const int32_t 
     for (int32_t q = q0; q < q1; ++q) {
       const int64_t e = idx[q];
 #pragma unroll
-      for (int c = 0; c < C; ++c) acc[c] += r[e * C + c];
+      for (int c = 0; c < C; ++c) acc[c] += kInKernelR ? __ldca(r + e * C + c) : r[e * C + c];
     }
   }
   if constexpr (MODE == 1) {
@@ -206,8 +211,12 @@ __global__ void source_kernel(int nsrc, int P, const int64_t *__restrict__ elem,
 // each thread keeps a Kahan-compensated FP64 partial per component, then a
 // fixed-order tree combines the partials (deterministic).
 // seis[(rec*C + c)*cap + step % cap] = sum_p l_p u_p.
+// kInKernelU: u was written earlier in the same launch (fused group steps),
+// so it is read with a coherent load (ld.global.ca, ordered by the waits'
+// fences), never through the non-coherent read-only path (ld.global.nc),
+// which is only defined for data that no thread writes during the launch.
 constexpr int kRecThreads = 128;
-template <typename real, int C>
+template <typename real, int C, bool kInKernelU = false>
 __device__ __forceinline__ void receiver_body(int rc, int P, const int64_t *__restrict__ elem,
                                               const double *__restrict__ lw,
                                               const int32_t *__restrict__ conn,
@@ -227,7 +236,8 @@ __device__ __forceinline__ void receiver_body(int rc, int P, const int64_t *__re
     const int64_t node = conn[e * P + p];
 #pragma unroll
     for (int c = 0; c < C; ++c) {
-      const double y = l * (double)u[node * C + c] - comp[c];
+      const real uc = kInKernelU ? __ldca(u + node * C + c) : u[node * C + c];
+      const double y = l * (double)uc - comp[c];
       const double tt = s[c] + y;
       comp[c] = (tt - s[c]) - y;
       s[c] = tt;

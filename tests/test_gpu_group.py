@@ -1,5 +1,6 @@
 """Problem groups: meshes of uneven size advanced together (one persistent
-work-queue launch per step, or one launch per stage) must give every member
+work-queue launch per step, one cooperative member-partitioned launch per
+step, or one launch per stage) must give every member
 exactly (bitwise) the seismograms and fields it gets alone, for acoustic quads and elastic hexahedra, with members that have
 no receivers, across graph-replayed chunks and remainders, and over several
 group runs."""
@@ -32,10 +33,11 @@ def make(kind, edge, seed, receivers=True):
     return m, p
 
 
-@pytest.mark.parametrize("form", ["persistent", "stages"])
+@pytest.mark.parametrize("form", ["persistent", "partitioned", "stages"])
 @pytest.mark.parametrize("kind,edges", [("quad", (10, 17, 24, 13)), ("hex", (3, 5, 4))])
 def test_group_matches_solo_bitwise(kind, edges, form, monkeypatch):
-    """persistent: one work-queue launch per step; stages: one launch per stage."""
+    """persistent: one work-queue launch per step; partitioned: one cooperative
+    launch per step, each member on its own CTAs; stages: one launch per stage."""
     monkeypatch.setenv("SALVUS_GROUP_STEP", form)
     runs = (75, 40)  # two chunks + remainder, then one chunk + remainder
     solo = []
