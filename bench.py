@@ -618,13 +618,18 @@ def main():
     v0 = np.zeros((G, 3))
     seis_holder = {}
 
-    def e2e_job():
+    def e2e_job(k, first):
         p2.set_field("u", u0)
         p2.set_field("v", v0)
-        p2.run(args.steps, core.RUN_GRAPH)
-        seis_holder["s"] = p2.seismograms(0, args.steps)
+        p2.run(k, core.RUN_GRAPH)
+        seis_holder["s"] = p2.seismograms(first, k)
 
-    ms_e2e = timed_on(p2, e2e_job)
+    # one untimed warm-up job (pinned staging buffers, graph capture), then
+    # the timed job
+    w_e2e = max(args.warmup, 32)
+    e2e_job(w_e2e, 0)
+    p2.synchronize()
+    ms_e2e = timed_on(p2, lambda: e2e_job(args.steps, w_e2e))
     e2e = replica_rate(G, args.steps, ms_e2e, world)
     h2d = 2 * G * 3 * 8 / args.steps
     d2h = len(cfg["receivers"]) * 3 * 8
