@@ -17,10 +17,13 @@
 //   GEMM 1   gradient:  D1[row][k*56 + q] = sum_j u_row[j] dphi_j/dxi_k (x_q)
 //            M = 128, N = 176 (3 directions x 56, padded), K = 56 (7 steps)
 //   pointwise  per node q: physical gradient, stress, reference flux
-//            F_row[k][q] (FP32, CUDA cores), written back to shared memory in
-//            chunks of 8 nodes
+//            F_row[k][q] (FP32, CUDA cores), split into hi and lo parts and
+//            stored to tensor memory in chunks of 8 nodes
 //   GEMM 2   divergence: D2[row][i] = sum_{k,q} F_row[k][q] dphi_i/dxi_k (x_q)
-//            M = 128, N = 64 (50 used), K = 3 x 8 per chunk, 7 chunks
+//            K = 3 x 8 per chunk, 7 chunks; A (the flux chunk) from tensor
+//            memory; per K step one M = 128, N = 128 MMA of F_hi against
+//            [B2_hi | B2_lo] and one N = 64 MMA of F_lo against B2_hi, three
+//            accumulators summed at read-out: hh + (hl + lh)
 //
 // The B operands are two constant tables, both K-major, loaded once per CTA
 // (hi and lo parts, 161 KB in all):
@@ -32,8 +35,8 @@
 // layout produced no output on sm_100a, so both tables are K-major.)
 //
 // Roles: warps 0-7 gather u, run the pointwise stage (warp group 0 takes the
-// even chunks, group 1 the odd ones, each group with one flux buffer) and
-// write the residual; warp 8 owns the
+// even chunks, group 1 the odd ones, each group with one tensor-memory flux
+// buffer written by tcgen05.st) and write the residual; warp 8 owns the
 // tensor memory and one elected lane issues every MMA in a fixed order, so
 // the accumulation order -- and the result -- is the same on every run.
 // Hand-offs go through mbarriers; every wait is bounded (about a second of
@@ -58,17 +61,18 @@ struct TetTcShape {
   static constexpr uint32_t B2_BYTES = 64 * 168 * 4;         // 43008 per part
   static constexpr uint32_t A1_SBO = 14 * 128;               // 56 K -> 14 chunks
   static constexpr uint32_t A1_BYTES = 128 * 56 * 4;         // 28672 per part
-  static constexpr uint32_t A2_SBO = 6 * 128;                // 24 K -> 6 chunks
-  static constexpr uint32_t A2_BYTES = 128 * 24 * 4;         // 12288 per part
   static constexpr uint32_t OFF_B1 = 0;
   static constexpr uint32_t OFF_B2 = 2 * B1_BYTES;
   static constexpr uint32_t TAB_BYTES = 2 * B1_BYTES + 2 * B2_BYTES;  // 164864
-  static constexpr uint32_t OFF_A = TAB_BYTES;               // A1 | A2 x 2 (aliased)
-  static constexpr uint32_t A_REGION = 2 * A1_BYTES;         // 57344 >= 4 A2_BYTES
-  static constexpr uint32_t OFF_BAR = OFF_A + A_REGION;
+  static constexpr uint32_t OFF_A = TAB_BYTES;               // A1 hi | lo
+  static constexpr uint32_t OFF_BAR = OFF_A + 2 * A1_BYTES;
   static constexpr uint32_t SMEM = OFF_BAR + 256;
-  static constexpr uint32_t TMEM_COLS = 256;
-  static constexpr uint32_t D2_COL = 192;
+  // tensor memory: D1 columns 0-175; GEMM 2 partial sums F_hi B_hi in
+  // 192-255, F_hi B_lo in 256-319 (one N = 128 MMA against B2 hi and lo,
+  // which lie one after the other), F_lo B_hi in 320-383; flux buffers
+  // 384 + 64 b (hi 24 columns, lo 32 columns further on), b = 0, 1
+  static constexpr uint32_t TMEM_COLS = 512;
+  static constexpr uint32_t D2_COL = 192, D2L_COL = 320, A2_COL = 384;
   static constexpr int RW = C == 1 ? 64 : 120;               // record words
 };
 
@@ -126,6 +130,28 @@ __device__ __forceinline__ void ld8(uint32_t taddr, float *v) {
 }
 __device__ __forceinline__ void ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// eight 32-bit columns of this thread's tensor-memory lane
+__device__ __forceinline__ void st8(uint32_t taddr, const float *v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+      : "memory");
+}
+__device__ __forceinline__ void st_wait() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+// D (tensor memory) += A (tensor memory, lane = row, column = K) x B (shared)
+__device__ __forceinline__ void mma_tf32_ta(uint32_t dtmem, uint32_t atmem, uint64_t b,
+                                            uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n}\n" ::"r"(dtmem),
+      "r"(atmem), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
 }
 
 // split x into its nearest TF32 value and the exact FP32 remainder
@@ -205,9 +231,20 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     // instructions at the end); lane 0 issues the MMAs and commits.
     constexpr uint32_t IG = tc::idesc_tf32(128, 176, false);
     constexpr uint32_t ID = tc::idesc_tf32(128, 64, false);
+    constexpr uint32_t IDW = tc::idesc_tf32(128, 128, false);
     const uint32_t b1_hi = sbase + S::OFF_B1, b1_lo = b1_hi + S::B1_BYTES;
-    const uint32_t b2_hi = sbase + S::OFF_B2, b2_lo = b2_hi + S::B2_BYTES;
+    const uint32_t b2_hi = sbase + S::OFF_B2;
     const uint32_t a1_hi = sbase + S::OFF_A, a1_lo = a1_hi + S::A1_BYTES;
+    // Descriptor bases: an operand start `off` bytes further on is the base
+    // plus off >> 4 (the 14-bit address field holds every shared address of
+    // the CTA, so the addition never carries out of it).  With the loops
+    // unrolled every MMA is one 64-bit add and the instruction itself.
+    const uint64_t dA1h = tc::desc(a1_hi, 128, S::A1_SBO), dA1l = tc::desc(a1_lo, 128, S::A1_SBO);
+    const uint64_t dB1h = tc::desc(b1_hi, 128, S::B1_SBO), dB1l = tc::desc(b1_lo, 128, S::B1_SBO);
+    // B2 hi and lo lie one after the other: rows 0-63 and 64-127 of one
+    // N = 128 operand with the same 8-row group stride
+    const uint64_t dB2h = tc::desc(b2_hi, 128, S::B2_SBO);
+    const uint32_t d2 = tmem + S::D2_COL, d2l = tmem + S::D2L_COL;
     const bool leader = lane == 0;
     auto wwait = [&](uint64_t *b, uint32_t p, int code) {
       return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
@@ -218,20 +255,18 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
       if (!wwait(&bar[0], par, 1100)) break;
       tc::fence_after();
       if (leader) {
+#pragma unroll
         for (int s = 0; s < S::KSTEPS; ++s) {
-          const uint32_t ko = (uint32_t)s * 256u;
-          const uint64_t ah = tc::desc(a1_hi + ko, 128, S::A1_SBO);
-          const uint64_t al = tc::desc(a1_lo + ko, 128, S::A1_SBO);
-          const uint64_t bh = tc::desc(b1_hi + ko, 128, S::B1_SBO);
-          const uint64_t bl = tc::desc(b1_lo + ko, 128, S::B1_SBO);
-          tc::mma_tf32(tmem, ah, bh, IG, s > 0);
-          tc::mma_tf32(tmem, al, bh, IG, 1);
-          tc::mma_tf32(tmem, ah, bl, IG, 1);
+          const uint64_t ko = (uint64_t)s * 16u;  // 256 bytes: one K step of 8
+          tc::mma_tf32(tmem, dA1h + ko, dB1h + ko, IG, s > 0);
+          tc::mma_tf32(tmem, dA1l + ko, dB1h + ko, IG, 1);
+          tc::mma_tf32(tmem, dA1h + ko, dB1l + ko, IG, 1);
         }
         tc::commit(&bar[1]);
       }
       __syncwarp();
       bool ok = true;
+#pragma unroll
       for (int c = 0; c < 7; ++c) {
         if (!wwait(&bar[2 + c], par, 1102 + c)) {
           ok = false;
@@ -239,18 +274,16 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
         }
         tc::fence_after();
         if (leader) {
-          const uint32_t a2_hi = sbase + S::OFF_A + (uint32_t)(c & 1) * 2u * S::A2_BYTES;
-          const uint32_t a2_lo = a2_hi + S::A2_BYTES;
+          // A: this chunk's flux in tensor-memory buffer c & 1 (hi, then lo 32 columns on)
+          const uint32_t a2 = tmem + S::A2_COL + 64u * (uint32_t)(c & 1);
+#pragma unroll
           for (int k = 0; k < 3; ++k) {
-            const uint64_t ah = tc::desc(a2_hi + (uint32_t)k * 256u, 128, S::A2_SBO);
-            const uint64_t al = tc::desc(a2_lo + (uint32_t)k * 256u, 128, S::A2_SBO);
             // K = kappa in [56 k + 8 c, 56 k + 8 c + 8): chunk (14 k + 2 c) of B2
-            const uint32_t kg = (uint32_t)(14 * k + 2 * c) * 128u;
-            const uint64_t bh = tc::desc(b2_hi + kg, 128, S::B2_SBO);
-            const uint64_t bl = tc::desc(b2_lo + kg, 128, S::B2_SBO);
-            tc::mma_tf32(tmem + S::D2_COL, ah, bh, ID, (c > 0 || k > 0) ? 1u : 0u);
-            tc::mma_tf32(tmem + S::D2_COL, al, bh, ID, 1);
-            tc::mma_tf32(tmem + S::D2_COL, ah, bl, ID, 1);
+            const uint64_t kg = (uint64_t)(14 * k + 2 * c) * 8u;  // 128-byte chunks
+            const uint32_t ah = a2 + 8u * (uint32_t)k, al = ah + 32u;
+            const uint32_t acc = (c > 0 || k > 0) ? 1u : 0u;
+            tc::mma_tf32_ta(d2, ah, dB2h + kg, IDW, acc);  // F_hi [B_hi | B_lo]
+            tc::mma_tf32_ta(d2l, al, dB2h + kg, ID, acc);  // F_lo B_hi
           }
           tc::commit(&bar[9 + c]);
         }
@@ -419,22 +452,18 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
           good = false;
           break;
         }
-        unsigned char *b_hi = sm + S::OFF_A + (uint32_t)(c & 1) * 2u * S::A2_BYTES;
-        unsigned char *b_lo = b_hi + S::A2_BYTES;
+        // flux chunk -> tensor-memory buffer c & 1 of this thread's lane
+        const uint32_t a2t = tmem + lane_base + S::A2_COL + 64u * (uint32_t)(c & 1);
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
+        for (int k = 0; k < 3; ++k) {
+          float h[8], l[8];
 #pragma unroll
-          for (int h4 = 0; h4 < 2; ++h4) {
-            float4 h, l;
-            tc::split(F[k][4 * h4 + 0], h.x, l.x);
-            tc::split(F[k][4 * h4 + 1], h.y, l.y);
-            tc::split(F[k][4 * h4 + 2], h.z, l.z);
-            tc::split(F[k][4 * h4 + 3], h.w, l.w);
-            const uint32_t off = tc::kmajor_off(row, 8 * k + 4 * h4, S::A2_SBO);
-            *reinterpret_cast<float4 *>(b_hi + off) = h;
-            *reinterpret_cast<float4 *>(b_lo + off) = l;
-          }
-        fence_proxy_async_smem();
+          for (int q = 0; q < 8; ++q) tc::split(F[k][q], h[q], l[q]);
+          tc::st8(a2t + 8u * (uint32_t)k, h);
+          tc::st8(a2t + 32u + 8u * (uint32_t)k, l);
+        }
+        tc::st_wait();
+        tc::fence_before();
         tc::arrive(&bar[2 + c]);
       }
       if (!good) break;
@@ -442,17 +471,24 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
       for (int t = 0; t < 28; ++t) uv[t] = cn[t] >= 0 ? __ldg(u + (int64_t)cn[t] * C + comp) : 0.f;
       if (!wwait(&bar[15], par, 1015)) break;
       tc::fence_after();
-      // residual columns 32 wg .. 32 wg + 31 of D2
-      float out[32];
+      // residual columns 32 wg .. 32 wg + 31: F_hi B_hi + (F_hi B_lo + F_lo B_hi)
 #pragma unroll
-      for (int g8 = 0; g8 < 4; ++g8)
-        tc::ld8(tmem + lane_base + S::D2_COL + (uint32_t)(32 * wg + 8 * g8), out + 8 * g8);
-      tc::ld_wait();
-      if (ok) {
+      for (int h = 0; h < 2; ++h) {
+        float hh[16], hl[16], lh[16];
+        const uint32_t col = (uint32_t)(32 * wg + 16 * h);
 #pragma unroll
-        for (int t = 0; t < 32; ++t) {
-          const int i = 32 * wg + t;
-          if (i < P) r[(e * P + i) * C + comp] = -out[t];
+        for (int g8 = 0; g8 < 2; ++g8) {
+          tc::ld8(tmem + lane_base + S::D2_COL + col + 8u * g8, hh + 8 * g8);
+          tc::ld8(tmem + lane_base + S::D2_COL + 64u + col + 8u * g8, hl + 8 * g8);
+          tc::ld8(tmem + lane_base + S::D2L_COL + col + 8u * g8, lh + 8 * g8);
+        }
+        tc::ld_wait();
+        if (ok) {
+#pragma unroll
+          for (int t = 0; t < 16; ++t) {
+            const int i = 32 * wg + 16 * h + t;
+            if (i < P) r[(e * P + i) * C + comp] = -(hh[t] + (hl[t] + lh[t]));
+          }
         }
       }
     }
