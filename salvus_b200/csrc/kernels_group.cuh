@@ -248,7 +248,7 @@ struct GroupBar {  // per member; the member's last CTA out zeroes it
 };
 
 template <int N, bool kHex, int C>
-__global__ void __launch_bounds__(128, kHex ? 5 : 8)
+__global__ void __launch_bounds__(128, kHex ? 5 : 10)
 group_partitioned_step(const GroupSlot *__restrict__ slots, const GroupPart *__restrict__ parts,
                        int J, GroupBar *__restrict__ bars, GroupSync *__restrict__ sync,
                        DMatrix<float> Dm, int P) {
