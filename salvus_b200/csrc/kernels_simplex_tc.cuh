@@ -193,9 +193,10 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint64_t *bar = reinterpret_cast<uint64_t *>(sm + S::OFF_BAR);
   // bar[0] A1 full (256) | bar[1] GEMM 1 done | bar[2+c] chunk c full (128) |
-  // bar[9+c] chunk c consumed | bar[16] drain
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + S::OFF_BAR + 17 * 8);
-  volatile int *flag = reinterpret_cast<volatile int *>(sm + S::OFF_BAR + 17 * 8 + 4);
+  // bar[9+c] chunk c consumed | bar[16] drain | bar[17] previous tile's
+  // GEMM 2 sums read out (256)
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + S::OFF_BAR + 18 * 8);
+  volatile int *flag = reinterpret_cast<volatile int *>(sm + S::OFF_BAR + 18 * 8 + 4);
   const uint32_t sbase = smem_addr(sm);
 
   for (int i = tid; i < (int)(S::TAB_BYTES / 16); i += S::THREADS)
@@ -208,6 +209,7 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
       mbar_init(&bar[9 + c], 1);
     }
     mbar_init(&bar[16], 1);
+    mbar_init(&bar[17], S::WORKERS);
     *flag = 0;
     fence_mbar_init();
   }
@@ -265,6 +267,8 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
         tc::commit(&bar[1]);
       }
       __syncwarp();
+      // GEMM 2 overwrites the previous tile's sums: every worker has read them
+      if (!wwait(&bar[17], par, 1117)) break;
       bool ok = true;
 #pragma unroll
       for (int c = 0; c < 7; ++c) {
@@ -346,6 +350,34 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
 #pragma unroll
       for (int t = 0; t < 28; ++t) uv[t] = cn[t] >= 0 ? __ldg(u + (int64_t)cn[t] * C + comp) : 0.f;
     }
+    // residual columns 32 wg .. 32 wg + 31 of a finished tile:
+    // F_hi B_hi + (F_hi B_lo + F_lo B_hi)
+    auto store_residual = [&](int64_t er, bool okr) {
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float hh[16], hl[16], lh[16];
+        const uint32_t col = (uint32_t)(32 * wg + 16 * h);
+#pragma unroll
+        for (int g8 = 0; g8 < 2; ++g8) {
+          tc::ld8(tmem + lane_base + S::D2_COL + col + 8u * g8, hh + 8 * g8);
+          tc::ld8(tmem + lane_base + S::D2_COL + 64u + col + 8u * g8, hl + 8 * g8);
+          tc::ld8(tmem + lane_base + S::D2L_COL + col + 8u * g8, lh + 8 * g8);
+        }
+        tc::ld_wait();
+        if (okr) {
+#pragma unroll
+          for (int t = 0; t < 16; ++t) {
+            const int i = 32 * wg + 16 * h + t;
+            if (i < P) r[(er * P + i) * C + comp] = -(hh[t] + (hl[t] + lh[t]));
+          }
+        }
+      }
+    };
+    // A tile's residual is read out and stored while the NEXT tile's
+    // gradient GEMM runs (its sums stay in tensor memory until that tile's
+    // first flux chunk, which these same threads hand over afterwards).
+    int64_t e_prev = 0;
+    bool ok_prev = false, have_prev = false, clean = true;
     uint32_t it = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
       const uint32_t par = it & 1;
@@ -384,7 +416,20 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
           cn[t] = okn && j < P ? __ldg(conn + en * P + j) : -1;
         }
       }
-      if (!wwait(&bar[1], par, 1001)) break;
+      if (have_prev) {
+        if (!wwait(&bar[15], par ^ 1u, 1015)) {
+          clean = false;
+          break;
+        }
+        tc::fence_after();
+        store_residual(e_prev, ok_prev);
+      }
+      tc::fence_before();
+      tc::arrive(&bar[17]);
+      if (!wwait(&bar[1], par, 1001)) {
+        clean = false;
+        break;
+      }
       tc::fence_after();
       bool good = true;
       for (int c = wg; c < 7; c += 2) {
@@ -466,31 +511,20 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
         tc::fence_before();
         tc::arrive(&bar[2 + c]);
       }
-      if (!good) break;
+      if (!good) {
+        clean = false;
+        break;
+      }
 #pragma unroll
       for (int t = 0; t < 28; ++t) uv[t] = cn[t] >= 0 ? __ldg(u + (int64_t)cn[t] * C + comp) : 0.f;
-      if (!wwait(&bar[15], par, 1015)) break;
+      e_prev = e;
+      ok_prev = ok;
+      have_prev = true;
+    }
+    // the last tile's residual (its parity is that of it - 1)
+    if (clean && have_prev && wwait(&bar[15], (it - 1u) & 1u, 1015)) {
       tc::fence_after();
-      // residual columns 32 wg .. 32 wg + 31: F_hi B_hi + (F_hi B_lo + F_lo B_hi)
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        float hh[16], hl[16], lh[16];
-        const uint32_t col = (uint32_t)(32 * wg + 16 * h);
-#pragma unroll
-        for (int g8 = 0; g8 < 2; ++g8) {
-          tc::ld8(tmem + lane_base + S::D2_COL + col + 8u * g8, hh + 8 * g8);
-          tc::ld8(tmem + lane_base + S::D2_COL + 64u + col + 8u * g8, hl + 8 * g8);
-          tc::ld8(tmem + lane_base + S::D2L_COL + col + 8u * g8, lh + 8 * g8);
-        }
-        tc::ld_wait();
-        if (ok) {
-#pragma unroll
-          for (int t = 0; t < 16; ++t) {
-            const int i = 32 * wg + 16 * h + t;
-            if (i < P) r[(e * P + i) * C + comp] = -(hh[t] + (hl[t] + lh[t]));
-          }
-        }
-      }
+      store_residual(e_prev, ok_prev);
     }
   }
   tc::fence_before();
