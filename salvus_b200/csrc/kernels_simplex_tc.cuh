@@ -436,7 +436,13 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
         float cur[NPRE];
 #pragma unroll
         for (int x = 0; x < NPRE; ++x) cur[x] = pre[x];
-        if (c + 2 < 7) load_chunk(rc, c + 2, pre);
+        if (c + 2 < 7) {
+          load_chunk(rc, c + 2, pre);
+        } else {
+          // the group's last chunk: the next tile's u is fetched under it
+#pragma unroll
+          for (int t = 0; t < 28; ++t) uv[t] = cn[t] >= 0 ? __ldg(u + (int64_t)cn[t] * C + comp) : 0.f;
+        }
         float gr[3][8];
 #pragma unroll
         for (int k = 0; k < 3; ++k) tc::ld8(tmem + lane_base + (uint32_t)(k * 56 + 8 * c), gr[k]);
@@ -515,8 +521,6 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
         clean = false;
         break;
       }
-#pragma unroll
-      for (int t = 0; t < 28; ++t) uv[t] = cn[t] >= 0 ? __ldg(u + (int64_t)cn[t] * C + comp) : 0.f;
       e_prev = e;
       ok_prev = ok;
       have_prev = true;
