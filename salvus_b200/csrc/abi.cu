@@ -1101,11 +1101,11 @@ static int ready(salvus_problem *p) {
 // problem groups: FP32 single-shot problems of one element class advance with
 // one launch per stage (kernels_group.cuh)
 template <int N>
-static int group_stiffness_t(const salvus_mesh *m0, const GroupSlot *slots, int J, int64_t blocks,
-                             cudaStream_t st) {
+static int group_stiffness_t(const salvus_mesh *m0, const GroupSlot *slots, const int32_t *owner,
+                             int64_t blocks, cudaStream_t st) {
   if (m0->shape == SALVUS_QUAD) {
     group_quad_acoustic_stiffness<N><<<(unsigned)blocks, QuadColShape<N, quad_col_epb<N>()>::THREADS,
-                                        0, st>>>(slots, J, dmatrix<float>(m0->basis));
+                                        0, st>>>(slots, owner, dmatrix<float>(m0->basis));
   } else if constexpr (N <= kMaxHexOrder) {
     constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
     using T = ElasticV2Shape<N, EPB, false>;
@@ -1116,25 +1116,25 @@ static int group_stiffness_t(const salvus_mesh *m0, const GroupSlot *slots, int 
       attr = true;
     }
     group_hex_elastic_stiffness<N, EPB><<<(unsigned)blocks, T::THREADS, T::SMEM, st>>>(
-        slots, J, dmatrix<float>(m0->basis));
+        slots, owner, dmatrix<float>(m0->basis));
   }
   g_launches++;
   return check_launch("group stiffness");
 }
 
-static int group_stiffness(const salvus_mesh *m0, const GroupSlot *slots, int J, int64_t blocks,
-                           cudaStream_t st) {
+static int group_stiffness(const salvus_mesh *m0, const GroupSlot *slots, const int32_t *owner,
+                           int64_t blocks, cudaStream_t st) {
   switch (m0->order) {
-    case 1: return group_stiffness_t<1>(m0, slots, J, blocks, st);
-    case 2: return group_stiffness_t<2>(m0, slots, J, blocks, st);
-    case 3: return group_stiffness_t<3>(m0, slots, J, blocks, st);
-    case 4: return group_stiffness_t<4>(m0, slots, J, blocks, st);
-    case 5: return group_stiffness_t<5>(m0, slots, J, blocks, st);
-    case 6: return group_stiffness_t<6>(m0, slots, J, blocks, st);
-    case 7: return group_stiffness_t<7>(m0, slots, J, blocks, st);
-    case 8: return group_stiffness_t<8>(m0, slots, J, blocks, st);
-    case 9: return group_stiffness_t<9>(m0, slots, J, blocks, st);
-    case 10: return group_stiffness_t<10>(m0, slots, J, blocks, st);
+    case 1: return group_stiffness_t<1>(m0, slots, owner, blocks, st);
+    case 2: return group_stiffness_t<2>(m0, slots, owner, blocks, st);
+    case 3: return group_stiffness_t<3>(m0, slots, owner, blocks, st);
+    case 4: return group_stiffness_t<4>(m0, slots, owner, blocks, st);
+    case 5: return group_stiffness_t<5>(m0, slots, owner, blocks, st);
+    case 6: return group_stiffness_t<6>(m0, slots, owner, blocks, st);
+    case 7: return group_stiffness_t<7>(m0, slots, owner, blocks, st);
+    case 8: return group_stiffness_t<8>(m0, slots, owner, blocks, st);
+    case 9: return group_stiffness_t<9>(m0, slots, owner, blocks, st);
+    case 10: return group_stiffness_t<10>(m0, slots, owner, blocks, st);
   }
   return fail(SALVUS_E_UNSUPPORTED, "no grouped stiffness for order %d", m0->order);
 }
@@ -1163,6 +1163,10 @@ struct salvus_group {
   int coop_slots = 0;  // co-resident CTAs of the partitioned kernel
   std::vector<salvus::GroupSlot> slots;
   salvus::DeviceBuffer d_slots;
+  // per-stage CTA -> member tables of the per-stage launches, one after the
+  // other: stiffness (n_stiff), gather (n_gather), receivers (n_rec)
+  std::vector<int32_t> owner;
+  salvus::DeviceBuffer d_owner;
   int64_t n_stiff = 0, n_gather = 0, n_rec = 0;
   // persistent single-launch step: work-item queue
   std::vector<salvus::GroupCounts> counts;
@@ -1236,6 +1240,19 @@ static int group_fill(salvus_group *g) {
   g->n_rec = br;
   int rc = group_upload(g->d_slots, g->slots.data(), sizeof(GroupSlot) * g->slots.size(), g->stream);
   if (rc) return rc;
+  g->owner.resize((size_t)(bs + bg + br));
+  {
+    int32_t *o = g->owner.data();
+    for (size_t k = 0; k < g->members.size(); ++k) {
+      const GroupSlot &sk = g->slots[k];
+      const salvus_mesh *mk = g->members[k]->mesh;
+      std::fill(o + sk.b_stiff, o + sk.b_stiff + group_stiff_blocks(mk), (int32_t)k);
+      std::fill(o + bs + sk.b_gather, o + bs + sk.b_gather + (mk->G + 255) / 256, (int32_t)k);
+      std::fill(o + bs + bg + sk.b_rec, o + bs + bg + sk.b_rec + sk.nrec, (int32_t)k);
+    }
+  }
+  if ((rc = group_upload(g->d_owner, g->owner.data(), sizeof(int32_t) * g->owner.size(), g->stream)))
+    return rc;
   // work-item queue of the persistent step: every member's stiffness items
   // (kStiffPer element groups each), then per member source (1), gather items
   // (kGatherPer CTA-wide node tiles each), receivers (1 each), advance (1)
@@ -1432,14 +1449,16 @@ static int group_step(salvus_group *g) {
   const int P = g->m0->P;
   const GroupSlot *slots = g->d_slots.as<GroupSlot>();
   int rc;
-  if ((rc = group_stiffness(g->m0, slots, J, g->n_stiff, g->stream))) return rc;
+  const int32_t *own = g->d_owner.as<int32_t>();
+  if ((rc = group_stiffness(g->m0, slots, own, g->n_stiff, g->stream))) return rc;
   if (g->c == 1) group_source<1><<<J, 256, 0, g->stream>>>(slots, P);
   else group_source<3><<<J, 256, 0, g->stream>>>(slots, P);
-  if (g->c == 1) group_gather_update<1><<<(unsigned)g->n_gather, 256, 0, g->stream>>>(slots, J);
-  else group_gather_update<3><<<(unsigned)g->n_gather, 256, 0, g->stream>>>(slots, J);
+  if (g->c == 1) group_gather_update<1><<<(unsigned)g->n_gather, 256, 0, g->stream>>>(slots, own + g->n_stiff);
+  else group_gather_update<3><<<(unsigned)g->n_gather, 256, 0, g->stream>>>(slots, own + g->n_stiff);
   if (g->n_rec > 0) {
-    if (g->c == 1) group_receivers<1><<<(unsigned)g->n_rec, kRecThreads, 0, g->stream>>>(slots, J, P);
-    else group_receivers<3><<<(unsigned)g->n_rec, kRecThreads, 0, g->stream>>>(slots, J, P);
+    const int32_t *own_rec = own + g->n_stiff + g->n_gather;
+    if (g->c == 1) group_receivers<1><<<(unsigned)g->n_rec, kRecThreads, 0, g->stream>>>(slots, own_rec, P);
+    else group_receivers<3><<<(unsigned)g->n_rec, kRecThreads, 0, g->stream>>>(slots, own_rec, P);
   }
   group_advance<<<1, 256, 0, g->stream>>>(slots, J);
   g_launches += g->n_rec > 0 ? 4 : 3;

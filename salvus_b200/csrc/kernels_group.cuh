@@ -46,33 +46,23 @@ struct GroupSlot {
   int64_t b_stiff, b_gather, b_rec;
 };
 
-// Index of the member whose CTA range holds blockIdx.x (ranges ascending).
-template <int64_t GroupSlot::*first>
-__device__ __forceinline__ int group_member(const GroupSlot *__restrict__ slots, int J) {
-  const int64_t b = blockIdx.x;
-  int lo = 0, hi = J - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (slots[mid].*first <= b) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
+// owner[b]: the member whose CTA range of this launch holds CTA b (a table
+// per stage, filled on the host; one load instead of a search).
 
 template <int N>
 __global__ void __launch_bounds__(QuadColShape<N, quad_col_epb<N>()>::THREADS)
-group_quad_acoustic_stiffness(const GroupSlot *__restrict__ slots, int J, DMatrix<float> Dm) {
-  const int s = group_member<&GroupSlot::b_stiff>(slots, J);
-  const GroupSlot &m = slots[s];
+group_quad_acoustic_stiffness(const GroupSlot *__restrict__ slots,
+                              const int32_t *__restrict__ owner, DMatrix<float> Dm) {
+  const GroupSlot &m = slots[owner[blockIdx.x]];
   acoustic_quad_col_body<N, quad_col_epb<N>(), float>(blockIdx.x - m.b_stiff, m.E, m.rec, m.conn,
                                                        m.u, m.r, Dm);
 }
 
 template <int N, int EPB>
 __global__ void __launch_bounds__(ElasticV2Shape<N, EPB, false>::THREADS)
-group_hex_elastic_stiffness(const GroupSlot *__restrict__ slots, int J, DMatrix<float> Dm) {
-  const int s = group_member<&GroupSlot::b_stiff>(slots, J);
-  const GroupSlot &m = slots[s];
+group_hex_elastic_stiffness(const GroupSlot *__restrict__ slots,
+                            const int32_t *__restrict__ owner, DMatrix<float> Dm) {
+  const GroupSlot &m = slots[owner[blockIdx.x]];
   elastic_hex_v2_body<N, EPB, false>(blockIdx.x - m.b_stiff, m.E, m.rec, m.u, m.r, Dm);
 }
 
@@ -84,18 +74,17 @@ __global__ void group_source(const GroupSlot *__restrict__ slots, int P) {
 }
 
 template <int C>
-__global__ void group_gather_update(const GroupSlot *__restrict__ slots, int J) {
-  const int s = group_member<&GroupSlot::b_gather>(slots, J);
-  const GroupSlot &m = slots[s];
+__global__ void group_gather_update(const GroupSlot *__restrict__ slots,
+                                    const int32_t *__restrict__ owner) {
+  const GroupSlot &m = slots[owner[blockIdx.x]];
   const int64_t g = (blockIdx.x - m.b_gather) * (int64_t)blockDim.x + threadIdx.x;
   gather_body<float, C, 0>(g, m.G, m.inc_off, m.inc_idx, m.r, m.mi, m.u, m.v, m.ap, m.a, m.dt);
 }
 
 template <int C>
 __global__ void __launch_bounds__(kRecThreads)
-group_receivers(const GroupSlot *__restrict__ slots, int J, int P) {
-  const int s = group_member<&GroupSlot::b_rec>(slots, J);
-  const GroupSlot &m = slots[s];
+group_receivers(const GroupSlot *__restrict__ slots, const int32_t *__restrict__ owner, int P) {
+  const GroupSlot &m = slots[owner[blockIdx.x]];
   receiver_body<float, C>((int)(blockIdx.x - m.b_rec), P, m.rec_elem, m.rec_l, m.conn, m.u, m.seis,
                           m.cap, m.step);
 }
