@@ -318,9 +318,9 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
       return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
     };
     // Loads are software-pipelined: the next tile's connectivity is fetched
-    // while this tile's GEMMs and pointwise stage run, its u values while this
-    // tile's residual is read out; each chunk's material while the previous
-    // chunk of the group is computed.
+    // while this tile's GEMMs and pointwise stage run, its u values under the
+    // group's last flux chunk; each chunk's material while the previous chunk
+    // of the group is computed.
     constexpr int NPRE = C == 1 ? 8 : 16;
     auto load_chunk = [&](const float *rcp, int c, float *dst) {
       const float4 *p4 = reinterpret_cast<const float4 *>(rcp);
