@@ -246,10 +246,17 @@ int salvus_problem_info(const salvus_problem *p, int32_t *n_shots, int32_t *n_re
  * stream and allocates nothing: the element-local residual lives in a
  * 32 MiB array inside the library that every GPU loading the library holds
  * until exit.  Meshes needing more (E * P * c * sizeof(real) > 32 MiB) are
- * rejected with SALVUS_E_INVALID.  All calls share that array: calls that
- * overlap on the GPU race and must be serialised by the caller.  The first
- * call on a device looks up the array's device address; make it before any
- * stream capture. */
+ * rejected with SALVUS_E_INVALID.  All calls share that array (and a status
+ * word beside it): calls that overlap on the GPU race and must be serialised
+ * by the caller.  The first call on a device looks up the array's device
+ * address; make it before any stream capture.  FP64 calls on meshes created
+ * with SALVUS_MESH_FP32_ONLY return SALVUS_E_STATE; fluid-solid
+ * (SALVUS_COUPLED2D) meshes return SALVUS_E_UNSUPPORTED, because their
+ * coupling terms act on the velocity field, which this call does not take.
+ * On meshes whose FP32 stiffness kernel has bounded device waits (tensor-core
+ * tetrahedra and triangles) the call synchronises the stream and returns
+ * SALVUS_E_TIMEOUT if a wait gave up; otherwise it returns once the work is
+ * queued.  The caller's current device is unchanged on return. */
 int salvus_apply_stiffness_noalloc(const salvus_mesh *mesh, int32_t precision, const void *u,
                                    void *a, void *stream);
 

@@ -22,6 +22,7 @@ LIB_PATH = os.path.join(HERE, "libsalvus_b200.so")
 QUAD, HEX, TRI, TET = 0, 1, 2, 3
 ACOUSTIC, ELASTIC3D, ELASTIC2D, COUPLED2D = 0, 1, 2, 3
 FP32, FP64 = 0, 1
+MESH_FP32_ONLY = 1  # salvus_mesh_desc.flags: build only the FP32 stiffness records
 FIELD_U, FIELD_V, FIELD_A, FIELD_A_PREV = 0, 1, 2, 3
 FORCE, MOMENT_TENSOR = 0, 1
 RUN_PLAIN, RUN_GRAPH = 0, 1
@@ -153,12 +154,12 @@ class Mesh:
     """Flattened mesh resident on one GPU (DMPlex mesh + Exodus model + the
     per-element precomputation of the reference, done once)."""
 
-    def __init__(self, shape, order, physics, vertices, cells, params, device=0):
+    def __init__(self, shape, order, physics, vertices, cells, params, device=0, flags=0):
         self.shape, self.order, self.physics = shape, order, physics
         self._v = np.ascontiguousarray(vertices, dtype=np.float64)
         self._c = np.ascontiguousarray(cells, dtype=np.int64)
         self._p = np.ascontiguousarray(params, dtype=np.float64)
-        d = MeshDesc(shape, order, physics, 0, self._v.shape[0], _dp(self._v), self._c.shape[0],
+        d = MeshDesc(shape, order, physics, flags, self._v.shape[0], _dp(self._v), self._c.shape[0],
                      self._c.ctypes.data_as(ctypes.POINTER(_I64)), _dp(self._p))
         h = _VP()
         _check(lib().salvus_mesh_create(ctypes.byref(d), device, ctypes.byref(h)))

@@ -1053,12 +1053,28 @@ static int newmark_t(salvus_problem *p) {
   return launch_receivers<real, C>(p);
 }
 
+// True when the FP32 stiffness launch of this mesh runs a kernel whose
+// bounded waits report a timeout through the error word (tensor-core
+// simplices, the TMA hexahedron variants); mirrors launch_stiffness.
+bool stiffness_reports_errors(const salvus_mesh *m, int precision) {
+  if (precision != SALVUS_FP32) return false;
+  if (m->shape == SALVUS_TET) return m->tet_kernel == 0;
+  if (m->shape == SALVUS_TRI) return m->tri_kernel == 0;
+  if (m->shape == SALVUS_HEX && m->physics == SALVUS_ELASTIC3D) {
+    const int v = hex_variant();
+    return v == HEX_TMA || v == HEX_PERSISTENT;
+  }
+  return false;
+}
+
 // a = -K u for caller-owned device buffers, with the element-local residual
-// in caller-provided scratch (used by salvus_apply_stiffness_noalloc).
+// in caller-provided scratch and timeouts of bounded device waits recorded in
+// the caller-provided device word `err` (used by
+// salvus_apply_stiffness_noalloc).
 template <typename real>
 static int apply_stiffness_into_t(const salvus_mesh *m, const real *rec, const real *u, real *a,
-                                  real *scratch, cudaStream_t st) {
-  int rc = launch_stiffness<real>(m, rec, u, scratch, st, nullptr);
+                                  real *scratch, int *err, cudaStream_t st) {
+  int rc = launch_stiffness<real>(m, rec, u, scratch, st, err);
   if (rc) return rc;
   return by_components(m->c, [&](auto cc) {
     gather_kernel<real, decltype(cc)::value, 1><<<blocks_for(m->G, 256), 256, 0, st>>>(
@@ -1070,12 +1086,14 @@ static int apply_stiffness_into_t(const salvus_mesh *m, const real *rec, const r
 }
 
 int apply_stiffness_into(const salvus_mesh *m, int precision, const void *u, void *a,
-                         void *scratch, cudaStream_t st) {
+                         void *scratch, int *err, cudaStream_t st) {
   if (precision == SALVUS_FP32)
     return apply_stiffness_into_t<float>(m, m->d_rec32.as<float>(), (const float *)u, (float *)a,
-                                         (float *)scratch, st);
+                                         (float *)scratch, err, st);
+  if (!m->d_rec64.ptr)
+    return fail(SALVUS_E_STATE, "mesh holds no FP64 records (created with SALVUS_MESH_FP32_ONLY)");
   return apply_stiffness_into_t<double>(m, m->d_rec64.as<double>(), (const double *)u,
-                                        (double *)a, (double *)scratch, st);
+                                        (double *)a, (double *)scratch, err, st);
 }
 
 // Reads the device error word (set by kernels whose bounded waits ran out).
@@ -2087,8 +2105,12 @@ int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
     cudaGraph_t graph;
     SALVUS_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
     int crc = SALVUS_OK;
+    const int64_t l0 = g_launches.load();
     for (int s = 0; s < chunk && crc == SALVUS_OK; ++s) crc = step_fused(p);
     cudaError_t ce = cudaStreamEndCapture(p->stream, &graph);
+    // captured launches run only when the graph is replayed: count them there
+    p->graph_launches = g_launches.load() - l0;
+    g_launches -= p->graph_launches;
     p->profiling = prof;
     if (crc) return crc;
     if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
@@ -2101,7 +2123,7 @@ int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
   while (n_steps - done >= p->graph_steps) {
     ProfScope ps(p, K_GRAPH);
     SALVUS_CUDA(cudaGraphLaunch(p->graph_exec, p->stream));
-    g_launches += (int64_t)p->graph_steps * (3 + (p->srcs.empty() ? 0 : 1));
+    g_launches += p->graph_launches;
     done += p->graph_steps;
     p->step += p->graph_steps;
   }

@@ -174,6 +174,7 @@ struct salvus_problem {
   // graphs
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;
+  int64_t graph_launches = 0;  // kernel launches in one replay of graph_exec
   cudaStream_t stream = nullptr;
   // profiling
   bool profiling = false;
