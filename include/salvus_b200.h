@@ -63,7 +63,13 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  * params are per element, per element vertex (Exodus NAME_0..NAME_k):
  *   acoustic : [1][n_elements][nv]  VP                    (Scalar.cpp:23-25)
  *   elastic3d: [3][n_elements][nv]  RHO, VP, VS  (isotropic form of
- *              Elastic3D.cpp:33-54 with VPV=VPH=VP, VSV=VSH=VS, ETA=1)
+ *              Elastic3D.cpp:33-54 with VPV=VPH=VP, VSV=VSH=VS, ETA=1), or
+ *              with flag SALVUS_MESH_ELASTIC_TI the reference's six
+ *              [6][n_elements][nv] RHO, VPV, VPH, VSV, VSH, ETA: transversely
+ *              isotropic with a vertical axis, c11 = c22 = rho VPH^2,
+ *              c33 = rho VPV^2, c44 = c55 = rho VSV^2, c66 = rho VSH^2,
+ *              c12 = c11 - 2 c66, c13 = c23 = ETA (c11 - 2 c44)
+ *              (Elastic3D.cpp:42-53, stress :106-118)
  *   elastic2d: [5][n_elements][4]   RHO, C11, C13, C33, C55
  *              (Elastic2D.cpp:29-37; fields ux, uy)
  *   coupled2d: [7][n_elements][4]   FLUID, VP, RHO, C11, C13, C33, C55:
@@ -79,6 +85,12 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  * per-mesh geometry memory; FP64 problems and the FP64 eigenvalue estimate
  * are then unavailable on that mesh). */
 #define SALVUS_MESH_FP32_ONLY 1
+/* salvus_mesh_desc.flags: elastic3d params are the six transversely isotropic
+ * parameters (see above).  A model that is isotropic everywhere (VPH = VPV,
+ * VSH = VSV, ETA = 1) runs the isotropic kernels; others store five folded
+ * constants per point.  Tetrahedra with such material run on CUDA cores;
+ * problem groups take isotropic meshes only. */
+#define SALVUS_MESH_ELASTIC_TI 2
 
 typedef struct {
   int32_t shape;   /* enum salvus_shape */
@@ -381,6 +393,11 @@ int salvus_exodus_variable(const salvus_exodus *file, const char *name, double *
  * when present, must equal VPV / VSV / 1); elastic2d RHO C11 C13 C33 C55;
  * coupled2d the "fluid" flag then VP RHO C11 C13 C33 C55 (absent names 0). */
 int salvus_exodus_params(const salvus_exodus *file, int32_t physics, double *params);
+/* The reference's six Elastic3D parameters (Elastic3D::attachMaterialProperties,
+ * Elastic3D.cpp:33-54), [6][n_elements][nv] RHO VPV VPH VSV VSH ETA, for a
+ * mesh created with SALVUS_MESH_ELASTIC_TI: VPV / VSV fall back to VP / VS,
+ * VPH / VSH default to VPV / VSV and ETA to 1 when the file lacks them. */
+int salvus_exodus_elastic3d_params(const salvus_exodus *file, double *params);
 int salvus_exodus_side_set_name(const salvus_exodus *file, int32_t i, char *buf, int32_t len);
 /* Global nodes of a mesh built from this file that lie on the named side set
  * (Mesh::setupTopology's "Face Sets", Mesh.cpp:286-312): count first (nodes

@@ -35,18 +35,38 @@ def ricker_2d(nel=40, order=4, L=1.0e4, vp=4000.0, f0=2.0, n_receivers=16, radiu
     return cfg
 
 
+def ti_params(rho, vp, vs, C, anisotropy):
+    """The reference's six Elastic3D parameters per element vertex
+    (Elastic3D.cpp:33-54), [6][E][nv] RHO VPV VPH VSV VSH ETA, for a vertical
+    symmetry axis: VPV = vp, VPH = vp sqrt(1 + 2 eps), VSV = vs,
+    VSH = vs sqrt(1 + 2 gamma), ETA = eta (Thomsen-style parameters from the
+    `anisotropy` dict eps, gamma, eta)."""
+    eps, gam, eta = anisotropy["eps"], anisotropy["gamma"], anisotropy["eta"]
+    pe = lambda x: meshgen.per_element_vertex(x, C)
+    return np.stack([pe(rho), pe(vp), pe(vp * np.sqrt(1 + 2 * eps)), pe(vs),
+                     pe(vs * np.sqrt(1 + 2 * gam)), pe(np.full_like(rho, eta))])
+
+
+VTI = dict(eps=0.08, gamma=0.06, eta=0.9)  # a moderately anisotropic layer
+
+
 def elastic_hex(nel=64, order=4, h=200.0, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
-                corr=1000.0, f0=1.5, n_receivers=64, seed=1):
+                corr=1000.0, f0=1.5, n_receivers=64, seed=1, anisotropy=None):
     """3-D elastic hex cube with a Gaussian random-field perturbation of
     vp, vs and rho, a moment-tensor Ricker source at the centre and receivers
-    at seeded positions on the top surface."""
+    at seeded positions on the top surface.  anisotropy (dict eps, gamma,
+    eta) makes the material transversely isotropic: six parameters per
+    vertex (ti_params)."""
     L = nel * h
     V, C = meshgen.structured_hex(nel, nel, nel, L, L, L)
     grf = meshgen.gaussian_random_field((nel + 1,) * 3, h, corr, seed)  # [z][y][x]
     pert = 1.0 + std * grf.ravel()
     vpv, vsv, rhov = vp * pert, vs * pert, rho * pert
-    params = np.stack([meshgen.per_element_vertex(rhov, C), meshgen.per_element_vertex(vpv, C),
-                       meshgen.per_element_vertex(vsv, C)])
+    if anisotropy is not None:
+        params = ti_params(rhov, vpv, vsv, C, anisotropy)
+    else:
+        params = np.stack([meshgen.per_element_vertex(rhov, C), meshgen.per_element_vertex(vpv, C),
+                           meshgen.per_element_vertex(vsv, C)])
     rng = np.random.default_rng(seed)
     mt = rng.standard_normal(6)
     rec_xy = rng.uniform(0.02 * L, 0.98 * L, size=(n_receivers, 2))
@@ -212,7 +232,7 @@ def simplex_tri(nx=448, ny=224, lx=2.0e4, ly=1.0e4, vp=4000.0, std=0.05, corr=10
 
 
 def simplex_tet(n=55, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
-                corr=1000.0, f0=1.0, n_receivers=64, seed=3):
+                corr=1000.0, f0=1.0, n_receivers=64, seed=3, anisotropy=None):
     """3-D P3 tetrahedra: jittered n^3 lattice over an L cube, 6 tetrahedra
     per cell (6 n^3 elements; n = 55 gives about 1M), material homogeneous
     times (1 + std GRF); elastic: seeded moment-tensor Ricker source, acoustic:
@@ -229,9 +249,12 @@ def simplex_tet(n=55, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700
         par = meshgen.per_element_vertex(vp * pert, C)[None]
         src = dict(location=loc, center_freq=f0, time_delay=1.2 / f0, amplitude=1.0, direction=[1.0])
     else:
-        par = np.stack([meshgen.per_element_vertex(rho * pert, C),
-                        meshgen.per_element_vertex(vp * pert, C),
-                        meshgen.per_element_vertex(vs * pert, C)])
+        if anisotropy is not None:
+            par = ti_params(rho * pert, vp * pert, vs * pert, C, anisotropy)
+        else:
+            par = np.stack([meshgen.per_element_vertex(rho * pert, C),
+                            meshgen.per_element_vertex(vp * pert, C),
+                            meshgen.per_element_vertex(vs * pert, C)])
         src = dict(location=loc, center_freq=f0, time_delay=1.2 / f0, amplitude=1.0e13,
                    moment_tensor=rng.standard_normal(6))
     return dict(shape=TET, order=3, physics=physics, vertices=V, cells=C, params=par, L=L,
@@ -241,7 +264,7 @@ def simplex_tet(n=55, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700
 def oracle_params(cfg):
     """Parameter array in the oracle's layout (elastic: RHO VPV VPH VSV VSH ETA)."""
     p = cfg["params"]
-    if cfg["physics"] in (ACOUSTIC, ELASTIC2D, COUPLED2D):
+    if cfg["physics"] in (ACOUSTIC, ELASTIC2D, COUPLED2D) or len(p) == 6:
         return p
     rho, vp, vs = p
     return np.stack([rho, vp, vp, vs, vs, np.ones_like(rho)])

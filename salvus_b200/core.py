@@ -23,6 +23,7 @@ QUAD, HEX, TRI, TET = 0, 1, 2, 3
 ACOUSTIC, ELASTIC3D, ELASTIC2D, COUPLED2D = 0, 1, 2, 3
 FP32, FP64 = 0, 1
 MESH_FP32_ONLY = 1  # salvus_mesh_desc.flags: build only the FP32 stiffness records
+MESH_ELASTIC_TI = 2  # salvus_mesh_desc.flags: elastic3d params RHO VPV VPH VSV VSH ETA
 FIELD_U, FIELD_V, FIELD_A, FIELD_A_PREV = 0, 1, 2, 3
 FORCE, MOMENT_TENSOR = 0, 1
 RUN_PLAIN, RUN_GRAPH = 0, 1
@@ -77,6 +78,7 @@ SIGNATURES = [
     ("salvus_exodus_variable_name", ctypes.c_int, [_VP, _I32, ctypes.c_char_p, _I32]),
     ("salvus_exodus_variable", ctypes.c_int, [_VP, ctypes.c_char_p, _DP]),
     ("salvus_exodus_params", ctypes.c_int, [_VP, _I32, _DP]),
+    ("salvus_exodus_elastic3d_params", ctypes.c_int, [_VP, _DP]),
     ("salvus_exodus_side_set_name", ctypes.c_int, [_VP, _I32, ctypes.c_char_p, _I32]),
     ("salvus_exodus_side_set_nodes", ctypes.c_int, [_VP, _VP, ctypes.c_char_p,
                                                     ctypes.POINTER(_I64), ctypes.POINTER(_I64)]),
@@ -159,6 +161,8 @@ class Mesh:
         self._v = np.ascontiguousarray(vertices, dtype=np.float64)
         self._c = np.ascontiguousarray(cells, dtype=np.int64)
         self._p = np.ascontiguousarray(params, dtype=np.float64)
+        if physics == ELASTIC3D and self._p.shape[0] == 6:
+            flags |= MESH_ELASTIC_TI  # RHO VPV VPH VSV VSH ETA
         d = MeshDesc(shape, order, physics, flags, self._v.shape[0], _dp(self._v), self._c.shape[0],
                      self._c.ctypes.data_as(ctypes.POINTER(_I64)), _dp(self._p))
         h = _VP()

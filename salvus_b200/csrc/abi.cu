@@ -17,7 +17,6 @@
 #include "kernels_setup.cuh"
 #include "kernels_stiffness.cuh"
 #include "kernels_step.cuh"
-#include "kernels_hex_tma.cuh"
 #include "kernels_hex_v2.cuh"
 #include "kernels_batch.cuh"
 #include "kernels_simplex.cuh"
@@ -105,132 +104,58 @@ static int launch_acoustic(const salvus_mesh *m, const real *rec, const real *u,
   return check_launch("acoustic stiffness");
 }
 
-// FP32 elastic hexahedra: SALVUS_HEX_KERNEL selects the variant
-//   v2e5 (default)   column threads, 32-bit shared planes, 128-thread CTAs
-//                    (whole warps: 5 order-4 elements)
-//   v2, v2e10, v2e14 the same kernel with 224 / 256 / 352-thread CTAs
-//   m-suffixed       the same with a resident-CTA register cap
-//   tma, persistent  TMA bulk-copied records (one group per CTA / double-
-//                    buffered persistent CTAs)
-//   v3               cp.async record heads
-//   classic          register/shared-memory baseline (also the FP64 path)
-enum HexVariant {
-  HEX_PERSISTENT = 0, HEX_TMA = 1, HEX_CLASSIC = 2, HEX_V2 = 3, HEX_V2_E4 = 4, HEX_V3 = 5,
-  HEX_V3_E4 = 6, HEX_V2_E10 = 7, HEX_V2_E5 = 8, HEX_V2_E10M4 = 9, HEX_V2_E5M8 = 10,
-  HEX_V2_E14 = 11, HEX_V2_E10M3 = 12, HEX_V2_E8M3 = 13, HEX_V2_E5M6 = 14, HEX_V2_E14M2 = 15
-};
-// Read at every launch (cheap), so a tuning sweep can switch variants
-// within one process.
-static int hex_variant() {
+// FP32 elastic hexahedra: the column-threaded kernel with 32-bit shared
+// planes and 128-thread CTAs (whole warps: 5 order-4 elements, 6 CTAs per
+// SM) by default; SALVUS_HEX_KERNEL=classic selects the register / shared-
+// memory kernel that also serves FP64 (read at every launch).
+static bool hex_classic() {
   const char *s = std::getenv("SALVUS_HEX_KERNEL");
-  if (!s) return HEX_V2_E5;  // measured fastest (whole 128-thread CTAs, 6 per SM)
-  static const struct { const char *name; int v; } kNames[] = {
-      {"v2", HEX_V2},           {"v3", HEX_V3},         {"classic", HEX_CLASSIC},
-      {"tma", HEX_TMA},         {"persistent", HEX_PERSISTENT}, {"v2e4", HEX_V2_E4},
-      {"v3e4", HEX_V3_E4},      {"v2e10", HEX_V2_E10},  {"v2e5", HEX_V2_E5},
-      {"v2e10m4", HEX_V2_E10M4}, {"v2e5m8", HEX_V2_E5M8}, {"v2e14", HEX_V2_E14},
-      {"v2e10m3", HEX_V2_E10M3}, {"v2e8m3", HEX_V2_E8M3}, {"v2e5m6", HEX_V2_E5M6},
-      {"v2e14m2", HEX_V2_E14M2}};
-  for (const auto &k : kNames)
-    if (std::strcmp(s, k.name) == 0) return k.v;
-  return HEX_V2_E5;
+  return s && std::strcmp(s, "classic") == 0;
 }
 
-template <int N, int EPB, bool kAsync, int MINB = 0>
+template <int N, bool TI>
 static int launch_elastic_v2(const salvus_mesh *m, const float *rec, const float *u, float *r,
                              cudaStream_t st) {
-  using T = ElasticV2Shape<N, EPB, kAsync>;
-  if constexpr (MINB > 0) {
-    static bool attr_m = false;
-    if (!attr_m) {
-      cudaFuncSetAttribute(elastic_hex_stiffness_v2m_kernel<N, EPB, MINB>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-      attr_m = true;
-    }
-    elastic_hex_stiffness_v2m_kernel<N, EPB, MINB>
-        <<<blocks_for(m->E, EPB), T::THREADS, T::SMEM, st>>>(m->E, rec, u, r, dmatrix<float>(m->basis));
-    g_launches++;
-    return check_launch("elastic stiffness (v2)");
-  }
+  constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
+  using T = ElasticV2Shape<N, EPB, TI>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(elastic_hex_stiffness_v2_kernel<N, EPB, kAsync>,
+    cudaFuncSetAttribute(elastic_hex_stiffness_v2_kernel<N, EPB, TI>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
-  const unsigned grid = blocks_for(m->E, EPB);
-  elastic_hex_stiffness_v2_kernel<N, EPB, kAsync><<<grid, T::THREADS, T::SMEM, st>>>(
+  elastic_hex_stiffness_v2_kernel<N, EPB, TI><<<blocks_for(m->E, EPB), T::THREADS, T::SMEM, st>>>(
       m->E, rec, u, r, dmatrix<float>(m->basis));
   g_launches++;
-  return check_launch("elastic stiffness (v2)");
+  return check_launch("elastic stiffness");
+}
+
+template <int N, typename real, bool TI>
+static int launch_elastic_classic(const salvus_mesh *m, const real *rec, const real *u, real *r,
+                                  cudaStream_t st) {
+  using S = ElasticShape<N, real>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(elastic_hex_stiffness_kernel<N, real, TI>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+    attr_set = true;
+  }
+  elastic_hex_stiffness_kernel<N, real, TI><<<blocks_for(m->E, S::EPB), S::THREADS, S::SMEM, st>>>(
+      m->E, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
+  g_launches++;
+  return check_launch("elastic stiffness");
 }
 
 template <int N, typename real>
 static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, real *r,
-                          cudaStream_t st, int *err) {
+                          cudaStream_t st) {
   if constexpr (std::is_same<real, float>::value) {
-    const int var = hex_variant();
-    constexpr int n2 = (N + 1) * (N + 1);
-    constexpr int E8 = 200 / n2 > 0 ? 200 / n2 : 1, E4 = 100 / n2 > 0 ? 100 / n2 : 1;
-    if (var == HEX_V2) return launch_elastic_v2<N, E8, false>(m, rec, u, r, st);
-    if (var == HEX_V2_E4) return launch_elastic_v2<N, E4, false>(m, rec, u, r, st);
-    if (var == HEX_V3) return launch_elastic_v2<N, E8, true>(m, rec, u, r, st);
-    if (var == HEX_V3_E4) return launch_elastic_v2<N, E4, true>(m, rec, u, r, st);
-    // element counts that fill whole warps at order 4 (n^2 = 25 threads each)
-    constexpr int E10 = 256 / n2 > 0 ? 256 / n2 : 1, E5 = 128 / n2 > 0 ? 128 / n2 : 1;
-    constexpr int E14 = 352 / n2 > 0 ? 352 / n2 : 1;
-    if (var == HEX_V2_E10) return launch_elastic_v2<N, E10, false>(m, rec, u, r, st);
-    if (var == HEX_V2_E5) return launch_elastic_v2<N, E5, false>(m, rec, u, r, st);
-    if (var == HEX_V2_E10M4) return launch_elastic_v2<N, E10, false, 4>(m, rec, u, r, st);
-    if (var == HEX_V2_E5M8) return launch_elastic_v2<N, E5, false, 8>(m, rec, u, r, st);
-    if (var == HEX_V2_E14) return launch_elastic_v2<N, E14, false>(m, rec, u, r, st);
-    if (var == HEX_V2_E10M3) return launch_elastic_v2<N, E10, false, 3>(m, rec, u, r, st);
-    if (var == HEX_V2_E8M3) return launch_elastic_v2<N, E8, false, 3>(m, rec, u, r, st);
-    if (var == HEX_V2_E5M6) return launch_elastic_v2<N, E5, false, 6>(m, rec, u, r, st);
-    if (var == HEX_V2_E14M2) return launch_elastic_v2<N, E14, false, 2>(m, rec, u, r, st);
-    if (var == HEX_TMA && err) {
-      using T = ElasticTmaShape<N>;
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(elastic_hex_stiffness_tma_kernel<N>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-        attr = true;
-      }
-      const unsigned grid = blocks_for(m->E, T::EPB);
-      elastic_hex_stiffness_tma_kernel<N><<<grid, T::THREADS, T::SMEM, st>>>(
-          m->E, rec, u, r, dmatrix<float>(m->basis), err);
-      g_launches++;
-      return check_launch("elastic stiffness (tma)");
-    }
-    if (var == HEX_PERSISTENT && err) {
-      using T = ElasticTmaShape<N>;
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(elastic_hex_stiffness_tma_persistent<N>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM_PERSISTENT);
-        attr = true;
-      }
-      const int64_t groups = (m->E + T::EPB - 1) / T::EPB;
-      const int64_t slots = (int64_t)m->sm_count * 2;
-      const unsigned grid = (unsigned)(groups < slots ? groups : slots);
-      elastic_hex_stiffness_tma_persistent<N><<<grid, T::THREADS, T::SMEM_PERSISTENT, st>>>(
-          m->E, rec, u, r, dmatrix<float>(m->basis), err);
-      g_launches++;
-      return check_launch("elastic stiffness (persistent)");
-    }
+    if (!hex_classic())
+      return m->ti ? launch_elastic_v2<N, true>(m, rec, u, r, st)
+                   : launch_elastic_v2<N, false>(m, rec, u, r, st);
   }
-  using S = ElasticShape<N, real>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(elastic_hex_stiffness_kernel<N, real>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
-    attr_set = true;
-  }
-  const unsigned grid = blocks_for(m->E, S::EPB);
-  elastic_hex_stiffness_kernel<N, real><<<grid, S::THREADS, S::SMEM, st>>>(
-      m->E, rec, m->d_conn.as<int32_t>(), u, r, dmatrix<real>(m->basis));
-  g_launches++;
-  return check_launch("elastic stiffness");
+  return m->ti ? launch_elastic_classic<N, real, true>(m, rec, u, r, st)
+               : launch_elastic_classic<N, real, false>(m, rec, u, r, st);
 }
 
 // Quadrilateral stiffness: column-threaded kernels (kernels_quad_col.cuh) by
@@ -335,17 +260,17 @@ static const real *simplex_tables(const salvus_mesh *m) {
   return sizeof(real) == 4 ? (const real *)m->d_sd32.ptr : (const real *)m->d_sd64.ptr;
 }
 
-template <typename real, int C>
+template <typename real, int C, bool TI = false>
 static int launch_tet(const salvus_mesh *m, const real *rec, const real *u, real *r,
                       cudaStream_t st) {
-  using S = TetShape<real, C>;
+  using S = TetShape<real, C, TI>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(tet_stiffness_kernel<real, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)S::SMEM);
+    cudaFuncSetAttribute(tet_stiffness_kernel<real, C, TI>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
     attr = true;
   }
-  tet_stiffness_kernel<real, C><<<blocks_for(m->E, S::EPB), S::THREADS, S::SMEM, st>>>(
+  tet_stiffness_kernel<real, C, TI><<<blocks_for(m->E, S::EPB), S::THREADS, S::SMEM, st>>>(
       m->E, rec, m->d_conn.as<int32_t>(), simplex_tables<real>(m), u, r);
   g_launches++;
   return check_launch("tetrahedron stiffness");
@@ -409,7 +334,8 @@ static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, 
     g_launches++;
     return check_launch("triangle stiffness");
   }
-  if (m->physics == SALVUS_ELASTIC3D) return launch_tet<real, 3>(m, rec, u, r, st);
+  if (m->physics == SALVUS_ELASTIC3D)
+    return m->ti ? launch_tet<real, 3, true>(m, rec, u, r, st) : launch_tet<real, 3>(m, rec, u, r, st);
   return launch_tet<real, 1>(m, rec, u, r, st);
 }
 
@@ -419,12 +345,12 @@ static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u
   if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st, err);
   if (m->physics == SALVUS_ELASTIC3D) {
     switch (m->order) {
-      case 1: return launch_elastic<1, real>(m, rec, u, r, st, err);
-      case 2: return launch_elastic<2, real>(m, rec, u, r, st, err);
-      case 3: return launch_elastic<3, real>(m, rec, u, r, st, err);
-      case 4: return launch_elastic<4, real>(m, rec, u, r, st, err);
-      case 5: return launch_elastic<5, real>(m, rec, u, r, st, err);
-      case 6: return launch_elastic<6, real>(m, rec, u, r, st, err);
+      case 1: return launch_elastic<1, real>(m, rec, u, r, st);
+      case 2: return launch_elastic<2, real>(m, rec, u, r, st);
+      case 3: return launch_elastic<3, real>(m, rec, u, r, st);
+      case 4: return launch_elastic<4, real>(m, rec, u, r, st);
+      case 5: return launch_elastic<5, real>(m, rec, u, r, st);
+      case 6: return launch_elastic<6, real>(m, rec, u, r, st);
     }
   } else if (m->shape == SALVUS_QUAD) {
     switch (m->order) {
@@ -457,7 +383,7 @@ static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u
 template <typename real>
 static int build_simplex_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &sd,
                                  DeviceBuffer &mass_local) {
-  const int rw = record_words(m->shape, m->physics, sizeof(real) == 8);
+  const int rw = record_words(m->shape, m->physics, sizeof(real) == 8, m->ti);
   int rc = out.alloc(sizeof(real) * (size_t)m->E * rw);
   if (rc) return rc;
   SimplexTable tab{};
@@ -467,7 +393,7 @@ static int build_simplex_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer
   }
   simplex_geometry_kernel<real><<<blocks_for(m->E, 128), 128, 0, m->stream>>>(
       m->E, m->shape, m->physics, m->P, rw, m->d_vtx.as<double>(), m->d_par.as<double>(), tab,
-      out.as<real>(), mass_local.as<double>());
+      out.as<real>(), mass_local.as<double>(), m->ti);
   g_launches++;
   if ((rc = check_launch("simplex geometry"))) return rc;
   std::vector<real> t(m->basis.SD.size());
@@ -561,7 +487,7 @@ static int build_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &mass_l
   if (is_simplex(m->shape))
     return build_simplex_records<real>(m, out, sizeof(real) == 4 ? m->d_sd32 : m->d_sd64,
                                        mass_local);
-  const int rw = record_words(m->shape, m->physics, sizeof(real) == 8);
+  const int rw = record_words(m->shape, m->physics, sizeof(real) == 8, m->ti);
   int rc = out.alloc(sizeof(real) * (size_t)(m->E * m->P) * rw);
   if (rc) return rc;
   GllTable gll{};
@@ -573,7 +499,7 @@ static int build_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &mass_l
   geometry_kernel<real, kPack><<<blocks_for(total, 128), 128, 0, m->stream>>>(
       m->E, m->dim, m->n, m->P, m->physics, rw, m->d_vtx.as<double>(), m->d_par.as<double>(),
       m->d_conn.as<int32_t>(), gll, out.as<real>(), mass_local.as<double>(),
-      m->d_cls_k.as<int32_t>(), m->n_fluid);
+      m->d_cls_k.as<int32_t>(), m->n_fluid, m->ti);
   g_launches++;
   return check_launch("geometry");
 }
@@ -1055,15 +981,11 @@ static int newmark_t(salvus_problem *p) {
 
 // True when the FP32 stiffness launch of this mesh runs a kernel whose
 // bounded waits report a timeout through the error word (tensor-core
-// simplices, the TMA hexahedron variants); mirrors launch_stiffness.
+// simplices); mirrors launch_stiffness.
 bool stiffness_reports_errors(const salvus_mesh *m, int precision) {
   if (precision != SALVUS_FP32) return false;
   if (m->shape == SALVUS_TET) return m->tet_kernel == 0;
   if (m->shape == SALVUS_TRI) return m->tri_kernel == 0;
-  if (m->shape == SALVUS_HEX && m->physics == SALVUS_ELASTIC3D) {
-    const int v = hex_variant();
-    return v == HEX_TMA || v == HEX_PERSISTENT;
-  }
   return false;
 }
 
@@ -1563,7 +1485,7 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
   m->n = m->basis.n;
   m->P = m->basis.P;
   m->c = physics_components(d->physics);
-  m->npar = physics_params(d->physics);
+  m->npar = physics_params(d->physics, d->reserved);
   m->E = d->n_elements;
   m->vtx.resize((size_t)(m->E * m->nv * m->dim));
   for (int64_t e = 0; e < m->E; ++e)
@@ -1595,6 +1517,27 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
   m->par.assign(d->params, d->params + npar_total);
   for (size_t i = 0; i < npar_total; ++i)
     if (!std::isfinite(m->par[i])) return fail(SALVUS_E_INVALID, "non-finite material parameter");
+  if (m->npar == 6) {
+    // RHO VPV VPH VSV VSH ETA (Elastic3D.cpp:33-54).  An isotropic model
+    // (VPH = VPV, VSH = VSV, ETA = 1 everywhere) keeps the two-constant
+    // records and kernels; anything else gets the five-constant ones.
+    const size_t K = (size_t)m->E * m->nv;
+    const double *pr = m->par.data();
+    bool iso = true;
+    for (size_t i = 0; i < K && iso; ++i)
+      iso = pr[2 * K + i] == pr[K + i] && pr[4 * K + i] == pr[3 * K + i] && pr[5 * K + i] == 1.0;
+    if (iso) {
+      std::vector<double> p3(3 * K);
+      std::copy(pr, pr + K, p3.begin());                    // RHO
+      std::copy(pr + K, pr + 2 * K, p3.begin() + K);        // VP = VPV
+      std::copy(pr + 3 * K, pr + 4 * K, p3.begin() + 2 * K);  // VS = VSV
+      m->par.swap(p3);
+      m->npar = 3;
+    } else {
+      m->ti = true;
+      m->tet_kernel = 1;  // tetrahedra: the CUDA-core kernel has the five-constant stress
+    }
+  }
   if ((rc = flatten_mesh(m.get(), d->cells, d->n_vertices))) return rc;
   if (m->physics == SALVUS_COUPLED2D && (rc = setup_coupled(m.get(), d->cells))) return rc;
   if (device >= 0) {
@@ -2309,6 +2252,10 @@ int salvus_group_create(salvus_problem *const *members, int32_t n, salvus_group 
       return fail(SALVUS_E_UNSUPPORTED, "group members must be FP32 single-shot problems");
     if (p->n_dir_pts > 0)
       return fail(SALVUS_E_UNSUPPORTED, "group members cannot carry Dirichlet boundaries");
+    if (m->ti)
+      return fail(SALVUS_E_UNSUPPORTED,
+                  "group members must have isotropic material (transversely isotropic meshes "
+                  "run as single problems)");
     if (m->shape != m0->shape || m->order != m0->order || m->physics != m0->physics ||
         m->device != m0->device)
       return fail(SALVUS_E_INVALID, "group members must share shape, order, physics and device");

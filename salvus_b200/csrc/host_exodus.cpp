@@ -529,8 +529,9 @@ int salvus_exodus_params(const salvus_exodus *x, int32_t physics, double *params
         const double *ref = k == 0 ? params + blk : k == 1 ? params + 2 * blk : nullptr;
         for (size_t i = 0; i < blk; ++i)
           if (t[i] != (ref ? ref[i] : 1.0))
-            return fail(SALVUS_E_UNSUPPORTED, "%s: anisotropic elastic model (%s differs); the 3-D "
-                        "elastic physics here is isotropic", x->path.c_str(), pairs[k][0]);
+            return fail(SALVUS_E_UNSUPPORTED, "%s: anisotropic elastic model (%s differs); read "
+                        "it with salvus_exodus_elastic3d_params for a SALVUS_MESH_ELASTIC_TI mesh",
+                        x->path.c_str(), pairs[k][0]);
       }
       return SALVUS_OK;
     }
@@ -554,6 +555,52 @@ int salvus_exodus_params(const salvus_exodus *x, int32_t physics, double *params
     }
   }
   return fail(SALVUS_E_INVALID, "unknown physics %d", physics);
+}
+
+int salvus_exodus_elastic3d_params(const salvus_exodus *x, double *params) {
+  if (!x || !params) return fail(SALVUS_E_INVALID, "null argument");
+  const size_t blk = (size_t)(x->n_elements * x->nv);
+  // per-vertex NAME_<i> (ExodusModel.cpp:439-470), VPV <-> VP and VSV <-> VS
+  // fallbacks as in the reference
+  auto read = [&](const char *name, const char *alt, double *out, double dflt, bool need) -> int {
+    std::string n = name;
+    if (find_name(x->var_names, n + "_0") < 0) {
+      if (alt && find_name(x->var_names, std::string(alt) + "_0") >= 0) {
+        n = alt;
+      } else if (!need) {
+        for (size_t i = 0; i < blk; ++i) out[i] = dflt;
+        return SALVUS_OK;
+      } else {
+        return fail(SALVUS_E_NOT_FOUND, "%s: elastic physics needs elemental variables %s_0..%s_%d",
+                    x->path.c_str(), name, name, x->nv - 1);
+      }
+    }
+    for (int i = 0; i < x->nv; ++i) {
+      const int k = find_name(x->var_names, n + "_" + std::to_string(i));
+      if (k < 0)
+        return fail(SALVUS_E_NOT_FOUND, "%s: no elemental variable %s_%d", x->path.c_str(), n.c_str(), i);
+      for (int64_t e = 0; e < x->n_elements; ++e)
+        out[e * x->nv + i] = x->var_vals[(size_t)k][(size_t)e];
+    }
+    return SALVUS_OK;
+  };
+  int rc;
+  if ((rc = read("RHO", nullptr, params, 0.0, true)) ||
+      (rc = read("VPV", "VP", params + blk, 0.0, true)) ||
+      (rc = read("VSV", "VS", params + 3 * blk, 0.0, true)))
+    return rc;
+  // horizontal velocities default to the vertical ones, ETA to 1 (isotropic)
+  if (find_name(x->var_names, "VPH_0") >= 0) {
+    if ((rc = read("VPH", nullptr, params + 2 * blk, 0.0, true))) return rc;
+  } else {
+    std::copy(params + blk, params + 2 * blk, params + 2 * blk);
+  }
+  if (find_name(x->var_names, "VSH_0") >= 0) {
+    if ((rc = read("VSH", nullptr, params + 4 * blk, 0.0, true))) return rc;
+  } else {
+    std::copy(params + 3 * blk, params + 4 * blk, params + 4 * blk);
+  }
+  return read("ETA", nullptr, params + 5 * blk, 1.0, false);
 }
 
 int salvus_exodus_side_set_nodes(const salvus_exodus *x, const salvus_mesh *m, const char *name,

@@ -370,11 +370,12 @@ int inverse_map(int shape, const double *vtx, const double *x, double *ref) {
   return fail(SALVUS_E_INVALID, "inverse coordinate transform did not converge");
 }
 
-int record_words(int shape, int physics, int fp64) {
+int record_words(int shape, int physics, int fp64, bool ti) {
   // simplices: one record per element (affine geometry), see kernels_simplex.cuh
   if (shape == SALVUS_TRI) return 16;                        // G(3) pad s[12]
-  if (shape == SALVUS_TET) return physics == SALVUS_ELASTIC3D ? 120 : 64;
-  if (physics == SALVUS_ELASTIC3D) return fp64 ? 11 : 12;  // invJ(9) lambda' mu' [conn]
+  if (shape == SALVUS_TET) return physics == SALVUS_ELASTIC3D ? (ti ? 280 : 120) : 64;
+  // invJ(9) lambda' mu' [conn]; transversely isotropic invJ(9) A' C' [conn] F' L' N' [0]
+  if (physics == SALVUS_ELASTIC3D) return ti ? (fp64 ? 14 : 16) : (fp64 ? 11 : 12);
   if (physics == SALVUS_ELASTIC2D) return 8;                // invJ(4) C11' C13' C33' C55'
   if (physics == SALVUS_COUPLED2D) return 8;                // per class: fluid 4 | 3, solid 8
   if (shape == SALVUS_QUAD) return fp64 ? 3 : 4;          // G00 G01 G11 [conn]

@@ -66,8 +66,10 @@ inline int physics_components(int physics) {
   return (physics == SALVUS_ELASTIC3D || physics == SALVUS_COUPLED2D) ? 3
                                                                       : (physics == SALVUS_ELASTIC2D ? 2 : 1);
 }
-inline int physics_params(int physics) {
-  return physics == SALVUS_ELASTIC3D ? 3
+// (flags: salvus_mesh_desc.reserved; SALVUS_MESH_ELASTIC_TI selects the six
+// transversely isotropic elastic 3-D parameters)
+inline int physics_params(int physics, int flags = 0) {
+  return physics == SALVUS_ELASTIC3D ? ((flags & SALVUS_MESH_ELASTIC_TI) ? 6 : 3)
          : physics == SALVUS_ELASTIC2D ? 5 : physics == SALVUS_COUPLED2D ? 7 : 1;
 }
 
@@ -81,8 +83,9 @@ struct DeviceBuffer {
 };
 
 // Number of float / double words per element-point record in the stiffness
-// kernels (geometry + folded material [+ packed connectivity for FP32]).
-int record_words(int shape, int physics, int fp64);
+// kernels (geometry + folded material [+ packed connectivity for FP32]);
+// ti: transversely isotropic elastic material (five constants per point).
+int record_words(int shape, int physics, int fp64, bool ti = false);
 
 }  // namespace salvus
 
@@ -94,6 +97,7 @@ struct salvus_mesh {
   int sm_count = 148;
   bool host_only = false;
   bool fp32_only = false;
+  bool ti = false;  // elastic 3-D with transversely isotropic material (6 parameters)
   int shape = 0, order = 0, physics = 0, dim = 0, nv = 0, n = 0, P = 0, c = 0, npar = 0;
   int64_t E = 0, G = 0;
   salvus::Basis basis;

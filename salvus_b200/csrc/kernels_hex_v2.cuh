@@ -12,50 +12,45 @@
 //  * connectivity comes from word 11 of each 48-byte record, so no separate
 //    connectivity stream is read; the record's last float4 (J8, lambda', mu',
 //    conn) is fetched first to start the displacement gather early;
-//  * records are three float4 planes per element ([E][3][P]), so the 32
-//    lanes of a warp load 512 contiguous bytes per instruction.
+//  * records are three (transversely isotropic: four) float4 planes per
+//    element ([E][3|4][P]), so the 32 lanes of a warp load 512 contiguous
+//    bytes per instruction.
 #pragma once
 
 #include <cstdint>
+
+#include "kernels_material.cuh"
 
 namespace salvus {
 
 // smallest w' >= w with w' = m (mod 32)
 __host__ __device__ constexpr int pad_to_mod32(int w, int m) { return w + ((m - (w % 32)) + 32) % 32; }
 
-template <int N, int EPB_, bool kAsync>
+template <int N, int EPB_, bool TI = false>
 struct ElasticV2Shape {
   static constexpr int n = N + 1, n2 = n * n, P = n2 * n;
   static constexpr int EPB = EPB_;
   static constexpr int THREADS = ((EPB * n2 + 31) / 32) * 32;
+  // float4 record planes per element: isotropic 3, transversely isotropic 4
+  static constexpr int PLANES = TI ? 4 : 3;
   // padded per-element strides (words): u planes 3P, F planes 6P
   static constexpr int US = pad_to_mod32(3 * P, n2 % 32);
   static constexpr int FS = pad_to_mod32(6 * P, n2 % 32);
-  // kAsync: record heads (invJ 0..7, two float4 per point) staged in shared
-  // memory by cp.async, in two planes [EPB*P] float4 each
-  static constexpr size_t REC = kAsync ? (size_t)2 * EPB * P * 16 : 0;
-  static constexpr size_t SMEM = REC + sizeof(float) * (size_t)EPB * (US + FS);
+  static constexpr size_t SMEM = sizeof(float) * (size_t)EPB * (US + FS);
 };
 
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_all;" ::: "memory");
-}
-
-template <int N, int EPB_, bool kAsync>
+// Records ([E][PLANES][P] float4): plane 0 = invJ 0-3, plane 1 = invJ 4-7,
+// plane 2 = (invJ 8, m0, m1, conn); TI adds plane 3 = (m2, m3, m4, 0), where
+// m = (lambda', mu') for isotropic and (A', C', F', L', N') for transversely
+// isotropic material (kernels_material.cuh).
+template <int N, int EPB_, bool TI>
 __device__ __forceinline__ void elastic_hex_v2_body(int64_t bid, int64_t E,
                                                     const float *__restrict__ rec,
                                                     const float *__restrict__ u,
                                                     float *__restrict__ r, const DMatrix<float> &Dm) {
-  using S = ElasticV2Shape<N, EPB_, kAsync>;
+  using S = ElasticV2Shape<N, EPB_, TI>;
   constexpr int n = S::n, n2 = S::n2, P = S::P, EPB = S::EPB;
-  extern __shared__ __align__(16) float smem_v2raw[];
-  float4 *sra = reinterpret_cast<float4 *>(smem_v2raw);  // [EPB*P] (kAsync)
-  float4 *srb = sra + (kAsync ? (size_t)EPB * P : 0);
-  float *smem_v2 = smem_v2raw + S::REC / sizeof(float);
+  extern __shared__ __align__(16) float smem_v2[];
   const int t = threadIdx.x;
   const int le = t / n2, ij = t - le * n2;
   const int i = ij % n, j = ij / n;
@@ -63,7 +58,7 @@ __device__ __forceinline__ void elastic_hex_v2_body(int64_t bid, int64_t E,
   const bool ok = le < EPB && e < E;
   float *su = smem_v2 + (size_t)(ok ? le : 0) * S::US;                      // [3][P]
   float *sF = smem_v2 + (size_t)EPB * S::US + (size_t)(ok ? le : 0) * S::FS;  // [3][2][P]
-  const float4 *rq = reinterpret_cast<const float4 *>(rec) + (e * 3) * P;  // planes [3][P]
+  const float4 *rq = reinterpret_cast<const float4 *>(rec) + (e * S::PLANES) * P;
 
   float Dri[n], Dsj[n], DTi[n], DTj[n];
 #pragma unroll
@@ -74,15 +69,7 @@ __device__ __forceinline__ void elastic_hex_v2_body(int64_t bid, int64_t E,
     DTj[l] = Dm.d[l * n + j];
   }
   float ux[n], uy[n], uz[n];
-  float4 rc[n];  // (J8, lambda', mu', conn) per point of the column
-  if (kAsync && ok) {
-#pragma unroll
-    for (int k = 0; k < n; ++k) {
-      const int p = ij + n2 * k;
-      cp_async16(sra + le * P + p, rq + p);
-      cp_async16(srb + le * P + p, rq + P + p);
-    }
-  }
+  float4 rc[n];  // (J8, m0, m1, conn) per point of the column
   if (ok) {
 #pragma unroll
     for (int k = 0; k < n; ++k) rc[k] = __ldg(rq + 2 * P + ij + n2 * k);
@@ -101,17 +88,15 @@ __device__ __forceinline__ void elastic_hex_v2_body(int64_t bid, int64_t E,
       su[2 * P + p] = uz[k];
     }
   }
-  if (kAsync) cp_async_wait_all();  // own points' record heads (read by this thread only)
   __syncthreads();
   float Ftx[n], Fty[n], Ftz[n];
   if (ok) {
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const int p = ij + n2 * k;
-      const float4 ra = kAsync ? sra[le * P + p] : __ldg(rq + p);
-      const float4 rb = kAsync ? srb[le * P + p] : __ldg(rq + P + p);
+      const float4 ra = __ldg(rq + p);
+      const float4 rb = __ldg(rq + P + p);
       const float J[9] = {ra.x, ra.y, ra.z, ra.w, rb.x, rb.y, rb.z, rb.w, rc[k].x};
-      const float lam = rc[k].y, mu = rc[k].z;
       float d[3][3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -132,14 +117,14 @@ __device__ __forceinline__ void elastic_hex_v2_body(int64_t bid, int64_t E,
 #pragma unroll
         for (int a = 0; a < 3; ++a)
           g[c][a] = J[a * 3 + 0] * d[c][0] + J[a * 3 + 1] * d[c][1] + J[a * 3 + 2] * d[c][2];
-      const float tr = g[0][0] + g[1][1] + g[2][2];
-      const float sxx = lam * tr + 2 * mu * g[0][0];
-      const float syy = lam * tr + 2 * mu * g[1][1];
-      const float szz = lam * tr + 2 * mu * g[2][2];
-      const float sxy = mu * (g[0][1] + g[1][0]);
-      const float sxz = mu * (g[0][2] + g[2][0]);
-      const float syz = mu * (g[1][2] + g[2][1]);
-      const float sig[3][3] = {{sxx, sxy, sxz}, {sxy, syy, syz}, {sxz, syz, szz}};
+      float sig[3][3];
+      if constexpr (TI) {
+        const float4 rt = __ldg(rq + 3 * P + p);
+        const float m[5] = {rc[k].y, rc[k].z, rt.x, rt.y, rt.z};
+        stress_ti<float>(g, m, sig);
+      } else {
+        stress_iso<float>(g, rc[k].y, rc[k].z, sig);
+      }
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const float F0 = J[0] * sig[c][0] + J[3] * sig[c][1] + J[6] * sig[c][2];
@@ -175,22 +160,12 @@ __device__ __forceinline__ void elastic_hex_v2_body(int64_t bid, int64_t E,
   }
 }
 
-// MINB = 0: the compiler picks the register count for THREADS threads per
-// CTA; MINB > 0 also asks for MINB resident CTAs per SM (register cap).
-template <int N, int EPB_, bool kAsync, int MINB = 0>
-__global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, kAsync>::THREADS)
+template <int N, int EPB_, bool TI>
+__global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, TI>::THREADS)
 elastic_hex_stiffness_v2_kernel(int64_t E, const float *__restrict__ rec,
                                 const float *__restrict__ u, float *__restrict__ r,
                                 DMatrix<float> Dm) {
-  elastic_hex_v2_body<N, EPB_, kAsync>(blockIdx.x, E, rec, u, r, Dm);
-}
-
-template <int N, int EPB_, int MINB>
-__global__ void __launch_bounds__(ElasticV2Shape<N, EPB_, false>::THREADS, MINB)
-elastic_hex_stiffness_v2m_kernel(int64_t E, const float *__restrict__ rec,
-                                 const float *__restrict__ u, float *__restrict__ r,
-                                 DMatrix<float> Dm) {
-  elastic_hex_v2_body<N, EPB_, false>(blockIdx.x, E, rec, u, r, Dm);
+  elastic_hex_v2_body<N, EPB_, TI>(blockIdx.x, E, rec, u, r, Dm);
 }
 
 }  // namespace salvus

@@ -13,6 +13,8 @@
 
 #include <cstdint>
 
+#include "kernels_material.cuh"
+
 namespace salvus {
 
 constexpr int kMaxN = 11;
@@ -90,10 +92,12 @@ __device__ __forceinline__ double p1_interp_dev(int dim, const double *vals, con
 // Records:
 //   acoustic : G = w detJ vp^2 invJ^T invJ (symmetric; 3 or 6 words)
 //   elastic  : invJ (row-major [x_a][xi_b], 9 words), lambda w detJ, mu w detJ
-// FP32 elastic records (12 words with connectivity) are stored as three
-// float4 planes per element, [E][3][P] float4: plane 0 = invJ 0-3, plane 1 =
-// invJ 4-7, plane 2 = (invJ 8, lambda', mu', conn), so that consecutive
-// points of one plane are consecutive 16-byte words (contiguous warp loads).
+//              (transversely isotropic: A C F L N w detJ, kernels_material.cuh)
+// FP32 elastic records (12 words with connectivity, 16 transversely
+// isotropic) are stored as float4 planes per element, [E][3|4][P] float4:
+// plane 0 = invJ 0-3, plane 1 = invJ 4-7, plane 2 = (invJ 8, m0, m1, conn),
+// plane 3 = (m2, m3, m4, 0), so that consecutive points of one plane are
+// consecutive 16-byte words (contiguous warp loads).
 // Meshes of fluid and solid quadrilaterals (physics 3): records are stored per
 // class, fluid elements first ([Ef] acoustic quad records) then solid ones
 // (elastic 2-D records); cls_k[e] is the element's index within its class.
@@ -102,7 +106,8 @@ __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, i
                                 const double *__restrict__ vtx, const double *__restrict__ par,
                                 const int32_t *__restrict__ conn, GllTable gll,
                                 real *__restrict__ rec, double *__restrict__ mass_local,
-                                const int32_t *__restrict__ cls_k = nullptr, int64_t Ef = 0) {
+                                const int32_t *__restrict__ cls_k = nullptr, int64_t Ef = 0,
+                                bool ti = false) {
   int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= E * P) return;
   const int64_t e = tid / P;
@@ -192,31 +197,38 @@ __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, i
     }
     mass_local[tid] = wd;  // Scalar mass: no density (Scalar.cpp:34-39)
   } else {
-    double vals[8], rho, vp, vs;
-    for (int a = 0; a < 8; ++a) vals[a] = par[(0 * E + e) * 8 + a];
-    rho = p1_interp_dev(3, vals, ref);
-    for (int a = 0; a < 8; ++a) vals[a] = par[(1 * E + e) * 8 + a];
-    vp = p1_interp_dev(3, vals, ref);
-    for (int a = 0; a < 8; ++a) vals[a] = par[(2 * E + e) * 8 + a];
-    vs = p1_interp_dev(3, vals, ref);
-    // c11 = rho vp^2, c66 = rho vs^2, c12 = c11 - 2 c66 (Elastic3D.cpp:42-53)
-    double mu = rho * vs * vs;
-    double lam = rho * vp * vp - 2.0 * mu;
+    // elastic 3-D: P1-interpolated RHO VP VS (isotropic) or RHO VPV VPH VSV
+    // VSH ETA (transversely isotropic), then the folded constants
+    // (Elastic3D.cpp:42-53, kernels_material.cuh)
+    const int npar = ti ? 6 : 3;
+    double pv[6];
+    for (int q = 0; q < npar; ++q) {
+      double vals[8];
+      for (int a = 0; a < 8; ++a) vals[a] = par[((int64_t)q * E + e) * 8 + a];
+      pv[q] = p1_interp_dev(3, vals, ref);
+    }
+    double mc[5];
+    const int nm = ti ? 5 : 2;
+    if (ti) elastic_constants_ti(pv, mc);
+    else elastic_constants_iso(pv[0], pv[1], pv[2], mc);
     if constexpr (kPackConn) {
-      real w12[12];
-      for (int a = 0; a < 9; ++a) w12[a] = (real)iJ[a];
-      w12[9] = (real)(wd * lam);
-      w12[10] = (real)(wd * mu);
-      const int32_t cn = conn[tid];
-      w12[11] = 0;
-      reinterpret_cast<int32_t *>(w12)[11] = cn;
-      for (int a = 0; a < 12; ++a) rec[((e * 3 + a / 4) * P + p) * 4 + a % 4] = w12[a];
+      // float4 planes [E][3|4][P]: invJ 0-3 | invJ 4-7 | invJ 8, m0, m1, conn
+      // | m2, m3, m4, 0 (transversely isotropic only)
+      const int planes = ti ? 4 : 3;
+      real w16[16];
+      for (int a = 0; a < 9; ++a) w16[a] = (real)iJ[a];
+      w16[9] = (real)(wd * mc[0]);
+      w16[10] = (real)(wd * mc[1]);
+      w16[11] = 0;
+      reinterpret_cast<int32_t *>(w16)[11] = conn[tid];
+      for (int a = 0; a < 4; ++a) w16[12 + a] = a < 3 && ti ? (real)(wd * mc[2 + a]) : (real)0;
+      for (int a = 0; a < 4 * planes; ++a)
+        rec[((e * planes + a / 4) * P + p) * 4 + a % 4] = w16[a];
     } else {
       for (int a = 0; a < 9; ++a) out[a] = (real)iJ[a];
-      out[9] = (real)(wd * lam);
-      out[10] = (real)(wd * mu);
+      for (int a = 0; a < nm; ++a) out[9 + a] = (real)(wd * mc[a]);
     }
-    mass_local[tid] = wd * rho;
+    mass_local[tid] = wd * pv[0];
     return;
   }
   if (kPackConn) {

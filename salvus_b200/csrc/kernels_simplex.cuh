@@ -29,13 +29,19 @@
 //   tetrahedron acoustic  [G00 G01 G02 G11 G12 G22 0 0 | s_0..s_49 | 0 x6]    64
 //   tetrahedron elastic   [invJ (9) 0 x3 | lw_0..lw_49 | 0 0 | mw_0..mw_49 | 0 x6]
 //                                                                            120
+//   tetrahedron elastic, transversely isotropic
+//                         [invJ (9) 0 x3 | A' 0 0 | C' 0 0 | F' 0 0 | L' 0 0 | N' | 0 x10]
+//                                                                            280
 // (padded so that every 8-node run of s / lw / mw starts on 16 bytes and an
 // 8-node run that starts at node 48 stays inside the record)
 // with G = detJ invJ^T invJ (invJ[x_a][xi_b] = d xi_b / d x_a), s_q = w_q vp_q^2,
-// lw_q = w_q detJ lambda_q, mw_q = w_q detJ mu_q.
+// lw_q = w_q detJ lambda_q, mw_q = w_q detJ mu_q, and the transversely
+// isotropic constants (kernels_material.cuh) times w_q detJ.
 #pragma once
 
 #include <cstdint>
+
+#include "kernels_material.cuh"
 
 namespace salvus {
 
@@ -44,15 +50,19 @@ struct SimplexTable {
   double w[50];     // nodal quadrature weights
 };
 
-constexpr int kTriRec = 16, kTetAcRec = 64, kTetElRec = 120;
+constexpr int kTriRec = 16, kTetAcRec = 64, kTetElRec = 120, kTetTiRec = 280;
 constexpr int kTetLambda = 12, kTetMu = 64;
+// per-node material arrays of elastic tetrahedra start at kTetLambda +
+// kTetMatStride * m (m = 0, 1 isotropic; m = 0..4 transversely isotropic)
+constexpr int kTetMatStride = 52;
 
 // One thread per element.
 template <typename real>
 __global__ void simplex_geometry_kernel(int64_t E, int shape, int physics, int P, int rw,
                                         const double *__restrict__ vtx,
                                         const double *__restrict__ par, SimplexTable tab,
-                                        real *__restrict__ rec, double *__restrict__ mass_local) {
+                                        real *__restrict__ rec, double *__restrict__ mass_local,
+                                        bool ti = false) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= E) return;
   const bool tri = shape == 2;
@@ -88,7 +98,7 @@ __global__ void simplex_geometry_kernel(int64_t E, int shape, int physics, int P
   }
   real *out = rec + e * rw;
   for (int a = 0; a < rw; ++a) out[a] = 0;
-  const int npar = physics == 0 ? 1 : 3;
+  const int npar = physics == 0 ? 1 : (ti ? 6 : 3);
   for (int q = 0; q < P; ++q) {
     const double r = tab.x[q][0], s = tab.x[q][1], t = tab.x[q][2];
     double lw[4];
@@ -97,7 +107,7 @@ __global__ void simplex_geometry_kernel(int64_t E, int shape, int physics, int P
     } else {
       lw[0] = 1.0 - r - s - t; lw[1] = s; lw[2] = r; lw[3] = t;
     }
-    double pv[3];
+    double pv[6];
     for (int k = 0; k < npar; ++k) {
       double acc = 0;
       for (int a = 0; a < nv; ++a) acc += lw[a] * par[((int64_t)k * E + e) * nv + a];
@@ -108,11 +118,12 @@ __global__ void simplex_geometry_kernel(int64_t E, int shape, int physics, int P
       out[(tri ? 4 : 8) + q] = (real)(tab.w[q] * pv[0] * pv[0]);
       mass_local[e * P + q] = wd;
     } else {
-      const double rho = pv[0], vp = pv[1], vs = pv[2];
-      const double mu = rho * vs * vs, lam = rho * vp * vp - 2.0 * mu;
-      out[kTetLambda + q] = (real)(wd * lam);
-      out[kTetMu + q] = (real)(wd * mu);
-      mass_local[e * P + q] = wd * rho;
+      double mc[5];
+      const int nm = ti ? 5 : 2;
+      if (ti) elastic_constants_ti(pv, mc);
+      else elastic_constants_iso(pv[0], pv[1], pv[2], mc);
+      for (int m = 0; m < nm; ++m) out[kTetLambda + kTetMatStride * m + q] = (real)(wd * mc[m]);
+      mass_local[e * P + q] = wd * pv[0];
     }
   }
   if (physics == 0) {
@@ -254,23 +265,23 @@ tri_acoustic_const_kernel(int64_t E, const real *__restrict__ rec,
 // element node, EPB elements per CTA.  The derivative table is held twice in
 // shared memory, [k][j][q] for the gradient (lanes walk q) and [k][q][i] for
 // the divergence (lanes walk i), so both contractions are bank-conflict-free.
-template <typename real, int C>
+template <typename real, int C, bool TI = false>
 struct TetShape {
   static constexpr int P = 50;
   static constexpr int EPB = sizeof(real) == 4 ? 8 : 4;
   static constexpr int THREADS = EPB * P;
-  static constexpr int RW = C == 1 ? kTetAcRec : kTetElRec;
+  static constexpr int RW = C == 1 ? kTetAcRec : (TI ? kTetTiRec : kTetElRec);
   static constexpr int NF = C == 1 ? 3 : 9;  // flux words per node
   static constexpr size_t SMEM =
       sizeof(real) * (size_t)(2 * 3 * P * P + EPB * P * C + EPB * P * NF + EPB * RW);
 };
 
-template <typename real, int C>
-__global__ void __launch_bounds__(TetShape<real, C>::THREADS)
+template <typename real, int C, bool TI = false>
+__global__ void __launch_bounds__(TetShape<real, C, TI>::THREADS)
 tet_stiffness_kernel(int64_t E, const real *__restrict__ rec, const int32_t *__restrict__ conn,
                      const real *__restrict__ SD, const real *__restrict__ u,
                      real *__restrict__ r) {
-  using S = TetShape<real, C>;
+  using S = TetShape<real, C, TI>;
   constexpr int P = S::P, EPB = S::EPB, RW = S::RW, NF = S::NF, PP = P * P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   real *sD = reinterpret_cast<real *>(smem_raw);  // [3][j][q]
@@ -329,13 +340,20 @@ tet_stiffness_kernel(int64_t E, const real *__restrict__ rec, const int32_t *__r
 #pragma unroll
         for (int x = 0; x < 3; ++x)
           g[a][x] = rc[x * 3 + 0] * gr[a][0] + rc[x * 3 + 1] * gr[a][1] + rc[x * 3 + 2] * gr[a][2];
-      const real lw = rc[kTetLambda + q], mw = rc[kTetMu + q];
-      const real tr = lw * (g[0][0] + g[1][1] + g[2][2]);
       real sig[3][3];
+      if constexpr (TI) {
+        real mc[5];
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
+        for (int m = 0; m < 5; ++m) mc[m] = rc[kTetLambda + kTetMatStride * m + q];
+        stress_ti<real>(g, mc, sig);
+      } else {
+        const real lw = rc[kTetLambda + q], mw = rc[kTetMu + q];
+        const real tr = lw * (g[0][0] + g[1][1] + g[2][2]);
 #pragma unroll
-        for (int x = 0; x < 3; ++x) sig[a][x] = mw * (g[a][x] + g[x][a]) + (a == x ? tr : real(0));
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+          for (int x = 0; x < 3; ++x) sig[a][x] = mw * (g[a][x] + g[x][a]) + (a == x ? tr : real(0));
+      }
       // reference flux F[a][k] = sum_x invJ[x][k] sigma[a][x]
 #pragma unroll
       for (int a = 0; a < 3; ++a)

@@ -45,7 +45,7 @@
 
 #include <cstdint>
 
-#include "kernels_hex_tma.cuh"  // smem_addr, mbarrier helpers
+#include "kernels_sync.cuh"  // smem_addr, mbarrier helpers
 
 namespace salvus {
 

@@ -17,6 +17,8 @@
 
 #include <cstdint>
 
+#include "kernels_material.cuh"
+
 namespace salvus {
 
 template <typename real>
@@ -163,27 +165,36 @@ struct ElasticShape {
   static constexpr size_t SMEM = sizeof(real) * (size_t)EPB * 9 * P;
 };
 
-// FP32 records: three float4 planes per element ([E][3][P], kernels_setup.cuh)
-__device__ __forceinline__ void load_elastic_rec(const float *__restrict__ rec,
-                                                 const int32_t *__restrict__, int64_t e, int p,
-                                                 int P, float *J, float *lam, float *mu) {
-  const float4 *q = reinterpret_cast<const float4 *>(rec) + e * 3 * P + p;
+// Records (kernels_setup.cuh): FP32 as float4 planes per element
+// ([E][3|4][P]: invJ 0-3, invJ 4-7, (invJ 8, m0, m1, conn)[, (m2, m3, m4, 0)]),
+// FP64 as [E][P][9 + kWords] (invJ, m); m = (lambda', mu') or, for
+// transversely isotropic material, (A', C', F', L', N').
+template <bool TI>
+__device__ __forceinline__ void load_elastic_rec(const float *__restrict__ rec, int64_t e, int p,
+                                                 int P, float *J, float *m) {
+  constexpr int PL = TI ? 4 : 3;
+  const float4 *q = reinterpret_cast<const float4 *>(rec) + e * PL * P + p;
   float4 a = __ldg(q), b = __ldg(q + P), c = __ldg(q + 2 * P);
   J[0] = a.x; J[1] = a.y; J[2] = a.z; J[3] = a.w;
   J[4] = b.x; J[5] = b.y; J[6] = b.z; J[7] = b.w;
-  J[8] = c.x; *lam = c.y; *mu = c.z;
+  J[8] = c.x; m[0] = c.y; m[1] = c.z;
+  if constexpr (TI) {
+    float4 d = __ldg(q + 3 * P);
+    m[2] = d.x; m[3] = d.y; m[4] = d.z;
+  }
 }
-__device__ __forceinline__ void load_elastic_rec(const double *__restrict__ rec,
-                                                 const int32_t *__restrict__, int64_t e, int p,
-                                                 int P, double *J, double *lam, double *mu) {
+template <bool TI>
+__device__ __forceinline__ void load_elastic_rec(const double *__restrict__ rec, int64_t e, int p,
+                                                 int P, double *J, double *m) {
+  constexpr int W = 9 + ElasticMat<TI>::kWords;
   const int64_t ep = e * P + p;
 #pragma unroll
-  for (int a = 0; a < 9; ++a) J[a] = rec[ep * 11 + a];
-  *lam = rec[ep * 11 + 9];
-  *mu = rec[ep * 11 + 10];
+  for (int a = 0; a < 9; ++a) J[a] = rec[ep * W + a];
+#pragma unroll
+  for (int a = 0; a < ElasticMat<TI>::kWords; ++a) m[a] = rec[ep * W + 9 + a];
 }
 
-template <int N, typename real>
+template <int N, typename real, bool TI = false>
 __global__ void __launch_bounds__(ElasticShape<N, real>::THREADS)
 elastic_hex_stiffness_kernel(int64_t E, const real *__restrict__ rec,
                              const int32_t *__restrict__ conn, const real *__restrict__ u,
@@ -228,8 +239,8 @@ elastic_hex_stiffness_kernel(int64_t E, const real *__restrict__ rec,
 #pragma unroll
     for (int k = 0; k < n; ++k) {
       const int p = ij + n2 * k;
-      real J[9], lam, mu;
-      load_elastic_rec(rec, conn, e, p, P, J, &lam, &mu);
+      real J[9], mat[ElasticMat<TI>::kWords];
+      load_elastic_rec<TI>(rec, e, p, P, J, mat);
       real d[3][3];  // d[c][b]: derivative of u_c along reference direction b
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
@@ -252,15 +263,10 @@ elastic_hex_stiffness_kernel(int64_t E, const real *__restrict__ rec,
 #pragma unroll
         for (int a = 0; a < 3; ++a)
           g[c][a] = J[a * 3 + 0] * d[c][0] + J[a * 3 + 1] * d[c][1] + J[a * 3 + 2] * d[c][2];
-      // isotropic Hooke with quadrature weight and detJ folded into lam, mu
-      const real tr = g[0][0] + g[1][1] + g[2][2];
-      const real sxx = lam * tr + 2 * mu * g[0][0];
-      const real syy = lam * tr + 2 * mu * g[1][1];
-      const real szz = lam * tr + 2 * mu * g[2][2];
-      const real sxy = mu * (g[0][1] + g[1][0]);
-      const real sxz = mu * (g[0][2] + g[2][0]);
-      const real syz = mu * (g[1][2] + g[2][1]);
-      const real sig[3][3] = {{sxx, sxy, sxz}, {sxy, syy, syz}, {sxz, syz, szz}};
+      // Hooke with quadrature weight and detJ folded into the constants
+      real sig[3][3];
+      if constexpr (TI) stress_ti<real>(g, mat, sig);
+      else stress_iso<real>(g, mat[0], mat[1], sig);
       // F_c[b] = sum_a invJ[a][b] sigma[c][a]
 #pragma unroll
       for (int c = 0; c < 3; ++c) {

@@ -73,8 +73,9 @@ int64_t estimate_bytes(const salvus_mesh_desc &d, int precision) {
   int64_t G = E;
   for (int k = 0; k < dim; ++k) G *= d.order;
   G = G * 5 / 4 + 4 * E;  // interior count plus a generous boundary allowance
-  const int64_t rw32 = salvus::record_words(d.shape, d.physics, 0);
-  const int64_t rw64 = salvus::record_words(d.shape, d.physics, 1);
+  const bool ti = (d.reserved & SALVUS_MESH_ELASTIC_TI) != 0;
+  const int64_t rw32 = salvus::record_words(d.shape, d.physics, 0, ti);
+  const int64_t rw64 = salvus::record_words(d.shape, d.physics, 1, ti);
   const int64_t rs = precision == SALVUS_FP64 ? 8 : 4;
   int64_t b = 0;
   b += E * P * (4 * rw32 + 4 /*conn*/ + 4 /*incidence*/ + 8 /*setup mass, transient*/);
@@ -83,7 +84,7 @@ int64_t estimate_bytes(const salvus_mesh_desc &d, int precision) {
   b += 4 * G * c * rs;             // u v a a_
   b += E * P * c * rs;             // element-local residual
   b += G * c * 8;                  // host-copy staging
-  b += E * 8 * dim * 8 + E * 8 * 3 * 8;  // vertices and vertex material
+  b += E * 8 * dim * 8 + E * 8 * 6 * 8;  // vertices and vertex material
   return b + (8 << 20);            // per-job slack (graphs, rings)
 }
 
@@ -320,7 +321,7 @@ int salvus_server_submit(salvus_server *s, const salvus_job_desc *d, int64_t *jo
   std::unique_ptr<Job> j(new Job());
   j->mesh = m;
   const int dim = m.shape == SALVUS_QUAD ? 2 : 3, nv = m.shape == SALVUS_QUAD ? 4 : 8;
-  const int npar = salvus::physics_params(m.physics);
+  const int npar = salvus::physics_params(m.physics, m.reserved);
   j->vertices.assign(m.vertices, m.vertices + m.n_vertices * dim);
   j->cells.assign(m.cells, m.cells + m.n_elements * nv);
   j->params.assign(m.params, m.params + (size_t)npar * m.n_elements * nv);

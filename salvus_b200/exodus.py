@@ -67,9 +67,20 @@ class ExodusFile:
         _check(lib().salvus_exodus_params(self.h, physics, _dp(out)))
         return out
 
+    def elastic3d_params(self):
+        """The reference's six Elastic3D parameters [6][n_elements][nv]
+        RHO VPV VPH VSV VSH ETA (transversely isotropic models)."""
+        out = np.zeros((6, self.n_elements, self.nv))
+        _check(lib().salvus_exodus_elastic3d_params(self.h, _dp(out)))
+        return out
+
     def mesh(self, physics, order, device=0):
+        """The file's mesh and model; elastic 3-D reads the six reference
+        parameters, so transversely isotropic models run as such (isotropic
+        ones keep the isotropic kernels)."""
         v, c = self.mesh_arrays()
-        return core.Mesh(self.shape, order, physics, v, c, self.params(physics), device=device)
+        par = self.elastic3d_params() if physics == core.ELASTIC3D else self.params(physics)
+        return core.Mesh(self.shape, order, physics, v, c, par, device=device)
 
     def side_set_nodes(self, mesh, name):
         n = ctypes.c_int64()

@@ -82,15 +82,36 @@ def test_hex_mesh_vertex_order_and_isotropic_elastic(tmp_path):
     assert np.all(m.node_coords()[z1, 2] == 200.0) and len(z1) == 7 * 5
 
 
-def test_anisotropic_elastic_rejected(tmp_path):
+def test_anisotropic_elastic_model(tmp_path):
+    """An anisotropic Elastic3D model: the isotropic reader refuses it, the
+    six-parameter reader returns RHO VPV VPH VSV VSH ETA (ETA defaulting to
+    1 when absent), and mesh() builds a transversely isotropic mesh."""
     V, C = meshgen.structured_hex(1, 1, 1, 1.0, 1.0, 1.0)
     ones = np.ones((1, 8))
     ev = {**vars_of("RHO", ones), **vars_of("VPV", ones), **vars_of("VPH", 2 * ones),
-          **vars_of("VSV", ones), **vars_of("VSH", ones)}
+          **vars_of("VSV", ones), **vars_of("VSH", 1.5 * ones)}
     path = str(tmp_path / "aniso.e")
     xf.write(path, V, [xf.to_exodus(C, "HEX8")], "HEX8", ev)
+    f = ExodusFile(path)
     with pytest.raises(core.SalvusError, match="anisotropic"):
-        ExodusFile(path).params(core.ELASTIC3D)
+        f.params(core.ELASTIC3D)
+    p6 = f.elastic3d_params()
+    want = np.stack([ones, ones, 2 * ones, ones, 1.5 * ones, ones])
+    assert np.array_equal(p6, want)
+    m = f.mesh(core.ELASTIC3D, 2, device=-1)
+    assert m.n_nodes == 27
+
+
+def test_isotropic_file_six_parameters(tmp_path):
+    """VP / VS only: the six-parameter form repeats them as VPV = VPH and
+    VSV = VSH with ETA = 1."""
+    V, C = meshgen.structured_hex(1, 1, 1, 1.0, 1.0, 1.0)
+    ones = np.ones((1, 8))
+    ev = {**vars_of("RHO", 3 * ones), **vars_of("VP", 2 * ones), **vars_of("VS", ones)}
+    path = str(tmp_path / "iso.e")
+    xf.write(path, V, [xf.to_exodus(C, "HEX8")], "HEX8", ev)
+    p6 = ExodusFile(path).elastic3d_params()
+    assert np.array_equal(p6, np.stack([3 * ones, 2 * ones, 2 * ones, ones, ones, ones]))
 
 
 @pytest.mark.parametrize("kind", ["tri", "tet"])
