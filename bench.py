@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-simplex", action="store_true", help="skip the P3 simplex leg")
     ap.add_argument("--no-elastic2d", action="store_true", help="skip the 2-D elastic quad leg")
+    ap.add_argument("--no-general", action="store_true",
+                    help="skip timing the per-point-geometry stiffness kernel")
     ap.add_argument("--profile-leg", default=None,
                     choices=["quad", "elastic2d", "coupled", "tri", "tet", "shots", "group"],
                     help="set up one workload and run --steps plain steps (for ncu captures)")
@@ -622,13 +624,27 @@ def main():
     p.profile(False)
 
     E, P = mesh.n_elements, mesh.points_per_element
-    # algorithmic bytes per stiffness launch: per point 48 B record (invJ 9,
-    # lambda wdetJ, mu wdetJ, conn) + compulsory u read 12 B/node + the
-    # element-local residual write 12 B/point
-    b_stiff = E * P * 48 + G * 12 + E * P * 12
-    # gather/update: residual read 12 B/point + incidence index 4 B/point +
-    # offsets 4 B/node + (u, v, a_) read and write 72 B/node + inverse mass 4 B/node
-    b_upd = E * P * 16 + G * (4 + 72 + 4)
+    affine, n_gather = mesh.layout()
+    n_int = G - n_gather  # element-interior nodes advanced in the stiffness kernel
+    if affine:
+        # parallelepiped layout, fused step: per point conn 4 B + lambda' mu'
+        # 8 B; per element invJ 36 B; u read 12 B/node; residual write
+        # 12 B/point for the points on element faces; interior nodes: inverse
+        # mass 4 B + (v, a_) read 24 B + (u, v, a_) write 36 B
+        b_stiff = E * P * 12 + E * 36 + G * 12 + (E * P - n_int) * 12 + n_int * 64
+        # shared-node gather: node list + offsets 8 B/node, residual 12 B +
+        # incidence index 4 B per face point, inverse mass 4 B + (u, v, a_)
+        # read and write 72 B per node
+        b_upd = n_gather * 8 + (E * P - n_int) * 16 + n_gather * 76
+        layout = "per-element inverse Jacobian, interior nodes advanced in the stiffness kernel"
+    else:
+        # per-point records: 48 B (invJ 9, lambda', mu', conn) + u read
+        # 12 B/node + the element-local residual write 12 B/point
+        b_stiff = E * P * 48 + G * 12 + E * P * 12
+        # gather/update: residual read 12 B/point + incidence index 4 B/point +
+        # offsets 4 B/node + (u, v, a_) read and write 72 B/node + inverse mass 4 B/node
+        b_upd = E * P * 16 + G * (4 + 72 + 4)
+        layout = "per-point inverse Jacobians"
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     k_ms, k_n = prof.get("stiffness", (0.0, 1))
@@ -639,9 +655,36 @@ def main():
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic_elastic_hex_stiffness.txt")
     if os.path.exists(tf):
+        key = "dram_bytes_per_launch_fullsize_affine=" if affine else "dram_bytes_per_launch_fullsize="
         for line in open(tf):
-            if line.startswith("dram_bytes_per_launch_fullsize="):
+            if line.startswith(key):
                 traffic = float(line.split("=")[1])
+
+    # the per-point-geometry kernel on the same workload (the layout whose
+    # canonical bytes are B_K = 4 P E (1 + 10 + 2) + 8 c G): its own launch
+    # time and fraction of HBM
+    general = None
+    if affine and not args.no_general:
+        mesh_g = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"],
+                           cfg["cells"], cfg["params"], device=local,
+                           flags=core.MESH_PER_POINT_GEOMETRY)
+        pg = core.Problem(mesh_g, core.FP32, dt=dt)
+        pg.run(3, core.RUN_PLAIN)
+        pg.profile(True)
+        pg.run(min(args.steps, 50), core.RUN_PLAIN)
+        prof_g = pg.profile_read()
+        pg.profile(False)
+        gk_ms, gk_n = prof_g.get("stiffness", (0.0, 1))
+        g_ms = gk_ms / max(gk_n, 1)
+        b_g = E * P * 48 + G * 12 + E * P * 12
+        b_canon = 4 * P * E * (1 + 10 + 2) + 8 * 3 * G
+        general = {"kernel": "elastic_hex_stiffness (per-point records)", "ms": g_ms,
+                   "achieved": b_g / (g_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                   "frac": b_g / (g_ms / 1e3) / 1e9 / peak, "algorithmic_bytes": b_g,
+                   "canonical_bytes": b_canon,
+                   "frac_canonical": b_canon / (g_ms / 1e3) / 1e9 / peak}
+        pg.close()
+        mesh_g.close()
 
     # end-to-end through the public API with host buffers: initial state from
     # host (u0, v0 FP64), K steps, seismograms back to the host
@@ -700,13 +743,20 @@ def main():
             "plain": {"value": plain, "unit": METRIC, "steps": kp, "ms_per_step": ms_plain / kp,
                       "form": "host-launched fused step"},
             "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
-            "roofline": {"bound": "hbm", "kernel": "elastic_hex_stiffness", "achieved": ach,
-                         "peak": peak, "unit": "GB/s", "frac": ach / peak, "traffic": traffic,
-                         "algorithmic_bytes": b_stiff,
+            "roofline": {"bound": "hbm", "kernel": "elastic_hex_stiffness", "layout": layout,
+                         "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "traffic": traffic, "algorithmic_bytes": b_stiff,
+                         "kernel_ms": st_ms,
                          "peak_source": "measured" if peaks else "fallback"},
             "roofline_update": {"kernel": "gather_update", "achieved": b_upd / (up_ms / 1e3) / 1e9,
-                                "peak": peak, "unit": "GB/s",
+                                "peak": peak, "unit": "GB/s", "algorithmic_bytes": b_upd,
+                                "kernel_ms": up_ms,
                                 "frac": b_upd / (up_ms / 1e3) / 1e9 / peak},
+            "roofline_step": {"bytes_per_step": b_stiff + b_upd, "ms_per_step": ms / args.steps,
+                              "achieved": (b_stiff + b_upd) / (ms / args.steps / 1e3) / 1e9,
+                              "peak": peak, "unit": "GB/s",
+                              "frac": (b_stiff + b_upd) / (ms / args.steps / 1e3) / 1e9 / peak},
+            "roofline_per_point_geometry": general,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "form": "C-ABI job: FP64 host u0/v0 upload, K graph-replayed steps, "

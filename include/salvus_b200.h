@@ -91,12 +91,20 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
  * constants per point.  Tetrahedra with such material run on CUDA cores;
  * problem groups take isotropic meshes only. */
 #define SALVUS_MESH_ELASTIC_TI 2
+/* salvus_mesh_desc.flags: keep per-point inverse Jacobians for elastic
+ * hexahedra even when every element is a parallelepiped.  By default such
+ * meshes store one inverse Jacobian per element and FP32 records of the
+ * material alone (12 instead of 48 bytes per point with the connectivity),
+ * and the fused FP32 step advances each element's interior nodes inside the
+ * stiffness kernel. */
+#define SALVUS_MESH_PER_POINT_GEOMETRY 4
 
 typedef struct {
   int32_t shape;   /* enum salvus_shape */
   int32_t order;   /* polynomial order: quad 1..10, hex 1..6, tri / tet 3 */
   int32_t physics; /* enum salvus_physics */
-  int32_t reserved; /* flags: SALVUS_MESH_FP32_ONLY */
+  int32_t reserved; /* flags: SALVUS_MESH_FP32_ONLY | SALVUS_MESH_ELASTIC_TI |
+                       SALVUS_MESH_PER_POINT_GEOMETRY */
   int64_t n_vertices;
   const double *vertices; /* [n_vertices][dim] */
   int64_t n_elements;
@@ -155,6 +163,14 @@ int salvus_mesh_destroy(salvus_mesh *mesh);
 /* Unique global GLL nodes G and components c. */
 int salvus_mesh_info(const salvus_mesh *mesh, int64_t *n_nodes, int32_t *n_components,
                      int32_t *points_per_element);
+/* Storage chosen for the mesh (no reference counterpart): *per_element_jacobian
+ * = 1 when every element is a parallelepiped and one inverse Jacobian per
+ * element is kept (elastic hexahedra, SALVUS_MESH_PER_POINT_GEOMETRY unset);
+ * *gathered_nodes = the nodes the fused FP32 step assembles by node gather
+ * (all G unless the interior nodes are advanced in the stiffness kernel).
+ * Either pointer may be NULL. */
+int salvus_mesh_layout(const salvus_mesh *mesh, int32_t *per_element_jacobian,
+                       int64_t *gathered_nodes);
 /* Node coordinates [G][dim] (QuadP1::buildNodalPoints QuadP1.cpp:176-216,
  * HexP1::buildNodalPoints HexP1.cpp:312-354). */
 int salvus_mesh_node_coords(const salvus_mesh *mesh, double *xyz);
@@ -238,6 +254,17 @@ int64_t salvus_problem_step_index(const salvus_problem *p);
 int salvus_problem_autotune(salvus_problem *p, int32_t *stiff_shot_lanes,
                             int32_t *stiff_elements, int32_t *gather_shot_lanes,
                             int32_t *gather_nodes);
+/* Device status of the problem (synchronises its stream): SALVUS_OK,
+ * SALVUS_E_NONFINITE when the displacement field held a NaN / Inf at one of
+ * the finite checks (after every 32 steps of salvus_run / salvus_step /
+ * salvus_take_time_step: an unstable time step or a non-finite input field),
+ * or SALVUS_E_TIMEOUT when a bounded device wait gave up.  The same status is
+ * returned by salvus_synchronize, salvus_problem_get_field and
+ * salvus_get_seismograms.  clear != 0 resets the status word afterwards (the
+ * fields are left as they are: set them again before continuing).  The
+ * reference reports such failures as exceptions caught in main
+ * (Main.cpp:70-74). */
+int salvus_problem_status(salvus_problem *p, int32_t clear);
 /* The problem's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events after this problem's kernels. */
 int salvus_problem_stream(const salvus_problem *p, void **stream);

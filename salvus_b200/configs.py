@@ -231,13 +231,18 @@ def simplex_tri(nx=448, ny=224, lx=2.0e4, ly=1.0e4, vp=4000.0, std=0.05, corr=10
                 receivers=meshgen.ring_positions(center, 0.3 * ly, n_receivers, seed))
 
 
-def simplex_tet(n=55, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
-                corr=1000.0, f0=1.0, n_receivers=64, seed=3, anisotropy=None):
-    """3-D P3 tetrahedra: jittered n^3 lattice over an L cube, 6 tetrahedra
-    per cell (6 n^3 elements; n = 55 gives about 1M), material homogeneous
-    times (1 + std GRF); elastic: seeded moment-tensor Ricker source, acoustic:
-    pressure source; receivers at seeded positions on the top surface."""
-    V, C = meshgen.kuhn_tet(n, n, n, L, L, L, seed=seed)
+def simplex_tet(n=53, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
+                corr=1000.0, f0=1.0, n_receivers=64, seed=3, anisotropy=None, mesh="delaunay"):
+    """3-D P3 tetrahedra over an L cube: a seeded Delaunay tetrahedralisation
+    of a jittered (n+1)^3 point lattice (about 6.7 n^3 elements; n = 53 gives
+    ~157k points and ~1M tetrahedra), or with mesh="kuhn" the lattice cells
+    split into 6 tetrahedra each; material homogeneous times (1 + std GRF);
+    elastic: seeded moment-tensor Ricker source, acoustic: pressure source;
+    receivers at seeded positions on the top surface."""
+    if mesh == "kuhn":
+        V, C = meshgen.kuhn_tet(n, n, n, L, L, L, seed=seed)
+    else:
+        V, C = meshgen.delaunay_tet(n, n, n, L, L, L, seed=seed)
     h = L / n
     grf = meshgen.gaussian_random_field((n + 1,) * 3, h, corr, seed).ravel()
     pert = 1.0 + std * grf

@@ -22,8 +22,10 @@ LIB_PATH = os.path.join(HERE, "libsalvus_b200.so")
 QUAD, HEX, TRI, TET = 0, 1, 2, 3
 ACOUSTIC, ELASTIC3D, ELASTIC2D, COUPLED2D = 0, 1, 2, 3
 FP32, FP64 = 0, 1
+E_INVALID, E_OOM, E_CUDA, E_TIMEOUT, E_NONFINITE, E_STATE, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
 MESH_FP32_ONLY = 1  # salvus_mesh_desc.flags: build only the FP32 stiffness records
 MESH_ELASTIC_TI = 2  # salvus_mesh_desc.flags: elastic3d params RHO VPV VPH VSV VSH ETA
+MESH_PER_POINT_GEOMETRY = 4  # salvus_mesh_desc.flags: per-point Jacobians for parallelepipeds too
 FIELD_U, FIELD_V, FIELD_A, FIELD_A_PREV = 0, 1, 2, 3
 FORCE, MOMENT_TENSOR = 0, 1
 RUN_PLAIN, RUN_GRAPH = 0, 1
@@ -63,6 +65,8 @@ SIGNATURES = [
     ("salvus_mesh_destroy", ctypes.c_int, [_VP]),
     ("salvus_mesh_info", ctypes.c_int, [_VP, ctypes.POINTER(_I64), ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
     ("salvus_mesh_node_coords", ctypes.c_int, [_VP, _DP]),
+    ("salvus_problem_status", ctypes.c_int, [_VP, _I32]),
+    ("salvus_mesh_layout", ctypes.c_int, [_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I64)]),
     ("salvus_mesh_connectivity", ctypes.c_int, [_VP, ctypes.POINTER(_I64)]),
     ("salvus_mesh_locate_point", ctypes.c_int, [_VP, _DP, ctypes.POINTER(_I64), _DP]),
     ("salvus_mesh_inverse_mass", ctypes.c_int, [_VP, _DP]),
@@ -184,6 +188,14 @@ class Mesh:
             self.close()
         except Exception:
             pass
+
+    def layout(self):
+        """(per_element_jacobian, gathered_nodes): whether one inverse
+        Jacobian per element is stored, and how many nodes the fused FP32
+        step assembles by node gather."""
+        a, g = _I32(), _I64()
+        _check(lib().salvus_mesh_layout(self.h, ctypes.byref(a), ctypes.byref(g)))
+        return bool(a.value), g.value
 
     def node_coords(self):
         x = np.zeros((self.n_nodes, self.dim))
@@ -319,6 +331,14 @@ class Problem:
 
     def run(self, n_steps, mode=RUN_GRAPH):
         _check(lib().salvus_run(self.h, int(n_steps), mode))
+
+    def status(self, clear=False):
+        """Raise SalvusError for a non-finite wavefield (SALVUS_E_NONFINITE) or
+        a bounded device wait that gave up; clear=True resets the status
+        word after reading it."""
+        rc = lib().salvus_problem_status(self.h, 1 if clear else 0)
+        if rc:
+            raise SalvusError(rc, lib().salvus_last_error().decode())
 
     def synchronize(self):
         _check(lib().salvus_synchronize(self.h))

@@ -18,6 +18,7 @@
 #include "kernels_stiffness.cuh"
 #include "kernels_step.cuh"
 #include "kernels_hex_v2.cuh"
+#include "kernels_hex_affine.cuh"
 #include "kernels_batch.cuh"
 #include "kernels_simplex.cuh"
 #include "kernels_simplex_tc.cuh"
@@ -146,10 +147,35 @@ static int launch_elastic_classic(const salvus_mesh *m, const real *rec, const r
   return check_launch("elastic stiffness");
 }
 
+// Parallelepiped meshes (m->affine): per-element inverse Jacobian, material
+// planes; kFuse also advances the interior nodes (kernels_hex_affine.cuh).
+template <int N, bool TI, bool kFuse>
+static int launch_elastic_affine(const salvus_mesh *m, const float *mat, float *u, float *r,
+                                 cudaStream_t st, const HexInteriorUpdate &iu) {
+  constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
+  using T = HexAffineShape<N, EPB, TI>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(elastic_hex_affine_kernel<N, EPB, TI, kFuse>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    attr = true;
+  }
+  elastic_hex_affine_kernel<N, EPB, TI, kFuse><<<blocks_for(m->E, EPB), T::THREADS, T::SMEM, st>>>(
+      m->E, m->d_jac32.as<float>(), mat, m->d_conn.as<int32_t>(), u, r, dmatrix<float>(m->basis),
+      iu);
+  g_launches++;
+  return check_launch(kFuse ? "elastic stiffness (fused interior)" : "elastic stiffness");
+}
+
 template <int N, typename real>
 static int launch_elastic(const salvus_mesh *m, const real *rec, const real *u, real *r,
                           cudaStream_t st) {
   if constexpr (std::is_same<real, float>::value) {
+    if (m->affine) {
+      HexInteriorUpdate none{};
+      return m->ti ? launch_elastic_affine<N, true, false>(m, rec, const_cast<float *>(u), r, st, none)
+                   : launch_elastic_affine<N, false, false>(m, rec, const_cast<float *>(u), r, st, none);
+    }
     if (!hex_classic())
       return m->ti ? launch_elastic_v2<N, true>(m, rec, u, r, st)
                    : launch_elastic_v2<N, false>(m, rec, u, r, st);
@@ -552,7 +578,44 @@ static int mesh_setup_device(salvus_mesh *m) {
   }
   DeviceBuffer mass_local;
   if ((rc = mass_local.alloc(sizeof(double) * EP))) return rc;
-  if ((rc = build_records<float, true>(m, m->d_rec32, mass_local))) return rc;
+  if (m->affine) {
+    // parallelepiped elastic hexahedra: material planes + per-element invJ
+    const int nm = m->ti ? 5 : 2;
+    if ((rc = m->d_rec32.alloc(sizeof(float) * (size_t)nm * EP)) ||
+        (rc = m->d_jac32.alloc(sizeof(float) * 9 * (size_t)m->E)))
+      return rc;
+    GllTable gll{};
+    for (int i = 0; i < m->n; ++i) {
+      gll.xi[i] = m->basis.xi[i];
+      gll.w[i] = m->basis.w[i];
+    }
+    affine_hex_records_kernel<<<blocks_for(EP, 128), 128, 0, m->stream>>>(
+        m->E, m->n, m->P, m->ti, m->d_vtx.as<double>(), m->d_par.as<double>(), gll,
+        m->d_rec32.as<float>(), m->d_jac32.as<float>(), mass_local.as<double>());
+    g_launches++;
+    if ((rc = check_launch("affine records"))) return rc;
+    // nodes the fused step gathers: all but the element-interior ones
+    if (m->order >= 2) {
+      std::vector<char> interior(m->G, 0);
+      const int n = m->n;
+      for (int64_t e = 0; e < m->E; ++e)
+        for (int k = 1; k < n - 1; ++k)
+          for (int j = 1; j < n - 1; ++j)
+            for (int i = 1; i < n - 1; ++i)
+              interior[m->conn[e * m->P + i + n * j + n * n * k]] = 1;
+      std::vector<int32_t> gn;
+      gn.reserve(m->G);
+      for (int64_t g = 0; g < m->G; ++g)
+        if (!interior[g]) gn.push_back((int32_t)g);
+      m->n_gnodes = (int64_t)gn.size();
+      if ((rc = m->d_gnodes.alloc(sizeof(int32_t) * (gn.empty() ? 1 : gn.size())))) return rc;
+      SALVUS_CUDA(cudaMemcpyAsync(m->d_gnodes.ptr, gn.data(), sizeof(int32_t) * gn.size(),
+                                  cudaMemcpyHostToDevice, m->stream));
+      SALVUS_CUDA(cudaStreamSynchronize(m->stream));
+    }
+  } else if ((rc = build_records<float, true>(m, m->d_rec32, mass_local))) {
+    return rc;
+  }
   if (!m->fp32_only && (rc = build_records<double, false>(m, m->d_rec64, mass_local))) return rc;
   mass_gather_kernel<<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
       m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), mass_local.as<double>(),
@@ -702,10 +765,77 @@ static const real *inv_mass(const salvus_problem *p) {
   return sizeof(real) == 4 ? (const real *)p->mesh->d_mi32.ptr : (const real *)p->mesh->d_mi64.ptr;
 }
 
+// The fused FP32 step of parallelepiped elastic hexahedra advances the
+// element-interior nodes inside the stiffness kernel and gathers the rest
+// (kernels_hex_affine.cuh).  Used when the problem has no Dirichlet points
+// and at most kFuseMaxSources sources (each interior thread scans them);
+// SALVUS_HEX_STEP=unfused selects the plain sequence (read at every step).
+constexpr int kFuseMaxSources = 16;
+static bool hex_interior_fusion(const salvus_problem *p) {
+  const salvus_mesh *m = p->mesh;
+  if (!(m->affine && m->n_gnodes > 0 && p->prec == SALVUS_FP32 && p->shots == 1 &&
+        p->n_dir_pts == 0 && (int)p->srcs.size() <= kFuseMaxSources))
+    return false;
+  const char *s = std::getenv("SALVUS_HEX_STEP");
+  return !(s && std::strcmp(s, "unfused") == 0);
+}
+
+template <bool TI>
+static int launch_fused_interior(salvus_problem *p, const HexInteriorUpdate &iu) {
+  const salvus_mesh *m = p->mesh;
+  const float *mat = m->d_rec32.as<float>();
+  float *u = F<float>(p->d_u), *r = F<float>(p->d_r);
+  switch (m->order) {
+    case 2: return launch_elastic_affine<2, TI, true>(m, mat, u, r, p->stream, iu);
+    case 3: return launch_elastic_affine<3, TI, true>(m, mat, u, r, p->stream, iu);
+    case 4: return launch_elastic_affine<4, TI, true>(m, mat, u, r, p->stream, iu);
+    case 5: return launch_elastic_affine<5, TI, true>(m, mat, u, r, p->stream, iu);
+    case 6: return launch_elastic_affine<6, TI, true>(m, mat, u, r, p->stream, iu);
+  }
+  return fail(SALVUS_E_UNSUPPORTED, "fused hexahedron step: order %d", m->order);
+}
+
+static int step_fused_hex_interior(salvus_problem *p) {
+  const salvus_mesh *m = p->mesh;
+  int rc;
+  {
+    ProfScope ps(p, K_STIFF);
+    HexInteriorUpdate iu{};
+    iu.mi = m->d_mi32.as<float>();
+    iu.v = F<float>(p->d_v);
+    iu.ap = F<float>(p->d_ap);
+    iu.dt = (float)p->dt;
+    iu.dtd = p->dt;
+    iu.nsrc = (int)p->srcs.size();
+    iu.src_elem = p->d_src_elem.as<int64_t>();
+    iu.src_par = p->d_src_par.as<double>();
+    iu.src_wts = p->d_src_wts.as<double>();
+    iu.step = p->d_step.as<int64_t>();
+    if ((rc = m->ti ? launch_fused_interior<true>(p, iu) : launch_fused_interior<false>(p, iu)))
+      return rc;
+  }
+  // the source kernel still adds into every point of its element; the
+  // interior ones were consumed above and are not gathered
+  if ((rc = launch_sources<float, 3>(p))) return rc;
+  {
+    ProfScope ps(p, K_UPDATE);
+    gather_list_kernel<float, 3, 0><<<blocks_for(m->n_gnodes, 256), 256, 0, p->stream>>>(
+        m->n_gnodes, m->d_gnodes.as<int32_t>(), m->d_inc_off.as<int32_t>(),
+        m->d_inc_idx.as<int32_t>(), F<float>(p->d_r), m->d_mi32.as<float>(), F<float>(p->d_u),
+        F<float>(p->d_v), F<float>(p->d_ap), F<float>(p->d_a), (float)p->dt);
+    g_launches++;
+    if ((rc = check_launch("gather update (shared nodes)"))) return rc;
+  }
+  return launch_receivers<float, 3>(p);
+}
+
 template <typename real, int C>
 static int step_fused_t(salvus_problem *p) {
   const salvus_mesh *m = p->mesh;
   int rc;
+  if constexpr (std::is_same<real, float>::value && C == 3) {
+    if (hex_interior_fusion(p)) return step_fused_hex_interior(p);
+  }
   {
     ProfScope ps(p, K_STIFF);
     if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
@@ -1018,13 +1148,34 @@ int apply_stiffness_into(const salvus_mesh *m, int precision, const void *u, voi
                                         (double *)a, (double *)scratch, err, st);
 }
 
-// Reads the device error word (set by kernels whose bounded waits ran out).
+// Reads the device status word: set by kernels whose bounded waits ran out
+// (the wait's code) or by the finite check (kNonFiniteCode).
 static int device_status(salvus_problem *p) {
   int h = 0;
   SALVUS_CUDA(cudaMemcpyAsync(&h, p->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
   SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  if (h == kNonFiniteCode)
+    return fail(SALVUS_E_NONFINITE,
+                "the wavefield became non-finite (NaN / Inf) by step %lld: the time step is "
+                "unstable or an input field is not finite",
+                (long long)p->step);
   if (h) return fail(SALVUS_E_TIMEOUT, "a bounded device wait gave up (code %d); results invalid", h);
   return SALVUS_OK;
+}
+
+// Finite check of u (all shots) into the status word; part of every 32-step
+// chunk (kFiniteEvery) of salvus_run and of the single-step entry points.
+constexpr int kFiniteEvery = 32;
+static int launch_finite_check(salvus_problem *p) {
+  const int64_t n = p->mesh->G * p->c * p->shots_pad;
+  const int64_t want = (n + 255) / 256, cap = (int64_t)p->mesh->sm_count * 8;
+  const unsigned grid = (unsigned)std::max<int64_t>(1, std::min(want, cap));
+  if (p->prec == SALVUS_FP32)
+    finite_check_kernel<float><<<grid, 256, 0, p->stream>>>(n, F<float>(p->d_u), p->d_err.as<int>());
+  else
+    finite_check_kernel<double><<<grid, 256, 0, p->stream>>>(n, F<double>(p->d_u), p->d_err.as<int>());
+  g_launches++;
+  return check_launch("finite check");
 }
 
 static int ready(salvus_problem *p) {
@@ -1135,6 +1286,19 @@ static int group_upload(salvus::DeviceBuffer &b, const void *src, size_t bytes, 
 
 static int group_partitioned(salvus_group *g, bool launch);
 
+// Problem groups run the per-point-geometry hexahedron body; parallelepiped
+// meshes build those records on first use.
+static int ensure_per_point_records(salvus_mesh *m) {
+  if (m->d_rec32g.ptr) return SALVUS_OK;
+  SALVUS_CUDA(cudaSetDevice(m->device));
+  DeviceBuffer mass_local;
+  int rc = mass_local.alloc(sizeof(double) * (size_t)(m->E * m->P));
+  if (rc) return rc;
+  if ((rc = build_records<float, true>(m, m->d_rec32g, mass_local))) return rc;
+  SALVUS_CUDA(cudaStreamSynchronize(m->stream));
+  return SALVUS_OK;
+}
+
 static int group_fill(salvus_group *g) {
   int64_t bs = 0, bg = 0, br = 0;
   g->slots.resize(g->members.size());
@@ -1144,7 +1308,8 @@ static int group_fill(salvus_group *g) {
     int rc = ready(p);
     if (rc) return rc;
     GroupSlot &s = g->slots[k];
-    s.rec = m->d_rec32.as<float>();
+    if (m->affine && (rc = ensure_per_point_records(const_cast<salvus_mesh *>(m)))) return rc;
+    s.rec = (m->affine ? m->d_rec32g : m->d_rec32).as<float>();
     s.conn = m->d_conn.as<int32_t>();
     s.inc_off = m->d_inc_off.as<int32_t>();
     s.inc_idx = m->d_inc_idx.as<int32_t>();
@@ -1538,6 +1703,27 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
       m->tet_kernel = 1;  // tetrahedra: the CUDA-core kernel has the five-constant stress
     }
   }
+  if (m->shape == SALVUS_HEX && m->physics == SALVUS_ELASTIC3D &&
+      !(d->reserved & SALVUS_MESH_PER_POINT_GEOMETRY)) {
+    // every element a parallelepiped: the inverse Jacobian at the eight
+    // corners equals the one at the centre (to 1e-12 relative)
+    bool affine = true;
+    for (int64_t e = 0; e < m->E && affine; ++e) {
+      const double *v = m->vtx.data() + e * 24;
+      double c0[3] = {0, 0, 0}, det0, J0[9];
+      p1_jacobian(m->shape, v, c0, &det0, J0);
+      double scale = 0;
+      for (int a = 0; a < 9; ++a) scale = std::max(scale, std::fabs(J0[a]));
+      for (int q = 0; q < 8 && affine; ++q) {
+        double ref[3], det, J[9];
+        for (int a = 0; a < 3; ++a) ref[a] = ((q >> a) & 1) ? 1.0 : -1.0;
+        p1_jacobian(m->shape, v, ref, &det, J);
+        for (int a = 0; a < 9; ++a)
+          if (std::fabs(J[a] - J0[a]) > 1e-12 * scale) affine = false;
+      }
+    }
+    m->affine = affine;
+  }
   if ((rc = flatten_mesh(m.get(), d->cells, d->n_vertices))) return rc;
   if (m->physics == SALVUS_COUPLED2D && (rc = setup_coupled(m.get(), d->cells))) return rc;
   if (device >= 0) {
@@ -1568,6 +1754,14 @@ int salvus_mesh_info(const salvus_mesh *m, int64_t *G, int32_t *c, int32_t *P) {
   if (G) *G = m->G;
   if (c) *c = m->c;
   if (P) *P = m->P;
+  return SALVUS_OK;
+}
+
+int salvus_mesh_layout(const salvus_mesh *m, int32_t *per_element_jacobian,
+                       int64_t *gathered_nodes) {
+  if (!m) return fail(SALVUS_E_INVALID, "null mesh");
+  if (per_element_jacobian) *per_element_jacobian = m->affine ? 1 : 0;
+  if (gathered_nodes) *gathered_nodes = m->n_gnodes > 0 ? m->n_gnodes : m->G;
   return SALVUS_OK;
 }
 
@@ -2016,6 +2210,7 @@ int salvus_take_time_step(salvus_problem *p) {
     return p->prec == SALVUS_FP32 ? newmark_t<float, C>(p) : newmark_t<double, C>(p);
   });
   if (rc == SALVUS_OK) p->step++;
+  if (rc == SALVUS_OK && p->step % kFiniteEvery == 0) rc = launch_finite_check(p);
   return rc;
 }
 
@@ -2025,6 +2220,18 @@ int salvus_step(salvus_problem *p) {
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
   rc = step_fused(p);
   if (rc == SALVUS_OK) p->step++;
+  if (rc == SALVUS_OK && p->step % kFiniteEvery == 0) rc = launch_finite_check(p);
+  return rc;
+}
+
+int salvus_problem_status(salvus_problem *p, int32_t clear) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  const int rc = device_status(p);
+  if (clear) {
+    SALVUS_CUDA(cudaMemsetAsync(p->d_err.ptr, 0, sizeof(int), p->stream));
+    SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  }
   return rc;
 }
 
@@ -2037,6 +2244,7 @@ int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
     for (int64_t s = 0; s < n_steps; ++s) {
       if ((rc = step_fused(p))) return rc;
       p->step++;
+      if (p->step % kFiniteEvery == 0 && (rc = launch_finite_check(p))) return rc;
     }
     return SALVUS_OK;
   }
@@ -2050,6 +2258,7 @@ int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
     int crc = SALVUS_OK;
     const int64_t l0 = g_launches.load();
     for (int s = 0; s < chunk && crc == SALVUS_OK; ++s) crc = step_fused(p);
+    if (crc == SALVUS_OK) crc = launch_finite_check(p);
     cudaError_t ce = cudaStreamEndCapture(p->stream, &graph);
     // captured launches run only when the graph is replayed: count them there
     p->graph_launches = g_launches.load() - l0;
@@ -2073,6 +2282,7 @@ int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
   for (; done < n_steps; ++done) {
     if ((rc = step_fused(p))) return rc;
     p->step++;
+    if (p->step % kFiniteEvery == 0 && (rc = launch_finite_check(p))) return rc;
   }
   return SALVUS_OK;
 }
@@ -2324,9 +2534,13 @@ int salvus_group_run(salvus_group *g, int64_t n_steps) {
   for (; done < n_steps; ++done)
     if ((rc = group_step(g))) return rc;
   for (auto *p : g->members) p->step += n_steps;
-  // members' later work waits for the group
+  // members' later work waits for the group; then each member's finite check
+  // on its own stream
   SALVUS_CUDA(cudaEventRecord(g->ev, g->stream));
-  for (auto *p : g->members) SALVUS_CUDA(cudaStreamWaitEvent(p->stream, g->ev, 0));
+  for (auto *p : g->members) {
+    SALVUS_CUDA(cudaStreamWaitEvent(p->stream, g->ev, 0));
+    if (n_steps > 0 && (rc = launch_finite_check(p))) return rc;
+  }
   return SALVUS_OK;
 }
 

@@ -119,6 +119,13 @@ struct salvus_mesh {
   salvus::DeviceBuffer d_conn, d_inc_off, d_inc_idx, d_vtx, d_par;
   salvus::DeviceBuffer d_mi64, d_mi32;
   salvus::DeviceBuffer d_rec32, d_rec64;  // stiffness records per precision
+  // elastic hexahedra that are all parallelepipeds: d_rec32 holds material
+  // planes [NM][E*P], d_jac32 the per-element invJ [E][9]; d_rec32g the
+  // per-point layout, built when a problem group needs it; d_gnodes lists
+  // the nodes that are not interior to an element (fused step gather)
+  bool affine = false;
+  salvus::DeviceBuffer d_jac32, d_rec32g, d_gnodes;
+  int64_t n_gnodes = 0;
   salvus::DeviceBuffer d_sd32, d_sd64;    // simplex derivative tables [dim][P][P]
   salvus::DeviceBuffer d_tc_tab;          // tetrahedra: tensor-core operand image (hi | lo)
   salvus::DeviceBuffer d_elist, d_cls_k, d_cpl_pts, d_cpl32, d_cpl64;

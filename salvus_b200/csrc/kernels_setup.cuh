@@ -238,6 +238,50 @@ __global__ void geometry_kernel(int64_t E, int dim, int n, int P, int physics, i
   }
 }
 
+// FP32 records of elastic hexahedra that are all parallelepipeds
+// (kernels_hex_affine.cuh): one thread per element point writes the folded
+// material planes mat[m][e*P + p] (w detJ at the point times the constants
+// of the P1-interpolated parameters, as geometry_kernel) and the
+// element-local mass; point 0 of each element also writes invJ at the
+// element centre to jac[e][9] (constant over an affine element).
+__global__ void affine_hex_records_kernel(int64_t E, int n, int P, bool ti,
+                                          const double *__restrict__ vtx,
+                                          const double *__restrict__ par, GllTable gll,
+                                          float *__restrict__ mat, float *__restrict__ jac,
+                                          double *__restrict__ mass_local) {
+  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= E * P) return;
+  const int64_t e = tid / P;
+  const int p = (int)(tid - e * P);
+  const int i = p % n, j = (p / n) % n, k = p / (n * n);
+  const double ref[3] = {gll.xi[i], gll.xi[j], gll.xi[k]};
+  const double wq = gll.w[i] * gll.w[j] * gll.w[k];
+  double v[24];
+  for (int a = 0; a < 24; ++a) v[a] = vtx[e * 24 + a];
+  double detJ, iJ[9];
+  p1_jac_dev(3, v, ref, &detJ, iJ);
+  const double wd = wq * detJ;
+  const int npar = ti ? 6 : 3;
+  double pv[6];
+  for (int q = 0; q < npar; ++q) {
+    double vals[8];
+    for (int a = 0; a < 8; ++a) vals[a] = par[((int64_t)q * E + e) * 8 + a];
+    pv[q] = p1_interp_dev(3, vals, ref);
+  }
+  double mc[5];
+  const int nm = ti ? 5 : 2;
+  if (ti) elastic_constants_ti(pv, mc);
+  else elastic_constants_iso(pv[0], pv[1], pv[2], mc);
+  for (int q = 0; q < nm; ++q) mat[(int64_t)q * E * P + tid] = (float)(wd * mc[q]);
+  mass_local[tid] = wd * pv[0];
+  if (p == 0) {
+    const double c0[3] = {0.0, 0.0, 0.0};
+    double d0, J0[9];
+    p1_jac_dev(3, v, c0, &d0, J0);
+    for (int a = 0; a < 9; ++a) jac[e * 9 + a] = (float)J0[a];
+  }
+}
+
 // Diagonal mass by node gather in ascending element order, then reciprocal.
 __global__ void mass_gather_kernel(int64_t G, const int32_t *__restrict__ off,
                                    const int32_t *__restrict__ idx,

@@ -121,6 +121,34 @@ __global__ void gather_kernel(int64_t G, const int32_t *__restrict__ off,
                              v, ap, a, dt);
 }
 
+// The gather / update over a list of nodes (the shared nodes of a fused
+// hexahedron step, whose interior nodes the stiffness kernel advanced).
+template <typename real, int C, int MODE>
+__global__ void gather_list_kernel(int64_t n, const int32_t *__restrict__ nodes,
+                                   const int32_t *__restrict__ off,
+                                   const int32_t *__restrict__ idx, const real *__restrict__ r,
+                                   const real *__restrict__ mi, real *__restrict__ u,
+                                   real *__restrict__ v, real *__restrict__ ap,
+                                   real *__restrict__ a, real dt) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  gather_body<real, C, MODE>(nodes[t], INT64_MAX, off, idx, r, mi, u, v, ap, a, dt);
+}
+
+// Blow-up detection: any NaN / Inf among n values sets the problem's device
+// status word to kNonFiniteCode (unless a wait timeout code is already
+// there).  Launched after every 32 steps on the displacement field: an
+// unstable explicit step grows without bound and reaches Inf / NaN in u.
+constexpr int kNonFiniteCode = 0x4e614e;  // distinct from the wait codes (1000-1099)
+template <typename real>
+__global__ void finite_check_kernel(int64_t n, const real *__restrict__ x, int *__restrict__ err) {
+  bool bad = false;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    bad |= !isfinite(x[i]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicCAS(err, 0, kNonFiniteCode);
+}
+
 // Homogeneous Dirichlet (HomogeneousDirichlet.cpp:65-73): zero the stiffness
 // rows of the listed element-local points (before sources are added).
 template <typename real, int C>

@@ -117,6 +117,25 @@ def delaunay_tri(nx, ny, lx, ly, jitter=0.3, seed=3):
     return pts, np.ascontiguousarray(cells[keep])
 
 
+def delaunay_tet(nx, ny, nz, lx, ly, lz, jitter=0.3, seed=3):
+    """Seeded Delaunay tetrahedralisation (scipy / qhull) of a jittered
+    (nx+1) x (ny+1) x (nz+1) point lattice over [0,lx] x [0,ly] x [0,lz]:
+    about 6.7 tetrahedra per lattice cell, in qhull's element order.  Flat
+    tetrahedra on the boundary faces (coplanar boundary points) are dropped;
+    cells are returned in TetP1 order with positive orientation."""
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    pts = _jittered_lattice((nx, ny, nz), (lx, ly, lz), jitter, rng)
+    cells = Delaunay(pts).simplices.astype(np.int64)
+    v = pts[cells]
+    det = np.einsum("ij,ij->i", v[:, 2] - v[:, 0], np.cross(v[:, 1] - v[:, 0], v[:, 3] - v[:, 0]))
+    neg = det < 0
+    cells[neg, 1], cells[neg, 2] = cells[neg, 2].copy(), cells[neg, 1].copy()
+    keep = np.abs(det) > 1e-9 * (lx * ly * lz / (nx * ny * nz))
+    return pts, np.ascontiguousarray(cells[keep])
+
+
 # Kuhn (Freudenthal) split of a cube into 6 tetrahedra along the main
 # diagonal 0 -> 7 (corner index = i + 2 j + 4 k).
 _KUHN = [(0, 1, 3, 7), (0, 1, 5, 7), (0, 2, 3, 7), (0, 2, 6, 7), (0, 4, 5, 7), (0, 4, 6, 7)]

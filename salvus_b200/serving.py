@@ -5,8 +5,8 @@ import ctypes
 
 import numpy as np
 
-from .core import (_D, _DP, _I32, _I64, _VP, MeshDesc, SalvusError, SourceDesc, _check, _dp,
-                   lib)
+from .core import (_D, _DP, _I32, _I64, _VP, ACOUSTIC, COUPLED2D, ELASTIC2D, ELASTIC3D,
+                   MESH_ELASTIC_TI, MeshDesc, SalvusError, SourceDesc, _check, _dp, lib)
 
 QUEUED, RUNNING, DONE, FAILED, CANCELLED = range(5)
 
@@ -95,13 +95,15 @@ class Server:
         for k, r in enumerate(cfg.get("receivers", [])):
             rec[k, : len(r)] = r
         rec = np.ascontiguousarray(rec)
-        m = MeshDesc(cfg["shape"], cfg["order"], cfg["physics"], 0, v.shape[0], _dp(v), c.shape[0],
-                     c.ctypes.data_as(ctypes.POINTER(_I64)), _dp(p))
+        flags = MESH_ELASTIC_TI if cfg["physics"] == ELASTIC3D and p.shape[0] == 6 else 0
+        m = MeshDesc(cfg["shape"], cfg["order"], cfg["physics"], flags, v.shape[0], _dp(v),
+                     c.shape[0], c.ctypes.data_as(ctypes.POINTER(_I64)), _dp(p))
         d = JobDesc(m, precision, len(cfg.get("sources", [])), srcs, len(cfg.get("receivers", [])), 0,
                     _dp(rec), float(dt), int(n_steps))
         jid = _I64()
         _check(lib().salvus_server_submit(self.h, ctypes.byref(d), ctypes.byref(jid)))
-        self._meta[jid.value] = (len(cfg.get("receivers", [])), 3 if cfg["physics"] == 1 else 1, n_steps)
+        comps = {ACOUSTIC: 1, ELASTIC3D: 3, ELASTIC2D: 2, COUPLED2D: 3}[cfg["physics"]]
+        self._meta[jid.value] = (len(cfg.get("receivers", [])), comps, n_steps)
         return jid.value
 
     def poll(self, job):

@@ -1,0 +1,138 @@
+"""FP32 accuracy at the benchmark sizes: every workload bench.py times, at
+its full size and step count, against an FP64 reference.
+
+  * 3-D elastic hexahedra, 64^3 elements, order 4, 4000 steps: FP32 and FP64
+    GPU seismograms against the FP64 CPU oracle's, stored in
+    tests/golden/hex_elastic_64cube_4000steps.npz (made by
+    tests/golden/make_hex_fullsize.py on the same seeded inputs);
+  * batched shots, 200^2 quads, order 4, 256 shots, 2000 steps: FP32 batched
+    shots against FP64 single-shot GPU runs, and one shot's FP64 GPU and FP32
+    batched seismograms against the FP64 CPU oracle (which pins the FP64 GPU
+    run as the transitive reference);
+  * P3 triangles (~200k, Delaunay) and elastic P3 tetrahedra (~1M, Delaunay),
+    3000 steps: FP32 (tensor cores for tetrahedra) against FP64 GPU runs on
+    the same mesh (the FP64 GPU path matches the oracle to 1e-10 at test
+    size).
+
+Target (the stated FP32 bound): seismogram rel-L2 <= 1e-4.  Measured errors
+are appended as JSON lines to $SALVUS_ACCURACY_LOG when it is set.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from salvus_b200 import configs, core
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURE = os.path.join(HERE, "golden", "hex_elastic_64cube_4000steps.npz")
+TOL32 = 1e-4
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+
+
+def log(name, **kw):
+    path = os.environ.get("SALVUS_ACCURACY_LOG")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps(dict(workload=name, **kw)) + "\n")
+
+
+def add_all(p, cfg, shots=False, only_shot=None):
+    for s in cfg["sources"]:
+        if only_shot is not None and s.get("shot", 0) != only_shot:
+            continue
+        kw = ({"moment_tensor": s["moment_tensor"]} if "moment_tensor" in s
+              else {"direction": s["direction"]})
+        if shots:
+            kw["shot"] = s["shot"]
+        p.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"], **kw)
+    for r in cfg["receivers"]:
+        p.add_receiver(r)
+
+
+def mesh_of(cfg, flags=0):
+    return core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                     cfg["params"], flags=flags)
+
+
+@pytest.mark.skipif(not os.path.exists(FIXTURE), reason="full-size FP64 fixture not generated")
+@pytest.mark.parametrize("precision", [core.FP32, core.FP64])
+def test_hex_64cube_4000_steps_against_fp64_oracle(precision):
+    fx = np.load(FIXTURE)
+    nel, steps, dt = int(fx["nel"]), int(fx["steps"]), float(fx["dt"])
+    cfg = configs.elastic_hex(nel=nel, order=int(fx["order"]))
+    p = core.Problem(mesh_of(cfg), precision, dt=dt)
+    add_all(p, cfg)
+    p.set_seismogram_capacity(steps + 8)
+    p.run(steps, core.RUN_GRAPH)
+    s = p.seismograms(0, steps)
+    err = rel_l2(s, fx["seis"])
+    log("hex elastic 64^3 order 4, 4000 steps", precision=["fp32", "fp64"][precision],
+        reference="FP64 CPU oracle", rel_l2=err)
+    assert err <= (TOL32 if precision == core.FP32 else 1e-9)
+
+
+def test_batched_shots_200sq_256shots_2000_steps():
+    cfg = configs.batched_quad(nel=200, order=4, n_shots=256)
+    mesh = mesh_of(cfg)
+    dt = 0.4 * mesh.critical_dt(iterations=60)
+    steps = 2000
+    pb = core.Problem(mesh, core.FP32, dt=dt, n_shots=256)
+    add_all(pb, cfg, shots=True)
+    pb.set_seismogram_capacity(steps + 8)
+    pb.run(steps, core.RUN_GRAPH)
+    sb = pb.seismograms(0, steps)  # [shot][rec][c][step]
+    errs = []
+    for shot in range(0, 256, 32):
+        q = core.Problem(mesh, core.FP64, dt=dt)
+        add_all(q, cfg, only_shot=shot)
+        q.set_seismogram_capacity(steps + 8)
+        q.run(steps, core.RUN_GRAPH)
+        s64 = q.seismograms(0, steps)
+        errs.append(rel_l2(sb[shot], s64))
+        if shot == 0:
+            o = po.Problem(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"],
+                           cfg["cells"], cfg["params"], threads=os.cpu_count() or 1)
+            s = cfg["sources"][0]
+            o.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
+                         s["direction"])
+            for r in cfg["receivers"]:
+                o.add_receiver(r)
+            so = o.run(steps, dt)
+            e64_orc = rel_l2(s64, so)
+            e32_orc = rel_l2(sb[0], so)
+    log("batched quads 200^2 order 4, 256 shots, 2000 steps", precision="fp32",
+        reference="FP64 single-shot GPU runs (8 shots)", rel_l2_max=max(errs),
+        rel_l2_shot0_vs_cpu_oracle=e32_orc, fp64_gpu_vs_cpu_oracle=e64_orc)
+    assert e64_orc <= 1e-10
+    assert e32_orc <= TOL32
+    assert max(errs) <= TOL32
+
+
+@pytest.mark.parametrize("which", ["tri", "tet"])
+def test_simplices_full_size_3000_steps(which):
+    cfg = configs.simplex_tri() if which == "tri" else configs.simplex_tet(physics=core.ELASTIC3D)
+    mesh = mesh_of(cfg)
+    dt = 0.4 * mesh.critical_dt(iterations=40)
+    steps = 3000
+    out = {}
+    for prec in (core.FP32, core.FP64):
+        p = core.Problem(mesh, prec, dt=dt)
+        add_all(p, cfg)
+        p.set_seismogram_capacity(steps + 8)
+        p.run(steps, core.RUN_GRAPH)
+        out[prec] = p.seismograms(0, steps)
+        p.close()
+    err = rel_l2(out[core.FP32], out[core.FP64])
+    log(f"P3 {'triangles' if which == 'tri' else 'elastic tetrahedra'} "
+        f"{mesh.n_elements} elements (Delaunay), 3000 steps", precision="fp32",
+        reference="FP64 GPU on the same mesh", rel_l2=err, dt=dt)
+    assert np.abs(out[core.FP64]).max() > 0
+    assert err <= TOL32
