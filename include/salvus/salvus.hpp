@@ -145,9 +145,11 @@ class Mesh {
  public:
   // vertices [n_vertices][dim]; cells [n_elements][nv] (PETSc right-hand
   // order for quads / hexes, TriP1 / TetP1 order for simplices); params per
-  // element vertex: acoustic VP [E][nv], elastic RHO, VP, VS [3][E][nv],
-  // 2-D elastic RHO, C11, C13, C33, C55 [5][E][4], fluid-solid FLUID, VP,
-  // RHO, C11, C13, C33, C55 [7][E][4].
+  // element vertex: acoustic VP [E][nv], elastic RHO, VP, VS [3][E][nv] or
+  // the reference's six RHO, VPV, VPH, VSV, VSH, ETA [6][E][nv]
+  // (Elastic3D.cpp:33-54; transversely isotropic), 2-D elastic RHO, C11,
+  // C13, C33, C55 [5][E][4], fluid-solid FLUID, VP, RHO, C11, C13, C33, C55
+  // [7][E][4].
   Mesh(int order, const std::vector<double> &vertices, const std::vector<int64_t> &cells,
        const std::vector<double> &params, int device = 0) {
     if (order < 1 || order > Element::max_order)
@@ -161,6 +163,9 @@ class Mesh {
     d.n_elements = (int64_t)(cells.size() / Element::vertices);
     d.cells = cells.data();
     d.params = params.data();
+    if (d.physics == SALVUS_ELASTIC3D &&
+        params.size() == (size_t)(6 * d.n_elements * Element::vertices))
+      d.reserved |= SALVUS_MESH_ELASTIC_TI;
     salvus_mesh *m = nullptr;
     check(salvus_mesh_create(&d, device, &m));
     mesh_.reset(m);

@@ -265,6 +265,14 @@ int salvus_problem_autotune(salvus_problem *p, int32_t *stiff_shot_lanes,
  * reference reports such failures as exceptions caught in main
  * (Main.cpp:70-74). */
 int salvus_problem_status(salvus_problem *p, int32_t clear);
+/* Bound, in SM clock cycles, of every device-side wait in this problem's
+ * kernels (the tensor-core simplex kernels' hand-offs between their MMA
+ * issuer and worker warps); <= 0 restores the default 2^31 (about a
+ * second).  A wait that runs out records its code in the status word
+ * (SALVUS_E_TIMEOUT, results invalid) and the kernel returns cleanly after
+ * draining its own MMAs under the default bound.  A short limit makes waits
+ * give up on purpose: for testing the timeout path. */
+int salvus_problem_set_wait_limit(salvus_problem *p, int64_t cycles);
 /* The problem's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events after this problem's kernels. */
 int salvus_problem_stream(const salvus_problem *p, void **stream);
@@ -317,6 +325,13 @@ typedef struct salvus_group salvus_group;
 int salvus_group_create(salvus_problem *const *members, int32_t n_members, salvus_group **out);
 int salvus_group_run(salvus_group *g, int64_t n_steps);
 int salvus_group_synchronize(salvus_group *g);
+/* Bound of the device waits of the single-launch group forms
+ * (SALVUS_GROUP_STEP=persistent / partitioned), as
+ * salvus_problem_set_wait_limit; salvus_group_synchronize then reports
+ * SALVUS_E_TIMEOUT.  salvus_group_clear_status resets the group's and its
+ * members' status words (set the members' fields again before continuing). */
+int salvus_group_set_wait_limit(salvus_group *g, int64_t cycles);
+int salvus_group_clear_status(salvus_group *g);
 int salvus_group_destroy(salvus_group *g);
 
 /* ---- serving: continuous batching of forward-modelling jobs ----

@@ -66,6 +66,9 @@ SIGNATURES = [
     ("salvus_mesh_info", ctypes.c_int, [_VP, ctypes.POINTER(_I64), ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
     ("salvus_mesh_node_coords", ctypes.c_int, [_VP, _DP]),
     ("salvus_problem_status", ctypes.c_int, [_VP, _I32]),
+    ("salvus_problem_set_wait_limit", ctypes.c_int, [_VP, _I64]),
+    ("salvus_group_set_wait_limit", ctypes.c_int, [_VP, _I64]),
+    ("salvus_group_clear_status", ctypes.c_int, [_VP]),
     ("salvus_mesh_layout", ctypes.c_int, [_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I64)]),
     ("salvus_mesh_connectivity", ctypes.c_int, [_VP, ctypes.POINTER(_I64)]),
     ("salvus_mesh_locate_point", ctypes.c_int, [_VP, _DP, ctypes.POINTER(_I64), _DP]),
@@ -332,6 +335,11 @@ class Problem:
     def run(self, n_steps, mode=RUN_GRAPH):
         _check(lib().salvus_run(self.h, int(n_steps), mode))
 
+    def set_wait_limit(self, cycles):
+        """Bound (SM cycles) of the device waits of this problem's kernels;
+        <= 0 restores the default (about a second)."""
+        _check(lib().salvus_problem_set_wait_limit(self.h, int(cycles)))
+
     def status(self, clear=False):
         """Raise SalvusError for a non-finite wavefield (SALVUS_E_NONFINITE) or
         a bounded device wait that gave up; clear=True resets the status
@@ -400,6 +408,12 @@ class Group:
 
     def synchronize(self):
         _check(lib().salvus_group_synchronize(self.h))
+
+    def set_wait_limit(self, cycles):
+        _check(lib().salvus_group_set_wait_limit(self.h, int(cycles)))
+
+    def clear_status(self):
+        _check(lib().salvus_group_clear_status(self.h))
 
     def close(self):
         if getattr(self, "h", None):

@@ -305,7 +305,7 @@ static int launch_tet(const salvus_mesh *m, const real *rec, const real *u, real
 // FP32 tetrahedra on the tensor cores (tcgen05, split TF32)
 template <int C>
 static int launch_tet_tc(const salvus_mesh *m, const float *rec, const float *u, float *r,
-                         cudaStream_t st, int *err) {
+                         cudaStream_t st, int *err, long long wlim) {
   using S = TetTcShape<C>;
   static bool attr = false;
   if (!attr) {
@@ -316,13 +316,13 @@ static int launch_tet_tc(const salvus_mesh *m, const float *rec, const float *u,
   const int64_t tiles = (m->E + S::NE - 1) / S::NE;
   const unsigned grid = (unsigned)(tiles < m->sm_count ? tiles : m->sm_count);
   tet_tc_kernel<C><<<grid, S::THREADS, S::SMEM, st>>>(
-      m->E, rec, m->d_conn.as<int32_t>(), m->d_tc_tab.as<uint4>(), u, r, err);
+      m->E, rec, m->d_conn.as<int32_t>(), m->d_tc_tab.as<uint4>(), u, r, err, wlim);
   g_launches++;
   return check_launch("tetrahedron stiffness (tensor cores)");
 }
 
 static int launch_tri_tc(const salvus_mesh *m, const float *rec, const float *u, float *r,
-                         cudaStream_t st, int *err) {
+                         cudaStream_t st, int *err, long long wlim) {
   using S = TriTcShape;
   static int per_sm = 0;
   if (!per_sm) {
@@ -335,19 +335,20 @@ static int launch_tri_tc(const salvus_mesh *m, const float *rec, const float *u,
   const int64_t slots = (int64_t)per_sm * m->sm_count;
   const unsigned grid = (unsigned)(tiles < slots ? tiles : slots);
   tri_tc_kernel<<<grid, S::THREADS, S::SMEM, st>>>(m->E, rec, m->d_conn.as<int32_t>(),
-                                                   m->d_tc_tab.as<uint4>(), u, r, err);
+                                                   m->d_tc_tab.as<uint4>(), u, r, err, wlim);
   g_launches++;
   return check_launch("triangle stiffness (tensor cores)");
 }
 
 template <typename real>
 static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, real *r,
-                          cudaStream_t st, int *err) {
+                          cudaStream_t st, int *err, long long wlim) {
   if constexpr (std::is_same<real, float>::value) {
-    if (m->shape == SALVUS_TRI && m->tri_kernel == 0) return launch_tri_tc(m, rec, u, r, st, err);
+    if (m->shape == SALVUS_TRI && m->tri_kernel == 0)
+      return launch_tri_tc(m, rec, u, r, st, err, wlim);
     if (m->shape == SALVUS_TET && m->tet_kernel == 0) {
-      if (m->physics == SALVUS_ELASTIC3D) return launch_tet_tc<3>(m, rec, u, r, st, err);
-      return launch_tet_tc<1>(m, rec, u, r, st, err);
+      if (m->physics == SALVUS_ELASTIC3D) return launch_tet_tc<3>(m, rec, u, r, st, err, wlim);
+      return launch_tet_tc<1>(m, rec, u, r, st, err, wlim);
     }
   }
   if (m->shape == SALVUS_TRI) {
@@ -367,8 +368,9 @@ static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, 
 
 template <typename real>
 static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u, real *r,
-                            cudaStream_t st, int *err = nullptr) {
-  if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st, err);
+                            cudaStream_t st, int *err = nullptr,
+                            long long wlim = salvus::kDefaultWaitLimit) {
+  if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st, err, wlim);
   if (m->physics == SALVUS_ELASTIC3D) {
     switch (m->order) {
       case 1: return launch_elastic<1, real>(m, rec, u, r, st);
@@ -594,27 +596,29 @@ static int mesh_setup_device(salvus_mesh *m) {
         m->d_rec32.as<float>(), m->d_jac32.as<float>(), mass_local.as<double>());
     g_launches++;
     if ((rc = check_launch("affine records"))) return rc;
-    // nodes the fused step gathers: all but the element-interior ones
-    if (m->order >= 2) {
-      std::vector<char> interior(m->G, 0);
-      const int n = m->n;
-      for (int64_t e = 0; e < m->E; ++e)
-        for (int k = 1; k < n - 1; ++k)
-          for (int j = 1; j < n - 1; ++j)
-            for (int i = 1; i < n - 1; ++i)
-              interior[m->conn[e * m->P + i + n * j + n * n * k]] = 1;
-      std::vector<int32_t> gn;
-      gn.reserve(m->G);
-      for (int64_t g = 0; g < m->G; ++g)
-        if (!interior[g]) gn.push_back((int32_t)g);
-      m->n_gnodes = (int64_t)gn.size();
-      if ((rc = m->d_gnodes.alloc(sizeof(int32_t) * (gn.empty() ? 1 : gn.size())))) return rc;
-      SALVUS_CUDA(cudaMemcpyAsync(m->d_gnodes.ptr, gn.data(), sizeof(int32_t) * gn.size(),
-                                  cudaMemcpyHostToDevice, m->stream));
-      SALVUS_CUDA(cudaStreamSynchronize(m->stream));
-    }
   } else if ((rc = build_records<float, true>(m, m->d_rec32, mass_local))) {
     return rc;
+  }
+  // nodes the fused step (parallelepiped elastic hexahedra) and the fused
+  // batched step (acoustic quadrilaterals) gather: all but the
+  // element-interior ones, which those steps advance in the stiffness kernel
+  if (m->order >= 2 && (m->affine || (m->shape == SALVUS_QUAD && m->physics == SALVUS_ACOUSTIC))) {
+    std::vector<char> interior(m->G, 0);
+    const int n = m->n, kmax = m->dim == 3 ? n - 1 : 2;
+    for (int64_t e = 0; e < m->E; ++e)
+      for (int k = m->dim == 3 ? 1 : 0; k < kmax; ++k)
+        for (int j = 1; j < n - 1; ++j)
+          for (int i = 1; i < n - 1; ++i)
+            interior[m->conn[e * m->P + i + n * j + n * n * k]] = 1;
+    std::vector<int32_t> gn;
+    gn.reserve(m->G);
+    for (int64_t g = 0; g < m->G; ++g)
+      if (!interior[g]) gn.push_back((int32_t)g);
+    m->n_gnodes = (int64_t)gn.size();
+    if ((rc = m->d_gnodes.alloc(sizeof(int32_t) * (gn.empty() ? 1 : gn.size())))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(m->d_gnodes.ptr, gn.data(), sizeof(int32_t) * gn.size(),
+                                cudaMemcpyHostToDevice, m->stream));
+    SALVUS_CUDA(cudaStreamSynchronize(m->stream));
   }
   if (!m->fp32_only && (rc = build_records<double, false>(m, m->d_rec64, mass_local))) return rc;
   mass_gather_kernel<<<blocks_for(m->G, 256), 256, 0, m->stream>>>(
@@ -839,7 +843,7 @@ static int step_fused_t(salvus_problem *p) {
   {
     ProfScope ps(p, K_STIFF);
     if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
-                                       p->d_err.as<int>())))
+                                       p->d_err.as<int>(), p->wait_limit)))
       return rc;
   }
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
@@ -870,67 +874,95 @@ static const BatchCfg kGatherCfg[] = {{32, 4, 1},  {32, 8, 1}, {64, 2, 1}, {64, 
 constexpr int kNumStiffCfg = sizeof(kStiffCfg) / sizeof(kStiffCfg[0]);
 constexpr int kNumGatherCfg = sizeof(kGatherCfg) / sizeof(kGatherCfg[0]);
 
+// Fused batched step (kernels_batch.cuh, kFuse): interior nodes advanced in
+// the stiffness kernel, edge nodes by the node-list gather.  Used when the
+// mesh has interior nodes (order >= 2); SALVUS_BATCH_STEP=unfused selects
+// the plain sequence (read at every step).
+static bool batch_fusion(const salvus_problem *p) {
+  if (p->mesh->n_gnodes <= 0) return false;
+  const char *s = std::getenv("SALVUS_BATCH_STEP");
+  return !(s && std::strcmp(s, "unfused") == 0);
+}
+
 template <int N, int SC, int EPC>
-static void launch_qb(const salvus_problem *p, cudaStream_t st) {
+static void launch_qb(const salvus_problem *p, cudaStream_t st, bool fuse) {
   const salvus_mesh *m = p->mesh;
   dim3 grid((unsigned)((m->E + EPC - 1) / EPC), (unsigned)(p->shots_pad / SC));
-  quad_acoustic_batched_kernel<N, SC, EPC><<<grid, SC * EPC, 0, st>>>(
-      m->E, p->shots_pad, m->d_rec32.as<float>(), F<float>(p->d_u), F<float>(p->d_r),
-      dmatrix<float>(m->basis));
+  BatchInterior bi{};
+  if (fuse) {
+    bi.mi = m->d_mi32.as<float>();
+    bi.w = F<float>(p->d_v);
+    bi.dt = (float)p->dt;
+    bi.dtd = p->dt;
+    bi.shot_off = p->srcs.empty() ? nullptr : p->d_shot_off.as<int32_t>();
+    bi.src_elem = p->d_src_elem.as<int64_t>();
+    bi.src_par = p->d_src_par.as<double>();
+    bi.src_wts = p->d_src_wts.as<double>();
+    bi.step = p->d_step.as<int64_t>();
+    quad_acoustic_batched_kernel<N, SC, EPC, true><<<grid, SC * EPC, 0, st>>>(
+        m->E, p->shots_pad, m->d_rec32.as<float>(), F<float>(p->d_u), F<float>(p->d_r),
+        dmatrix<float>(m->basis), bi);
+  } else {
+    quad_acoustic_batched_kernel<N, SC, EPC, false><<<grid, SC * EPC, 0, st>>>(
+        m->E, p->shots_pad, m->d_rec32.as<float>(), F<float>(p->d_u), F<float>(p->d_r),
+        dmatrix<float>(m->basis), bi);
+  }
 }
 
 template <int N>
-static int launch_qb_cfg(const salvus_problem *p, int cfg, cudaStream_t st) {
+static int launch_qb_cfg(const salvus_problem *p, int cfg, cudaStream_t st, bool fuse) {
   switch (cfg) {
-    case 0: launch_qb<N, 32, 1>(p, st); break;
-    case 1: launch_qb<N, 32, 2>(p, st); break;
-    case 2: launch_qb<N, 32, 4>(p, st); break;
-    case 3: launch_qb<N, 64, 1>(p, st); break;
-    case 4: launch_qb<N, 64, 2>(p, st); break;
-    case 5: launch_qb<N, 128, 1>(p, st); break;
-    case 6: launch_qb<N, 128, 2>(p, st); break;
-    case 7: launch_qb<N, 256, 1>(p, st); break;
+    case 0: launch_qb<N, 32, 1>(p, st, fuse); break;
+    case 1: launch_qb<N, 32, 2>(p, st, fuse); break;
+    case 2: launch_qb<N, 32, 4>(p, st, fuse); break;
+    case 3: launch_qb<N, 64, 1>(p, st, fuse); break;
+    case 4: launch_qb<N, 64, 2>(p, st, fuse); break;
+    case 5: launch_qb<N, 128, 1>(p, st, fuse); break;
+    case 6: launch_qb<N, 128, 2>(p, st, fuse); break;
+    case 7: launch_qb<N, 256, 1>(p, st, fuse); break;
     default: return fail(SALVUS_E_INVALID, "bad batch config %d", cfg);
   }
   g_launches++;
   return check_launch("batched stiffness");
 }
 
-static int batched_stiffness(const salvus_problem *p, int cfg, cudaStream_t st) {
+static int batched_stiffness(const salvus_problem *p, int cfg, cudaStream_t st, bool fuse) {
   switch (p->mesh->order) {
-    case 1: return launch_qb_cfg<1>(p, cfg, st);
-    case 2: return launch_qb_cfg<2>(p, cfg, st);
-    case 3: return launch_qb_cfg<3>(p, cfg, st);
-    case 4: return launch_qb_cfg<4>(p, cfg, st);
-    case 5: return launch_qb_cfg<5>(p, cfg, st);
-    case 6: return launch_qb_cfg<6>(p, cfg, st);
+    case 1: return launch_qb_cfg<1>(p, cfg, st, false);  // no interior nodes
+    case 2: return launch_qb_cfg<2>(p, cfg, st, fuse);
+    case 3: return launch_qb_cfg<3>(p, cfg, st, fuse);
+    case 4: return launch_qb_cfg<4>(p, cfg, st, fuse);
+    case 5: return launch_qb_cfg<5>(p, cfg, st, fuse);
+    case 6: return launch_qb_cfg<6>(p, cfg, st, fuse);
   }
   return fail(SALVUS_E_UNSUPPORTED, "batched quads support orders 1..6");
 }
 
 template <int SC, int NPB, int NPT = 1>
-static void launch_bg(const salvus_problem *p, cudaStream_t st) {
+static void launch_bg(const salvus_problem *p, cudaStream_t st, bool fuse) {
   const salvus_mesh *m = p->mesh;
-  dim3 grid((unsigned)((m->G + NPB * NPT - 1) / (NPB * NPT)), (unsigned)(p->shots_pad / SC));
+  const int64_t n = fuse ? m->n_gnodes : m->G;
+  dim3 grid((unsigned)((n + NPB * NPT - 1) / (NPB * NPT)), (unsigned)(p->shots_pad / SC));
   batched_gather_update_kernel<SC, NPB, NPT><<<grid, SC * NPB, 0, st>>>(
-      m->G, p->shots_pad, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(),
-      F<float>(p->d_r), m->d_mi32.as<float>(), F<float>(p->d_u), F<float>(p->d_v), (float)p->dt);
+      n, p->shots_pad, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(),
+      F<float>(p->d_r), m->d_mi32.as<float>(), F<float>(p->d_u), F<float>(p->d_v), (float)p->dt,
+      fuse ? m->d_gnodes.as<int32_t>() : nullptr);
 }
 
-static int batched_gather(const salvus_problem *p, int cfg, cudaStream_t st) {
+static int batched_gather(const salvus_problem *p, int cfg, cudaStream_t st, bool fuse) {
   switch (cfg) {
-    case 0: launch_bg<32, 4>(p, st); break;
-    case 1: launch_bg<32, 8>(p, st); break;
-    case 2: launch_bg<64, 2>(p, st); break;
-    case 3: launch_bg<64, 4>(p, st); break;
-    case 4: launch_bg<128, 1>(p, st); break;
-    case 5: launch_bg<128, 2>(p, st); break;
-    case 6: launch_bg<256, 1>(p, st); break;
-    case 7: launch_bg<32, 4, 2>(p, st); break;
-    case 8: launch_bg<64, 2, 2>(p, st); break;
-    case 9: launch_bg<128, 1, 2>(p, st); break;
-    case 10: launch_bg<128, 1, 4>(p, st); break;
-    case 11: launch_bg<256, 1, 2>(p, st); break;
+    case 0: launch_bg<32, 4>(p, st, fuse); break;
+    case 1: launch_bg<32, 8>(p, st, fuse); break;
+    case 2: launch_bg<64, 2>(p, st, fuse); break;
+    case 3: launch_bg<64, 4>(p, st, fuse); break;
+    case 4: launch_bg<128, 1>(p, st, fuse); break;
+    case 5: launch_bg<128, 2>(p, st, fuse); break;
+    case 6: launch_bg<256, 1>(p, st, fuse); break;
+    case 7: launch_bg<32, 4, 2>(p, st, fuse); break;
+    case 8: launch_bg<64, 2, 2>(p, st, fuse); break;
+    case 9: launch_bg<128, 1, 2>(p, st, fuse); break;
+    case 10: launch_bg<128, 1, 4>(p, st, fuse); break;
+    case 11: launch_bg<256, 1, 2>(p, st, fuse); break;
     default: return fail(SALVUS_E_INVALID, "bad gather config %d", cfg);
   }
   g_launches++;
@@ -984,26 +1016,29 @@ static int autotune(salvus_problem *p) {
     }
     return best;
   };
-  float bs = 1e30f;
-  int cs = -1;
-  for (int c = 0; c < kNumStiffCfg && rc == SALVUS_OK; ++c) {
-    if (p->shots_pad % kStiffCfg[c].sc) continue;
-    float t = time_it([&] { return batched_stiffness(p, c, p->stream); });
-    if (t < bs) { bs = t; cs = c; }
-  }
-  // gather timing on scratch copies of u and w
+  // both kernels are timed on zeroed scratch copies of u and w (the fused
+  // stiffness kernel also advances interior nodes), so the problem's state
+  // is untouched
+  const bool fuse = batch_fusion(p);
   const size_t nf = (size_t)p->mesh->G * p->shots_pad * sizeof(float);
   DeviceBuffer su, sw;
+  float bs = 1e30f;
+  int cs = -1;
   if (rc == SALVUS_OK && ((rc = su.alloc(nf)) == SALVUS_OK) && ((rc = sw.alloc(nf)) == SALVUS_OK)) {
     std::swap(p->d_u.ptr, su.ptr);
     std::swap(p->d_v.ptr, sw.ptr);
     cudaMemsetAsync(p->d_u.ptr, 0, nf, p->stream);
     cudaMemsetAsync(p->d_v.ptr, 0, nf, p->stream);
+    for (int c = 0; c < kNumStiffCfg && rc == SALVUS_OK; ++c) {
+      if (p->shots_pad % kStiffCfg[c].sc) continue;
+      float t = time_it([&] { return batched_stiffness(p, c, p->stream, fuse); });
+      if (t < bs) { bs = t; cs = c; }
+    }
     float bg = 1e30f;
     int cg = -1;
     for (int c = 0; c < kNumGatherCfg && rc == SALVUS_OK; ++c) {
       if (p->shots_pad % kGatherCfg[c].sc) continue;
-      float t = time_it([&] { return batched_gather(p, c, p->stream); });
+      float t = time_it([&] { return batched_gather(p, c, p->stream, fuse); });
       if (t < bg) { bg = t; cg = c; }
     }
     std::swap(p->d_u.ptr, su.ptr);
@@ -1026,7 +1061,7 @@ static int step_batched(salvus_problem *p) {
   int rc;
   {
     ProfScope ps(p, K_STIFF);
-    if ((rc = batched_stiffness(p, p->tune_stiff, p->stream))) return rc;
+    if ((rc = batched_stiffness(p, p->tune_stiff, p->stream, batch_fusion(p)))) return rc;
   }
   if (!p->srcs.empty()) {
     ProfScope ps(p, K_SRC);
@@ -1040,7 +1075,7 @@ static int step_batched(salvus_problem *p) {
   }
   {
     ProfScope ps(p, K_UPDATE);
-    if ((rc = batched_gather(p, p->tune_gather, p->stream))) return rc;
+    if ((rc = batched_gather(p, p->tune_gather, p->stream, batch_fusion(p)))) return rc;
   }
   ProfScope ps(p, K_REC);
   if (!p->recs.empty()) {
@@ -1071,7 +1106,7 @@ static int assemble_t(salvus_problem *p) {
   {
     ProfScope ps(p, K_STIFF);
     if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
-                                       p->d_err.as<int>())))
+                                       p->d_err.as<int>(), p->wait_limit)))
       return rc;
   }
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
@@ -1265,6 +1300,7 @@ struct salvus_group {
   int64_t total = 0;
   int grid = 0;
   salvus::DeviceBuffer d_counts, d_work, d_done, d_sync;
+  long long wait_limit = salvus::kDefaultWaitLimit;  // bound of the device waits, SM cycles
   cudaStream_t stream = nullptr;
   cudaEvent_t ev = nullptr;
   std::vector<cudaEvent_t> member_ev;
@@ -1416,7 +1452,7 @@ static int group_persistent_t(salvus_group *g) {
   kern<<<grid, threads, smem, g->stream>>>(
       g->d_slots.as<GroupSlot>(), g->d_counts.as<GroupCounts>(), (int)g->members.size(),
       g->d_work.as<GroupWork>(), g->total, g->d_done.as<int32_t>(), g->d_sync.as<GroupSync>(),
-      dmatrix<float>(g->m0->basis), g->m0->P);
+      dmatrix<float>(g->m0->basis), g->m0->P, g->wait_limit);
   g_launches++;
   return check_launch("group persistent step");
 }
@@ -1514,7 +1550,8 @@ static int group_partitioned_t(salvus_group *g, bool launch) {
   SALVUS_CUDA(cudaLaunchKernelEx(&cfg, kern, (const GroupSlot *)g->d_slots.as<GroupSlot>(),
                                  (const GroupPart *)g->d_parts.as<GroupPart>(), J,
                                  g->d_bars.as<GroupBar>(), g->d_sync.as<GroupSync>(),
-                                 dmatrix<float>(g->m0->basis), g->m0->P));
+                                 dmatrix<float>(g->m0->basis), g->m0->P,
+                                 (long long)g->wait_limit));
   g_launches++;
   return check_launch("group partitioned step");
 }
@@ -2018,20 +2055,38 @@ int salvus_problem_set_seismogram_capacity(salvus_problem *p, int64_t steps) {
 // the host copy into (out of) one chunk overlaps the DMA of the other, which
 // runs at pinned-memory speed instead of the staged pageable path.  Small
 // copies go directly.
-static constexpr size_t kPinChunk = size_t(16) << 20;
-// host copy of one chunk, split over a few threads (one thread's memcpy is
-// slower than the DMA it feeds)
-static void par_memcpy(void *dst, const void *src, size_t n) {
-  constexpr int kThreads = 4;
-  const size_t part = (n / kThreads + 63) & ~size_t(63);
-  std::thread th[kThreads - 1];
-  int used = 0;
-  for (int t = 1; t < kThreads && (size_t)t * part < n; ++t, ++used) {
-    const size_t o = (size_t)t * part, m = std::min(part, n - o);
-    th[t - 1] = std::thread([=] { std::memcpy((char *)dst + o, (const char *)src + o, m); });
+static constexpr size_t kPinChunk = size_t(32) << 20;
+// Host work on one chunk, split over the host threads (one thread's memcpy
+// or conversion is slower than the DMA it feeds): fn(lo, hi) on [0, n).
+static int host_threads() {
+  static const int n = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+  return n;
+}
+extern "C++" {
+template <typename Fn>
+static void par_range(size_t n, Fn fn) {
+  const int T = host_threads();
+  const size_t part = ((n + T - 1) / T + 63) & ~size_t(63);
+  std::vector<std::thread> th;
+  for (int t = 1; t < T && (size_t)t * part < n; ++t) {
+    const size_t lo = (size_t)t * part, hi = std::min(n, lo + part);
+    th.emplace_back([=] { fn(lo, hi); });
   }
-  std::memcpy(dst, src, std::min(part, n));
-  for (int t = 0; t < used; ++t) th[t].join();
+  fn(0, std::min(part, n));
+  for (auto &x : th) x.join();
+}
+}  // extern "C++"
+static void par_memcpy(void *dst, const void *src, size_t n) {
+  par_range(n, [=](size_t lo, size_t hi) {
+    std::memcpy((char *)dst + lo, (const char *)src + lo, hi - lo);
+  });
+}
+// FP64 -> FP32 with round-to-nearest-even, the rounding of the device's
+// conversion (cvt.rn.f32.f64), so both give the same bits.
+static void par_convert(float *dst, const double *src, size_t n) {
+  par_range(n, [=](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; ++i) dst[i] = (float)src[i];
+  });
 }
 static int pin_ready(salvus_problem *p) {
   for (int b = 0; b < 2; ++b) {
@@ -2056,6 +2111,26 @@ static int copy_h2d(salvus_problem *p, void *dst, const void *src, size_t bytes)
     SALVUS_CUDA(cudaMemcpyAsync((char *)dst + off, p->h_pin[b], n, cudaMemcpyHostToDevice, p->stream));
     SALVUS_CUDA(cudaEventRecord(p->pin_ev[b], p->stream));
     off += n;
+  }
+  return SALVUS_OK;
+}
+// FP64 host array -> FP32 device field: the host threads convert each chunk
+// into a pinned buffer while the previous chunk's DMA runs (half the bytes
+// of an FP64 transfer cross PCIe).
+static int copy_h2d_f32(salvus_problem *p, float *dst, const double *src, size_t n) {
+  int rc = pin_ready(p);
+  if (rc) return rc;
+  const size_t per = kPinChunk / sizeof(float);
+  size_t off = 0;
+  for (int k = 0; off < n; ++k) {
+    const int b = k & 1;
+    const size_t m = std::min(per, n - off);
+    if (k >= 2) SALVUS_CUDA(cudaEventSynchronize(p->pin_ev[b]));  // chunk free again
+    par_convert(static_cast<float *>(p->h_pin[b]), src + off, m);
+    SALVUS_CUDA(cudaMemcpyAsync(dst + off, p->h_pin[b], m * sizeof(float), cudaMemcpyHostToDevice,
+                                p->stream));
+    SALVUS_CUDA(cudaEventRecord(p->pin_ev[b], p->stream));
+    off += m;
   }
   return SALVUS_OK;
 }
@@ -2132,14 +2207,9 @@ int salvus_problem_set_field(salvus_problem *p, int32_t f, int32_t shot, const d
     int rc = copy_h2d(p, b->ptr, vals, 8 * N);
     if (rc) return rc;
   } else {
-    // FP64 host array -> FP64 staging on the device -> FP32 field
-    int rc;
-    if (p->d_stage.bytes < 8 * N && (rc = p->d_stage.alloc(8 * N))) return rc;
-    if ((rc = copy_h2d(p, p->d_stage.ptr, vals, 8 * N))) return rc;
-    convert_kernel<double, float><<<blocks_for((int64_t)N, 256), 256, 0, p->stream>>>(
-        (int64_t)N, p->d_stage.as<double>(), b->as<float>());
-    g_launches++;
-    if ((rc = check_launch("convert"))) return rc;
+    // FP64 host array -> FP32 on the host threads -> FP32 field
+    int rc = copy_h2d_f32(p, b->as<float>(), vals, N);
+    if (rc) return rc;
   }
   SALVUS_CUDA(cudaStreamSynchronize(p->stream));
   return SALVUS_OK;
@@ -2224,6 +2294,13 @@ int salvus_step(salvus_problem *p) {
   return rc;
 }
 
+int salvus_problem_set_wait_limit(salvus_problem *p, int64_t cycles) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  p->wait_limit = cycles > 0 ? (long long)cycles : salvus::kDefaultWaitLimit;
+  drop_graph(p);  // captured launches hold the old bound
+  return SALVUS_OK;
+}
+
 int salvus_problem_status(salvus_problem *p, int32_t clear) {
   if (!p) return fail(SALVUS_E_INVALID, "null problem");
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
@@ -2301,7 +2378,7 @@ static int energy_t(salvus_problem *p, double *kinetic, double *strain) {
       (rc = p->d_epart.alloc(2 * kBlocks * sizeof(double))))
     return rc;
   if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
-                                   p->d_err.as<int>())))
+                                   p->d_err.as<int>(), p->wait_limit)))
     return rc;
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
   gather_kernel<real, C, 1><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(
@@ -2540,6 +2617,26 @@ int salvus_group_run(salvus_group *g, int64_t n_steps) {
   for (auto *p : g->members) {
     SALVUS_CUDA(cudaStreamWaitEvent(p->stream, g->ev, 0));
     if (n_steps > 0 && (rc = launch_finite_check(p))) return rc;
+  }
+  return SALVUS_OK;
+}
+
+int salvus_group_set_wait_limit(salvus_group *g, int64_t cycles) {
+  if (!g) return fail(SALVUS_E_INVALID, "null group");
+  g->wait_limit = cycles > 0 ? (long long)cycles : salvus::kDefaultWaitLimit;
+  if (g->graph) cudaGraphExecDestroy(g->graph);  // captured launches hold the old bound
+  g->graph = nullptr;
+  return SALVUS_OK;
+}
+
+int salvus_group_clear_status(salvus_group *g) {
+  if (!g) return fail(SALVUS_E_INVALID, "null group");
+  SALVUS_CUDA(cudaSetDevice(g->m0->device));
+  SALVUS_CUDA(cudaStreamSynchronize(g->stream));
+  if (g->d_sync.ptr) SALVUS_CUDA(cudaMemset(g->d_sync.ptr, 0, sizeof(GroupSync)));
+  for (auto *p : g->members) {
+    SALVUS_CUDA(cudaMemsetAsync(p->d_err.ptr, 0, sizeof(int), p->stream));
+    SALVUS_CUDA(cudaStreamSynchronize(p->stream));
   }
   return SALVUS_OK;
 }

@@ -15,6 +15,8 @@ namespace salvus {
 // quads, Hexahedra.h:14-17 with order7_hex.c missing for hexes).
 constexpr int kMaxQuadOrder = 10;
 constexpr int kMaxHexOrder = 6;
+// Default bound of every device-side wait, in SM clock cycles (~1 s).
+constexpr long long kDefaultWaitLimit = 1ll << 31;
 
 void set_error(const char *fmt, ...);
 int fail(int code, const char *fmt, ...);
@@ -151,7 +153,8 @@ struct salvus_problem {
   // the first large copy) and the events that guard their reuse
   void *h_pin[2] = {nullptr, nullptr};
   cudaEvent_t pin_ev[2] = {nullptr, nullptr};
-  salvus::DeviceBuffer d_err;    // int: device-side error word (bounded waits)
+  salvus::DeviceBuffer d_err;    // int: device-side status word (bounded waits, finite check)
+  long long wait_limit = salvus::kDefaultWaitLimit;  // bound of device waits, SM cycles
   // homogeneous Dirichlet: element-local points (e*P + p) whose stiffness
   // rows are zeroed
   salvus::DeviceBuffer d_dir_pts;

@@ -16,14 +16,42 @@
 
 namespace salvus {
 
+// Interior-node update of the fused batched step (kFuse): the points with
+// both local indices in 1..N-1 are nodes of this element alone, so the
+// stiffness thread of (element, shot) finishes them -- the shot's sources in
+// attach order (batched_source_kernel's arithmetic), the one-term assembly
+// 0 + r, the inverse mass and the half-step-velocity update
+// (batched_gather_update_kernel's arithmetic) -- and writes residuals only
+// for the element's edge points.  Same operations in the same order as the
+// unfused sequence, so both forms give bitwise the same wavefields.
+struct BatchInterior {
+  const float *mi;
+  float *w;
+  float dt;
+  double dtd;
+  const int32_t *shot_off;
+  const int64_t *src_elem;
+  const double *src_par;  // [k][3] f0 t0 amp
+  const double *src_wts;  // [k][P]
+  const int64_t *step;
+};
+
+// half-step-velocity update of one node (one shot): w += dt a; u += dt w,
+// with explicitly rounded operations so that every kernel applying it gives
+// the same bits
+__device__ __forceinline__ void half_step_update(float acc, float m, float dt, float &w, float &u) {
+  w = __fmaf_rn(dt, __fmul_rn(acc, m), w);
+  u = __fmaf_rn(dt, w, u);
+}
+
 // One thread = one shot of one quad element; the element's n^2 values of
 // that shot live in registers, so the tensor-product contractions need no
 // shared memory.  CTA = EPC elements x SC shots.
-template <int N, int SC, int EPC>
+template <int N, int SC, int EPC, bool kFuse = false>
 __global__ void __launch_bounds__(SC *EPC)
 quad_acoustic_batched_kernel(int64_t E, int S, const float *__restrict__ rec,
-                             const float *__restrict__ u, float *__restrict__ r,
-                             DMatrix<float> Dm) {
+                             float *__restrict__ u, float *__restrict__ r,
+                             DMatrix<float> Dm, BatchInterior bi) {
   constexpr int n = N + 1, P = n * n;
   __shared__ float4 sg[EPC * P];  // G00 G01 G11 conn of the CTA's elements
   const int64_t e0 = (int64_t)blockIdx.x * EPC;
@@ -40,7 +68,11 @@ quad_acoustic_batched_kernel(int64_t E, int S, const float *__restrict__ rec,
   const float4 *g = sg + ey * P;
   float uu[P];
 #pragma unroll
-  for (int p = 0; p < P; ++p) uu[p] = __ldg(u + (int64_t)__float_as_int(g[p].w) * S + s);
+  for (int p = 0; p < P; ++p) {
+    // the fused form writes u of interior nodes during the launch: coherent loads
+    const float *up = u + (int64_t)__float_as_int(g[p].w) * S + s;
+    uu[p] = kFuse ? *up : __ldg(up);
+  }
   float Fr[P], Fs[P];
 #pragma unroll
   for (int p = 0; p < P; ++p) {
@@ -65,7 +97,28 @@ quad_acoustic_batched_kernel(int64_t E, int S, const float *__restrict__ rec,
       o += Dm.d[l * n + i] * Fr[l + n * j];
       o += Dm.d[l * n + j] * Fs[i + n * l];
     }
-    out[(int64_t)p * S] = -o;
+    if (!kFuse || i < 1 || i > n - 2 || j < 1 || j > n - 2) {
+      out[(int64_t)p * S] = -o;
+      continue;
+    }
+    if constexpr (kFuse) {
+      float rv = -o;
+      const int k0 = bi.shot_off ? bi.shot_off[s] : 0, k1 = bi.shot_off ? bi.shot_off[s + 1] : 0;
+      if (k1 > k0) {
+        const double t = (double)(*bi.step) * bi.dtd;
+        for (int k = k0; k < k1; ++k) {
+          if (bi.src_elem[k] != e) continue;
+          const double stf = ricker_dev(t, bi.src_par[3 * k], bi.src_par[3 * k + 1],
+                                        bi.src_par[3 * k + 2]);
+          rv += (float)(bi.src_wts[(int64_t)k * P + p] * stf);
+        }
+      }
+      const int64_t x = (int64_t)__float_as_int(g[p].w) * S + s;
+      float wv = bi.w[x], uv = uu[p];
+      half_step_update(__fadd_rn(0.f, rv), __ldg(bi.mi + __float_as_int(g[p].w)), bi.dt, wv, uv);
+      bi.w[x] = wv;
+      u[x] = uv;
+    }
   }
 }
 
@@ -92,12 +145,15 @@ __global__ void batched_source_kernel(int S, int P, const int32_t *__restrict__ 
 // nodes' dependent load chains (offsets -> incidence -> residual) are issued
 // side by side so that more bytes are in flight per thread; the per-node
 // arithmetic and summation order do not depend on NPT.
+// nodes != nullptr: thread slot t handles node nodes[t] (the edge nodes of
+// the fused form), G is then the list's length.
 template <int SC, int NPB, int NPT>
 __global__ void __launch_bounds__(SC *NPB)
 batched_gather_update_kernel(int64_t G, int S, const int32_t *__restrict__ off,
                              const int32_t *__restrict__ idx, const float *__restrict__ r,
                              const float *__restrict__ mi, float *__restrict__ u,
-                             float *__restrict__ w, float dt) {
+                             float *__restrict__ w, float dt,
+                             const int32_t *__restrict__ nodes = nullptr) {
   const int ny = threadIdx.x / SC, lane = threadIdx.x - ny * SC;
   const int64_t g0 = ((int64_t)blockIdx.x * NPB + ny) * NPT;
   const int s = blockIdx.y * SC + lane;
@@ -105,10 +161,12 @@ batched_gather_update_kernel(int64_t G, int S, const int32_t *__restrict__ off,
   constexpr int kFast = 4;  // quadrilateral valence bound
   float uo[NPT], wo[NPT], m[NPT];
   int32_t q0[NPT], cnt[NPT];
+  int64_t gk[NPT];
 #pragma unroll
   for (int k = 0; k < NPT; ++k) {
-    const int64_t g = g0 + k;
-    const bool live = g < G;
+    const bool live = g0 + k < G;
+    const int64_t g = !live ? 0 : nodes ? (int64_t)__ldg(nodes + g0 + k) : g0 + k;
+    gk[k] = g;
     const int64_t i = g * S + s;
     uo[k] = live ? u[i] : 0.f;
     wo[k] = live ? w[i] : 0.f;
@@ -130,8 +188,8 @@ batched_gather_update_kernel(int64_t G, int S, const int32_t *__restrict__ off,
       rv[k][q] = q < cnt[k] ? __ldg(r + (int64_t)ep[k][q] * S + s) : 0.f;
 #pragma unroll
   for (int k = 0; k < NPT; ++k) {
-    const int64_t g = g0 + k;
-    if (g >= G) break;
+    if (g0 + k >= G) break;
+    const int64_t g = gk[k];
     // summed in ascending element order
     float acc = 0.f;
     if (cnt[k] <= kFast) {
@@ -142,10 +200,11 @@ batched_gather_update_kernel(int64_t G, int S, const int32_t *__restrict__ off,
       for (int32_t q = q0[k]; q < q0[k] + cnt[k]; ++q)
         acc += __ldg(r + (int64_t)__ldg(idx + q) * S + s);
     }
-    const float wn = wo[k] + dt * (acc * m[k]);
+    float wn = wo[k], un = uo[k];
+    half_step_update(acc, m[k], dt, wn, un);
     const int64_t i = g * S + s;
     w[i] = wn;
-    u[i] = uo[k] + dt * wn;
+    u[i] = un;
   }
 }
 

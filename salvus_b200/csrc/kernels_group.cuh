@@ -107,12 +107,14 @@ struct GroupSync {
   int err;
 };
 
-// spin (bounded, ~1 s of clock) until *c >= target; thread 0 only
-__device__ __forceinline__ bool group_wait(const int32_t *c, int32_t target, GroupSync *sync) {
+// spin (bounded: `limit` SM cycles, 2^31 -- about a second -- by default)
+// until *c >= target; thread 0 only
+__device__ __forceinline__ bool group_wait(const int32_t *c, int32_t target, GroupSync *sync,
+                                           long long limit) {
   const long long t0 = clock64();
   while (*(volatile const int32_t *)c < target) {
     if (*(volatile int *)&sync->err) return false;
-    if (clock64() - t0 > (1ll << 31)) {
+    if (clock64() - t0 > limit) {
       atomicExch(&sync->err, 1);
       return false;
     }
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(128)
 group_persistent_step(const GroupSlot *__restrict__ slots, const GroupCounts *__restrict__ counts,
                       int J, const GroupWork *__restrict__ work, int64_t total,
                       int32_t *__restrict__ done /* [J][4] */, GroupSync *__restrict__ sync,
-                      DMatrix<float> Dm, int P) {
+                      DMatrix<float> Dm, int P, long long wait_limit) {
   constexpr int n2 = (N + 1) * (N + 1);
   constexpr int EPB = kHex ? (128 / n2 > 0 ? 128 / n2 : 1) : 1;
   __shared__ long long s_item;
@@ -158,11 +160,11 @@ group_persistent_step(const GroupSlot *__restrict__ slots, const GroupCounts *__
     // dependencies (thread 0 waits, the CTA follows)
     if (t == 0) {
       bool ok = true;
-      if (w.type == GI_SRC) ok = group_wait(dj + GI_STIFF, cn.stiff, sync);
-      else if (w.type == GI_GATHER) ok = group_wait(dj + GI_SRC, 1, sync);
-      else if (w.type == GI_REC) ok = group_wait(dj + GI_GATHER, cn.gather, sync);
+      if (w.type == GI_SRC) ok = group_wait(dj + GI_STIFF, cn.stiff, sync, wait_limit);
+      else if (w.type == GI_GATHER) ok = group_wait(dj + GI_SRC, 1, sync, wait_limit);
+      else if (w.type == GI_REC) ok = group_wait(dj + GI_GATHER, cn.gather, sync, wait_limit);
       else if (w.type == GI_ADV)
-        ok = group_wait(dj + GI_GATHER, cn.gather, sync) && group_wait(dj + GI_REC, cn.rec, sync);
+        ok = group_wait(dj + GI_GATHER, cn.gather, sync, wait_limit) && group_wait(dj + GI_REC, cn.rec, sync, wait_limit);
       s_ok = ok;
     }
     __syncthreads();
@@ -240,7 +242,7 @@ template <int N, bool kHex, int C>
 __global__ void __launch_bounds__(128, kHex ? 5 : 10)
 group_partitioned_step(const GroupSlot *__restrict__ slots, const GroupPart *__restrict__ parts,
                        int J, GroupBar *__restrict__ bars, GroupSync *__restrict__ sync,
-                       DMatrix<float> Dm, int P) {
+                       DMatrix<float> Dm, int P, long long wait_limit) {
   constexpr int n2 = (N + 1) * (N + 1);
   constexpr int EPB = kHex ? (128 / n2 > 0 ? 128 / n2 : 1) : 1;
   __shared__ int s_ok;
@@ -257,7 +259,7 @@ group_partitioned_step(const GroupSlot *__restrict__ slots, const GroupPart *__r
   GroupBar *gb = bars + lo;
   const int b = (int)blockIdx.x - pt.cta_first, nb = pt.cta_count;
   auto member_wait = [&](const int32_t *c, int32_t target) {
-    if (t == 0) s_ok = group_wait(c, target, sync);
+    if (t == 0) s_ok = group_wait(c, target, sync, wait_limit);
     __syncthreads();
     return s_ok != 0;
   };

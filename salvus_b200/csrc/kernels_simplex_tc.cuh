@@ -162,16 +162,20 @@ __device__ __forceinline__ void split(float x, float &hi, float &lo) {
   lo = x - hi;
 }
 
-// Bounded wait: clock-based limit (~1 s); a failure anywhere in the CTA
+// Bounded wait: clock-based limit (`limit` SM cycles, 2^31 -- about a second
+// -- unless the problem sets another); a failure anywhere in the CTA
 // (*flag != 0) ends every later wait at once.  The flag records which wait
 // gave up: 1000 + 100 * role + barrier index (role 0 workers, 1 issuer).
+// The issuer's final drain of its own MMAs keeps the fixed 2^31 bound
+// whatever `limit` is, so tensor memory is never released under MMAs in
+// flight.
 __device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, volatile int *flag,
-                                     int code) {
+                                     int code, long long limit) {
   const long long t0 = clock64();
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*flag) return false;
-    if (clock64() - t0 > (1ll << 31)) {
+    if (clock64() - t0 > limit) {
       atomicCAS((int *)flag, 0, code);
       return false;
     }
@@ -186,7 +190,7 @@ template <int C>
 __global__ void __launch_bounds__(288, 1)
 tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restrict__ conn,
               const uint4 *__restrict__ table, const float *__restrict__ u, float *__restrict__ r,
-              int *__restrict__ err) {
+              int *__restrict__ err, long long wait_limit) {
   using S = TetTcShape<C>;
   constexpr int P = S::P, NE = S::NE, RW = S::RW;
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -249,7 +253,7 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     const uint32_t d2 = tmem + S::D2_COL, d2l = tmem + S::D2L_COL;
     const bool leader = lane == 0;
     auto wwait = [&](uint64_t *b, uint32_t p, int code) {
-      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
+      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code, wait_limit) ? 1 : 0) != 0;
     };
     uint32_t it = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
@@ -315,7 +319,7 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     // warp-uniform outcome, so that every lane reaches the .sync.aligned
     // tensor-memory loads together
     auto wwait = [&](uint64_t *b, uint32_t p, int code) {
-      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
+      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code, wait_limit) ? 1 : 0) != 0;
     };
     // Loads are software-pipelined: the next tile's connectivity is fetched
     // while this tile's GEMMs and pointwise stage run, its u values under the

@@ -55,7 +55,7 @@ struct TriTcShape {
 __global__ void __launch_bounds__(160)
 tri_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restrict__ conn,
               const uint4 *__restrict__ table, const float *__restrict__ u, float *__restrict__ r,
-              int *__restrict__ err) {
+              int *__restrict__ err, long long wait_limit) {
   using S = TriTcShape;
   constexpr int P = S::P, NE = S::NE;
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -102,7 +102,7 @@ tri_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     const uint32_t a2_hi = sbase + S::OFF_A2, a2_lo = a2_hi + S::A2_BYTES;
     const bool leader = lane == 0;
     auto wwait = [&](uint64_t *b, uint32_t p, int code) {
-      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
+      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code, wait_limit) ? 1 : 0) != 0;
     };
     uint32_t it = 0;
     for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
@@ -155,7 +155,7 @@ tri_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     unsigned char *a1h = sm + S::OFF_A1, *a1l = a1h + S::A1_BYTES;
     unsigned char *a2h = sm + S::OFF_A2, *a2l = a2h + S::A2_BYTES;
     auto wwait = [&](uint64_t *b, uint32_t p, int code) {
-      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code) ? 1 : 0) != 0;
+      return __all_sync(0xffffffffu, tc::wait(b, p, flag, code, wait_limit) ? 1 : 0) != 0;
     };
     // The next tile's connectivity, record and u are loaded while this
     // tile's MMAs and pointwise stage run (software pipelining across tiles).

@@ -97,3 +97,22 @@ def test_batched_fields_and_tuning(setup):
     p.run(50)
     assert np.abs(p.get_field("u", shot=2)).max() > 0.5
     assert np.all(p.get_field("u", shot=4) == 0)
+
+
+@pytest.mark.parametrize("order", [2, 4, 6])
+def test_fused_batched_step_equals_unfused(order, monkeypatch):
+    """The fused batched step (interior nodes advanced in the stiffness
+    kernel, edge nodes gathered) gives bitwise the wavefields and
+    seismograms of the unfused sequence (stiffness, sources, gather)."""
+    cfg = configs.batched_quad(nel=16, order=order, n_shots=40, n_receivers=6, seed=7)
+    mesh = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                     cfg["params"])
+    dt = 0.4 * mesh.critical_dt(iterations=100)
+    a = batched(cfg, dt, mesh, 120)
+    monkeypatch.setenv("SALVUS_BATCH_STEP", "unfused")
+    b = batched(cfg, dt, mesh, 120)
+    assert np.abs(a.seismograms()).max() > 0
+    assert np.array_equal(a.seismograms(), b.seismograms())
+    for shot in (0, 17, 39):
+        assert np.array_equal(a.get_field("u", shot=shot), b.get_field("u", shot=shot))
+        assert np.array_equal(a.get_field("v", shot=shot), b.get_field("v", shot=shot))

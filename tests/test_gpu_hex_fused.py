@@ -152,3 +152,17 @@ def test_distorted_hexahedra_against_oracle(precision, tol):
     s_o = orc.run(n, dt)
     assert np.abs(s_o).max() > 0
     assert rel_l2(p.seismograms(), s_o) <= tol
+
+
+def test_fp32_field_upload_rounds_like_a_float32_cast():
+    """salvus_problem_set_field converts FP64 host values to FP32 on host
+    threads in pinned chunks; the bits equal a float32 cast of each value
+    (round to nearest even), across chunk boundaries (86 MB of FP32 here)."""
+    cfg = configs.elastic_hex(nel=48, order=4, n_receivers=2)
+    p = problem(cfg)
+    G = p.mesh.n_nodes
+    vals = np.random.default_rng(4).standard_normal((G, 3)) * 10.0 ** np.random.default_rng(5).integers(-30, 30, (G, 3))
+    vals[::997, 1] = 1.0 + 2.0 ** -24  # a tie: rounds to even (1.0)
+    p.set_field("v", vals)
+    got = p.get_field("v")
+    assert np.array_equal(got, vals.astype(np.float32).astype(np.float64))
