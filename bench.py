@@ -209,16 +209,22 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
                  direction=s["direction"])
     for r in cfg["receivers"]:
         q.add_receiver(r)
-    q.set_seismogram_capacity(steps + 64)
+    q.set_seismogram_capacity(2 * steps + 128)
     q.run(5, core.RUN_PLAIN)
     q.synchronize()
     ms_p = timed(q, lambda: q.run(steps, core.RUN_PLAIN))
+    # the same single shot with its time loop replayed from a CUDA graph
+    q.run(64, core.RUN_GRAPH)
+    q.synchronize()
+    ms_g = timed(q, lambda: q.run(steps, core.RUN_GRAPH))
     batched = G * n_shots * steps / (ms_b / 1e3)
     plain = G * steps / (ms_p / 1e3)
     return {"workload": f"acoustic quad {nel}^2 order 4, {n_shots} Ricker shots, GRF model, "
                         f"{len(cfg['receivers'])} receivers",
             "value": batched, "unit": METRIC, "ms_per_step": ms_b / steps,
             "plain_value": plain, "plain_ms_per_step": ms_p / steps,
+            "single_graph_value": G * steps / (ms_g / 1e3), "single_graph_ms_per_step": ms_g / steps,
+            "form": "fused batched step (interior nodes in the stiffness kernel), CUDA graph",
             "shot_throughput_ratio": batched / plain, "steps": steps,
             "tuning": {"stiffness_shot_lanes": tune[0], "stiffness_elements_per_cta": tune[1],
                        "gather_shot_lanes": tune[2], "gather_nodes_per_cta": tune[3]}}

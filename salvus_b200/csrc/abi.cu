@@ -532,6 +532,34 @@ static int build_records(salvus_mesh *m, DeviceBuffer &out, DeviceBuffer &mass_l
   return check_launch("geometry");
 }
 
+// Nodes the fused step (parallelepiped elastic hexahedra) and the fused
+// batched step (acoustic quadrilaterals) gather: all but the element-interior
+// ones (every local index in 1..N-1), which those steps advance in the
+// stiffness kernel.  Host-side, ascending node ids.
+static void interior_free_nodes(salvus_mesh *m) {
+  m->gnodes.clear();
+  m->n_gnodes = 0;
+  const bool quad = m->shape == SALVUS_QUAD && m->physics == SALVUS_ACOUSTIC;
+  if (m->order < 2 || !(m->affine || quad)) return;
+  const int n = m->n;
+  std::vector<char> interior((size_t)m->G, 0);
+  for (int64_t e = 0; e < m->E; ++e) {
+    const int32_t *cn = m->conn.data() + e * m->P;
+    if (m->dim == 2) {
+      for (int j = 1; j < n - 1; ++j)
+        for (int i = 1; i < n - 1; ++i) interior[(size_t)cn[i + n * j]] = 1;
+    } else {
+      for (int k = 1; k < n - 1; ++k)
+        for (int j = 1; j < n - 1; ++j)
+          for (int i = 1; i < n - 1; ++i) interior[(size_t)cn[i + n * j + n * n * k]] = 1;
+    }
+  }
+  m->gnodes.reserve((size_t)m->G);
+  for (int64_t g = 0; g < m->G; ++g)
+    if (!interior[(size_t)g]) m->gnodes.push_back((int32_t)g);
+  m->n_gnodes = (int64_t)m->gnodes.size();
+}
+
 static int mesh_setup_device(salvus_mesh *m) {
   int rc;
   SALVUS_CUDA(cudaSetDevice(m->device));
@@ -599,24 +627,10 @@ static int mesh_setup_device(salvus_mesh *m) {
   } else if ((rc = build_records<float, true>(m, m->d_rec32, mass_local))) {
     return rc;
   }
-  // nodes the fused step (parallelepiped elastic hexahedra) and the fused
-  // batched step (acoustic quadrilaterals) gather: all but the
-  // element-interior ones, which those steps advance in the stiffness kernel
-  if (m->order >= 2 && (m->affine || (m->shape == SALVUS_QUAD && m->physics == SALVUS_ACOUSTIC))) {
-    std::vector<char> interior(m->G, 0);
-    const int n = m->n, kmax = m->dim == 3 ? n - 1 : 2;
-    for (int64_t e = 0; e < m->E; ++e)
-      for (int k = m->dim == 3 ? 1 : 0; k < kmax; ++k)
-        for (int j = 1; j < n - 1; ++j)
-          for (int i = 1; i < n - 1; ++i)
-            interior[m->conn[e * m->P + i + n * j + n * n * k]] = 1;
-    std::vector<int32_t> gn;
-    gn.reserve(m->G);
-    for (int64_t g = 0; g < m->G; ++g)
-      if (!interior[g]) gn.push_back((int32_t)g);
-    m->n_gnodes = (int64_t)gn.size();
-    if ((rc = m->d_gnodes.alloc(sizeof(int32_t) * (gn.empty() ? 1 : gn.size())))) return rc;
-    SALVUS_CUDA(cudaMemcpyAsync(m->d_gnodes.ptr, gn.data(), sizeof(int32_t) * gn.size(),
+  // the node list of the fused steps (interior_free_nodes, at creation)
+  if (m->n_gnodes > 0) {
+    if ((rc = m->d_gnodes.alloc(sizeof(int32_t) * (size_t)m->n_gnodes))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(m->d_gnodes.ptr, m->gnodes.data(), sizeof(int32_t) * m->gnodes.size(),
                                 cudaMemcpyHostToDevice, m->stream));
     SALVUS_CUDA(cudaStreamSynchronize(m->stream));
   }
@@ -1763,6 +1777,7 @@ int salvus_mesh_create(const salvus_mesh_desc *d, int device, salvus_mesh **out)
   }
   if ((rc = flatten_mesh(m.get(), d->cells, d->n_vertices))) return rc;
   if (m->physics == SALVUS_COUPLED2D && (rc = setup_coupled(m.get(), d->cells))) return rc;
+  interior_free_nodes(m.get());
   if (device >= 0) {
     if ((rc = mesh_setup_device(m.get()))) return rc;
   } else {

@@ -127,6 +127,7 @@ struct salvus_mesh {
   // the nodes that are not interior to an element (fused step gather)
   bool affine = false;
   salvus::DeviceBuffer d_jac32, d_rec32g, d_gnodes;
+  std::vector<int32_t> gnodes;  // host copy of d_gnodes
   int64_t n_gnodes = 0;
   salvus::DeviceBuffer d_sd32, d_sd64;    // simplex derivative tables [dim][P][P]
   salvus::DeviceBuffer d_tc_tab;          // tetrahedra: tensor-core operand image (hi | lo)

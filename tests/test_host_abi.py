@@ -194,3 +194,33 @@ def test_invalid_physics_meshes_rejected():
         core.Mesh(core.QUAD, 3, core.COUPLED2D, V, C, mixed, device=-1)
     with pytest.raises(core.SalvusError):
         core.Mesh(core.QUAD, 3, 7, V, C, par, device=-1)
+
+
+def test_interior_node_lists_on_the_host():
+    """The fused steps gather every node except the element-interior ones:
+    G - E (N-1)^d for acoustic quads and parallelepiped elastic hexahedra,
+    all G otherwise (order 1, distorted or acoustic hexahedra, per-point
+    geometry requested)."""
+    def layout(cfg, flags=0):
+        m = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                      cfg["params"], device=-1, flags=flags)
+        return m.layout(), m.n_nodes, len(cfg["cells"])
+
+    (aff, gathered), G, E = layout(configs.standing_wave_2d(nel=10, order=4))
+    assert not aff and G == 41 * 41 and gathered == G - E * 9
+    (aff, gathered), G, E = layout(configs.standing_wave_2d(nel=6, order=1))
+    assert gathered == G
+    (aff, gathered), G, E = layout(configs.elastic_hex(nel=3, order=4, n_receivers=2))
+    assert aff and G == 13 ** 3 and gathered == G - E * 27
+    (aff, gathered), G, E = layout(configs.elastic_hex(nel=3, order=4, n_receivers=2),
+                                   flags=core.MESH_PER_POINT_GEOMETRY)
+    assert not aff and gathered == G
+    (aff, gathered), G, E = layout(configs.acoustic_hex(nel=3, order=4))
+    assert not aff and gathered == G
+    cfg = configs.elastic_hex(nel=3, order=3, n_receivers=2)
+    V = cfg["vertices"].copy()
+    inner = np.all((V > 1.0) & (V < cfg["L"] - 1.0), axis=1)
+    V[inner] += 37.0
+    cfg["vertices"] = V
+    (aff, gathered), G, E = layout(cfg)
+    assert not aff and gathered == G
