@@ -54,8 +54,9 @@ def parse():
                     help="2-D elastic leg: nel x nel quads (default 720, ~8.3M nodes)")
     ap.add_argument("--simplex-only", action="store_true",
                     help="run only the P3 simplex leg (profiling / quick checks)")
-    ap.add_argument("--tet-n", type=int, default=55,
-                    help="tetrahedral lattice cells per side (6 n^3 elements; 55 -> ~1M)")
+    ap.add_argument("--tet-n", type=int, default=44,
+                    help="tetrahedral mesh cells per side (Delaunay of a jittered BCC point "
+                         "set, ~12 n^3 elements; 44 -> ~1.02M)")
     ap.add_argument("--serving-jobs", type=int, default=24)
     ap.add_argument("--serving-only", action="store_true",
                     help="run only the serving leg (e.g. --serving-jobs 500) and print its JSON")
@@ -327,8 +328,8 @@ def profile_leg(core, configs, name, steps, device=0):
     """One workload at a capture-friendly size (inputs larger than L2, a few
     GB at most), `steps` host-launched plain steps, nothing timed: the command
     that ncu captures.  quad: 1000^2 acoustic quads N=4; elastic2d / coupled:
-    720^2 quads N=4; tri: 1400 x 700 x 2 P3 triangles; tet: 40^3 x 6 elastic
-    P3 tetrahedra; shots: 200^2 quads x 256 shots; group: 12 acoustic quad
+    720^2 quads N=4; tri: 1400 x 700 x 2 P3 triangles; tet: ~393k elastic
+    P3 tetrahedra (Delaunay, 32^3 BCC cells); shots: 200^2 quads x 256 shots; group: 12 acoustic quad
     meshes of 100^2..320^2 in one problem group."""
     def populate(p, cfg, shots=False):
         for s in cfg.get("sources", []):
@@ -361,7 +362,7 @@ def profile_leg(core, configs, name, steps, device=0):
            "elastic2d": lambda: configs.elastic_2d(nel=720, order=4),
            "coupled": lambda: configs.coupled_2d(nel=720, order=4),
            "tri": lambda: configs.simplex_tri(nx=1400, ny=700),
-           "tet": lambda: configs.simplex_tet(n=40, physics=core.ELASTIC3D),
+           "tet": lambda: configs.simplex_tet(n=32, physics=core.ELASTIC3D),
            "shots": lambda: configs.batched_quad(nel=200, order=4, n_shots=256)}[name]()
     mesh = build(cfg)
     shots = name == "shots"

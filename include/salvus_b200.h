@@ -273,6 +273,12 @@ int salvus_problem_status(salvus_problem *p, int32_t clear);
  * draining its own MMAs under the default bound.  A short limit makes waits
  * give up on purpose: for testing the timeout path. */
 int salvus_problem_set_wait_limit(salvus_problem *p, int64_t cycles);
+/* Testing the timeout path (no reference counterpart): with enable != 0 the
+ * worker warps of the tensor-core simplex kernels first wait on a barrier
+ * that nothing arrives on, so every such launch runs out of its wait limit,
+ * returns cleanly and the problem reports SALVUS_E_TIMEOUT (results
+ * invalid); enable = 0 restores normal launches.  Other kernels ignore it. */
+int salvus_problem_hold_device_waits(salvus_problem *p, int32_t enable);
 /* The problem's CUDA stream (a cudaStream_t), for callers that order their
  * own work or timing events after this problem's kernels. */
 int salvus_problem_stream(const salvus_problem *p, void **stream);

@@ -231,20 +231,25 @@ def simplex_tri(nx=448, ny=224, lx=2.0e4, ly=1.0e4, vp=4000.0, std=0.05, corr=10
                 receivers=meshgen.ring_positions(center, 0.3 * ly, n_receivers, seed))
 
 
-def simplex_tet(n=53, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
+def simplex_tet(n=44, L=1.0e4, physics=ELASTIC3D, vp=6000.0, vs=3464.0, rho=2700.0, std=0.05,
                 corr=1000.0, f0=1.0, n_receivers=64, seed=3, anisotropy=None, mesh="delaunay"):
     """3-D P3 tetrahedra over an L cube: a seeded Delaunay tetrahedralisation
-    of a jittered (n+1)^3 point lattice (about 6.7 n^3 elements; n = 53 gives
-    ~157k points and ~1M tetrahedra), or with mesh="kuhn" the lattice cells
-    split into 6 tetrahedra each; material homogeneous times (1 + std GRF);
+    of a jittered body-centred cubic point set on n^3 cells (about 12 n^3
+    elements; n = 44 gives 176k points and ~1.02M tetrahedra), or with
+    mesh="kuhn" a jittered lattice whose cells are split into 6 tetrahedra
+    each; material homogeneous times (1 + std GRF);
     elastic: seeded moment-tensor Ricker source, acoustic: pressure source;
     receivers at seeded positions on the top surface."""
+    h = L / n
     if mesh == "kuhn":
         V, C = meshgen.kuhn_tet(n, n, n, L, L, L, seed=seed)
+        grf = meshgen.gaussian_random_field((n + 1,) * 3, h, corr, seed).ravel()
     else:
         V, C = meshgen.delaunay_tet(n, n, n, L, L, L, seed=seed)
-    h = L / n
-    grf = meshgen.gaussian_random_field((n + 1,) * 3, h, corr, seed).ravel()
+        # the field on the doubled lattice: cell corners at even, cell
+        # centres at odd indices (the point order of delaunay_tet)
+        g2 = meshgen.gaussian_random_field((2 * n + 1,) * 3, h / 2, corr, seed)
+        grf = np.concatenate([g2[::2, ::2, ::2].ravel(), g2[1::2, 1::2, 1::2].ravel()])
     pert = 1.0 + std * grf
     rng = np.random.default_rng(seed)
     rec_xy = rng.uniform(0.02 * L, 0.98 * L, size=(n_receivers, 2))

@@ -67,6 +67,7 @@ SIGNATURES = [
     ("salvus_mesh_node_coords", ctypes.c_int, [_VP, _DP]),
     ("salvus_problem_status", ctypes.c_int, [_VP, _I32]),
     ("salvus_problem_set_wait_limit", ctypes.c_int, [_VP, _I64]),
+    ("salvus_problem_hold_device_waits", ctypes.c_int, [_VP, _I32]),
     ("salvus_group_set_wait_limit", ctypes.c_int, [_VP, _I64]),
     ("salvus_group_clear_status", ctypes.c_int, [_VP]),
     ("salvus_mesh_layout", ctypes.c_int, [_VP, ctypes.POINTER(_I32), ctypes.POINTER(_I64)]),
@@ -339,6 +340,11 @@ class Problem:
         """Bound (SM cycles) of the device waits of this problem's kernels;
         <= 0 restores the default (about a second)."""
         _check(lib().salvus_problem_set_wait_limit(self.h, int(cycles)))
+
+    def hold_device_waits(self, enable=True):
+        """Test hook: the tensor-core simplex kernels' workers wait on a
+        barrier nothing arrives on, so launches time out (SALVUS_E_TIMEOUT)."""
+        _check(lib().salvus_problem_hold_device_waits(self.h, 1 if enable else 0))
 
     def status(self, clear=False):
         """Raise SalvusError for a non-finite wavefield (SALVUS_E_NONFINITE) or

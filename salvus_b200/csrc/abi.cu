@@ -305,7 +305,7 @@ static int launch_tet(const salvus_mesh *m, const real *rec, const real *u, real
 // FP32 tetrahedra on the tensor cores (tcgen05, split TF32)
 template <int C>
 static int launch_tet_tc(const salvus_mesh *m, const float *rec, const float *u, float *r,
-                         cudaStream_t st, int *err, long long wlim) {
+                         cudaStream_t st, int *err, long long wlim, int hold) {
   using S = TetTcShape<C>;
   static bool attr = false;
   if (!attr) {
@@ -316,13 +316,13 @@ static int launch_tet_tc(const salvus_mesh *m, const float *rec, const float *u,
   const int64_t tiles = (m->E + S::NE - 1) / S::NE;
   const unsigned grid = (unsigned)(tiles < m->sm_count ? tiles : m->sm_count);
   tet_tc_kernel<C><<<grid, S::THREADS, S::SMEM, st>>>(
-      m->E, rec, m->d_conn.as<int32_t>(), m->d_tc_tab.as<uint4>(), u, r, err, wlim);
+      m->E, rec, m->d_conn.as<int32_t>(), m->d_tc_tab.as<uint4>(), u, r, err, wlim, hold);
   g_launches++;
   return check_launch("tetrahedron stiffness (tensor cores)");
 }
 
 static int launch_tri_tc(const salvus_mesh *m, const float *rec, const float *u, float *r,
-                         cudaStream_t st, int *err, long long wlim) {
+                         cudaStream_t st, int *err, long long wlim, int hold) {
   using S = TriTcShape;
   static int per_sm = 0;
   if (!per_sm) {
@@ -335,20 +335,21 @@ static int launch_tri_tc(const salvus_mesh *m, const float *rec, const float *u,
   const int64_t slots = (int64_t)per_sm * m->sm_count;
   const unsigned grid = (unsigned)(tiles < slots ? tiles : slots);
   tri_tc_kernel<<<grid, S::THREADS, S::SMEM, st>>>(m->E, rec, m->d_conn.as<int32_t>(),
-                                                   m->d_tc_tab.as<uint4>(), u, r, err, wlim);
+                                                   m->d_tc_tab.as<uint4>(), u, r, err, wlim, hold);
   g_launches++;
   return check_launch("triangle stiffness (tensor cores)");
 }
 
 template <typename real>
 static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, real *r,
-                          cudaStream_t st, int *err, long long wlim) {
+                          cudaStream_t st, int *err, long long wlim, int hold) {
   if constexpr (std::is_same<real, float>::value) {
     if (m->shape == SALVUS_TRI && m->tri_kernel == 0)
-      return launch_tri_tc(m, rec, u, r, st, err, wlim);
+      return launch_tri_tc(m, rec, u, r, st, err, wlim, hold);
     if (m->shape == SALVUS_TET && m->tet_kernel == 0) {
-      if (m->physics == SALVUS_ELASTIC3D) return launch_tet_tc<3>(m, rec, u, r, st, err, wlim);
-      return launch_tet_tc<1>(m, rec, u, r, st, err, wlim);
+      if (m->physics == SALVUS_ELASTIC3D)
+        return launch_tet_tc<3>(m, rec, u, r, st, err, wlim, hold);
+      return launch_tet_tc<1>(m, rec, u, r, st, err, wlim, hold);
     }
   }
   if (m->shape == SALVUS_TRI) {
@@ -369,8 +370,8 @@ static int launch_simplex(const salvus_mesh *m, const real *rec, const real *u, 
 template <typename real>
 static int launch_stiffness(const salvus_mesh *m, const real *rec, const real *u, real *r,
                             cudaStream_t st, int *err = nullptr,
-                            long long wlim = salvus::kDefaultWaitLimit) {
-  if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st, err, wlim);
+                            long long wlim = salvus::kDefaultWaitLimit, int hold = 0) {
+  if (is_simplex(m->shape)) return launch_simplex<real>(m, rec, u, r, st, err, wlim, hold);
   if (m->physics == SALVUS_ELASTIC3D) {
     switch (m->order) {
       case 1: return launch_elastic<1, real>(m, rec, u, r, st);
@@ -857,7 +858,7 @@ static int step_fused_t(salvus_problem *p) {
   {
     ProfScope ps(p, K_STIFF);
     if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
-                                       p->d_err.as<int>(), p->wait_limit)))
+                                       p->d_err.as<int>(), p->wait_limit, p->hold_waits)))
       return rc;
   }
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
@@ -1120,7 +1121,7 @@ static int assemble_t(salvus_problem *p) {
   {
     ProfScope ps(p, K_STIFF);
     if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
-                                       p->d_err.as<int>(), p->wait_limit)))
+                                       p->d_err.as<int>(), p->wait_limit, p->hold_waits)))
       return rc;
   }
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
@@ -1336,19 +1337,6 @@ static int group_upload(salvus::DeviceBuffer &b, const void *src, size_t bytes, 
 
 static int group_partitioned(salvus_group *g, bool launch);
 
-// Problem groups run the per-point-geometry hexahedron body; parallelepiped
-// meshes build those records on first use.
-static int ensure_per_point_records(salvus_mesh *m) {
-  if (m->d_rec32g.ptr) return SALVUS_OK;
-  SALVUS_CUDA(cudaSetDevice(m->device));
-  DeviceBuffer mass_local;
-  int rc = mass_local.alloc(sizeof(double) * (size_t)(m->E * m->P));
-  if (rc) return rc;
-  if ((rc = build_records<float, true>(m, m->d_rec32g, mass_local))) return rc;
-  SALVUS_CUDA(cudaStreamSynchronize(m->stream));
-  return SALVUS_OK;
-}
-
 static int group_fill(salvus_group *g) {
   int64_t bs = 0, bg = 0, br = 0;
   g->slots.resize(g->members.size());
@@ -1358,8 +1346,8 @@ static int group_fill(salvus_group *g) {
     int rc = ready(p);
     if (rc) return rc;
     GroupSlot &s = g->slots[k];
-    if (m->affine && (rc = ensure_per_point_records(const_cast<salvus_mesh *>(m)))) return rc;
-    s.rec = (m->affine ? m->d_rec32g : m->d_rec32).as<float>();
+    s.rec = m->d_rec32.as<float>();
+    s.jac = m->affine ? m->d_jac32.as<float>() : nullptr;
     s.conn = m->d_conn.as<int32_t>();
     s.inc_off = m->d_inc_off.as<int32_t>();
     s.inc_idx = m->d_inc_idx.as<int32_t>();
@@ -2316,6 +2304,13 @@ int salvus_problem_set_wait_limit(salvus_problem *p, int64_t cycles) {
   return SALVUS_OK;
 }
 
+int salvus_problem_hold_device_waits(salvus_problem *p, int32_t enable) {
+  if (!p) return fail(SALVUS_E_INVALID, "null problem");
+  p->hold_waits = enable ? 1 : 0;
+  drop_graph(p);  // captured launches hold the old setting
+  return SALVUS_OK;
+}
+
 int salvus_problem_status(salvus_problem *p, int32_t clear) {
   if (!p) return fail(SALVUS_E_INVALID, "null problem");
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
@@ -2393,7 +2388,7 @@ static int energy_t(salvus_problem *p, double *kinetic, double *strain) {
       (rc = p->d_epart.alloc(2 * kBlocks * sizeof(double))))
     return rc;
   if ((rc = launch_stiffness<real>(m, records<real>(p), F<real>(p->d_u), F<real>(p->d_r), p->stream,
-                                   p->d_err.as<int>(), p->wait_limit)))
+                                   p->d_err.as<int>(), p->wait_limit, p->hold_waits)))
     return rc;
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
   gather_kernel<real, C, 1><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(

@@ -122,11 +122,10 @@ struct salvus_mesh {
   salvus::DeviceBuffer d_mi64, d_mi32;
   salvus::DeviceBuffer d_rec32, d_rec64;  // stiffness records per precision
   // elastic hexahedra that are all parallelepipeds: d_rec32 holds material
-  // planes [NM][E*P], d_jac32 the per-element invJ [E][9]; d_rec32g the
-  // per-point layout, built when a problem group needs it; d_gnodes lists
-  // the nodes that are not interior to an element (fused step gather)
+  // planes [NM][E*P], d_jac32 the per-element invJ [E][9]; d_gnodes lists
+  // the nodes that are not interior to an element (fused steps' gather)
   bool affine = false;
-  salvus::DeviceBuffer d_jac32, d_rec32g, d_gnodes;
+  salvus::DeviceBuffer d_jac32, d_gnodes;
   std::vector<int32_t> gnodes;  // host copy of d_gnodes
   int64_t n_gnodes = 0;
   salvus::DeviceBuffer d_sd32, d_sd64;    // simplex derivative tables [dim][P][P]
@@ -156,6 +155,7 @@ struct salvus_problem {
   cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   salvus::DeviceBuffer d_err;    // int: device-side status word (bounded waits, finite check)
   long long wait_limit = salvus::kDefaultWaitLimit;  // bound of device waits, SM cycles
+  int hold_waits = 0;  // test hook: tensor-core workers wait on a barrier nothing arrives on
   // homogeneous Dirichlet: element-local points (e*P + p) whose stiffness
   // rows are zeroed
   salvus::DeviceBuffer d_dir_pts;

@@ -25,8 +25,9 @@
 namespace salvus {
 
 struct GroupSlot {
-  // mesh
-  const float *rec;
+  // mesh (hexahedra: jac != nullptr for parallelepiped meshes, whose rec holds
+  // the material planes of kernels_hex_affine.cuh)
+  const float *rec, *jac;
   const int32_t *conn, *inc_off, *inc_idx;
   const float *mi;
   int64_t E, G;
@@ -46,6 +47,20 @@ struct GroupSlot {
   int64_t b_stiff, b_gather, b_rec;
 };
 
+// Stiffness of element group bid of one member: the body its solo run uses
+// (parallelepiped records or per-point records), so the result is the same.
+template <int N, int EPB>
+__device__ __forceinline__ void group_hex_body(const GroupSlot &m, int64_t bid,
+                                               const DMatrix<float> &Dm) {
+  if (m.jac) {
+    const HexInteriorUpdate none{};
+    elastic_hex_affine_body<N, EPB, false, false>(bid, m.E, m.jac, m.rec, m.conn, m.u, m.r, Dm,
+                                                  none);
+  } else {
+    elastic_hex_v2_body<N, EPB, false>(bid, m.E, m.rec, m.u, m.r, Dm);
+  }
+}
+
 // owner[b]: the member whose CTA range of this launch holds CTA b (a table
 // per stage, filled on the host; one load instead of a search).
 
@@ -63,7 +78,7 @@ __global__ void __launch_bounds__(ElasticV2Shape<N, EPB, false>::THREADS)
 group_hex_elastic_stiffness(const GroupSlot *__restrict__ slots,
                             const int32_t *__restrict__ owner, DMatrix<float> Dm) {
   const GroupSlot &m = slots[owner[blockIdx.x]];
-  elastic_hex_v2_body<N, EPB, false>(blockIdx.x - m.b_stiff, m.E, m.rec, m.u, m.r, Dm);
+  group_hex_body<N, EPB>(m, blockIdx.x - m.b_stiff, Dm);
 }
 
 // one CTA per member
@@ -173,7 +188,7 @@ group_persistent_step(const GroupSlot *__restrict__ slots, const GroupCounts *__
       case GI_STIFF:
         for (int b = w.first; b < w.first + w.count; ++b) {
           if constexpr (kHex)
-            elastic_hex_v2_body<N, EPB, false>(b, m.E, m.rec, m.u, m.r, Dm);
+            group_hex_body<N, EPB>(m, b, Dm);
           else
             acoustic_quad_col_body<N, quad_col_epb<N>(), float>(b, m.E, m.rec, m.conn, m.u, m.r, Dm);
           __syncthreads();
@@ -273,7 +288,7 @@ group_partitioned_step(const GroupSlot *__restrict__ slots, const GroupPart *__r
   // stiffness
   for (int k = b; k < pt.n_stiff; k += nb) {
     if constexpr (kHex)
-      elastic_hex_v2_body<N, EPB, false>(k, m.E, m.rec, m.u, m.r, Dm);
+      group_hex_body<N, EPB>(m, k, Dm);
     else
       acoustic_quad_col_body<N, quad_col_epb<N>(), float>(k, m.E, m.rec, m.conn, m.u, m.r, Dm);
     __syncthreads();

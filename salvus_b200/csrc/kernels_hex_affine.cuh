@@ -58,18 +58,20 @@ struct HexAffineShape {
   static constexpr size_t SMEM = V2::SMEM;
 };
 
+// One group of EPB elements (bid), all threads of the CTA (contains
+// __syncthreads); also the body of the grouped hexahedron steps.
 template <int N, int EPB_, bool TI, bool kFuse>
-__global__ void __launch_bounds__(HexAffineShape<N, EPB_, TI>::THREADS)
-elastic_hex_affine_kernel(int64_t E, const float *__restrict__ jac, const float *__restrict__ mat,
-                          const int32_t *__restrict__ conn, float *__restrict__ u,
-                          float *__restrict__ r, DMatrix<float> Dm, HexInteriorUpdate iu) {
+__device__ __forceinline__ void elastic_hex_affine_body(
+    int64_t bid, int64_t E, const float *__restrict__ jac, const float *__restrict__ mat,
+    const int32_t *__restrict__ conn, float *__restrict__ u, float *__restrict__ r,
+    const DMatrix<float> &Dm, const HexInteriorUpdate &iu) {
   using S = HexAffineShape<N, EPB_, TI>;
   constexpr int n = S::n, n2 = S::n2, P = S::P, EPB = S::EPB, NM = S::NM;
   extern __shared__ __align__(16) float smem_af[];
   const int t = threadIdx.x;
   const int le = t / n2, ij = t - le * n2;
   const int i = ij % n, j = ij / n;
-  const int64_t e = (int64_t)blockIdx.x * EPB + le;
+  const int64_t e = bid * EPB + le;
   const bool ok = le < EPB && e < E;
   float *su = smem_af + (size_t)(ok ? le : 0) * S::US;                      // [3][P]
   float *sF = smem_af + (size_t)EPB * S::US + (size_t)(ok ? le : 0) * S::FS;  // [3][2][P]
@@ -212,6 +214,14 @@ elastic_hex_affine_kernel(int64_t E, const float *__restrict__ jac, const float 
       }
     }
   }
+}
+
+template <int N, int EPB_, bool TI, bool kFuse>
+__global__ void __launch_bounds__(HexAffineShape<N, EPB_, TI>::THREADS)
+elastic_hex_affine_kernel(int64_t E, const float *__restrict__ jac, const float *__restrict__ mat,
+                          const int32_t *__restrict__ conn, float *__restrict__ u,
+                          float *__restrict__ r, DMatrix<float> Dm, HexInteriorUpdate iu) {
+  elastic_hex_affine_body<N, EPB_, TI, kFuse>(blockIdx.x, E, jac, mat, conn, u, r, Dm, iu);
 }
 
 }  // namespace salvus

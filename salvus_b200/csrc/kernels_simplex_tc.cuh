@@ -190,7 +190,7 @@ template <int C>
 __global__ void __launch_bounds__(288, 1)
 tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restrict__ conn,
               const uint4 *__restrict__ table, const float *__restrict__ u, float *__restrict__ r,
-              int *__restrict__ err, long long wait_limit) {
+              int *__restrict__ err, long long wait_limit, int hold) {
   using S = TetTcShape<C>;
   constexpr int P = S::P, NE = S::NE, RW = S::RW;
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -201,6 +201,8 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
   // GEMM 2 sums read out (256)
   uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + S::OFF_BAR + 18 * 8);
   volatile int *flag = reinterpret_cast<volatile int *>(sm + S::OFF_BAR + 18 * 8 + 4);
+  // a barrier nothing arrives on (hold != 0: the timeout-path test)
+  uint64_t *never = reinterpret_cast<uint64_t *>(sm + S::OFF_BAR + 20 * 8);
   const uint32_t sbase = smem_addr(sm);
 
   for (int i = tid; i < (int)(S::TAB_BYTES / 16); i += S::THREADS)
@@ -214,6 +216,7 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     }
     mbar_init(&bar[16], 1);
     mbar_init(&bar[17], S::WORKERS);
+    mbar_init(never, 1);
     *flag = 0;
     fence_mbar_init();
   }
@@ -382,8 +385,11 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     // first flux chunk, which these same threads hand over afterwards).
     int64_t e_prev = 0;
     bool ok_prev = false, have_prev = false, clean = true;
+    // hold: wait first on a barrier nothing arrives on, so that the wait runs
+    // out after wait_limit cycles and the CTA takes its timeout path
+    if (hold && !wwait(never, 0u, 1099)) clean = false;
     uint32_t it = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    for (int64_t tile = blockIdx.x; clean && tile < ntiles; tile += gridDim.x, ++it) {
       const uint32_t par = it & 1;
       const int64_t e = tile * NE + slot;
       const bool ok = row_ok && e < E;

@@ -55,7 +55,7 @@ struct TriTcShape {
 __global__ void __launch_bounds__(160)
 tri_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restrict__ conn,
               const uint4 *__restrict__ table, const float *__restrict__ u, float *__restrict__ r,
-              int *__restrict__ err, long long wait_limit) {
+              int *__restrict__ err, long long wait_limit, int hold) {
   using S = TriTcShape;
   constexpr int P = S::P, NE = S::NE;
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -65,6 +65,8 @@ tri_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
   // bar[3] GEMM 2 done | bar[4] drain
   uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + S::OFF_BAR + 5 * 8);
   volatile int *flag = reinterpret_cast<volatile int *>(sm + S::OFF_BAR + 5 * 8 + 4);
+  // a barrier nothing arrives on (hold != 0: the timeout-path test)
+  uint64_t *never = reinterpret_cast<uint64_t *>(sm + S::OFF_BAR + 7 * 8);
   const uint32_t sbase = smem_addr(sm);
 
   for (int i = tid; i < (int)(S::TAB_BYTES / 16); i += S::THREADS)
@@ -75,6 +77,7 @@ tri_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     mbar_init(&bar[2], S::WORKERS);
     mbar_init(&bar[3], 1);
     mbar_init(&bar[4], 1);
+    mbar_init(never, 1);
     *flag = 0;
     fence_mbar_init();
   }
@@ -188,8 +191,11 @@ tri_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
       for (int j = 12; j < 16; ++j) uv[j] = 0.f;
     };
     load_tile(blockIdx.x);
+    // hold: wait first on a barrier nothing arrives on, so that the wait runs
+    // out after wait_limit cycles and the CTA takes its timeout path
+    const bool held = hold && !wwait(never, 0u, 1099);
     uint32_t it = 0;
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+    for (int64_t tile = blockIdx.x; !held && tile < ntiles; tile += gridDim.x, ++it) {
       const uint32_t par = it & 1;
       const int64_t e = tile * NE + row;
       const bool ok = e < E;

@@ -9,7 +9,7 @@
 //              jobs' kernels overlap on the device), then collects each
 //              chunk: streams the new seismogram samples to the host and
 //              retires finished jobs, freeing their device memory.
-//   workers    (up to 4) prepare admitted jobs (mesh flattening on the host,
+//   workers    (up to 8) prepare admitted jobs (mesh flattening on the host,
 //              device setup, sources, receivers) while the scheduler keeps
 //              running jobs busy.
 // Jobs never share device state, so a job's result does not depend on the
@@ -304,7 +304,7 @@ int salvus_server_create(int device, int64_t budget, int32_t max_running, int32_
   s->chunk = chunk;
   s->sched = std::thread(scheduler_loop, s);
   const unsigned hw = std::thread::hardware_concurrency();
-  const int nw = (int)std::max(1u, std::min(4u, hw / 2));
+  const int nw = (int)std::max(1u, std::min(8u, hw / 2));
   for (int w = 0; w < nw; ++w) s->workers.emplace_back(worker_loop, s);
   *out = s;
   return SALVUS_OK;

@@ -81,7 +81,9 @@ def test_group_member_blow_up_leaves_the_others_alone():
     probs[1].set_field("u", u)
     g = core.Group(probs)
     g.run(64)
-    g.synchronize()
+    with pytest.raises(core.SalvusError) as e:
+        g.synchronize()  # reports the members' status
+    assert e.value.code == core.E_NONFINITE
     probs[0].status()
     probs[2].status()
     with pytest.raises(core.SalvusError) as e:
@@ -97,8 +99,10 @@ def test_serving_fails_the_diverging_job_and_finishes_the_rest():
     ids = [srv.submit(c, 1.5e-3, 200) for c in good[:2]]
     jb = srv.submit(bad, 0.2, 2000)  # far beyond the stability limit of a 500 m mesh
     ids.append(srv.submit(good[2], 1.5e-3, 200))
-    for j in ids + [jb]:
+    for j in ids:
         srv.wait(j, 300)
+    with pytest.raises(core.SalvusError, match="non-finite"):
+        srv.wait(jb, 300)  # a failed job's wait returns its error
     st, done, _ = srv.poll(jb)
     assert st == serving.FAILED
     assert b"non-finite" in core.lib().salvus_last_error()

@@ -120,7 +120,7 @@ def test_batched_shots_200sq_256shots_2000_steps():
 def test_simplices_full_size_3000_steps(which):
     cfg = configs.simplex_tri() if which == "tri" else configs.simplex_tet(physics=core.ELASTIC3D)
     mesh = mesh_of(cfg)
-    dt = 0.4 * mesh.critical_dt(iterations=40)
+    dt = 0.4 * mesh.critical_dt(iterations=100)
     steps = 3000
     out = {}
     for prec in (core.FP32, core.FP64):

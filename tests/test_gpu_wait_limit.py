@@ -1,6 +1,8 @@
-"""Bounded device waits, exercised: a very short wait limit (one SM cycle)
-makes the hand-off waits of the tensor-core tetrahedron / triangle kernels
-and the member barriers of the partitioned group step give up.  The kernels
+"""Bounded device waits, exercised: the tensor-core tetrahedron / triangle
+kernels' worker warps are made to wait first on a barrier that nothing
+arrives on (salvus_problem_hold_device_waits) under a short wait limit, and
+a one-cycle limit makes the member barriers of the partitioned group step
+give up.  The kernels
 record the wait's code, return cleanly (the MMA issuer drains its own MMAs
 under the default bound before tensor memory is freed) and the host reports
 SALVUS_E_TIMEOUT.  After the status is cleared and the default limit is
@@ -51,7 +53,10 @@ def test_tensor_core_wait_gives_up_and_recovers(which, monkeypatch):
     ref.run(40, core.RUN_GRAPH)
     ref.status()
     p = core.Problem(mesh, core.FP32, dt=dt)
-    p.set_wait_limit(1)
+    # the workers first wait on a barrier nothing arrives on: every launch
+    # runs out of a ~2 ms wait limit and takes the timeout path
+    p.set_wait_limit(1 << 22)
+    p.hold_device_waits(True)
     start(p, u0)
     p.run(40, core.RUN_GRAPH)
     with pytest.raises(core.SalvusError) as e:
@@ -59,6 +64,7 @@ def test_tensor_core_wait_gives_up_and_recovers(which, monkeypatch):
     assert e.value.code == core.E_TIMEOUT
     assert "code 1" in str(e.value)  # wait codes 1000-1199
     p.status()  # cleared
+    p.hold_device_waits(False)
     p.set_wait_limit(0)
     start(p, u0)
     p.run(40, core.RUN_GRAPH)
