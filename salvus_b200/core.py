@@ -12,6 +12,7 @@ field dictionary live on the GPU, so they are not passed around), plus fused
 message, as the reference throws std::runtime_error.
 """
 import ctypes
+import weakref
 import os
 
 import numpy as np
@@ -176,6 +177,7 @@ class Mesh:
         h = _VP()
         _check(lib().salvus_mesh_create(ctypes.byref(d), device, ctypes.byref(h)))
         self.h = h
+        self._problems = weakref.WeakSet()
         G, c, P = _I64(), _I32(), _I32()
         _check(lib().salvus_mesh_info(self.h, ctypes.byref(G), ctypes.byref(c), ctypes.byref(P)))
         self.n_nodes, self.n_components, self.points_per_element = G.value, c.value, P.value
@@ -183,6 +185,10 @@ class Mesh:
         self.n_elements = self._c.shape[0]
 
     def close(self):
+        # problems on this mesh first (when both are found unreachable in a
+        # reference cycle, the collector may finalise the mesh first)
+        for p in list(getattr(self, "_problems", ())):
+            p.close()
         if getattr(self, "h", None):
             lib().salvus_mesh_destroy(self.h)
             self.h = None
@@ -250,6 +256,7 @@ class Problem:
         h = _VP()
         _check(lib().salvus_problem_create(mesh.h, precision, n_shots, ctypes.byref(h)))
         self.h = h
+        mesh._problems.add(self)
         self.n_shots = n_shots
         self.precision = precision
         self.c = mesh.n_components

@@ -1316,6 +1316,7 @@ struct salvus_group {
   int grid = 0;
   salvus::DeviceBuffer d_counts, d_work, d_done, d_sync;
   long long wait_limit = salvus::kDefaultWaitLimit;  // bound of the device waits, SM cycles
+  int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev = nullptr;
   std::vector<cudaEvent_t> member_ev;
@@ -1913,6 +1914,7 @@ int salvus_problem_create(salvus_mesh *m, int32_t precision, int32_t n_shots, sa
   SALVUS_CUDA(cudaSetDevice(m->device));
   std::unique_ptr<salvus_problem> p(new salvus_problem());
   p->mesh = m;
+  p->device = m->device;
   p->prec = precision;
   p->shots = n_shots;
   p->shots_pad = n_shots == 1 ? 1 : (n_shots + 31) / 32 * 32;
@@ -1942,7 +1944,8 @@ int salvus_problem_create(salvus_mesh *m, int32_t precision, int32_t n_shots, sa
 
 int salvus_problem_destroy(salvus_problem *p) {
   if (!p) return SALVUS_OK;
-  cudaSetDevice(p->mesh->device);
+  // the problem's own device: its mesh may already be gone
+  cudaSetDevice(p->device);
   cudaStreamSynchronize(p->stream);
   drop_graph(p);
   for (auto &e : p->events) {
@@ -2562,6 +2565,7 @@ int salvus_group_create(salvus_problem *const *members, int32_t n, salvus_group 
   std::unique_ptr<salvus_group> g(new salvus_group());
   g->members.assign(members, members + n);
   g->m0 = m0;
+  g->device = m0->device;
   g->c = m0->physics == SALVUS_ELASTIC3D ? 3 : 1;
   {
     // measured: one launch per stage beats both single-launch forms (the
@@ -2669,7 +2673,8 @@ cudaStream_t salvus_group_stream_internal(const salvus_group *g) { return g ? g-
 
 int salvus_group_destroy(salvus_group *g) {
   if (!g) return SALVUS_OK;
-  cudaSetDevice(g->m0->device);
+  // the group's own device: its members' meshes may already be gone
+  cudaSetDevice(g->device);
   if (g->stream) cudaStreamSynchronize(g->stream);
   if (g->graph) cudaGraphExecDestroy(g->graph);
   for (auto e : g->member_ev)

@@ -138,6 +138,7 @@ struct salvus_mesh {
 
 struct salvus_problem {
   salvus_mesh *mesh = nullptr;
+  int device = 0;  // the mesh's device, kept for teardown after the mesh is gone
   int prec = SALVUS_FP32;
   int shots = 1;
   int c = 1;

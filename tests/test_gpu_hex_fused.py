@@ -131,8 +131,13 @@ def distorted_hex(nel=4, order=3, seed=9):
     inner = np.all((V > 0.5 * h) & (V < cfg["L"] - 0.5 * h), axis=1)
     V[inner] += np.random.default_rng(seed).uniform(-0.15 * h, 0.15 * h, size=(inner.sum(), 3))
     cfg["vertices"] = V
-    # receivers a little below the top surface, inside the top elements
-    cfg["receivers"] = [(x, y, cfg["L"] - 0.3 * h) for x, y, _ in cfg["receivers"]]
+    # source and receivers at cell centres: on distorted hexahedra a point
+    # close to a face can fall outside both neighbours' hull tests (the
+    # reference's HexP1::checkHull, HexP1.cpp:8-84, restated)
+    L = cfg["L"]
+    cfg["sources"][0]["location"] = (L / 2 + 0.5 * h, L / 2 - 0.5 * h, L / 2 + 0.5 * h)
+    cfg["receivers"] = [((i + 0.5) * h, (j + 0.5) * h, L - 0.5 * h)
+                        for i, j in ((0, 1), (1, 3), (2, 0), (3, 2), (1, 1), (2, 2))]
     return cfg
 
 
