@@ -154,13 +154,14 @@ static int launch_elastic_affine(const salvus_mesh *m, const float *mat, float *
                                  cudaStream_t st, const HexInteriorUpdate &iu) {
   constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
   using T = HexAffineShape<N, EPB, TI>;
+  auto kern = kFuse ? elastic_hex_affine_fused_kernel<N, EPB, TI>
+                    : elastic_hex_affine_kernel<N, EPB, TI>;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(elastic_hex_affine_kernel<N, EPB, TI, kFuse>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
     attr = true;
   }
-  elastic_hex_affine_kernel<N, EPB, TI, kFuse><<<blocks_for(m->E, EPB), T::THREADS, T::SMEM, st>>>(
+  kern<<<blocks_for(m->E, EPB), T::THREADS, T::SMEM, st>>>(
       m->E, m->d_jac32.as<float>(), mat, m->d_conn.as<int32_t>(), u, r, dmatrix<float>(m->basis),
       iu);
   g_launches++;
@@ -690,7 +691,17 @@ static int upload_sources(salvus_problem *p) {
                                 cudaMemcpyHostToDevice, p->stream));
     SALVUS_CUDA(cudaMemcpyAsync(p->d_src_wts.ptr, w.data(), sizeof(double) * w.size(),
                                 cudaMemcpyHostToDevice, p->stream));
+    // distinct source elements, first appearance order (fused hexahedron step)
+    std::vector<int64_t> ue;
+    for (int64_t x : el)
+      if (std::find(ue.begin(), ue.end(), x) == ue.end()) ue.push_back(x);
+    if ((rc = p->d_src_uelem.alloc(sizeof(int64_t) * ue.size()))) return rc;
+    SALVUS_CUDA(cudaMemcpyAsync(p->d_src_uelem.ptr, ue.data(), sizeof(int64_t) * ue.size(),
+                                cudaMemcpyHostToDevice, p->stream));
+    p->n_src_uelem = (int)ue.size();
     SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  } else {
+    p->n_src_uelem = 0;
   }
   p->src_dirty = false;
   return SALVUS_OK;
@@ -824,18 +835,34 @@ static int step_fused_hex_interior(salvus_problem *p) {
     iu.v = F<float>(p->d_v);
     iu.ap = F<float>(p->d_ap);
     iu.dt = (float)p->dt;
-    iu.dtd = p->dt;
-    iu.nsrc = (int)p->srcs.size();
-    iu.src_elem = p->d_src_elem.as<int64_t>();
-    iu.src_par = p->d_src_par.as<double>();
-    iu.src_wts = p->d_src_wts.as<double>();
-    iu.step = p->d_step.as<int64_t>();
+    iu.nsrc_elem = p->n_src_uelem;
+    iu.src_elem = p->d_src_uelem.as<int64_t>();
     if ((rc = m->ti ? launch_fused_interior<true>(p, iu) : launch_fused_interior<false>(p, iu)))
       return rc;
   }
-  // the source kernel still adds into every point of its element; the
-  // interior ones were consumed above and are not gathered
-  if ((rc = launch_sources<float, 3>(p))) return rc;
+  // sources, then the source elements' interior nodes
+  if (!p->srcs.empty()) {
+    ProfScope ps(p, K_SRC);
+    auto go = [&](auto nt) {
+      constexpr int N = decltype(nt)::value;
+      source_fused_hex_kernel<N><<<1, 256, 0, p->stream>>>(
+          (int)p->srcs.size(), m->P, p->d_src_elem.as<int64_t>(), p->d_src_par.as<double>(),
+          p->d_src_wts.as<double>(), p->d_step.as<int64_t>(), p->dt, F<float>(p->d_r),
+          p->n_src_uelem, p->d_src_uelem.as<int64_t>(), m->d_conn.as<int32_t>(),
+          m->d_mi32.as<float>(), F<float>(p->d_u), F<float>(p->d_v), F<float>(p->d_ap),
+          (float)p->dt);
+    };
+    switch (m->order) {
+      case 2: go(std::integral_constant<int, 2>{}); break;
+      case 3: go(std::integral_constant<int, 3>{}); break;
+      case 4: go(std::integral_constant<int, 4>{}); break;
+      case 5: go(std::integral_constant<int, 5>{}); break;
+      case 6: go(std::integral_constant<int, 6>{}); break;
+      default: return fail(SALVUS_E_UNSUPPORTED, "fused hexahedron step: order %d", m->order);
+    }
+    g_launches++;
+    if ((rc = check_launch("source (fused step)"))) return rc;
+  }
   {
     ProfScope ps(p, K_UPDATE);
     gather_list_kernel<float, 3, 0><<<blocks_for(m->n_gnodes, 256), 256, 0, p->stream>>>(
@@ -908,12 +935,8 @@ static void launch_qb(const salvus_problem *p, cudaStream_t st, bool fuse) {
     bi.mi = m->d_mi32.as<float>();
     bi.w = F<float>(p->d_v);
     bi.dt = (float)p->dt;
-    bi.dtd = p->dt;
     bi.shot_off = p->srcs.empty() ? nullptr : p->d_shot_off.as<int32_t>();
     bi.src_elem = p->d_src_elem.as<int64_t>();
-    bi.src_par = p->d_src_par.as<double>();
-    bi.src_wts = p->d_src_wts.as<double>();
-    bi.step = p->d_step.as<int64_t>();
     quad_acoustic_batched_kernel<N, SC, EPC, true><<<grid, SC * EPC, 0, st>>>(
         m->E, p->shots_pad, m->d_rec32.as<float>(), F<float>(p->d_u), F<float>(p->d_r),
         dmatrix<float>(m->basis), bi);
@@ -1081,10 +1104,13 @@ static int step_batched(salvus_problem *p) {
   if (!p->srcs.empty()) {
     ProfScope ps(p, K_SRC);
     const int threads = 256, total = p->shots_pad * m->P;
+    // fused step: the source elements' interior nodes are finished here
+    const bool fuse = batch_fusion(p) && m->order >= 2;
     batched_source_kernel<<<(total + threads - 1) / threads, threads, 0, p->stream>>>(
         p->shots_pad, m->P, p->d_shot_off.as<int32_t>(), p->d_src_elem.as<int64_t>(),
         p->d_src_par.as<double>(), p->d_src_wts.as<double>(), p->d_step.as<int64_t>(), p->dt,
-        F<float>(p->d_r));
+        F<float>(p->d_r), fuse ? m->n : 0, m->d_conn.as<int32_t>(), m->d_mi32.as<float>(),
+        F<float>(p->d_u), F<float>(p->d_v), (float)p->dt);
     g_launches++;
     if ((rc = check_launch("batched sources"))) return rc;
   }

@@ -170,6 +170,8 @@ struct salvus_problem {
   };
   std::vector<Src> srcs;
   salvus::DeviceBuffer d_src_elem, d_src_par, d_src_wts;
+  salvus::DeviceBuffer d_src_uelem;  // distinct source elements (fused hexahedron step)
+  int n_src_uelem = 0;
   bool src_dirty = true;
   // receivers
   struct Rec {

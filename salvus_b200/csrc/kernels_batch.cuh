@@ -18,22 +18,20 @@ namespace salvus {
 
 // Interior-node update of the fused batched step (kFuse): the points with
 // both local indices in 1..N-1 are nodes of this element alone, so the
-// stiffness thread of (element, shot) finishes them -- the shot's sources in
-// attach order (batched_source_kernel's arithmetic), the one-term assembly
+// stiffness thread of (element, shot) finishes them -- the one-term assembly
 // 0 + r, the inverse mass and the half-step-velocity update
 // (batched_gather_update_kernel's arithmetic) -- and writes residuals only
-// for the element's edge points.  Same operations in the same order as the
-// unfused sequence, so both forms give bitwise the same wavefields.
+// for the element's edge points.  Where the shot has a source in the element
+// the interior residuals are written too, and batched_source_kernel adds the
+// source terms and then finishes those nodes.  Same operations in the same
+// order as the unfused sequence, so both forms give bitwise the same
+// wavefields.
 struct BatchInterior {
   const float *mi;
   float *w;
   float dt;
-  double dtd;
-  const int32_t *shot_off;
+  const int32_t *shot_off;  // sources of shot s: [shot_off[s], shot_off[s + 1])
   const int64_t *src_elem;
-  const double *src_par;  // [k][3] f0 t0 amp
-  const double *src_wts;  // [k][P]
-  const int64_t *step;
 };
 
 // half-step-velocity update of one node (one shot): w += dt a; u += dt w,
@@ -73,6 +71,25 @@ quad_acoustic_batched_kernel(int64_t E, int S, const float *__restrict__ rec,
     const float *up = u + (int64_t)__float_as_int(g[p].w) * S + s;
     uu[p] = kFuse ? *up : __ldg(up);
   }
+  // fused form: whether one of this shot's sources sits in this element (then
+  // the unfused form for its interior points), and the interior nodes' w,
+  // loaded before the arithmetic so that their latency overlaps it (w is
+  // written below; the read-only inverse mass is read where it is used)
+  bool fuse_here = kFuse;
+  float wpre[P];
+  if constexpr (kFuse) {
+    if (bi.shot_off)
+      for (int k = bi.shot_off[s]; k < bi.shot_off[s + 1] && fuse_here; ++k)
+        fuse_here = __ldg(bi.src_elem + k) != e;
+    if (fuse_here) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        const int i = p % n, j = p / n;
+        if (i < 1 || i > n - 2 || j < 1 || j > n - 2) continue;
+        wpre[p] = bi.w[(int64_t)__float_as_int(g[p].w) * S + s];
+      }
+    }
+  }
   float Fr[P], Fs[P];
 #pragma unroll
   for (int p = 0; p < P; ++p) {
@@ -97,25 +114,14 @@ quad_acoustic_batched_kernel(int64_t E, int S, const float *__restrict__ rec,
       o += Dm.d[l * n + i] * Fr[l + n * j];
       o += Dm.d[l * n + j] * Fs[i + n * l];
     }
-    if (!kFuse || i < 1 || i > n - 2 || j < 1 || j > n - 2) {
+    if (!fuse_here || i < 1 || i > n - 2 || j < 1 || j > n - 2) {
       out[(int64_t)p * S] = -o;
       continue;
     }
     if constexpr (kFuse) {
-      float rv = -o;
-      const int k0 = bi.shot_off ? bi.shot_off[s] : 0, k1 = bi.shot_off ? bi.shot_off[s + 1] : 0;
-      if (k1 > k0) {
-        const double t = (double)(*bi.step) * bi.dtd;
-        for (int k = k0; k < k1; ++k) {
-          if (bi.src_elem[k] != e) continue;
-          const double stf = ricker_dev(t, bi.src_par[3 * k], bi.src_par[3 * k + 1],
-                                        bi.src_par[3 * k + 2]);
-          rv += (float)(bi.src_wts[(int64_t)k * P + p] * stf);
-        }
-      }
       const int64_t x = (int64_t)__float_as_int(g[p].w) * S + s;
-      float wv = bi.w[x], uv = uu[p];
-      half_step_update(__fadd_rn(0.f, rv), __ldg(bi.mi + __float_as_int(g[p].w)), bi.dt, wv, uv);
+      float wv = wpre[p], uv = uu[p];
+      half_step_update(__fadd_rn(0.f, -o), __ldg(bi.mi + __float_as_int(g[p].w)), bi.dt, wv, uv);
       bi.w[x] = wv;
       u[x] = uv;
     }
@@ -123,13 +129,21 @@ quad_acoustic_batched_kernel(int64_t E, int S, const float *__restrict__ rec,
 }
 
 // Ricker sources of every shot into the element-local residual.  Thread =
-// (shot, point); a shot's sources are applied in attach order.
+// (shot, point); a shot's sources are applied in attach order.  Fused step
+// (n > 0, the element's points per line): afterwards the thread of an
+// interior point finishes that node of each distinct source element of its
+// shot -- the node the fused stiffness kernel left to it -- with the
+// gather's arithmetic (one-term assembly 0 + r, inverse mass, update).
 __global__ void batched_source_kernel(int S, int P, const int32_t *__restrict__ shot_off,
                                       const int64_t *__restrict__ elem,
                                       const double *__restrict__ par,
                                       const double *__restrict__ wts,
                                       const int64_t *__restrict__ step, double dt,
-                                      float *__restrict__ r) {
+                                      float *__restrict__ r, int n = 0,
+                                      const int32_t *__restrict__ conn = nullptr,
+                                      const float *__restrict__ mi = nullptr,
+                                      float *__restrict__ u = nullptr,
+                                      float *__restrict__ w = nullptr, float dtf = 0.f) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= S * P) return;
   const int p = q % P, s = q / P;
@@ -137,6 +151,21 @@ __global__ void batched_source_kernel(int S, int P, const int32_t *__restrict__ 
   for (int k = shot_off[s]; k < shot_off[s + 1]; ++k) {
     const double stf = ricker_dev(t, par[3 * k], par[3 * k + 1], par[3 * k + 2]);
     r[(elem[k] * P + p) * S + s] += (float)(wts[(int64_t)k * P + p] * stf);
+  }
+  if (n == 0) return;
+  const int i = p % n, j = p / n;
+  if (i < 1 || i > n - 2 || j < 1 || j > n - 2) return;
+  for (int k = shot_off[s]; k < shot_off[s + 1]; ++k) {
+    bool first = true;  // each distinct source element once
+    for (int k2 = shot_off[s]; k2 < k && first; ++k2) first = elem[k2] != elem[k];
+    if (!first) continue;
+    const int64_t e = elem[k];
+    const int32_t node = conn[e * P + p];
+    const int64_t x = (int64_t)node * S + s;
+    float wv = w[x], uv = u[x];
+    half_step_update(__fadd_rn(0.f, r[(e * P + p) * S + s]), mi[node], dtf, wv, uv);
+    w[x] = wv;
+    u[x] = uv;
   }
 }
 

@@ -13,12 +13,13 @@
 //
 // Fused step form (kFuse): the interior GLL points of an element (all three
 // local indices in 1..N-1) are nodes that no other element touches, so the
-// kernel finishes them itself -- the source terms of this element in attach
-// order (source_body's arithmetic), the one-term assembly 0 + r (the node
+// kernel finishes them itself -- the one-term assembly 0 + r (the node
 // gather's first addition), the inverse mass and the Newmark update
 // (newmark_point) -- and writes element-local residuals only for the points
 // on the element's faces, which the node gather then assembles over the
-// shared nodes alone.  Every operation and its order is the one of the
+// shared nodes alone.  In the few elements that hold a source the interior
+// residuals are written too; the source kernel adds the source terms in
+// attach order and then finishes those nodes (source_interior_body).  Every operation and its order is the one of the
 // unfused sequence (stiffness, sources, gather, update), so the two forms
 // give bitwise the same wavefield.  In the fused form u is written for
 // interior nodes during the launch, so u is read with coherent loads (the
@@ -34,18 +35,15 @@
 
 namespace salvus {
 
-// Interior-node update of the fused step: Newmark state, inverse mass and the
-// problem's sources (kernels_step.cuh source_body layout).
+// Interior-node update of the fused step: Newmark state, inverse mass, and
+// the elements that hold a source (their interior nodes are finished by the
+// source kernel after the source terms are added: source_interior_body).
 struct HexInteriorUpdate {
   const float *mi;
   float *v, *ap;
   float dt;
-  double dtd;
-  int nsrc;
-  const int64_t *src_elem;
-  const double *src_par;  // [nsrc][3] f0 t0 amp
-  const double *src_wts;  // [nsrc][P][3]
-  const int64_t *step;
+  int nsrc_elem;
+  const int64_t *src_elem;  // distinct source elements
 };
 
 template <int N, int EPB_, bool TI>
@@ -163,8 +161,32 @@ __device__ __forceinline__ void elastic_hex_affine_body(
   if (!ok) return;
   // interior column: both in-plane indices strictly inside the element
   const bool icol = kFuse && i >= 1 && i <= n - 2 && j >= 1 && j <= n - 2;
-  double t_now = 0;
-  if (icol && iu.nsrc > 0) t_now = (double)(*iu.step) * iu.dtd;
+  // Elements holding a source keep the unfused form for their interior
+  // points (residuals written; the source kernel adds the source terms and
+  // finishes those nodes).  For the others, the interior operands (v, a_)
+  // are loaded here, before the divergence, so that their latency overlaps
+  // it (after the stores below the compiler could not reorder them: the
+  // pointers may alias as far as it knows).
+  bool fuse_here = icol;
+  if constexpr (kFuse) {
+    for (int s = 0; s < iu.nsrc_elem && fuse_here; ++s) fuse_here = __ldg(iu.src_elem + s) != e;
+  }
+  float vpre[n][3], apre[n][3];
+  if constexpr (kFuse) {
+    if (fuse_here) {
+      const float *__restrict__ vv = iu.v;
+      const float *__restrict__ aa = iu.ap;
+#pragma unroll
+      for (int k = 1; k < n - 1; ++k) {
+        const int64_t g = node[k];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          vpre[k][c] = vv[g * 3 + c];
+          apre[k][c] = aa[g * 3 + c];
+        }
+      }
+    }
+  }
 #pragma unroll
   for (int k = 0; k < n; ++k) {
     const int p = ij + n2 * k;
@@ -182,30 +204,21 @@ __device__ __forceinline__ void elastic_hex_affine_body(
       }
       o[c] = -acc;
     }
-    const bool interior = icol && k >= 1 && k <= n - 2;
+    const bool interior = fuse_here && k >= 1 && k <= n - 2;
     if (!interior) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) r[(e * P + p) * 3 + c] = o[c];
       continue;
     }
     if constexpr (kFuse) {
-      // sources of this element in attach order (source_body)
-      for (int s = 0; s < iu.nsrc; ++s) {
-        if (iu.src_elem[s] != e) continue;
-        const double stf = ricker_dev(t_now, iu.src_par[3 * s], iu.src_par[3 * s + 1],
-                                      iu.src_par[3 * s + 2]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          o[c] += (float)(iu.src_wts[((int64_t)s * P + p) * 3 + c] * stf);
-      }
       // assembly (one incident point: 0 + r), inverse mass, Newmark
       const int64_t g = node[k];
-      const float mm = iu.mi[g];
+      const float mm = __ldg(iu.mi + g);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         const int64_t x = g * 3 + c;
         float uo = c == 0 ? ux[k] : (c == 1 ? uy[k] : uz[k]);
-        float vo = iu.v[x], apo = iu.ap[x];
+        float vo = vpre[k][c], apo = apre[k][c];
         const float acc = add_rn(0.f, o[c]);
         newmark_point<float>(mul_rn(acc, mm), apo, vo, uo, iu.dt);
         u[x] = uo;
@@ -216,12 +229,56 @@ __device__ __forceinline__ void elastic_hex_affine_body(
   }
 }
 
-template <int N, int EPB_, bool TI, bool kFuse>
+// Source kernel of the fused step (one CTA): the source terms in attach
+// order into the element-local residual (source_body), then the interior
+// nodes of the distinct source elements -- which the fused stiffness kernel
+// left to it -- with the one-term assembly 0 + r, the inverse mass and the
+// Newmark update: the arithmetic of the node gather, so the result is the
+// unfused sequence's.
+template <int N>
+__global__ void source_fused_hex_kernel(int nsrc, int P, const int64_t *__restrict__ elem,
+                                       const double *__restrict__ par,
+                                       const double *__restrict__ wts,
+                                       const int64_t *__restrict__ step, double dtd,
+                                       float *__restrict__ r, int nse,
+                                       const int64_t *__restrict__ src_elems,
+                                       const int32_t *__restrict__ conn,
+                                       const float *__restrict__ mi, float *__restrict__ u,
+                                       float *__restrict__ v, float *__restrict__ ap, float dt) {
+  source_body<float, 3>(nsrc, P, elem, par, wts, step, dtd, r);  // ends with __syncthreads
+  constexpr int n = N + 1, m = N - 1, NI = m * m * m;
+  for (int t = threadIdx.x; t < nse * NI * 3; t += blockDim.x) {
+    const int se = t / (NI * 3), rem = t - se * NI * 3, q = rem / 3, c = rem - q * 3;
+    const int i = 1 + q % m, j = 1 + (q / m) % m, k = 1 + q / (m * m);
+    const int64_t e = src_elems[se];
+    const int pt = i + n * j + n * n * k;
+    const int64_t g = conn[e * P + pt], x = g * 3 + c;
+    float uo = u[x], vo = v[x], apo = ap[x];
+    newmark_point<float>(mul_rn(add_rn(0.f, r[(e * P + pt) * 3 + c]), mi[g]), apo, vo, uo, dt);
+    u[x] = uo;
+    v[x] = vo;
+    ap[x] = apo;
+  }
+}
+
+template <int N, int EPB_, bool TI>
 __global__ void __launch_bounds__(HexAffineShape<N, EPB_, TI>::THREADS)
 elastic_hex_affine_kernel(int64_t E, const float *__restrict__ jac, const float *__restrict__ mat,
                           const int32_t *__restrict__ conn, float *__restrict__ u,
                           float *__restrict__ r, DMatrix<float> Dm, HexInteriorUpdate iu) {
-  elastic_hex_affine_body<N, EPB_, TI, kFuse>(blockIdx.x, E, jac, mat, conn, u, r, Dm, iu);
+  elastic_hex_affine_body<N, EPB_, TI, false>(blockIdx.x, E, jac, mat, conn, u, r, Dm, iu);
+}
+
+// The fused form asks for kFuseMinBlocks resident CTAs per SM (a register
+// cap): its interior-update registers would otherwise cost two CTAs per SM.
+constexpr int kFuseMinBlocks = 6;
+template <int N, int EPB_, bool TI>
+__global__ void __launch_bounds__(HexAffineShape<N, EPB_, TI>::THREADS, kFuseMinBlocks)
+elastic_hex_affine_fused_kernel(int64_t E, const float *__restrict__ jac,
+                                const float *__restrict__ mat, const int32_t *__restrict__ conn,
+                                float *__restrict__ u, float *__restrict__ r, DMatrix<float> Dm,
+                                HexInteriorUpdate iu) {
+  elastic_hex_affine_body<N, EPB_, TI, true>(blockIdx.x, E, jac, mat, conn, u, r, Dm, iu);
 }
 
 }  // namespace salvus

@@ -118,7 +118,20 @@ def test_batched_shots_200sq_256shots_2000_steps():
 
 @pytest.mark.parametrize("which", ["tri", "tet"])
 def test_simplices_full_size_3000_steps(which):
+    """3000 steps at 0.4 dt_crit cover 0.62 s (triangles) / 0.67 s
+    (tetrahedra) of a 1 Hz Ricker with t0 = 1.2 s.  The triangle receivers
+    (3 km ring) see the arriving wave; the tetrahedron workload's surface
+    receivers, 5 km above the source, do not yet (their traces are the
+    pre-arrival numerical floor, ~1e-12 against ~1e-7 near the source), so
+    the tetrahedron check uses 8 more receivers on a 1.5 km ring around the
+    source and logs the surface traces' error separately."""
     cfg = configs.simplex_tri() if which == "tri" else configs.simplex_tet(physics=core.ELASTIC3D)
+    near = []
+    if which == "tet":
+        c = cfg["sources"][0]["location"]
+        near = [(c[0] + 1500 * np.cos(a), c[1] + 1500 * np.sin(a), c[2])
+                for a in np.linspace(0, 2 * np.pi, 8, endpoint=False)]
+        cfg = dict(cfg, receivers=list(cfg["receivers"]) + near)
     mesh = mesh_of(cfg)
     dt = 0.4 * mesh.critical_dt(iterations=100)
     steps = 3000
@@ -130,9 +143,17 @@ def test_simplices_full_size_3000_steps(which):
         p.run(steps, core.RUN_GRAPH)
         out[prec] = p.seismograms(0, steps)
         p.close()
-    err = rel_l2(out[core.FP32], out[core.FP64])
+    R = len(cfg["receivers"]) - len(near)
+    err = rel_l2(out[core.FP32][R:] if near else out[core.FP32],
+                 out[core.FP64][R:] if near else out[core.FP64])
+    extra = {}
+    if near:
+        extra = dict(receivers="8 on a 1.5 km ring around the source",
+                     rel_l2_surface_receivers=rel_l2(out[core.FP32][:R], out[core.FP64][:R]),
+                     surface_amplitude=float(np.abs(out[core.FP64][:R]).max()),
+                     near_amplitude=float(np.abs(out[core.FP64][R:]).max()))
     log(f"P3 {'triangles' if which == 'tri' else 'elastic tetrahedra'} "
         f"{mesh.n_elements} elements (Delaunay), 3000 steps", precision="fp32",
-        reference="FP64 GPU on the same mesh", rel_l2=err, dt=dt)
+        reference="FP64 GPU on the same mesh", rel_l2=err, dt=dt, **extra)
     assert np.abs(out[core.FP64]).max() > 0
     assert err <= TOL32
