@@ -641,8 +641,9 @@ def main():
 
     E, P = mesh.n_elements, mesh.points_per_element
     affine, n_gather = mesh.layout()
-    n_int = G - n_gather  # element-interior nodes advanced in the stiffness kernel
-    if affine:
+    fused = affine and os.environ.get("SALVUS_HEX_STEP") == "fused"
+    n_int = G - n_gather  # element-interior nodes (advanced in the stiffness kernel when fused)
+    if fused:
         # parallelepiped layout, fused step: per point conn 4 B + lambda' mu'
         # 8 B; per element invJ 36 B; u read 12 B/node; residual write
         # 12 B/point for the points on element faces; interior nodes: inverse
@@ -653,6 +654,13 @@ def main():
         # read and write 72 B per node
         b_upd = n_gather * 8 + (E * P - n_int) * 16 + n_gather * 76
         layout = "per-element inverse Jacobian, interior nodes advanced in the stiffness kernel"
+    elif affine:
+        # parallelepiped layout (default): per point conn 4 B + lambda' mu'
+        # 8 B; per element invJ 36 B; u read 12 B/node; the element-local
+        # residual write 12 B/point
+        b_stiff = E * P * 12 + E * 36 + G * 12 + E * P * 12
+        b_upd = E * P * 16 + G * (4 + 72 + 4)
+        layout = "per-element inverse Jacobian (parallelepiped elements)"
     else:
         # per-point records: 48 B (invJ 9, lambda', mu', conn) + u read
         # 12 B/node + the element-local residual write 12 B/point

@@ -94,9 +94,10 @@ enum salvus_run_mode { SALVUS_RUN_PLAIN = 0, SALVUS_RUN_GRAPH = 1 };
 /* salvus_mesh_desc.flags: keep per-point inverse Jacobians for elastic
  * hexahedra even when every element is a parallelepiped.  By default such
  * meshes store one inverse Jacobian per element and FP32 records of the
- * material alone (12 instead of 48 bytes per point with the connectivity),
- * and the fused FP32 step advances each element's interior nodes inside the
- * stiffness kernel. */
+ * material alone (12 instead of 48 bytes per point with the connectivity);
+ * with SALVUS_HEX_STEP=fused in the environment the FP32 step also advances
+ * each element's interior nodes inside the stiffness kernel (bitwise the
+ * same result; measured slower on the order-4 benchmark mesh). */
 #define SALVUS_MESH_PER_POINT_GEOMETRY 4
 
 typedef struct {
@@ -167,7 +168,8 @@ int salvus_mesh_info(const salvus_mesh *mesh, int64_t *n_nodes, int32_t *n_compo
  * = 1 when every element is a parallelepiped and one inverse Jacobian per
  * element is kept (elastic hexahedra, SALVUS_MESH_PER_POINT_GEOMETRY unset);
  * *gathered_nodes = the nodes the fused FP32 step assembles by node gather
- * (all G unless the interior nodes are advanced in the stiffness kernel).
+ * when it advances the interior nodes in the stiffness kernel (fused
+ * hexahedron step, fused shot-batched step), all G otherwise.
  * Either pointer may be NULL. */
 int salvus_mesh_layout(const salvus_mesh *mesh, int32_t *per_element_jacobian,
                        int64_t *gathered_nodes);

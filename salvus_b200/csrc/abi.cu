@@ -797,9 +797,12 @@ static const real *inv_mass(const salvus_problem *p) {
 
 // The fused FP32 step of parallelepiped elastic hexahedra advances the
 // element-interior nodes inside the stiffness kernel and gathers the rest
-// (kernels_hex_affine.cuh).  Used when the problem has no Dirichlet points
-// and at most kFuseMaxSources sources (each interior thread scans them);
-// SALVUS_HEX_STEP=unfused selects the plain sequence (read at every step).
+// (kernels_hex_affine.cuh).  Measured on the 64^3 order-4 workload it is
+// slower than the plain sequence on the same records (0.97 against 0.80 ms
+// per step: the interior update costs the stiffness kernel more than the
+// shorter gather saves), so it runs only with SALVUS_HEX_STEP=fused (read at
+// every step), for problems without Dirichlet points and with at most
+// kFuseMaxSources sources (each interior column scans their elements).
 constexpr int kFuseMaxSources = 16;
 static bool hex_interior_fusion(const salvus_problem *p) {
   const salvus_mesh *m = p->mesh;
@@ -807,7 +810,7 @@ static bool hex_interior_fusion(const salvus_problem *p) {
         p->n_dir_pts == 0 && (int)p->srcs.size() <= kFuseMaxSources))
     return false;
   const char *s = std::getenv("SALVUS_HEX_STEP");
-  return !(s && std::strcmp(s, "unfused") == 0);
+  return s && std::strcmp(s, "fused") == 0;
 }
 
 template <bool TI>

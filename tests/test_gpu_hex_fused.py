@@ -1,14 +1,16 @@
 """The FP32 step of elastic hexahedra that are all parallelepipeds.
 
 Such meshes keep one inverse Jacobian per element and per-point material
-records only, and the fused step advances each element's interior nodes in
-the stiffness kernel (sources, one-term assembly, inverse mass, Newmark)
-while the node gather handles the shared nodes.  Checked here:
-  * fused step == three-call sequence == graph replay, bitwise (the interior
-    arithmetic repeats the unfused order exactly), also with a source inside
-    an element's interior and with more sources than the fused kernel scans
-    (the plain sequence then runs);
-  * the fused step == SALVUS_HEX_STEP=unfused, bitwise;
+records only.  The fused step (SALVUS_HEX_STEP=fused; measured slower than
+the default plain sequence on these records, kept as an option) advances
+each element's interior nodes in the stiffness kernel (one-term assembly,
+inverse mass, Newmark; elements holding a source are finished by the source
+kernel) while the node gather handles the shared nodes.  Checked here:
+  * both step forms == three-call sequence == graph replay, bitwise (the
+    interior arithmetic repeats the unfused order exactly), also with
+    sources inside an element and with more sources than the fused kernel
+    scans (the plain sequence then runs);
+  * the fused step == the default step, bitwise;
   * parallelepiped records against per-point records
     (SALVUS_MESH_PER_POINT_GEOMETRY): same physics, FP32 rounding only;
   * a mesh of distorted hexahedra (per-point records, the column kernel)
@@ -59,8 +61,15 @@ def assert_same(a, b):
         assert np.array_equal(x, y)
 
 
+@pytest.fixture(params=["default", "fused"])
+def step_form(request, monkeypatch):
+    if request.param == "fused":
+        monkeypatch.setenv("SALVUS_HEX_STEP", "fused")
+    return request.param
+
+
 @pytest.mark.parametrize("order", [2, 4, 6])
-def test_fused_equals_three_call_and_graph(order):
+def test_fused_equals_three_call_and_graph(order, step_form):
     cfg = configs.elastic_hex(nel=3, order=order, n_receivers=6)
     n = 70
     m = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
@@ -76,7 +85,7 @@ def test_fused_equals_three_call_and_graph(order):
     assert_same(pa, pc)
 
 
-def test_source_inside_an_element_interior():
+def test_source_inside_an_element_interior(step_form):
     """A force at an interior GLL point's neighbourhood: the source element's
     interior nodes get their source terms in the stiffness kernel."""
     cfg = configs.elastic_hex(nel=3, order=4, n_receivers=4)
@@ -91,7 +100,7 @@ def test_source_inside_an_element_interior():
     assert_same(pa, pb)
 
 
-def test_many_sources_run_the_plain_sequence():
+def test_many_sources_run_the_plain_sequence(step_form):
     cfg = configs.elastic_hex(nel=3, order=4, n_receivers=4)
     rng = np.random.default_rng(3)
     src = [dict(location=tuple(rng.uniform(0.1, 0.9, 3) * cfg["L"]), center_freq=1.5,
@@ -103,11 +112,11 @@ def test_many_sources_run_the_plain_sequence():
     assert_same(pa, pb)
 
 
-def test_unfused_switch_is_bitwise_equal(monkeypatch):
+def test_fused_switch_is_bitwise_equal(monkeypatch):
     cfg = configs.elastic_hex(nel=4, order=4, n_receivers=4)
     pa = problem(cfg)
     pa.run(60, core.RUN_PLAIN)
-    monkeypatch.setenv("SALVUS_HEX_STEP", "unfused")
+    monkeypatch.setenv("SALVUS_HEX_STEP", "fused")
     pb = problem(cfg)
     pb.run(60, core.RUN_PLAIN)
     assert_same(pa, pb)
