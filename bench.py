@@ -58,10 +58,15 @@ def parse():
                     help="tetrahedral mesh cells per side (Delaunay of a jittered BCC point "
                          "set, ~12 n^3 elements; 44 -> ~1.02M)")
     ap.add_argument("--serving-jobs", type=int, default=24)
+    ap.add_argument("--serving-max-running", type=int, default=16,
+                    help="serving leg: jobs admitted at once (running or being prepared)")
     ap.add_argument("--serving-only", action="store_true",
                     help="run only the serving leg (e.g. --serving-jobs 500) and print its JSON")
     ap.add_argument("--profile-only", action="store_true",
                     help="run a few steps only (for ncu captures); prints no JSON")
+    ap.add_argument("--per-point-geometry", action="store_true",
+                    help="build the hexahedron mesh with per-point geometry records "
+                         "(profiling the general layout with --profile-only)")
     return ap.parse_args()
 
 
@@ -386,13 +391,42 @@ def unit_dt(core, meshgen, kind, order=4):
     return m.critical_dt(iterations=300)
 
 
-def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8):
+def hex_rate_64cube(core, configs, device=0, steps=64):
+    """Graph-replayed FP32 rate of the 64^3 elastic hexahedron workload
+    (GLL-point updates/s): the per-node rate used for the serving leg's
+    device-time floor when the full workload leg did not run."""
+    import torch
+    cfg = configs.elastic_hex(nel=64, order=4)
+    m = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                  cfg["params"], device=device)
+    p = core.Problem(m, core.FP32, dt=1e-4)
+    p.run(32, core.RUN_GRAPH)
+    p.synchronize()
+    stream = torch.cuda.ExternalStream(p.stream_handle())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    p.run(steps, core.RUN_GRAPH)
+    b.record(stream)
+    torch.cuda.synchronize()
+    rate = m.n_nodes * steps / (a.elapsed_time(b) / 1e3)
+    p.close()
+    m.close()
+    return rate
+
+
+def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8, hex_rate=None,
+                max_running=16):
     """Config 4 (bounded sample): a seeded stream of n_jobs jobs, half 2-D
     acoustic quads (edge U{50..400}), half 3-D elastic hexes (edge
     U{16..48}), order 4, own model and source each, steps U{1000..6000}.
     First every job runs alone, one after the other (plain form, mesh
     preparation included); then the same jobs arrive as a Poisson stream at
-    load x the serial service rate and the server runs them."""
+    load x the serial service rate and the server runs them.
+
+    hex_rate (GLL-point updates/s of the 64^3 hexahedron workload on this
+    GPU) gives a device-time floor: the hexahedron jobs' updates alone need
+    sum(G * steps) / hex_rate seconds of device time, so no served form can
+    beat serial_s / that floor."""
     from salvus_b200 import serving
     ud = {k: unit_dt(core, meshgen, k) for k in ("quad", "hex")}
     stream = configs.serving_stream(n_jobs, seed=seed)
@@ -425,18 +459,19 @@ def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8):
         m.close()
     serial_s = time.perf_counter() - t0
     # capacity: all jobs submitted at once
-    srv = serving.Server(budget_bytes=150 * 10**9, max_running=16, chunk_steps=64)
+    srv = serving.Server(budget_bytes=150 * 10**9, max_running=max_running, chunk_steps=64)
     t0 = time.perf_counter()
     ids = [srv.submit(cfg, dt, n) for kind, cfg, dt, n in jobs]
     for j in ids:
         srv.wait(j, 3600)
     burst_s = time.perf_counter() - t0
-    burst_updates = srv.stats()["gll_point_updates"]
+    burst_stats = srv.stats()
+    burst_updates = burst_stats["gll_point_updates"]
     srv.close()
     # served stream at `load` times the measured capacity
     rng = np.random.default_rng(seed + 1)
     gaps = rng.exponential(burst_s / n_jobs / load, size=n_jobs)
-    srv = serving.Server(budget_bytes=150 * 10**9, max_running=16, chunk_steps=64)
+    srv = serving.Server(budget_bytes=150 * 10**9, max_running=max_running, chunk_steps=64)
     t0 = time.perf_counter()
     ids = []
     for (kind, cfg, dt, n), gap in zip(jobs, gaps):
@@ -447,6 +482,17 @@ def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8):
     wall = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
+    floor = None
+    if hex_rate:
+        # G of an edge^3 hexahedron mesh of order N: (N edge + 1)^3 nodes
+        hex_updates = sum((jobs[0][1]["order"] * edge + 1) ** 3 * n
+                          for (kind, edge, _, n, _) in stream if kind == "hex")
+        floor = {"hex_updates": hex_updates, "hex_rate_64cube": hex_rate,
+                 "hex_device_floor_s": hex_updates / hex_rate,
+                 "ratio_ceiling": serial_s / (hex_updates / hex_rate),
+                 "form": "hexahedron jobs' updates at the 64^3 workload's graph-replayed "
+                         "per-node rate (quadrilateral jobs excluded, so the true floor is "
+                         "higher and the ceiling lower)"}
     return {"workload": f"{n_jobs} jobs: 2-D acoustic quads 50^2-400^2 and 3-D elastic hexes "
                         f"16^3-48^3, order 4, 1000-6000 steps; latency under Poisson arrivals at "
                         f"{load:.0%} of the measured capacity (bounded sample of the 2000-job stream)",
@@ -460,7 +506,10 @@ def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8):
             "serial_form": "each job alone, one after the other, plain host-launched steps, "
                            "preparation included",
             "throughput_ratio": (burst_updates / burst_s) / (serial_updates / serial_s),
-            "peak_device_bytes": st["peak_device_bytes"]}
+            "peak_device_bytes": st["peak_device_bytes"],
+            "prep_seconds_burst": burst_stats["prep_seconds"],
+            "prep_seconds_stream": st["prep_seconds"], "max_running": max_running,
+            "device_floor": floor}
 
 
 REFERENCE_BUDGET_S = 150.0  # timed CPU work of the reference arm, at most
@@ -544,7 +593,9 @@ def main():
 
     if args.serving_only:
         from salvus_b200 import meshgen
-        out = {"serving": serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs)}
+        out = {"serving": serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs,
+                                      hex_rate=hex_rate_64cube(core, configs, device=local),
+                                      max_running=args.serving_max_running)}
         if rank == 0:
             print(json.dumps(out), flush=True)
         return
@@ -573,7 +624,8 @@ def main():
 
     cfg = configs.elastic_hex(nel=args.nel, order=args.order)
     mesh = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
-                     cfg["params"], device=local)
+                     cfg["params"], device=local,
+                     flags=core.MESH_PER_POINT_GEOMETRY if args.per_point_geometry else 0)
     G = mesh.n_nodes
     # profile-only runs (ncu captures) skip the power iteration to keep the
     # launch list short
@@ -641,7 +693,8 @@ def main():
 
     E, P = mesh.n_elements, mesh.points_per_element
     affine, n_gather = mesh.layout()
-    fused = affine and os.environ.get("SALVUS_HEX_STEP") == "fused"
+    form, epc = p.step_config()  # the hexahedron autotuner's choice
+    fused = affine and form == core.STEP_FUSED_INTERIOR
     n_int = G - n_gather  # element-interior nodes (advanced in the stiffness kernel when fused)
     if fused:
         # parallelepiped layout, fused step: per point conn 4 B + lambda' mu'
@@ -742,7 +795,9 @@ def main():
     serve = None
     if not args.no_serving and rank == 0 and world == 1:
         from salvus_b200 import meshgen
-        serve = serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs)
+        serve = serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs,
+                            hex_rate=value if args.nel == 64 and args.order == 4 else None,
+                            max_running=args.serving_max_running)
 
     simplex = None
     if not args.no_simplex:
@@ -772,7 +827,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "elastic_hex_stiffness", "layout": layout,
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                          "traffic": traffic, "algorithmic_bytes": b_stiff,
-                         "kernel_ms": st_ms,
+                         "kernel_ms": st_ms, "elements_per_cta": epc,
                          "peak_source": "measured" if peaks else "fallback"},
             "roofline_update": {"kernel": "gather_update", "achieved": b_upd / (up_ms / 1e3) / 1e9,
                                 "peak": peak, "unit": "GB/s", "algorithmic_bytes": b_upd,

@@ -256,6 +256,24 @@ int64_t salvus_problem_step_index(const salvus_problem *p);
 int salvus_problem_autotune(salvus_problem *p, int32_t *stiff_shot_lanes,
                             int32_t *stiff_elements, int32_t *gather_shot_lanes,
                             int32_t *gather_nodes);
+/* Step form the problem runs, as chosen by the autotuners (no reference
+ * counterpart; the reference has one form of Problem::takeTimeStep):
+ *   form  SALVUS_STEP_PLAIN (stiffness kernel, then the node gather / Newmark
+ *         update over every node) or SALVUS_STEP_FUSED_INTERIOR (the
+ *         stiffness kernel also advances each element's interior nodes; the
+ *         gather covers the shared nodes only).  Both forms give bitwise the
+ *         same fields.
+ *   elements_per_cta  elements per CTA of the stiffness kernel where it is
+ *         tuned (FP32 parallelepiped elastic hexahedra: 128 / (N+1)^2 or twice
+ *         that; shot-batched quads: the batched kernel's elements), else 0.
+ * FP32 single-shot elastic hexahedron meshes of parallelepipeds are tuned by
+ * timing every admissible (form, CTA width) on scratch copies of the fields
+ * before the first run (cached per mesh size and device for the process;
+ * SALVUS_HEX_CONFIG="form,wide" pins the choice, SALVUS_HEX_STEP=fused or
+ * plain forces the form).  Runs the tuning if it has not run yet. */
+#define SALVUS_STEP_PLAIN 0
+#define SALVUS_STEP_FUSED_INTERIOR 1
+int salvus_problem_step_config(salvus_problem *p, int32_t *form, int32_t *elements_per_cta);
 /* Device status of the problem (synchronises its stream): SALVUS_OK,
  * SALVUS_E_NONFINITE when the displacement field held a NaN / Inf at one of
  * the finite checks (after every 32 steps of salvus_run / salvus_step /
@@ -373,6 +391,7 @@ typedef struct {
   double gll_point_updates; /* sum over completed jobs of G * steps */
   double busy_seconds;      /* wall time with at least one job admitted */
   int64_t peak_device_bytes;
+  double prep_seconds;      /* sum over jobs of host + device preparation time (worker threads) */
 } salvus_server_stats;
 
 typedef struct salvus_server salvus_server;

@@ -24,6 +24,7 @@ QUAD, HEX, TRI, TET = 0, 1, 2, 3
 ACOUSTIC, ELASTIC3D, ELASTIC2D, COUPLED2D = 0, 1, 2, 3
 FP32, FP64 = 0, 1
 E_INVALID, E_OOM, E_CUDA, E_TIMEOUT, E_NONFINITE, E_STATE, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
+STEP_PLAIN, STEP_FUSED_INTERIOR = 0, 1  # salvus_problem_step_config forms
 MESH_FP32_ONLY = 1  # salvus_mesh_desc.flags: build only the FP32 stiffness records
 MESH_ELASTIC_TI = 2  # salvus_mesh_desc.flags: elastic3d params RHO VPV VPH VSV VSH ETA
 MESH_PER_POINT_GEOMETRY = 4  # salvus_mesh_desc.flags: per-point Jacobians for parallelepipeds too
@@ -120,6 +121,7 @@ SIGNATURES = [
     ("salvus_launch_count", _I64, []),
     ("salvus_apply_stiffness_noalloc", ctypes.c_int, [_VP, _I32, _VP, _VP, _VP]),
     ("salvus_problem_autotune", ctypes.c_int, [_VP] + [ctypes.POINTER(_I32)] * 4),
+    ("salvus_problem_step_config", ctypes.c_int, [_VP] + [ctypes.POINTER(_I32)] * 2),
 ]
 
 _LIB = None
@@ -388,6 +390,14 @@ class Problem:
         """(stiffness shot lanes, elements per CTA, gather shot lanes, nodes per CTA)."""
         v = [_I32() for _ in range(4)]
         _check(lib().salvus_problem_autotune(self.h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def step_config(self):
+        """(form, elements per CTA) the autotuners chose: form STEP_PLAIN or
+        STEP_FUSED_INTERIOR (bitwise the same fields); runs the tuning first
+        if needed."""
+        v = [_I32() for _ in range(2)]
+        _check(lib().salvus_problem_step_config(self.h, *[ctypes.byref(x) for x in v]))
         return tuple(x.value for x in v)
 
     def profile(self, enable=True):

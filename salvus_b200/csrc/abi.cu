@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <thread>
 #include <vector>
@@ -149,10 +150,11 @@ static int launch_elastic_classic(const salvus_mesh *m, const real *rec, const r
 
 // Parallelepiped meshes (m->affine): per-element inverse Jacobian, material
 // planes; kFuse also advances the interior nodes (kernels_hex_affine.cuh).
-template <int N, bool TI, bool kFuse>
-static int launch_elastic_affine(const salvus_mesh *m, const float *mat, float *u, float *r,
-                                 cudaStream_t st, const HexInteriorUpdate &iu) {
-  constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
+// CTAs hold EPB elements: 128 / (N+1)^2 or, when the hexahedron autotuner
+// found it faster on this mesh (m->hex_wide), twice as many.
+template <int N, int EPB, bool TI, bool kFuse>
+static int launch_elastic_affine_epb(const salvus_mesh *m, const float *mat, float *u, float *r,
+                                     cudaStream_t st, const HexInteriorUpdate &iu) {
   using T = HexAffineShape<N, EPB, TI>;
   auto kern = kFuse ? elastic_hex_affine_fused_kernel<N, EPB, TI>
                     : elastic_hex_affine_kernel<N, EPB, TI>;
@@ -166,6 +168,13 @@ static int launch_elastic_affine(const salvus_mesh *m, const float *mat, float *
       iu);
   g_launches++;
   return check_launch(kFuse ? "elastic stiffness (fused interior)" : "elastic stiffness");
+}
+template <int N, bool TI, bool kFuse>
+static int launch_elastic_affine(const salvus_mesh *m, const float *mat, float *u, float *r,
+                                 cudaStream_t st, const HexInteriorUpdate &iu) {
+  constexpr int n2 = (N + 1) * (N + 1), EPB = 128 / n2 > 0 ? 128 / n2 : 1;
+  return m->hex_wide ? launch_elastic_affine_epb<N, 2 * EPB, TI, kFuse>(m, mat, u, r, st, iu)
+                     : launch_elastic_affine_epb<N, EPB, TI, kFuse>(m, mat, u, r, st, iu);
 }
 
 template <int N, typename real>
@@ -798,19 +807,24 @@ static const real *inv_mass(const salvus_problem *p) {
 // The fused FP32 step of parallelepiped elastic hexahedra advances the
 // element-interior nodes inside the stiffness kernel and gathers the rest
 // (kernels_hex_affine.cuh).  Measured on the 64^3 order-4 workload it is
-// slower than the plain sequence on the same records (0.97 against 0.80 ms
-// per step: the interior update costs the stiffness kernel more than the
-// shorter gather saves), so it runs only with SALVUS_HEX_STEP=fused (read at
-// every step), for problems without Dirichlet points and with at most
+// slower than the plain sequence on the same records (the interior update
+// costs the stiffness kernel more than the shorter gather saves), so the
+// hexahedron autotuner (tune_hex) picks between the two per problem;
+// SALVUS_HEX_STEP=fused / plain forces the form (read at every step).  It is
+// admissible for problems without Dirichlet points and with at most
 // kFuseMaxSources sources (each interior column scans their elements).
 constexpr int kFuseMaxSources = 16;
-static bool hex_interior_fusion(const salvus_problem *p) {
+static bool hex_fusion_admissible(const salvus_problem *p) {
   const salvus_mesh *m = p->mesh;
-  if (!(m->affine && m->n_gnodes > 0 && p->prec == SALVUS_FP32 && p->shots == 1 &&
-        p->n_dir_pts == 0 && (int)p->srcs.size() <= kFuseMaxSources))
-    return false;
+  return m->affine && m->n_gnodes > 0 && p->prec == SALVUS_FP32 && p->shots == 1 &&
+         p->n_dir_pts == 0 && (int)p->srcs.size() <= kFuseMaxSources;
+}
+static bool hex_interior_fusion(const salvus_problem *p) {
+  if (!hex_fusion_admissible(p)) return false;
   const char *s = std::getenv("SALVUS_HEX_STEP");
-  return s && std::strcmp(s, "fused") == 0;
+  if (s && std::strcmp(s, "fused") == 0) return true;
+  if (s && std::strcmp(s, "plain") == 0) return false;
+  return p->hex_form == 1;
 }
 
 template <bool TI>
@@ -1022,14 +1036,18 @@ static int autotune(salvus_problem *p) {
     int64_t E;
     int dev;
   };
+  static std::mutex cache_mu;
   static std::vector<std::pair<Key, std::pair<int, int>>> cache;
-  for (auto &c : cache)
-    if (c.first.order == p->mesh->order && c.first.shots == p->shots_pad && c.first.E == p->mesh->E &&
-        c.first.dev == p->mesh->device) {
-      p->tune_stiff = c.second.first;
-      p->tune_gather = c.second.second;
-      return SALVUS_OK;
-    }
+  {
+    std::lock_guard<std::mutex> lk(cache_mu);
+    for (auto &c : cache)
+      if (c.first.order == p->mesh->order && c.first.shots == p->shots_pad &&
+          c.first.E == p->mesh->E && c.first.dev == p->mesh->device) {
+        p->tune_stiff = c.second.first;
+        p->tune_gather = c.second.second;
+        return SALVUS_OK;
+      }
+  }
   const char *env = std::getenv("SALVUS_BATCH_CONFIG");  // "stiff,gather" fixes the choice
   if (env) {
     int a = -1, b = -1;
@@ -1092,6 +1110,7 @@ static int autotune(salvus_problem *p) {
   if (rc) return rc;
   if (cs < 0 || p->tune_gather < 0) return fail(SALVUS_E_INVALID, "no admissible batch configuration");
   p->tune_stiff = cs;
+  std::lock_guard<std::mutex> lk(cache_mu);
   cache.push_back({{p->mesh->order, p->shots_pad, p->mesh->E, p->mesh->device},
                    {p->tune_stiff, p->tune_gather}});
   return SALVUS_OK;
@@ -1229,10 +1248,7 @@ int apply_stiffness_into(const salvus_mesh *m, int precision, const void *u, voi
 
 // Reads the device status word: set by kernels whose bounded waits ran out
 // (the wait's code) or by the finite check (kNonFiniteCode).
-static int device_status(salvus_problem *p) {
-  int h = 0;
-  SALVUS_CUDA(cudaMemcpyAsync(&h, p->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
-  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+int status_error(const salvus_problem *p, int h) {
   if (h == kNonFiniteCode)
     return fail(SALVUS_E_NONFINITE,
                 "the wavefield became non-finite (NaN / Inf) by step %lld: the time step is "
@@ -1240,6 +1256,29 @@ static int device_status(salvus_problem *p) {
                 (long long)p->step);
   if (h) return fail(SALVUS_E_TIMEOUT, "a bounded device wait gave up (code %d); results invalid", h);
   return SALVUS_OK;
+}
+
+static int device_status(salvus_problem *p) {
+  int h = 0;
+  SALVUS_CUDA(cudaMemcpyAsync(&h, p->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  SALVUS_CUDA(cudaStreamSynchronize(p->stream));
+  return status_error(p, h);
+}
+
+int enqueue_seis_copy(salvus_problem *p, double *ring, int *status) {
+  if (!p || !ring || !status) return fail(SALVUS_E_INVALID, "null argument");
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  const int64_t rows = (int64_t)p->shots * p->recs.size() * p->c;
+  if (rows > 0 && p->d_seis.ptr)
+    SALVUS_CUDA(cudaMemcpyAsync(ring, p->d_seis.ptr, sizeof(double) * rows * p->seis_cap,
+                                cudaMemcpyDeviceToHost, p->stream));
+  SALVUS_CUDA(cudaMemcpyAsync(status, p->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  return SALVUS_OK;
+}
+
+void seis_ring_shape(const salvus_problem *p, int64_t *rows, int64_t *capacity) {
+  if (rows) *rows = (int64_t)p->shots * p->recs.size() * p->c;
+  if (capacity) *capacity = p->seis_cap;
 }
 
 // Finite check of u (all shots) into the status word; part of every 32-step
@@ -1257,6 +1296,141 @@ static int launch_finite_check(salvus_problem *p) {
   return check_launch("finite check");
 }
 
+// Hexahedron autotuner (FP32 elastic meshes of parallelepipeds, one shot):
+// times the plain step (stiffness, node gather/update) and, where the fused
+// interior form is admissible, that form, each with CTAs of 128 / (N+1)^2
+// elements and with twice as many, on zeroed scratch copies of u, v, a_ and
+// a, and keeps the fastest.  All of them give bitwise the same wavefield
+// (the same arithmetic per element and per node, in the same order), so the
+// choice changes only the time.  Results are cached per (order, elements,
+// nodes, anisotropy, admissible forms, device) for the process; the CTA
+// width belongs to the mesh, the form to the problem.
+// SALVUS_HEX_CONFIG="form,wide" fixes both; SALVUS_HEX_STEP still forces
+// the form.  Without room for the scratch fields the defaults (plain, 128 /
+// (N+1)^2) are kept.
+static int tune_hex(salvus_problem *p) {
+  if (p->hex_form >= 0) return SALVUS_OK;
+  salvus_mesh *m = p->mesh;
+  if (!(m->shape == SALVUS_HEX && m->affine && m->physics == SALVUS_ELASTIC3D &&
+        p->prec == SALVUS_FP32 && p->shots == 1 && !m->host_only)) {
+    p->hex_form = 0;
+    return SALVUS_OK;
+  }
+  const bool fusable = hex_fusion_admissible(p) && m->order >= 2 && m->order <= 6;
+  struct Key {
+    int order;
+    int64_t E, G;
+    bool ti, fusable;
+    int dev;
+  };
+  if (const char *env = std::getenv("SALVUS_HEX_CONFIG")) {
+    int a = -1, b = -1;
+    if (std::sscanf(env, "%d,%d", &a, &b) == 2 && (a == 0 || (a == 1 && fusable)) &&
+        (b == 0 || b == 1)) {
+      p->hex_form = a;
+      m->hex_wide = b;
+      return SALVUS_OK;
+    }
+  }
+  // problems are prepared on several threads (the job server)
+  static std::mutex cache_mu;
+  static std::vector<std::pair<Key, std::pair<int, int>>> cache;
+  {
+    std::lock_guard<std::mutex> lk(cache_mu);
+    for (auto &c : cache)
+      if (c.first.order == m->order && c.first.E == m->E && c.first.G == m->G &&
+          c.first.ti == m->ti && c.first.fusable == fusable && c.first.dev == m->device) {
+        p->hex_form = c.second.first;
+        m->hex_wide = c.second.second;
+        return SALVUS_OK;
+      }
+  }
+  p->hex_form = 0;
+  const size_t nf = (size_t)m->G * 3 * sizeof(float);
+  DeviceBuffer su, sv, sap, sa;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < 4 * nf + (size_t(1) << 30) ||
+      su.alloc(nf) || sv.alloc(nf) || sap.alloc(nf) || sa.alloc(nf)) {
+    cudaGetLastError();
+    return SALVUS_OK;
+  }
+  SALVUS_CUDA(cudaMemsetAsync(su.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(sv.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(sap.ptr, 0, nf, p->stream));
+  SALVUS_CUDA(cudaMemsetAsync(sa.ptr, 0, nf, p->stream));
+  std::swap(p->d_u.ptr, su.ptr);
+  std::swap(p->d_v.ptr, sv.ptr);
+  std::swap(p->d_ap.ptr, sap.ptr);
+  std::swap(p->d_a.ptr, sa.ptr);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int rc = SALVUS_OK;
+  // one step of either form without sources and receivers (the same in both)
+  auto sequence = [&](int form) -> int {
+    int r;
+    if (form == 0) {
+      if ((r = launch_stiffness<float>(m, records<float>(p), F<float>(p->d_u), F<float>(p->d_r),
+                                       p->stream, p->d_err.as<int>(), p->wait_limit, 0)))
+        return r;
+      gather_kernel<float, 3, 0><<<blocks_for(m->G, 256), 256, 0, p->stream>>>(
+          m->G, m->d_inc_off.as<int32_t>(), m->d_inc_idx.as<int32_t>(), F<float>(p->d_r),
+          m->d_mi32.as<float>(), F<float>(p->d_u), F<float>(p->d_v), F<float>(p->d_ap),
+          F<float>(p->d_a), (float)p->dt);
+    } else {
+      HexInteriorUpdate iu{};
+      iu.mi = m->d_mi32.as<float>();
+      iu.v = F<float>(p->d_v);
+      iu.ap = F<float>(p->d_ap);
+      iu.dt = (float)p->dt;
+      if ((r = m->ti ? launch_fused_interior<true>(p, iu) : launch_fused_interior<false>(p, iu)))
+        return r;
+      gather_list_kernel<float, 3, 0><<<blocks_for(m->n_gnodes, 256), 256, 0, p->stream>>>(
+          m->n_gnodes, m->d_gnodes.as<int32_t>(), m->d_inc_off.as<int32_t>(),
+          m->d_inc_idx.as<int32_t>(), F<float>(p->d_r), m->d_mi32.as<float>(), F<float>(p->d_u),
+          F<float>(p->d_v), F<float>(p->d_ap), F<float>(p->d_a), (float)p->dt);
+    }
+    g_launches++;
+    return check_launch("hexahedron autotuner");
+  };
+  float best = 1e30f;
+  int bf = 0, bw = 0;
+  for (int w = 0; w < 2 && rc == SALVUS_OK; ++w) {
+    m->hex_wide = w;
+    for (int f = 0; f < (fusable ? 2 : 1) && rc == SALVUS_OK; ++f) {
+      if ((rc = sequence(f))) break;  // first launch (attributes, caches)
+      float t = 1e30f;
+      for (int rep = 0; rep < 3 && rc == SALVUS_OK; ++rep) {
+        cudaEventRecord(e0, p->stream);
+        for (int k = 0; k < 4 && rc == SALVUS_OK; ++k) rc = sequence(f);
+        cudaEventRecord(e1, p->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t = std::min(t, ms);
+      }
+      if (rc == SALVUS_OK && t < best) {
+        best = t;
+        bf = f;
+        bw = w;
+      }
+    }
+  }
+  cudaStreamSynchronize(p->stream);
+  std::swap(p->d_u.ptr, su.ptr);
+  std::swap(p->d_v.ptr, sv.ptr);
+  std::swap(p->d_ap.ptr, sap.ptr);
+  std::swap(p->d_a.ptr, sa.ptr);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  m->hex_wide = bw;
+  if (rc) return rc;
+  p->hex_form = bf;
+  std::lock_guard<std::mutex> lk(cache_mu);
+  cache.push_back({{m->order, m->E, m->G, m->ti, fusable, m->device}, {bf, bw}});
+  return SALVUS_OK;
+}
+
 static int ready(salvus_problem *p) {
   if (!p) return fail(SALVUS_E_INVALID, "null problem");
   if (!p->dt_set) return fail(SALVUS_E_STATE, "time step not set (salvus_problem_set_dt)");
@@ -1264,6 +1438,7 @@ static int ready(salvus_problem *p) {
   if ((rc = upload_sources(p))) return rc;
   if ((rc = upload_receivers(p))) return rc;
   if (p->shots > 1 && (rc = autotune(p))) return rc;
+  if ((rc = tune_hex(p))) return rc;
   return SALVUS_OK;
 }
 
@@ -2489,6 +2664,25 @@ int salvus_problem_autotune(salvus_problem *p, int32_t *stiff_shot_lanes, int32_
   if (stiff_elements) *stiff_elements = kStiffCfg[p->tune_stiff].epc;
   if (gather_shot_lanes) *gather_shot_lanes = kGatherCfg[p->tune_gather].sc;
   if (gather_nodes) *gather_nodes = kGatherCfg[p->tune_gather].epc * kGatherCfg[p->tune_gather].npt;
+  return SALVUS_OK;
+}
+
+int salvus_problem_step_config(salvus_problem *p, int32_t *form, int32_t *elements_per_cta) {
+  int rc = ready(p);
+  if (rc) return rc;
+  const salvus_mesh *m = p->mesh;
+  int32_t f = SALVUS_STEP_PLAIN, epc = 0;
+  if (p->shots > 1) {
+    f = batch_fusion(p) && m->order >= 2 ? SALVUS_STEP_FUSED_INTERIOR : SALVUS_STEP_PLAIN;
+    epc = kStiffCfg[p->tune_stiff].epc;
+  } else if (m->shape == SALVUS_HEX && m->affine && p->prec == SALVUS_FP32 &&
+             m->physics == SALVUS_ELASTIC3D) {
+    f = hex_interior_fusion(p) ? SALVUS_STEP_FUSED_INTERIOR : SALVUS_STEP_PLAIN;
+    const int n2 = (m->order + 1) * (m->order + 1), e1 = 128 / n2 > 0 ? 128 / n2 : 1;
+    epc = e1 * (m->hex_wide ? 2 : 1);
+  }
+  if (form) *form = f;
+  if (elements_per_cta) *elements_per_cta = epc;
   return SALVUS_OK;
 }
 

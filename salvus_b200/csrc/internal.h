@@ -91,6 +91,19 @@ int record_words(int shape, int physics, int fp64, bool ti = false);
 
 }  // namespace salvus
 
+// Server support (server.cpp): non-blocking chunk collection.  Enqueues on
+// the problem's stream, without synchronising, a copy of the seismogram ring
+// ([shots][receivers][c][capacity] doubles, step s at column s % capacity)
+// and of the status word into host buffers (page-locked for overlap);
+// reports the ring's rows and capacity.  status_error turns a status word
+// read that way into the error salvus_problem_status would return.
+struct salvus_problem;
+namespace salvus {
+int enqueue_seis_copy(salvus_problem *p, double *ring, int *status);
+void seis_ring_shape(const salvus_problem *p, int64_t *rows, int64_t *capacity);
+int status_error(const salvus_problem *p, int status);
+}  // namespace salvus
+
 // stream of a problem group (server scheduling)
 cudaStream_t salvus_group_stream_internal(const salvus_group *g);
 
@@ -125,6 +138,9 @@ struct salvus_mesh {
   // planes [NM][E*P], d_jac32 the per-element invJ [E][9]; d_gnodes lists
   // the nodes that are not interior to an element (fused steps' gather)
   bool affine = false;
+  // parallelepiped hexahedron kernels: CTAs of 128 / (N+1)^2 elements (0) or
+  // twice that (1), set by the hexahedron autotuner
+  int hex_wide = 0;
   salvus::DeviceBuffer d_jac32, d_gnodes;
   std::vector<int32_t> gnodes;  // host copy of d_gnodes
   int64_t n_gnodes = 0;
@@ -189,6 +205,7 @@ struct salvus_problem {
   int shots_pad = 1;
   salvus::DeviceBuffer d_shot_off;
   int tune_stiff = -1, tune_gather = -1;  // autotuner choices (indices)
+  int hex_form = -1;  // hexahedron step form: 0 plain, 1 fused interior update (-1 untuned)
   // graphs
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;

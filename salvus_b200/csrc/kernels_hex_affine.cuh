@@ -269,11 +269,16 @@ elastic_hex_affine_kernel(int64_t E, const float *__restrict__ jac, const float 
   elastic_hex_affine_body<N, EPB_, TI, false>(blockIdx.x, E, jac, mat, conn, u, r, Dm, iu);
 }
 
-// The fused form asks for kFuseMinBlocks resident CTAs per SM (a register
-// cap): its interior-update registers would otherwise cost two CTAs per SM.
-constexpr int kFuseMinBlocks = 6;
+// The fused form asks for 768 resident threads per SM (six 128-thread CTAs,
+// a register cap): its interior-update registers would otherwise cost two
+// CTAs per SM.
+template <int THREADS>
+constexpr int fuse_min_blocks() {
+  return 768 / THREADS > 0 ? 768 / THREADS : 1;
+}
 template <int N, int EPB_, bool TI>
-__global__ void __launch_bounds__(HexAffineShape<N, EPB_, TI>::THREADS, kFuseMinBlocks)
+__global__ void __launch_bounds__(HexAffineShape<N, EPB_, TI>::THREADS,
+                                  fuse_min_blocks<HexAffineShape<N, EPB_, TI>::THREADS>())
 elastic_hex_affine_fused_kernel(int64_t E, const float *__restrict__ jac,
                                 const float *__restrict__ mat, const int32_t *__restrict__ conn,
                                 float *__restrict__ u, float *__restrict__ r, DMatrix<float> Dm,

@@ -22,8 +22,9 @@
 //   GEMM 2   divergence: D2[row][i] = sum_{k,q} F_row[k][q] dphi_i/dxi_k (x_q)
 //            K = 3 x 8 per chunk, 7 chunks; A (the flux chunk) from tensor
 //            memory; per K step one M = 128, N = 128 MMA of F_hi against
-//            [B2_hi | B2_lo] and one N = 64 MMA of F_lo against B2_hi, three
-//            accumulators summed at read-out: hh + (hl + lh)
+//            [B2_hi | B2_lo] and one N = 64 MMA of F_lo against B2_hi onto
+//            the F_hi B2_lo sums: two accumulators, read out as
+//            hh + (hl + lh)
 //
 // The B operands are two constant tables, both K-major, loaded once per CTA
 // (hi and lo parts, 161 KB in all):
@@ -68,11 +69,12 @@ struct TetTcShape {
   static constexpr uint32_t OFF_BAR = OFF_A + 2 * A1_BYTES;
   static constexpr uint32_t SMEM = OFF_BAR + 256;
   // tensor memory: D1 columns 0-175; GEMM 2 partial sums F_hi B_hi in
-  // 192-255, F_hi B_lo in 256-319 (one N = 128 MMA against B2 hi and lo,
-  // which lie one after the other), F_lo B_hi in 320-383; flux buffers
-  // 384 + 64 b (hi 24 columns, lo 32 columns further on), b = 0, 1
+  // 192-255 and F_hi B_lo + F_lo B_hi in 256-319 (one N = 128 MMA against
+  // B2 hi and lo, which lie one after the other, then an N = 64 MMA of F_lo
+  // onto the second half); 320-383 unused; flux buffers 384 + 64 b (hi 24
+  // columns, lo 32 columns further on), b = 0, 1
   static constexpr uint32_t TMEM_COLS = 512;
-  static constexpr uint32_t D2_COL = 192, D2L_COL = 320, A2_COL = 384;
+  static constexpr uint32_t D2_COL = 192, D2C_COL = 256, A2_COL = 384;
   static constexpr int RW = C == 1 ? 64 : 120;               // record words
 };
 
@@ -253,7 +255,7 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     // B2 hi and lo lie one after the other: rows 0-63 and 64-127 of one
     // N = 128 operand with the same 8-row group stride
     const uint64_t dB2h = tc::desc(b2_hi, 128, S::B2_SBO);
-    const uint32_t d2 = tmem + S::D2_COL, d2l = tmem + S::D2L_COL;
+    const uint32_t d2 = tmem + S::D2_COL, d2c = tmem + S::D2C_COL;
     const bool leader = lane == 0;
     auto wwait = [&](uint64_t *b, uint32_t p, int code) {
       return __all_sync(0xffffffffu, tc::wait(b, p, flag, code, wait_limit) ? 1 : 0) != 0;
@@ -294,7 +296,7 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
             const uint32_t ah = a2 + 8u * (uint32_t)k, al = ah + 32u;
             const uint32_t acc = (c > 0 || k > 0) ? 1u : 0u;
             tc::mma_tf32_ta(d2, ah, dB2h + kg, IDW, acc);  // F_hi [B_hi | B_lo]
-            tc::mma_tf32_ta(d2l, al, dB2h + kg, ID, acc);  // F_lo B_hi
+            tc::mma_tf32_ta(d2c, al, dB2h + kg, ID, 1u);   // + F_lo B_hi
           }
           tc::commit(&bar[9 + c]);
         }
@@ -362,20 +364,19 @@ tet_tc_kernel(int64_t E, const float *__restrict__ rec, const int32_t *__restric
     auto store_residual = [&](int64_t er, bool okr) {
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        float hh[16], hl[16], lh[16];
+        float hh[16], cc[16];
         const uint32_t col = (uint32_t)(32 * wg + 16 * h);
 #pragma unroll
         for (int g8 = 0; g8 < 2; ++g8) {
           tc::ld8(tmem + lane_base + S::D2_COL + col + 8u * g8, hh + 8 * g8);
-          tc::ld8(tmem + lane_base + S::D2_COL + 64u + col + 8u * g8, hl + 8 * g8);
-          tc::ld8(tmem + lane_base + S::D2L_COL + col + 8u * g8, lh + 8 * g8);
+          tc::ld8(tmem + lane_base + S::D2C_COL + col + 8u * g8, cc + 8 * g8);
         }
         tc::ld_wait();
         if (okr) {
 #pragma unroll
           for (int t = 0; t < 16; ++t) {
             const int i = 32 * wg + 16 * h + t;
-            if (i < P) r[(er * P + i) * C + comp] = -(hh[t] + (hl[t] + lh[t]));
+            if (i < P) r[(er * P + i) * C + comp] = -(hh[t] + cc[t]);
           }
         }
       }

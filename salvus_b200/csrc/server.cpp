@@ -4,11 +4,15 @@
 // Threads:
 //   scheduler  admits queued jobs while the device-memory budget and the
 //              running-job limit allow (any queued job that fits may pass a
-//              larger one ahead of it), enqueues one graph-replayed chunk of
-//              steps for every running job on the job's own stream (so the
-//              jobs' kernels overlap on the device), then collects each
-//              chunk: streams the new seismogram samples to the host and
-//              retires finished jobs, freeing their device memory.
+//              larger one ahead of it) and keeps every running job two
+//              graph-replayed chunks of steps ahead on the job's own stream
+//              (so the jobs' kernels overlap on the device and no job waits
+//              for another's chunk): each chunk ends with an asynchronous
+//              copy of the job's seismogram ring and status word into
+//              page-locked host buffers and an event; the scheduler polls
+//              the events, streams each finished chunk's samples into the
+//              job's result, enqueues the next chunk, and retires finished
+//              jobs, freeing their device memory.
 //   workers    (up to 8) prepare admitted jobs (mesh flattening on the host,
 //              device setup, sources, receivers) while the scheduler keeps
 //              running jobs busy.
@@ -61,7 +65,15 @@ struct Job {
   Clock::time_point submitted, done;
   salvus_mesh *m = nullptr;
   salvus_problem *p = nullptr;
-  int64_t chunk_first = 0, chunk_count = 0;
+  // chunks in flight (at most two, in order from `head`): first step, step
+  // count, completion event, host copies of the seismogram ring and status
+  cudaStream_t stream = nullptr;
+  int64_t enq_steps = 0, rows = 0, cap = 0;
+  int head = 0, inflight = 0;
+  int64_t first[2] = {0, 0}, count[2] = {0, 0};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double *ring[2] = {nullptr, nullptr};
+  int *status[2] = {nullptr, nullptr};
 };
 
 int64_t estimate_bytes(const salvus_mesh_desc &d, int precision) {
@@ -109,7 +121,7 @@ struct salvus_server {
   // stats
   std::vector<double> latencies;
   double updates = 0;
-  double busy = 0;
+  double busy = 0, prep = 0;
   int64_t submitted = 0, completed = 0, failed = 0;
   Clock::time_point busy_since;
   bool busy_now = false;
@@ -133,10 +145,21 @@ void finish_locked(salvus_server *s, Job *j, int state) {
 }
 
 void release_device(Job *j) {
+  if (j->stream && j->inflight > 0) cudaStreamSynchronize(j->stream);
+  j->inflight = 0;
+  for (int k = 0; k < 2; ++k) {
+    if (j->ev[k]) cudaEventDestroy(j->ev[k]);
+    if (j->ring[k]) cudaFreeHost(j->ring[k]);
+    if (j->status[k]) cudaFreeHost(j->status[k]);
+    j->ev[k] = nullptr;
+    j->ring[k] = nullptr;
+    j->status[k] = nullptr;
+  }
   if (j->p) salvus_problem_destroy(j->p);
   if (j->m) salvus_mesh_destroy(j->m);
   j->p = nullptr;
   j->m = nullptr;
+  j->stream = nullptr;
 }
 
 // Host + device preparation of one job (worker thread).
@@ -161,6 +184,20 @@ int prepare(salvus_server *s, Job *j) {
   for (int64_t r = 0; r < R; ++r)
     if ((rc = salvus_problem_add_receiver(j->p, &j->receivers[3 * r]))) return rc;
   j->seis.assign((size_t)(R * j->c * j->n_steps), 0.0);
+  // sources and receivers on the device, step form tuned, here rather than
+  // in the scheduler's first chunk
+  if ((rc = salvus_problem_step_config(j->p, nullptr, nullptr))) return rc;
+  void *st = nullptr;
+  if ((rc = salvus_problem_stream(j->p, &st))) return rc;
+  j->stream = (cudaStream_t)st;
+  salvus::seis_ring_shape(j->p, &j->rows, &j->cap);
+  for (int k = 0; k < 2; ++k) {
+    if (cudaEventCreateWithFlags(&j->ev[k], cudaEventDisableTiming) != cudaSuccess ||
+        cudaMallocHost((void **)&j->status[k], sizeof(int)) != cudaSuccess ||
+        cudaMallocHost((void **)&j->ring[k], sizeof(double) * std::max<int64_t>(1, j->rows * j->cap)) !=
+            cudaSuccess)
+      return salvus::fail(SALVUS_E_CUDA, "job %lld: chunk buffers", (long long)j->id);
+  }
   return SALVUS_OK;
 }
 
@@ -175,9 +212,11 @@ void worker_loop(salvus_server *s) {
       j = s->to_prepare.front();
       s->to_prepare.pop_front();
     }
+    const auto t0 = Clock::now();
     int rc = j->cancel ? SALVUS_E_STATE : prepare(s, j);
     std::string err = rc ? salvus::last_error() : "";
     std::lock_guard<std::mutex> lk(s->mu);
+    s->prep += std::chrono::duration<double>(Clock::now() - t0).count();
     s->n_preparing--;
     if (rc) {
       release_device(j);
@@ -238,37 +277,48 @@ void scheduler_loop(salvus_server *s) {
       run = s->running;
     }
     if (run.empty()) continue;
-    // enqueue one chunk per running job (their streams run concurrently)
-    for (Job *j : run) {
-      j->chunk_first = j->steps_done;
-      j->chunk_count = std::min<int64_t>(s->chunk, j->n_steps - j->steps_done);
-      if (j->cancel) j->chunk_count = 0;
-      if (j->chunk_count > 0 && salvus_run(j->p, j->chunk_count, SALVUS_RUN_GRAPH)) {
-        j->error = salvus::last_error();
-        j->chunk_count = -1;
-      }
-    }
-    // collect: stream samples back, retire finished jobs
+    bool progressed = false;
     for (Job *j : run) {
       int rc = SALVUS_OK;
-      if (j->chunk_count > 0) {
-        const int64_t R = (int64_t)j->receivers.size() / 3, rows = R * j->c;
-        std::vector<double> tmp((size_t)(rows * j->chunk_count));
-        if (rows) rc = salvus_get_seismograms(j->p, j->chunk_first, j->chunk_count, tmp.data());
-        else rc = salvus_synchronize(j->p);
-        if (rc == SALVUS_OK) {
-          for (int64_t q = 0; q < rows; ++q)
-            std::memcpy(&j->seis[(size_t)(q * j->n_steps + j->chunk_first)], &tmp[(size_t)(q * j->chunk_count)],
-                        sizeof(double) * j->chunk_count);
-          j->steps_done += j->chunk_count;
-        } else {
-          j->error = salvus::last_error();
+      // collect this job's finished chunks, in order
+      while (j->inflight > 0) {
+        const int k = j->head;
+        const cudaError_t q = cudaEventQuery(j->ev[k]);
+        if (q == cudaErrorNotReady) break;
+        if (q != cudaSuccess) {
+          rc = salvus::fail(SALVUS_E_CUDA, "job %lld: %s", (long long)j->id, cudaGetErrorString(q));
+          break;
         }
-      } else if (j->chunk_count < 0) {
-        rc = SALVUS_E_CUDA;
+        if ((rc = salvus::status_error(j->p, *j->status[k]))) break;
+        const int64_t f = j->first[k], n = j->count[k];
+        for (int64_t r = 0; r < j->rows; ++r)
+          for (int64_t t = 0; t < n; ++t)
+            j->seis[(size_t)(r * j->n_steps + f + t)] = j->ring[k][r * j->cap + (f + t) % j->cap];
+        j->steps_done += n;
+        j->head ^= 1;
+        j->inflight--;
+        progressed = true;
       }
+      // keep two chunks in flight
+      while (rc == SALVUS_OK && !j->cancel && j->inflight < 2 && j->enq_steps < j->n_steps) {
+        const int k = (j->head + j->inflight) & 1;
+        const int64_t n = std::min<int64_t>(s->chunk, j->n_steps - j->enq_steps);
+        if ((rc = salvus_run(j->p, n, SALVUS_RUN_GRAPH))) break;
+        if ((rc = salvus::enqueue_seis_copy(j->p, j->ring[k], j->status[k]))) break;
+        if (cudaEventRecord(j->ev[k], j->stream) != cudaSuccess) {
+          rc = salvus::fail(SALVUS_E_CUDA, "job %lld: event record", (long long)j->id);
+          break;
+        }
+        j->first[k] = j->enq_steps;
+        j->count[k] = n;
+        j->enq_steps += n;
+        j->inflight++;
+        progressed = true;
+      }
+      if (rc != SALVUS_OK) j->error = salvus::last_error();
       const bool cancelled = j->cancel;
-      const bool finished = rc != SALVUS_OK || cancelled || j->steps_done >= j->n_steps;
+      const bool finished = rc != SALVUS_OK || (cancelled && j->inflight == 0) ||
+                            j->steps_done >= j->n_steps;
       if (finished) {
         release_device(j);
         std::lock_guard<std::mutex> lk(s->mu);
@@ -278,6 +328,8 @@ void scheduler_loop(salvus_server *s) {
                                             : SALVUS_JOB_DONE);
       }
     }
+    // nothing finished or started: let the device work before polling again
+    if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(50));
   }
 }
 
@@ -432,6 +484,7 @@ int salvus_server_stats_read(salvus_server *s, salvus_server_stats *o) {
   o->gll_point_updates = s->updates;
   o->busy_seconds = s->busy + (s->busy_now ? std::chrono::duration<double>(Clock::now() - s->busy_since).count() : 0.0);
   o->peak_device_bytes = s->peak_mem;
+  o->prep_seconds = s->prep;
   return SALVUS_OK;
 }
 

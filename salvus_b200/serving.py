@@ -21,7 +21,7 @@ class Stats(ctypes.Structure):
     _fields_ = [("submitted", _I64), ("completed", _I64), ("failed", _I64), ("running", _I64),
                 ("queued", _I64), ("p50_latency_s", _D), ("p99_latency_s", _D),
                 ("mean_latency_s", _D), ("gll_point_updates", _D), ("busy_seconds", _D),
-                ("peak_device_bytes", _I64)]
+                ("peak_device_bytes", _I64), ("prep_seconds", _D)]
 
 
 _BOUND = False

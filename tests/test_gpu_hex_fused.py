@@ -1,8 +1,8 @@
 """The FP32 step of elastic hexahedra that are all parallelepipeds.
 
 Such meshes keep one inverse Jacobian per element and per-point material
-records only.  The fused step (SALVUS_HEX_STEP=fused; measured slower than
-the default plain sequence on these records, kept as an option) advances
+records only.  The fused step (picked by the hexahedron autotuner when it is
+the faster form on the problem, forced by SALVUS_HEX_STEP=fused) advances
 each element's interior nodes in the stiffness kernel (one-term assembly,
 inverse mass, Newmark; elements holding a source are finished by the source
 kernel) while the node gather handles the shared nodes.  Checked here:
@@ -14,7 +14,9 @@ kernel) while the node gather handles the shared nodes.  Checked here:
   * parallelepiped records against per-point records
     (SALVUS_MESH_PER_POINT_GEOMETRY): same physics, FP32 rounding only;
   * a mesh of distorted hexahedra (per-point records, the column kernel)
-    against the FP64 oracle.
+    against the FP64 oracle;
+  * every configuration the autotuner chooses between (form x CTA width)
+    pinned in turn == the tuned default, bitwise.
 """
 import numpy as np
 import pytest
@@ -185,3 +187,28 @@ def test_fp32_field_upload_rounds_like_a_float32_cast():
     p.set_field("v", vals)
     got = p.get_field("v")
     assert np.array_equal(got, vals.astype(np.float32).astype(np.float64))
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_autotuned_configurations_agree_bitwise(order, monkeypatch):
+    """The hexahedron autotuner times the plain and fused forms with CTAs of
+    128 / (N+1)^2 elements and twice that; every one of the four,
+    pinned through SALVUS_HEX_CONFIG, gives the tuned default's fields and
+    seismograms bitwise, and step_config reports what was pinned."""
+    monkeypatch.delenv("SALVUS_HEX_STEP", raising=False)
+    cfg = configs.elastic_hex(nel=4, order=order, n_receivers=5)
+    m = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
+                  cfg["params"])
+    dt = 0.4 * m.critical_dt(iterations=100)
+    ref = problem(cfg, dt=dt)
+    form, epc = ref.step_config()
+    e1 = 128 // (order + 1) ** 2
+    assert form in (core.STEP_PLAIN, core.STEP_FUSED_INTERIOR) and epc in (e1, 2 * e1)
+    ref.run(80, core.RUN_GRAPH)
+    for f in (0, 1):
+        for w in (0, 1):
+            monkeypatch.setenv("SALVUS_HEX_CONFIG", f"{f},{w}")
+            p = problem(cfg, dt=dt)  # a new mesh: the CTA width belongs to the mesh
+            assert p.step_config() == (f, e1 * (1 + w))
+            p.run(80, core.RUN_GRAPH)
+            assert_same(p, ref)
