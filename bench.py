@@ -58,7 +58,7 @@ def parse():
                     help="tetrahedral mesh cells per side (Delaunay of a jittered BCC point "
                          "set, ~12 n^3 elements; 44 -> ~1.02M)")
     ap.add_argument("--serving-jobs", type=int, default=24)
-    ap.add_argument("--serving-max-running", type=int, default=16,
+    ap.add_argument("--serving-max-running", type=int, default=32,
                     help="serving leg: jobs admitted at once (running or being prepared)")
     ap.add_argument("--serving-only", action="store_true",
                     help="run only the serving leg (e.g. --serving-jobs 500) and print its JSON")
@@ -391,15 +391,17 @@ def unit_dt(core, meshgen, kind, order=4):
     return m.critical_dt(iterations=300)
 
 
-def hex_rate_64cube(core, configs, device=0, steps=64):
-    """Graph-replayed FP32 rate of the 64^3 elastic hexahedron workload
-    (GLL-point updates/s): the per-node rate used for the serving leg's
-    device-time floor when the full workload leg did not run."""
+def class_rate(core, configs, kind, device=0, steps=64):
+    """Graph-replayed FP32 rate (GLL-point updates/s) of one large mesh of a
+    serving job class: 64^3 elastic hexahedra or 1000^2 acoustic quads,
+    order 4 -- the per-node rates behind the serving leg's device-time
+    floor."""
     import torch
-    cfg = configs.elastic_hex(nel=64, order=4)
+    cfg = (configs.elastic_hex(nel=64, order=4) if kind == "hex"
+           else configs.batched_quad(nel=1000, order=4, n_shots=1))
     m = core.Mesh(cfg["shape"], cfg["order"], cfg["physics"], cfg["vertices"], cfg["cells"],
                   cfg["params"], device=device)
-    p = core.Problem(m, core.FP32, dt=1e-4)
+    p = core.Problem(m, core.FP32, dt=1e-5)
     p.run(32, core.RUN_GRAPH)
     p.synchronize()
     stream = torch.cuda.ExternalStream(p.stream_handle())
@@ -415,7 +417,7 @@ def hex_rate_64cube(core, configs, device=0, steps=64):
 
 
 def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8, hex_rate=None,
-                max_running=16):
+                quad_rate=None, max_running=32):
     """Config 4 (bounded sample): a seeded stream of n_jobs jobs, half 2-D
     acoustic quads (edge U{50..400}), half 3-D elastic hexes (edge
     U{16..48}), order 4, own model and source each, steps U{1000..6000}.
@@ -423,10 +425,11 @@ def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8, hex_rate=No
     preparation included); then the same jobs arrive as a Poisson stream at
     load x the serial service rate and the server runs them.
 
-    hex_rate (GLL-point updates/s of the 64^3 hexahedron workload on this
-    GPU) gives a device-time floor: the hexahedron jobs' updates alone need
-    sum(G * steps) / hex_rate seconds of device time, so no served form can
-    beat serial_s / that floor."""
+    hex_rate and quad_rate (GLL-point updates/s of a 64^3 hexahedron and a
+    1000^2 quadrilateral mesh on this GPU, graph-replayed) give a
+    device-time floor: the jobs' updates need at least sum(G * steps) /
+    rate of their class seconds of device time, so no served form can beat
+    serial_s / that floor."""
     from salvus_b200 import serving
     ud = {k: unit_dt(core, meshgen, k) for k in ("quad", "hex")}
     stream = configs.serving_stream(n_jobs, seed=seed)
@@ -483,16 +486,19 @@ def serving_leg(core, configs, meshgen, n_jobs=24, seed=4, load=0.8, hex_rate=No
     st = srv.stats()
     srv.close()
     floor = None
-    if hex_rate:
-        # G of an edge^3 hexahedron mesh of order N: (N edge + 1)^3 nodes
-        hex_updates = sum((jobs[0][1]["order"] * edge + 1) ** 3 * n
-                          for (kind, edge, _, n, _) in stream if kind == "hex")
-        floor = {"hex_updates": hex_updates, "hex_rate_64cube": hex_rate,
-                 "hex_device_floor_s": hex_updates / hex_rate,
-                 "ratio_ceiling": serial_s / (hex_updates / hex_rate),
-                 "form": "hexahedron jobs' updates at the 64^3 workload's graph-replayed "
-                         "per-node rate (quadrilateral jobs excluded, so the true floor is "
-                         "higher and the ceiling lower)"}
+    if hex_rate and quad_rate:
+        # G of an edge^d mesh of order N: (N edge + 1)^d nodes
+        order = jobs[0][1]["order"]
+        upd = {"hex": 0, "quad": 0}
+        for kind, edge, _, n, _ in stream:
+            upd[kind] += (order * edge + 1) ** (3 if kind == "hex" else 2) * n
+        fl = upd["hex"] / hex_rate + upd["quad"] / quad_rate
+        floor = {"hex_updates": upd["hex"], "quad_updates": upd["quad"],
+                 "hex_rate_64cube": hex_rate, "quad_rate_1000sq": quad_rate,
+                 "device_floor_s": fl, "ratio_ceiling": serial_s / fl,
+                 "form": "each class's updates at the graph-replayed per-node rate of one large "
+                         "mesh of that class (a lower bound on the device time of any served "
+                         "form, so serial_s / floor bounds the throughput ratio)"}
     return {"workload": f"{n_jobs} jobs: 2-D acoustic quads 50^2-400^2 and 3-D elastic hexes "
                         f"16^3-48^3, order 4, 1000-6000 steps; latency under Poisson arrivals at "
                         f"{load:.0%} of the measured capacity (bounded sample of the 2000-job stream)",
@@ -594,7 +600,8 @@ def main():
     if args.serving_only:
         from salvus_b200 import meshgen
         out = {"serving": serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs,
-                                      hex_rate=hex_rate_64cube(core, configs, device=local),
+                                      hex_rate=class_rate(core, configs, "hex", local),
+                                      quad_rate=class_rate(core, configs, "quad", local),
                                       max_running=args.serving_max_running)}
         if rank == 0:
             print(json.dumps(out), flush=True)
@@ -796,7 +803,9 @@ def main():
     if not args.no_serving and rank == 0 and world == 1:
         from salvus_b200 import meshgen
         serve = serving_leg(core, configs, meshgen, n_jobs=args.serving_jobs,
-                            hex_rate=value if args.nel == 64 and args.order == 4 else None,
+                            hex_rate=(value if args.nel == 64 and args.order == 4
+                                      else class_rate(core, configs, "hex", local)),
+                            quad_rate=class_rate(core, configs, "quad", local),
                             max_running=args.serving_max_running)
 
     simplex = None
