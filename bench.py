@@ -209,6 +209,13 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
     p.run(5, core.RUN_GRAPH)
     p.synchronize()
     ms_b = timed(p, lambda: p.run(steps, core.RUN_GRAPH))
+    # per-kernel device times of the same step (host-launched, event-timed):
+    # what a single launch per step could save is at most the graph step
+    # minus their sum
+    p.profile(True)
+    p.run(min(steps, 50), core.RUN_PLAIN)
+    kern = {k: v[0] / max(v[1], 1) for k, v in p.profile_read().items()}
+    p.profile(False)
     q = core.Problem(mesh, core.FP32, dt=dt)
     s = cfg["sources"][0]
     q.add_source(s["location"], s["center_freq"], s["time_delay"], s["amplitude"],
@@ -232,6 +239,8 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
             "single_graph_value": G * steps / (ms_g / 1e3), "single_graph_ms_per_step": ms_g / steps,
             "form": "fused batched step (interior nodes in the stiffness kernel), CUDA graph",
             "shot_throughput_ratio": batched / plain, "steps": steps,
+            "kernels_ms": kern,
+            "launch_gaps_ms_per_step": ms_b / steps - sum(kern.values()),
             "tuning": {"stiffness_shot_lanes": tune[0], "stiffness_elements_per_cta": tune[1],
                        "gather_shot_lanes": tune[2], "gather_nodes_per_cta": tune[3]}}
 
@@ -729,6 +738,16 @@ def main():
         # offsets 4 B/node + (u, v, a_) read and write 72 B/node + inverse mass 4 B/node
         b_upd = E * P * 16 + G * (4 + 72 + 4)
         layout = "per-point inverse Jacobians"
+    # what bounds the kernel (ncu at 32^3, same kernels): the per-point
+    # layout streams 48 B of records per point and is HBM-bound; the
+    # parallelepiped layout reads 2.2x fewer DRAM bytes and is held by the
+    # L1 / shared-memory pipe instead (its tensor-product contractions read
+    # 60 shared-memory words per point)
+    limiter = ("L1/shared-memory pipe (ncu l1tex throughput 86 % of peak, DRAM ~34 %): with "
+               "the per-element Jacobian the kernel moves 2.2x fewer bytes than the per-point "
+               "layout and is no longer HBM-bound" if affine and not fused else
+               "HBM (DRAM bytes equal the algorithmic bytes)" if not affine else
+               "L1/shared-memory pipe and occupancy (80 registers)")
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     k_ms, k_n = prof.get("stiffness", (0.0, 1))
@@ -835,6 +854,7 @@ def main():
             "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
             "roofline": {"bound": "hbm", "kernel": "elastic_hex_stiffness", "layout": layout,
                          "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                         "limiter": limiter,
                          "traffic": traffic, "algorithmic_bytes": b_stiff,
                          "kernel_ms": st_ms, "elements_per_cta": epc,
                          "peak_source": "measured" if peaks else "fallback"},

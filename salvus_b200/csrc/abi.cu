@@ -4,8 +4,12 @@
 //   mass + Newmark -> receivers.
 #include <cuda_runtime.h>
 
+#include <unistd.h>
+
 #include <atomic>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -2272,18 +2276,81 @@ static int host_threads() {
   static const int n = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
   return n;
 }
+// Persistent host workers for those copies: a field of the 64^3 workload
+// is 13 chunks, and creating and joining a fresh set of threads for every
+// chunk cost about as much as the conversion itself.  One parallel job runs
+// at a time (callers serialise on run_mu); the calling thread takes part 0.
+// The pool is created on first use and never destroyed (its threads are
+// detached and end with the process); a process forked after that has no
+// workers, so it runs the parts itself.
 extern "C++" {
+class HostPool {
+ public:
+  static HostPool &get() {
+    static HostPool *pool = new HostPool(host_threads());
+    return *pool;
+  }
+  int threads() const { return T_; }
+  void run(size_t n, size_t part, const std::function<void(size_t, size_t)> &fn) {
+    if (getpid() != pid_ || T_ == 1) {
+      for (size_t lo = 0; lo < n; lo += part) fn(lo, std::min(n, lo + part));
+      return;
+    }
+    std::lock_guard<std::mutex> rl(run_mu_);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      fn_ = &fn;
+      n_ = n;
+      part_ = part;
+      remaining_ = T_ - 1;
+      ++gen_;
+    }
+    cv_work_.notify_all();
+    fn(0, std::min(part, n));
+    std::unique_lock<std::mutex> lk(mu_);
+    cv_done_.wait(lk, [&] { return remaining_ == 0; });
+    fn_ = nullptr;
+  }
+
+ private:
+  explicit HostPool(int T) : T_(T), pid_(getpid()) {
+    for (int t = 1; t < T_; ++t) std::thread([this, t] { loop(t); }).detach();
+  }
+  void loop(int t) {
+    uint64_t seen = 0;
+    for (;;) {
+      const std::function<void(size_t, size_t)> *fn;
+      size_t lo, hi;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_work_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        fn = fn_;
+        lo = std::min(n_, (size_t)t * part_);
+        hi = std::min(n_, lo + part_);
+      }
+      if (lo < hi) (*fn)(lo, hi);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (--remaining_ == 0) cv_done_.notify_one();
+    }
+  }
+  const int T_;
+  const pid_t pid_;
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_work_, cv_done_;
+  const std::function<void(size_t, size_t)> *fn_ = nullptr;
+  size_t n_ = 0, part_ = 0;
+  uint64_t gen_ = 0;
+  int remaining_ = 0;
+};
+
 template <typename Fn>
 static void par_range(size_t n, Fn fn) {
-  const int T = host_threads();
+  HostPool &pool = HostPool::get();
+  const int T = pool.threads();
   const size_t part = ((n + T - 1) / T + 63) & ~size_t(63);
-  std::vector<std::thread> th;
-  for (int t = 1; t < T && (size_t)t * part < n; ++t) {
-    const size_t lo = (size_t)t * part, hi = std::min(n, lo + part);
-    th.emplace_back([=] { fn(lo, hi); });
-  }
-  fn(0, std::min(part, n));
-  for (auto &x : th) x.join();
+  const std::function<void(size_t, size_t)> f = fn;
+  pool.run(n, part, f);
 }
 }  // extern "C++"
 static void par_memcpy(void *dst, const void *src, size_t n) {
