@@ -210,6 +210,7 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
     p.set_seismogram_capacity(steps + 64)
     tune = p.autotune()
     p.run(5, core.RUN_GRAPH)
+    p.prepare_run(steps)
     p.synchronize()
     ms_b = timed(p, lambda: p.run(steps, core.RUN_GRAPH))
     # per-kernel device times of the same step (host-launched, event-timed):
@@ -231,6 +232,7 @@ def shots_leg(core, configs, timed, steps, n_shots=256, nel=200, device=0):
     ms_p = timed(q, lambda: q.run(steps, core.RUN_PLAIN))
     # the same single shot with its time loop replayed from a CUDA graph
     q.run(64, core.RUN_GRAPH)
+    q.prepare_run(steps)
     q.synchronize()
     ms_g = timed(q, lambda: q.run(steps, core.RUN_GRAPH))
     batched = G * n_shots * steps / (ms_b / 1e3)
@@ -271,6 +273,7 @@ def simplex_leg(core, configs, timed, steps, device=0, tet_n=55):
             p.add_receiver(r)
         p.set_seismogram_capacity(steps + 64)
         p.run(5, core.RUN_GRAPH)
+        p.prepare_run(steps)
         p.synchronize()
         ms = timed(p, lambda: p.run(steps, core.RUN_GRAPH))
         p.profile(True)
@@ -315,6 +318,7 @@ def elastic2d_leg(core, configs, timed, steps, device=0, nel=720, peak=None):
         p.add_receiver(r)
     p.set_seismogram_capacity(steps + 64)
     p.run(5, core.RUN_GRAPH)
+    p.prepare_run(steps)
     p.synchronize()
     ms = timed(p, lambda: p.run(steps, core.RUN_GRAPH))
     p.profile(True)
@@ -690,8 +694,10 @@ def main():
         return timed_on(p, fn)
 
     clocks = Clocks(local)
-    # warm-up (graph capture happens here)
+    # warm-up steps, then the capture of the graphs a K-step run replays
+    # (nothing runs in the capture)
     p.run(args.warmup, core.RUN_GRAPH)
+    p.prepare_run(args.steps)
     p.synchronize()
     # the K-step region is timed R times back to back; value = the median
     R = max(1, args.repeats)
@@ -755,6 +761,10 @@ def main():
                "layout and is no longer HBM-bound" if affine and not fused else
                "HBM (DRAM bytes equal the algorithmic bytes)" if not affine else
                "L1/shared-memory pipe and occupancy (80 registers)")
+    # the canonical step bytes of a per-GLL-point geometry layout (isotropic
+    # elastic: d = 3, m = 2 material words; c = 3): the compulsory traffic a
+    # straightforward implementation of the step moves
+    b_canon_step = 4 * P * E * (1 + 9 + 1 + 2) + 8 * 3 * G + (28 * 3 + 4) * G
     peaks = measured_peaks()
     peak = peaks["hbm_gbs"] if peaks else 6650.0
     k_ms, k_n = prof.get("stiffness", (0.0, 1))
@@ -799,6 +809,7 @@ def main():
     # end-to-end through the public API with host buffers: initial state from
     # host (u0, v0 FP64), K steps, seismograms back to the host
     p2 = make_problem()
+    p2.set_seismogram_capacity(max(args.warmup, 32) + max(1, args.repeats) * args.steps + 64)
     rng = np.random.default_rng(7)
     u0 = (1e-6 * rng.standard_normal((G, 3)))
     v0 = np.zeros((G, 3))
@@ -814,8 +825,12 @@ def main():
     # the timed job
     w_e2e = max(args.warmup, 32)
     e2e_job(w_e2e, 0)
+    p2.prepare_run(args.steps)
     p2.synchronize()
-    ms_e2e = timed_on(p2, lambda: e2e_job(args.steps, w_e2e))
+    # the job is timed R times (each one uploads u0 / v0 again); the median
+    e2e_runs = [timed_on(p2, lambda i=i: e2e_job(args.steps, w_e2e + i * args.steps))
+                for i in range(R)]
+    ms_e2e = float(np.median(e2e_runs))
     e2e = replica_rate(G, args.steps, ms_e2e, world)
     # u0 and v0 cross PCIe as FP32 (converted on the host threads from the
     # caller's FP64 arrays), amortised over the K steps of the job
@@ -872,11 +887,17 @@ def main():
             "roofline_step": {"bytes_per_step": b_stiff + b_upd, "ms_per_step": ms / args.steps,
                               "achieved": (b_stiff + b_upd) / (ms / args.steps / 1e3) / 1e9,
                               "peak": peak, "unit": "GB/s",
-                              "frac": (b_stiff + b_upd) / (ms / args.steps / 1e3) / 1e9 / peak},
+                              "frac": (b_stiff + b_upd) / (ms / args.steps / 1e3) / 1e9 / peak,
+                              "canonical_bytes": b_canon_step,
+                              "frac_canonical": b_canon_step / (ms / args.steps / 1e3) / 1e9 / peak,
+                              "canonical_form": "per-GLL-point geometry layout: B_K = 4 P E (1 + "
+                                                "d^2 + 1 + m) + 8 c G, B_U = (28 c + 4) G"},
             "roofline_per_point_geometry": general,
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "host_input_bytes": 2 * G * 3 * 8,
+                    "repeats": {"n": len(e2e_runs), "ms_median": ms_e2e,
+                                "ms_min": min(e2e_runs), "ms_max": max(e2e_runs)},
                     "form": "C-ABI job: FP64 host u0/v0 (converted to FP32 on host threads, "
                             "pinned DMA), K graph-replayed steps, seismogram read-back; h2d "
                             "amortised over K"},

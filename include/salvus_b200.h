@@ -242,8 +242,17 @@ int salvus_take_time_step(salvus_problem *p);
  * launch).  Same result as the three-call sequence. */
 int salvus_step(salvus_problem *p);
 /* n steps of the Main.cpp:45-66 loop; mode PLAIN launches each step from the
- * host, GRAPH replays a captured CUDA graph of steps. */
+ * host, GRAPH replays captured CUDA graphs of steps: a 32-step graph n / 32
+ * times, then a graph of the remaining steps when there are at least 8
+ * (the last remainder length is kept), else host launches for them.  In
+ * the graphs each step's receivers run on a second stream of the problem,
+ * overlapped with the next step's stiffness launch, and every graph ends
+ * with them joined to the problem's stream (results are those of single
+ * salvus_step calls). */
 int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode);
+/* Capture (without running) the graphs a GRAPH run of n_steps replays, so
+ * that the run itself launches no capture.  No reference counterpart. */
+int salvus_problem_prepare_run(salvus_problem *p, int64_t n_steps);
 int salvus_synchronize(salvus_problem *p);
 int64_t salvus_problem_step_index(const salvus_problem *p);
 /* Shot batching (n_shots > 1; FP32 acoustic quads): picks, by timing on this

@@ -110,6 +110,7 @@ SIGNATURES = [
     ("salvus_take_time_step", ctypes.c_int, [_VP]),
     ("salvus_step", ctypes.c_int, [_VP]),
     ("salvus_run", ctypes.c_int, [_VP, _I64, _I32]),
+    ("salvus_problem_prepare_run", ctypes.c_int, [_VP, _I64]),
     ("salvus_synchronize", ctypes.c_int, [_VP]),
     ("salvus_problem_step_index", _I64, [_VP]),
     ("salvus_problem_stream", ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
@@ -341,6 +342,10 @@ class Problem:
     # -- fused forms
     def step(self):
         _check(lib().salvus_step(self.h))
+
+    def prepare_run(self, n_steps):
+        """Capture the graphs a graph run of n_steps replays (nothing runs)."""
+        _check(lib().salvus_problem_prepare_run(self.h, n_steps))
 
     def run(self, n_steps, mode=RUN_GRAPH):
         _check(lib().salvus_run(self.h, int(n_steps), mode))

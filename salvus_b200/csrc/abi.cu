@@ -749,6 +749,9 @@ static void drop_graph(salvus_problem *p) {
   if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
   p->graph_exec = nullptr;
   p->graph_steps = 0;
+  if (p->tail_exec) cudaGraphExecDestroy(p->tail_exec);
+  p->tail_exec = nullptr;
+  p->tail_steps = 0;
 }
 
 // fluid-solid coupling integrals (meshes of fluid and solid quadrilaterals)
@@ -783,19 +786,45 @@ static int launch_sources(salvus_problem *p) {
   return check_launch("source");
 }
 
+// Receivers of step n read u after its update and advance the device step
+// counter; step n + 1's stiffness launch only reads u.  In the steps a
+// graph run captures (rec_overlap) they therefore run on a second stream,
+// forked after the node update, and step n + 1 joins them after its
+// stiffness launch, before its sources (which read the step counter) and
+// its node update (which writes u); the captured sequence ends joined, so
+// every later operation on the problem's stream is ordered after them.
+// Host-launched and profiled steps keep them on the problem's stream.
+static int join_receivers(salvus_problem *p) {
+  if (!p->rec_pending) return SALVUS_OK;
+  p->rec_pending = false;
+  SALVUS_CUDA(cudaStreamWaitEvent(p->stream, p->ev_recorded, 0));
+  return SALVUS_OK;
+}
+
 template <typename real, int C>
 static int launch_receivers(salvus_problem *p) {
   ProfScope ps(p, K_REC);
+  cudaStream_t st = p->stream;
+  const bool fork = p->rec_overlap && !p->profiling && p->rec_stream;
+  if (fork) {
+    SALVUS_CUDA(cudaEventRecord(p->ev_updated, p->stream));
+    SALVUS_CUDA(cudaStreamWaitEvent(p->rec_stream, p->ev_updated, 0));
+    st = p->rec_stream;
+  }
   const int nr = (int)p->recs.size();
   if (nr > 0) {
-    receiver_kernel<real, C><<<nr, kRecThreads, 0, p->stream>>>(
+    receiver_kernel<real, C><<<nr, kRecThreads, 0, st>>>(
         p->mesh->P, p->d_rec_elem.as<int64_t>(), p->d_rec_l.as<double>(),
         p->mesh->d_conn.as<int32_t>(), F<real>(p->d_u), p->d_seis.as<double>(), p->seis_cap,
         p->d_step.as<int64_t>());
     g_launches++;
   }
-  advance_step_kernel<<<1, 1, 0, p->stream>>>(p->d_step.as<int64_t>());
+  advance_step_kernel<<<1, 1, 0, st>>>(p->d_step.as<int64_t>());
   g_launches++;
+  if (fork) {
+    SALVUS_CUDA(cudaEventRecord(p->ev_recorded, p->rec_stream));
+    p->rec_pending = true;
+  }
   return check_launch("receivers");
 }
 
@@ -849,6 +878,9 @@ static int launch_fused_interior(salvus_problem *p, const HexInteriorUpdate &iu)
 static int step_fused_hex_interior(salvus_problem *p) {
   const salvus_mesh *m = p->mesh;
   int rc;
+  // this stiffness launch writes u (interior nodes): the previous step's
+  // receivers, which read u, finish first
+  if ((rc = join_receivers(p))) return rc;
   {
     ProfScope ps(p, K_STIFF);
     HexInteriorUpdate iu{};
@@ -909,6 +941,7 @@ static int step_fused_t(salvus_problem *p) {
                                        p->d_err.as<int>(), p->wait_limit, p->hold_waits)))
       return rc;
   }
+  if ((rc = join_receivers(p))) return rc;  // the previous step's receivers
   if ((rc = launch_dirichlet<real, C>(p))) return rc;
   if ((rc = launch_coupling<real>(p))) return rc;
   if ((rc = launch_sources<real, C>(p))) return rc;
@@ -2164,6 +2197,12 @@ int salvus_problem_destroy(salvus_problem *p) {
     if (p->h_pin[b]) cudaFreeHost(p->h_pin[b]);
     if (p->pin_ev[b]) cudaEventDestroy(p->pin_ev[b]);
   }
+  if (p->rec_stream) {
+    cudaStreamSynchronize(p->rec_stream);
+    cudaStreamDestroy(p->rec_stream);
+    cudaEventDestroy(p->ev_updated);
+    cudaEventDestroy(p->ev_recorded);
+  }
   cudaStream_t s = p->stream;
   delete p;
   if (s) cudaStreamDestroy(s);
@@ -2596,56 +2635,126 @@ int salvus_problem_status(salvus_problem *p, int32_t clear) {
   return rc;
 }
 
+// Time loops replay CUDA graphs of captured fused steps: a run of n steps
+// replays the 32-step graph n / 32 times and a graph of the remainder (the
+// last remainder length is kept) when it is at least 8 steps, else launches
+// those steps from the host.  Each graph ends with a finite check of u (the
+// 32-step graph at every 32nd step, as host-launched runs do; a remainder
+// graph at its end).
+constexpr int kGraphChunk = 32, kGraphMin = 8;
+
+static int capture_steps(salvus_problem *p, int steps, cudaGraphExec_t *exec, int64_t *launches) {
+  const bool prof = p->profiling;
+  p->profiling = false;
+  // receivers forked onto the second stream in the captured steps only (in
+  // host-launched steps the extra event calls would cost more host time
+  // than the overlap saves on small meshes)
+  p->rec_overlap = p->shots == 1 && p->rec_stream;
+  cudaGraph_t graph;
+  SALVUS_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+  int crc = SALVUS_OK;
+  const int64_t l0 = g_launches.load();
+  for (int s = 0; s < steps && crc == SALVUS_OK; ++s) crc = step_fused(p);
+  if (crc == SALVUS_OK) crc = launch_finite_check(p);
+  // the captured sequence ends joined (a forked stream must rejoin the
+  // capture), so every replay is self-contained
+  const int jrc = join_receivers(p);
+  if (crc == SALVUS_OK) crc = jrc;
+  p->rec_overlap = false;
+  cudaError_t ce = cudaStreamEndCapture(p->stream, &graph);
+  // captured launches run only when the graph is replayed: count them there
+  *launches = g_launches.load() - l0;
+  g_launches -= *launches;
+  p->profiling = prof;
+  if (crc) {
+    if (ce == cudaSuccess) cudaGraphDestroy(graph);
+    return crc;
+  }
+  if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+  return SALVUS_OK;
+}
+
+// the graphs a graph run of n_steps replays, captured if missing
+static int prepare_graphs(salvus_problem *p, int64_t n_steps) {
+  int rc;
+  if (n_steps >= kGraphChunk && !p->graph_exec) {
+    if ((rc = capture_steps(p, kGraphChunk, &p->graph_exec, &p->graph_launches))) return rc;
+    p->graph_steps = kGraphChunk;
+  }
+  const int rem = (int)(n_steps % kGraphChunk);
+  if (rem >= kGraphMin && p->tail_steps != rem) {
+    if (p->tail_exec) cudaGraphExecDestroy(p->tail_exec);
+    p->tail_exec = nullptr;
+    p->tail_steps = 0;
+    if ((rc = capture_steps(p, rem, &p->tail_exec, &p->tail_launches))) return rc;
+    p->tail_steps = rem;
+  }
+  return SALVUS_OK;
+}
+
+static int rec_stream_ready(salvus_problem *p) {
+  if (p->shots == 1 && !p->rec_stream) {  // created outside any graph capture
+    SALVUS_CUDA(cudaStreamCreateWithFlags(&p->rec_stream, cudaStreamNonBlocking));
+    SALVUS_CUDA(cudaEventCreateWithFlags(&p->ev_updated, cudaEventDisableTiming));
+    SALVUS_CUDA(cudaEventCreateWithFlags(&p->ev_recorded, cudaEventDisableTiming));
+  }
+  return SALVUS_OK;
+}
+
+static int run_steps(salvus_problem *p, int64_t n_steps, int32_t mode);
 int salvus_run(salvus_problem *p, int64_t n_steps, int32_t mode) {
   int rc = ready(p);
   if (rc) return rc;
   if (n_steps < 0) return fail(SALVUS_E_INVALID, "negative step count");
+  if (mode != SALVUS_RUN_PLAIN && mode != SALVUS_RUN_GRAPH)
+    return fail(SALVUS_E_INVALID, "unknown run mode %d", mode);
   SALVUS_CUDA(cudaSetDevice(p->mesh->device));
-  if (mode == SALVUS_RUN_PLAIN || n_steps < 8) {
-    for (int64_t s = 0; s < n_steps; ++s) {
-      if ((rc = step_fused(p))) return rc;
-      p->step++;
-      if (p->step % kFiniteEvery == 0 && (rc = launch_finite_check(p))) return rc;
-    }
-    return SALVUS_OK;
+  if ((rc = rec_stream_ready(p))) return rc;
+  return run_steps(p, n_steps, mode);
+}
+
+int salvus_problem_prepare_run(salvus_problem *p, int64_t n_steps) {
+  int rc = ready(p);
+  if (rc) return rc;
+  if (n_steps < 0) return fail(SALVUS_E_INVALID, "negative step count");
+  SALVUS_CUDA(cudaSetDevice(p->mesh->device));
+  if ((rc = rec_stream_ready(p))) return rc;
+  return prepare_graphs(p, n_steps);
+}
+
+static int plain_steps(salvus_problem *p, int64_t n) {
+  int rc;
+  for (int64_t s = 0; s < n; ++s) {
+    if ((rc = step_fused(p))) return rc;
+    p->step++;
+    if (p->step % kFiniteEvery == 0 && (rc = launch_finite_check(p))) return rc;
   }
-  if (mode != SALVUS_RUN_GRAPH) return fail(SALVUS_E_INVALID, "unknown run mode %d", mode);
-  const int chunk = 32;
-  if (!p->graph_exec) {
-    const bool prof = p->profiling;
-    p->profiling = false;
-    cudaGraph_t graph;
-    SALVUS_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
-    int crc = SALVUS_OK;
-    const int64_t l0 = g_launches.load();
-    for (int s = 0; s < chunk && crc == SALVUS_OK; ++s) crc = step_fused(p);
-    if (crc == SALVUS_OK) crc = launch_finite_check(p);
-    cudaError_t ce = cudaStreamEndCapture(p->stream, &graph);
-    // captured launches run only when the graph is replayed: count them there
-    p->graph_launches = g_launches.load() - l0;
-    g_launches -= p->graph_launches;
-    p->profiling = prof;
-    if (crc) return crc;
-    if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
-    ce = cudaGraphInstantiate(&p->graph_exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (ce != cudaSuccess) return fail(SALVUS_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
-    p->graph_steps = chunk;
-  }
+  return SALVUS_OK;
+}
+
+static int run_steps(salvus_problem *p, int64_t n_steps, int32_t mode) {
+  if (mode == SALVUS_RUN_PLAIN || n_steps < kGraphMin) return plain_steps(p, n_steps);
+  int rc = prepare_graphs(p, n_steps);
+  if (rc) return rc;
   int64_t done = 0;
-  while (n_steps - done >= p->graph_steps) {
+  while (n_steps - done >= p->graph_steps && p->graph_exec) {
     ProfScope ps(p, K_GRAPH);
     SALVUS_CUDA(cudaGraphLaunch(p->graph_exec, p->stream));
     g_launches += p->graph_launches;
     done += p->graph_steps;
     p->step += p->graph_steps;
   }
-  for (; done < n_steps; ++done) {
-    if ((rc = step_fused(p))) return rc;
-    p->step++;
-    if (p->step % kFiniteEvery == 0 && (rc = launch_finite_check(p))) return rc;
+  if (p->tail_exec && n_steps - done == p->tail_steps) {
+    ProfScope ps(p, K_GRAPH);
+    SALVUS_CUDA(cudaGraphLaunch(p->tail_exec, p->stream));
+    g_launches += p->tail_launches;
+    done += p->tail_steps;
+    p->step += p->tail_steps;
   }
-  return SALVUS_OK;
+  return plain_steps(p, n_steps - done);
 }
 
 // Energy of the current state: -K u into a scratch field (stiffness and

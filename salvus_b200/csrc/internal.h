@@ -210,7 +210,19 @@ struct salvus_problem {
   cudaGraphExec_t graph_exec = nullptr;
   int graph_steps = 0;
   int64_t graph_launches = 0;  // kernel launches in one replay of graph_exec
+  // the graph of the last remainder length (a run's steps after its whole
+  // 32-step replays, when at least 8)
+  cudaGraphExec_t tail_exec = nullptr;
+  int tail_steps = 0;
+  int64_t tail_launches = 0;
   cudaStream_t stream = nullptr;
+  // receivers of the fused step on a second stream inside salvus_run
+  // (overlapped with the next step's stiffness launch): the stream, the
+  // fork / join events, whether a launch is still to be joined, and whether
+  // the current call allows the overlap
+  cudaStream_t rec_stream = nullptr;
+  cudaEvent_t ev_updated = nullptr, ev_recorded = nullptr;
+  bool rec_pending = false, rec_overlap = false;
   // profiling
   bool profiling = false;
   struct Ev {

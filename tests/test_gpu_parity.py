@@ -176,6 +176,23 @@ def test_three_call_sequence_equals_fused_step(cfg0, precision):
     assert np.array_equal(p_lit.seismograms(), p_graph.seismograms())
 
 
+def test_run_with_overlapped_receivers_equals_single_steps(cfg1_small):
+    """salvus_run samples the receivers of each step on a second stream,
+    overlapped with the next step's stiffness launch; the seismograms and
+    the wavefield equal those of single salvus_step calls (receivers on the
+    problem's own stream), bitwise, in graph and plain runs."""
+    probs = [build_pair(cfg1_small, core.FP32, cfg1_small["dt"])[1] for _ in range(3)]
+    n = 77
+    for _ in range(n):
+        probs[0].step()
+    probs[1].run(n, core.RUN_GRAPH)
+    probs[2].run(n, core.RUN_PLAIN)
+    s0 = probs[0].seismograms()
+    for q in probs[1:]:
+        assert np.array_equal(s0, q.seismograms())
+        assert np.array_equal(probs[0].get_field("u"), q.get_field("u"))
+
+
 def test_deterministic_rerun(cfg1_small):
     outs = []
     for _ in range(2):
