@@ -90,10 +90,29 @@ __device__ __forceinline__ void gather_body(int64_t g, int64_t G, const int32_t 
         for (int c = 0; c < C; ++c) acc[c] += rv[q][c];
       }
   } else {
-    for (int32_t q = q0; q < q1; ++q) {
-      const int64_t e = idx[q];
+    // high-valence nodes (tetrahedron vertices: about two dozen incident
+    // points): batches of kBatch independent loads, summed in the same
+    // ascending order as one at a time
+    constexpr int kBatch = 4;
+    for (int32_t qb = q0; qb < q1; qb += kBatch) {
+      const int nq = q1 - qb < kBatch ? q1 - qb : kBatch;
+      int32_t ep[kBatch];
 #pragma unroll
-      for (int c = 0; c < C; ++c) acc[c] += kInKernelR ? __ldca(r + e * C + c) : r[e * C + c];
+      for (int q = 0; q < kBatch; ++q) ep[q] = q < nq ? idx[qb + q] : 0;
+      real rv[kBatch][C];
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q)
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+          const real *rp = r + (int64_t)ep[q] * C + c;
+          rv[q][c] = q < nq ? (kInKernelR ? __ldca(rp) : *rp) : real(0);
+        }
+#pragma unroll
+      for (int q = 0; q < kBatch; ++q)
+        if (q < nq) {
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[c] += rv[q][c];
+        }
     }
   }
   if constexpr (MODE == 1) {
