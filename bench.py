@@ -585,7 +585,9 @@ def reference_arm(args, rank, world):
             "higher_is_better": True,
             "ms_per_step": 1e3 * el / k_run, "dtype": "f64", "data": "synthetic",
             "scaling": "weak", "vs_baseline": None,
-            "config": workload(args),
+            # the GPU arm's config at one GPU (one CPU instance runs here
+            # whatever the rank count)
+            "config": dict(workload(args), parallelism="replicas x1"),
             "cpu_baseline": {"value": rate, "unit": METRIC, "cores": thr, "kind": "port",
                              "sample": sample},
             "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
@@ -872,7 +874,8 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded GRF model, structured hex mesh)",
-            "config": dict(workload(args), parallelism=f"replicas x{world}", form="graph-replayed fused step"),
+            "config": dict(workload(args), parallelism=f"replicas x{world}"),
+            "form": "graph-replayed fused step",
             "plain": {"value": plain, "unit": METRIC, "steps": kp, "ms_per_step": ms_plain / kp,
                       "form": "host-launched fused step"},
             "kernels_ms": {k: v[0] / max(v[1], 1) for k, v in prof.items()},
