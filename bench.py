@@ -103,6 +103,12 @@ def workload(args):
             "fields": "fp32 (geometry computed fp64)", "l2": "inputs larger than L2 (no flush)"}
 
 
+def arm_config(args, world=1):
+    """The `config` object of both arms' JSON lines: the workload and the
+    replica count (the reference arm is one CPU instance, so world = 1)."""
+    return dict(workload(args), parallelism=f"replicas x{world}")
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -585,9 +591,7 @@ def reference_arm(args, rank, world):
             "higher_is_better": True,
             "ms_per_step": 1e3 * el / k_run, "dtype": "f64", "data": "synthetic",
             "scaling": "weak", "vs_baseline": None,
-            # the GPU arm's config at one GPU (one CPU instance runs here
-            # whatever the rank count)
-            "config": dict(workload(args), parallelism="replicas x1"),
+            "config": arm_config(args),
             "cpu_baseline": {"value": rate, "unit": METRIC, "cores": thr, "kind": "port",
                              "sample": sample},
             "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0,
@@ -874,7 +878,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded GRF model, structured hex mesh)",
-            "config": dict(workload(args), parallelism=f"replicas x{world}"),
+            "config": arm_config(args, world),
             "form": "graph-replayed fused step",
             "plain": {"value": plain, "unit": METRIC, "steps": kp, "ms_per_step": ms_plain / kp,
                       "form": "host-launched fused step"},

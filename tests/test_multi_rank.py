@@ -70,3 +70,20 @@ def test_reference_arm_under_torchrun():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["steps"] == 2 and d["warmup"] == 1
     assert d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_both_arms_print_the_same_config_at_one_gpu():
+    """The reference arm's `config` equals the GPU arm's at N = 1 (the same
+    64^3 workload, one replica), so the two lines compare like for like."""
+    sys.path.insert(0, ROOT)
+    import bench
+    sys_argv = sys.argv
+    try:
+        sys.argv = ["bench.py"]
+        args = bench.parse()
+    finally:
+        sys.argv = sys_argv
+    ours, ref = bench.arm_config(args, 1), bench.arm_config(args)
+    assert ours == ref
+    assert ref["elements"] == 64 ** 3 and ref["parallelism"] == "replicas x1"
+
